@@ -1,0 +1,575 @@
+// The C ABI (include/falcondb_b200.h): context lifecycle, resident tables,
+// result accessors and the operator layer.  Every entry point catches engine
+// errors, stores the message in a thread-local string and returns a code, in
+// the manner of FalconDB's c_ffi.rs (src/api/c_ffi.rs:27-144).
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cstdio>
+#include <cstring>
+#include <sstream>
+
+#include "../../include/falcondb_b200.h"
+#include "engine.h"
+#include "result.h"
+
+struct fdb_db {
+  fdb::Ctx ctx;
+};
+struct fdb_hash {
+  fdb::HashTable* h = nullptr;
+  fdb_db* db = nullptr;
+};
+
+namespace fdb {
+
+static thread_local std::string g_last_error;
+
+void fail(int code, const std::string& msg) { throw Error(code, msg); }
+
+void cuda_check(cudaError_t e, const char* what) {
+  if (e == cudaSuccess) return;
+  const int code = (e == cudaErrorMemoryAllocation) ? FDB_E_OOM : FDB_E_CUDA;
+  throw Error(code, std::string("CUDA error ") + cudaGetErrorName(e) + " (" + cudaGetErrorString(e) +
+                        ") in " + what);
+}
+
+int dtype_size(int32_t dtype) { return dtype == FDB_UTF8 ? 4 : 8; }
+
+int Table::find(const std::string& n) const {
+  for (size_t i = 0; i < cols.size(); ++i)
+    if (cols[i].name == n) return (int)i;
+  return -1;
+}
+
+Ctx::~Ctx() {
+  tables.clear();
+  if (scratch.ptr) cudaFree(scratch.ptr);
+  if (d_err) cudaFree(d_err);
+  if (ev0) cudaEventDestroy(ev0);
+  if (ev1) cudaEventDestroy(ev1);
+  if (stream) cudaStreamDestroy(stream);
+  if (upload) cudaStreamDestroy(upload);
+}
+
+void* Ctx::dev_alloc(size_t bytes) {
+  if (bytes == 0) bytes = 16;
+  if (in_use.load() + bytes > budget)
+    fail(FDB_E_OOM, "device memory budget exceeded: " + std::to_string(in_use.load() + bytes) + " > " +
+                        std::to_string(budget) + " bytes");
+  void* p = nullptr;
+  cudaError_t e = cudaMalloc(&p, bytes);
+  if (e != cudaSuccess) {
+    cudaGetLastError();
+    fail(FDB_E_OOM, std::string("cudaMalloc failed: ") + cudaGetErrorString(e));
+  }
+  in_use += bytes;
+  return p;
+}
+void Ctx::dev_free(void* p, size_t bytes) {
+  if (!p) return;
+  cudaFree(p);
+  in_use -= bytes ? bytes : 16;
+}
+DevBuf Ctx::alloc_buf(size_t bytes) {
+  DevBuf b;
+  b.ptr = dev_alloc(bytes);
+  b.bytes = bytes ? bytes : 16;
+  return b;
+}
+void Ctx::free_buf(DevBuf& b) {
+  dev_free(b.ptr, b.bytes);
+  b.ptr = nullptr;
+  b.bytes = 0;
+}
+
+void Ctx::ensure_scratch(size_t bytes) {
+  if (scratch.bytes >= bytes) return;
+  // Work already queued may use the old arena: drain the stream first.
+  FDB_CUDA(cudaStreamSynchronize(stream));
+  size_t want = std::max(bytes, scratch.bytes * 2);
+  want = (want + (1u << 20) - 1) & ~size_t((1u << 20) - 1);
+  if (scratch.ptr) free_buf(scratch);
+  scratch = alloc_buf(want);
+}
+
+void* Ctx::scratch_take(size_t bytes) {
+  const size_t aligned = (bytes + 255) & ~size_t(255);
+  if (scratch_top + aligned > scratch.bytes)
+    fail(FDB_E_OOM, "operator scratch exceeds the reserved arena (" + std::to_string(scratch.bytes) +
+                        " bytes); reserve more before the call");
+  void* p = static_cast<char*>(scratch.ptr) + scratch_top;
+  scratch_top += aligned;
+  return p;
+}
+
+int Ctx::check_device_error() {
+  FDB_CUDA(cudaStreamSynchronize(stream));
+  int e = 0;
+  FDB_CUDA(cudaMemcpy(&e, d_err, sizeof(int), cudaMemcpyDeviceToHost));
+  if (e) {
+    // Clear the error word and the ticket so the context stays usable.
+    FDB_CUDA(cudaMemset(d_err, 0, kTicketBytes));
+    return e == kDevErrTimeout ? FDB_E_TIMEOUT : FDB_E_CAPACITY;
+  }
+  return 0;
+}
+
+}  // namespace fdb
+
+using namespace fdb;
+
+namespace {
+
+int set_error(int code, const std::string& msg) {
+  fdb::g_last_error = msg;
+  return code;
+}
+
+template <class F>
+int guarded(F&& f) {
+  try {
+    f();
+    fdb::g_last_error.clear();
+    return FDB_OK;
+  } catch (const Error& e) {
+    return set_error(e.code, e.what());
+  } catch (const std::bad_alloc&) {
+    return set_error(FDB_E_OOM, "host allocation failed");
+  } catch (const std::exception& e) {
+    return set_error(FDB_E_GENERIC, e.what());
+  } catch (...) {
+    return set_error(FDB_E_GENERIC, "unknown error");
+  }
+}
+
+// Lock, make the context's device current, and reserve scratch for one call.
+struct CallScope {
+  std::lock_guard<std::recursive_mutex> lk;
+  Ctx& c;
+  CallScope(fdb_db* db, size_t scratch_bytes) : lk(db->ctx.mu), c(db->ctx) {
+    FDB_CUDA(cudaSetDevice(c.device));
+    c.scratch_reset();
+    c.ensure_scratch(scratch_bytes);
+  }
+};
+
+size_t default_scratch(Ctx& c) { return (size_t)64 << 20; }
+
+void need(bool ok, const char* msg) {
+  if (!ok) fail(FDB_E_ARG, msg);
+}
+
+}  // namespace
+
+extern "C" {
+
+const char* fdb_version(void) { return "falcondb_b200 0.1.0 (sm_100a)"; }
+
+const char* fdb_last_error(void) { return fdb::g_last_error.c_str(); }
+
+int fdb_open(int device, uint64_t mem_budget_bytes, fdb_db** out) {
+  if (!out) return set_error(FDB_E_ARG, "fdb_open: out is NULL");
+  *out = nullptr;
+  std::unique_ptr<fdb_db> db(new fdb_db());
+  const int rc = guarded([&] {
+    Ctx& c = db->ctx;
+    int ndev = 0;
+    FDB_CUDA(cudaGetDeviceCount(&ndev));
+    if (device < 0 || device >= ndev) fail(FDB_E_ARG, "fdb_open: no such CUDA device");
+    c.device = device;
+    FDB_CUDA(cudaSetDevice(device));
+    cudaDeviceProp prop;
+    FDB_CUDA(cudaGetDeviceProperties(&prop, device));
+    if (prop.major < 10) fail(FDB_E_CUDA, "fdb_open: this build targets sm_100a (B200)");
+    c.sm_count = prop.multiProcessorCount;
+    size_t free_b = 0, total_b = 0;
+    FDB_CUDA(cudaMemGetInfo(&free_b, &total_b));
+    c.budget = mem_budget_bytes ? (size_t)mem_budget_bytes : (size_t)(free_b * 0.9);
+    FDB_CUDA(cudaStreamCreateWithFlags(&c.stream, cudaStreamNonBlocking));
+    FDB_CUDA(cudaStreamCreateWithFlags(&c.upload, cudaStreamNonBlocking));
+    FDB_CUDA(cudaEventCreate(&c.ev0));
+    FDB_CUDA(cudaEventCreate(&c.ev1));
+    c.d_err = static_cast<int*>(c.dev_alloc(Ctx::kTicketBytes));
+    FDB_CUDA(cudaMemset(c.d_err, 0, Ctx::kTicketBytes));
+    c.d_ticket = reinterpret_cast<unsigned int*>(reinterpret_cast<char*>(c.d_err) + 64);
+    c.ensure_scratch(default_scratch(c));
+  });
+  if (rc == FDB_OK) *out = db.release();
+  return rc;
+}
+
+void fdb_close(fdb_db* db) {
+  if (!db) return;
+  cudaSetDevice(db->ctx.device);
+  cudaStreamSynchronize(db->ctx.stream);
+  cudaStreamSynchronize(db->ctx.upload);
+  {
+    std::lock_guard<std::recursive_mutex> lk(db->ctx.mu);
+    for (auto& kv : db->ctx.tables)
+      for (auto& col : kv.second->cols) {
+        db->ctx.free_buf(col.values);
+        db->ctx.free_buf(col.validity);
+        if (col.ready) cudaEventDestroy(col.ready);
+      }
+    db->ctx.tables.clear();
+  }
+  delete db;
+}
+
+int64_t fdb_table_from_columns(fdb_db* db, const char* name, const fdb_column* cols, int32_t ncols,
+                               uint64_t nrows) {
+  if (!db || !name || (!cols && ncols > 0) || ncols < 0)
+    return set_error(FDB_E_ARG, "fdb_table_from_columns: bad arguments");
+  int rc = guarded([&] {
+    std::lock_guard<std::recursive_mutex> lk(db->ctx.mu);
+    Ctx& c = db->ctx;
+    FDB_CUDA(cudaSetDevice(c.device));
+    // Same name, row count and column layout as a resident table: overwrite its
+    // device buffers in place (no free/allocate), once every operator already
+    // queued on the context stream has read them.
+    {
+      auto it = c.tables.find(name);
+      bool same = it != c.tables.end() && it->second->nrows == nrows && (int)it->second->cols.size() == ncols;
+      for (int i = 0; same && i < ncols; ++i) {
+        const Column& old = it->second->cols[i];
+        same = cols[i].name && old.name == cols[i].name && old.dtype == cols[i].dtype &&
+               (old.validity.ptr != nullptr) == (cols[i].validity != nullptr) &&
+               (nrows == 0 || cols[i].values != nullptr);
+      }
+      if (same) {
+        cudaEvent_t done;
+        FDB_CUDA(cudaEventCreateWithFlags(&done, cudaEventDisableTiming));
+        FDB_CUDA(cudaEventRecord(done, c.stream));
+        FDB_CUDA(cudaStreamWaitEvent(c.upload, done, 0));
+        FDB_CUDA(cudaEventDestroy(done));
+        for (int i = 0; i < ncols; ++i) {
+          Column& col = it->second->cols[i];
+          const fdb_column& hc = cols[i];
+          const size_t vbytes = nrows * dtype_size(hc.dtype);
+          if (vbytes)
+            FDB_CUDA(cudaMemcpyAsync(col.values.ptr, hc.values, vbytes, cudaMemcpyHostToDevice, c.upload));
+          if (hc.validity && nrows)
+            FDB_CUDA(cudaMemcpyAsync(col.validity.ptr, hc.validity, ((nrows + 63) / 64) * 8,
+                                     cudaMemcpyHostToDevice, c.upload));
+          if (hc.dtype == FDB_UTF8) {
+            col.dict.clear();
+            for (uint32_t d = 0; d < hc.dict_len; ++d) col.dict.emplace_back(hc.dict[d] ? hc.dict[d] : "");
+          }
+          FDB_CUDA(cudaEventRecord(col.ready, c.upload));
+        }
+        return;
+      }
+    }
+    auto t = std::make_shared<Table>();
+    t->name = name;
+    t->nrows = nrows;
+    try {
+      for (int i = 0; i < ncols; ++i) {
+        const fdb_column& hc = cols[i];
+        need(hc.name != nullptr, "column without a name");
+        need(hc.dtype == FDB_INT64 || hc.dtype == FDB_FLOAT64 || hc.dtype == FDB_UTF8,
+             "unsupported column type");
+        need(nrows == 0 || hc.values != nullptr, "column without values");
+        for (auto& prev : t->cols)
+          if (prev.name == hc.name) fail(FDB_E_ARG, std::string("duplicate column ") + hc.name);
+        Column col;
+        col.name = hc.name;
+        col.dtype = hc.dtype;
+        const size_t vbytes = nrows * dtype_size(hc.dtype);
+        col.values = c.alloc_buf(vbytes);
+        if (vbytes) FDB_CUDA(cudaMemcpyAsync(col.values.ptr, hc.values, vbytes, cudaMemcpyHostToDevice, c.upload));
+        if (hc.validity) {
+          const size_t wbytes = ((nrows + 63) / 64) * 8;
+          col.validity = c.alloc_buf(wbytes);
+          if (wbytes)
+            FDB_CUDA(cudaMemcpyAsync(col.validity.ptr, hc.validity, wbytes, cudaMemcpyHostToDevice, c.upload));
+        }
+        if (hc.dtype == FDB_UTF8) {
+          need(hc.dict != nullptr || hc.dict_len == 0, "Utf8 column without a dictionary");
+          for (uint32_t d = 0; d < hc.dict_len; ++d) col.dict.emplace_back(hc.dict[d] ? hc.dict[d] : "");
+        }
+        FDB_CUDA(cudaEventCreateWithFlags(&col.ready, cudaEventDisableTiming));
+        FDB_CUDA(cudaEventRecord(col.ready, c.upload));
+        t->cols.push_back(std::move(col));
+      }
+    } catch (...) {
+      for (auto& col : t->cols) {
+        c.free_buf(col.values);
+        c.free_buf(col.validity);
+        if (col.ready) cudaEventDestroy(col.ready);
+      }
+      throw;
+    }
+    auto it = c.tables.find(name);
+    if (it != c.tables.end()) {
+      FDB_CUDA(cudaStreamSynchronize(c.stream));
+      for (auto& col : it->second->cols) {
+        c.free_buf(col.values);
+        c.free_buf(col.validity);
+        if (col.ready) cudaEventDestroy(col.ready);
+      }
+      c.tables.erase(it);
+    }
+    c.tables[name] = t;
+  });
+  return rc == FDB_OK ? (int64_t)nrows : (int64_t)rc;
+}
+
+uint64_t fdb_table_row_count(const fdb_db* db, const char* name) {
+  if (!db || !name) return 0;
+  auto& c = const_cast<fdb_db*>(db)->ctx;
+  std::lock_guard<std::recursive_mutex> lk(c.mu);
+  auto it = c.tables.find(name);
+  return it == c.tables.end() ? 0 : it->second->nrows;
+}
+
+int fdb_table_drop(fdb_db* db, const char* name) {
+  if (!db || !name) return set_error(FDB_E_ARG, "fdb_table_drop: bad arguments");
+  return guarded([&] {
+    std::lock_guard<std::recursive_mutex> lk(db->ctx.mu);
+    Ctx& c = db->ctx;
+    auto it = c.tables.find(name);
+    if (it == c.tables.end()) fail(FDB_E_NOTFOUND, std::string("no table ") + name);
+    FDB_CUDA(cudaSetDevice(c.device));
+    FDB_CUDA(cudaStreamSynchronize(c.stream));
+    for (auto& col : it->second->cols) {
+      c.free_buf(col.values);
+      c.free_buf(col.validity);
+      if (col.ready) cudaEventDestroy(col.ready);
+    }
+    c.tables.erase(it);
+  });
+}
+
+int fdb_table_column(const fdb_db* db, const char* table, const char* column, fdb_dev_column* out,
+                     uint64_t* nrows) {
+  if (!db || !table || !column || !out) return set_error(FDB_E_ARG, "fdb_table_column: bad arguments");
+  fdb_db* d = const_cast<fdb_db*>(db);
+  return guarded([&] {
+    std::lock_guard<std::recursive_mutex> lk(d->ctx.mu);
+    auto it = d->ctx.tables.find(table);
+    if (it == d->ctx.tables.end()) fail(FDB_E_NOTFOUND, std::string("no table ") + table);
+    const int ci = it->second->find(column);
+    if (ci < 0) fail(FDB_E_NOTFOUND, std::string("no column ") + column);
+    const Column& col = it->second->cols[ci];
+    // Later operators on the context stream see the uploaded values.
+    FDB_CUDA(cudaSetDevice(d->ctx.device));
+    FDB_CUDA(cudaStreamWaitEvent(d->ctx.stream, col.ready, 0));
+    out->dtype = col.dtype;
+    out->_pad = 0;
+    out->values = col.values.ptr;
+    out->validity = static_cast<const uint64_t*>(col.validity.ptr);
+    out->validity_offset = 0;
+    if (nrows) *nrows = it->second->nrows;
+  });
+}
+
+int fdb_sql(fdb_db* db, const char* sql, fdb_result** out) {
+  if (out) *out = nullptr;
+  if (!db || !sql || !out) return set_error(FDB_E_ARG, "fdb_sql: bad arguments");
+  return guarded([&] {
+    std::lock_guard<std::recursive_mutex> lk(db->ctx.mu);
+    FDB_CUDA(cudaSetDevice(db->ctx.device));
+    *out = fdb::run_sql(db->ctx, sql);
+  });
+}
+
+uint64_t fdb_result_row_count(const fdb_result* r) { return r ? r->rows : 0; }
+int32_t fdb_result_num_columns(const fdb_result* r) { return r ? (int32_t)r->cols.size() : 0; }
+const char* fdb_result_column_name(const fdb_result* r, int32_t col) {
+  if (!r || col < 0 || col >= (int32_t)r->cols.size()) return nullptr;
+  return r->cols[col].name.c_str();
+}
+int32_t fdb_result_column_dtype(const fdb_result* r, int32_t col) {
+  if (!r || col < 0 || col >= (int32_t)r->cols.size()) return 0;
+  return r->cols[col].dtype;
+}
+const void* fdb_result_column_values(const fdb_result* r, int32_t col) {
+  if (!r || col < 0 || col >= (int32_t)r->cols.size()) return nullptr;
+  const auto& c = r->cols[col];
+  if (c.dtype == FDB_INT64) return c.i64.data();
+  if (c.dtype == FDB_FLOAT64) return c.f64.data();
+  return c.str_ptrs.data();
+}
+const uint8_t* fdb_result_column_nulls(const fdb_result* r, int32_t col) {
+  if (!r || col < 0 || col >= (int32_t)r->cols.size()) return nullptr;
+  const auto& c = r->cols[col];
+  return c.has_nulls() ? c.nulls.data() : nullptr;
+}
+const char* fdb_result_display(fdb_result* r) { return r ? r->display.c_str() : nullptr; }
+void fdb_result_free(fdb_result* r) { delete r; }
+
+double fdb_last_kernel_ms(const fdb_db* db) { return db ? db->ctx.last_kernel_ms : 0.0; }
+
+void* fdb_stream(fdb_db* db) { return db ? (void*)db->ctx.stream : nullptr; }
+
+int fdb_synchronize(fdb_db* db) {
+  if (!db) return set_error(FDB_E_ARG, "fdb_synchronize: db is NULL");
+  int dev_err = 0;
+  const int rc = guarded([&] {
+    std::lock_guard<std::recursive_mutex> lk(db->ctx.mu);
+    FDB_CUDA(cudaSetDevice(db->ctx.device));
+    FDB_CUDA(cudaStreamSynchronize(db->ctx.upload));
+    dev_err = db->ctx.check_device_error();
+  });
+  if (rc != FDB_OK) return rc;
+  if (dev_err) return set_error(dev_err, dev_err == FDB_E_TIMEOUT ? "a device-side wait timed out"
+                                                                  : "an output buffer was too small");
+  return FDB_OK;
+}
+
+// ----------------------------- operator layer ------------------------------
+
+int fdb_filter_mask(fdb_db* db, const fdb_dev_column* cols, int32_t ncols, uint64_t nrows,
+                    const fdb_pred_term* prog, int32_t nterms, uint64_t* d_mask) {
+  if (!db || !cols || !d_mask || (nterms && !prog)) return set_error(FDB_E_ARG, "fdb_filter_mask: bad arguments");
+  return guarded([&] {
+    CallScope s(db, default_scratch(db->ctx));
+    op_filter_mask(s.c, cols, ncols, nrows, prog, nterms, d_mask);
+  });
+}
+
+int fdb_filter_count(fdb_db* db, const fdb_dev_column* cols, int32_t ncols, uint64_t nrows,
+                     const fdb_pred_term* prog, int32_t nterms, uint64_t* d_count) {
+  if (!db || !cols || !d_count || (nterms && !prog)) return set_error(FDB_E_ARG, "fdb_filter_count: bad arguments");
+  return guarded([&] {
+    CallScope s(db, default_scratch(db->ctx));
+    op_filter_count(s.c, cols, ncols, nrows, prog, nterms, d_count);
+  });
+}
+
+int fdb_compact_mask(fdb_db* db, const uint64_t* d_mask, uint64_t nrows, uint32_t* d_rows, uint64_t capacity,
+                     uint64_t* d_count) {
+  if (!db || (!d_mask && nrows) || !d_count || (!d_rows && capacity))
+    return set_error(FDB_E_ARG, "fdb_compact_mask: bad arguments");
+  if (nrows >= 0xFFFFFFFFull) return set_error(FDB_E_ARG, "fdb_compact_mask: rows are uint32");
+  return guarded([&] {
+    CallScope s(db, default_scratch(db->ctx));
+    op_compact_mask(s.c, d_mask, nrows, d_rows, capacity, d_count);
+  });
+}
+
+int fdb_gather(fdb_db* db, const fdb_dev_column* col, const uint32_t* d_rows, uint64_t n, void* d_out_values,
+               uint64_t* d_out_validity) {
+  if (!db || !col || (n && (!d_rows || !d_out_values))) return set_error(FDB_E_ARG, "fdb_gather: bad arguments");
+  return guarded([&] {
+    CallScope s(db, default_scratch(db->ctx));
+    op_gather(s.c, *col, d_rows, n, d_out_values, d_out_validity);
+  });
+}
+
+int fdb_aggregate(fdb_db* db, const fdb_dev_column* cols, int32_t ncols, uint64_t nrows,
+                  const fdb_pred_term* prog, int32_t nterms, const fdb_agg_spec* aggs, int32_t naggs,
+                  fdb_agg_value* d_out) {
+  if (!db || !cols || !aggs || !d_out || (nterms && !prog)) return set_error(FDB_E_ARG, "fdb_aggregate: bad arguments");
+  return guarded([&] {
+    CallScope s(db, default_scratch(db->ctx));
+    op_aggregate(s.c, cols, ncols, nrows, prog, nterms, aggs, naggs, d_out);
+  });
+}
+
+int fdb_distinct_codes(fdb_db* db, const fdb_dev_column* cols, int32_t ncols, uint64_t nrows,
+                       const fdb_pred_term* prog, int32_t nterms, int32_t code_col, uint32_t dict_len,
+                       uint64_t* d_bitmap) {
+  if (!db || !cols || (!d_bitmap && dict_len) || (nterms && !prog))
+    return set_error(FDB_E_ARG, "fdb_distinct_codes: bad arguments");
+  return guarded([&] {
+    CallScope s(db, default_scratch(db->ctx));
+    op_distinct_codes(s.c, cols, ncols, nrows, prog, nterms, code_col, dict_len, d_bitmap);
+  });
+}
+
+int fdb_group_by_codes(fdb_db* db, const fdb_dev_column* cols, int32_t ncols, uint64_t nrows,
+                       const fdb_pred_term* prog, int32_t nterms, int32_t key_col, uint32_t dict_len,
+                       const fdb_agg_spec* aggs, int32_t naggs, fdb_agg_value* d_out, int64_t* d_group_rows) {
+  if (!db || !cols || !aggs || !d_out || !d_group_rows || (nterms && !prog))
+    return set_error(FDB_E_ARG, "fdb_group_by_codes: bad arguments");
+  return guarded([&] {
+    CallScope s(db, default_scratch(db->ctx));
+    op_group_by_codes(s.c, cols, ncols, nrows, prog, nterms, key_col, dict_len, aggs, naggs, d_out,
+                      d_group_rows);
+  });
+}
+
+int fdb_group_by_i64(fdb_db* db, const fdb_dev_column* key, const fdb_dev_column* value, uint64_t nrows,
+                     const fdb_pred_term* prog, int32_t nterms, const fdb_dev_column* pred_cols,
+                     int32_t npred_cols, uint64_t expected_groups, double load_factor, fdb_group_i64* d_groups,
+                     uint64_t capacity, uint64_t* d_ngroups) {
+  if (!db || !key || !value || !d_ngroups || (!d_groups && capacity) || (nterms && !prog) ||
+      (npred_cols && !pred_cols))
+    return set_error(FDB_E_ARG, "fdb_group_by_i64: bad arguments");
+  return guarded([&] {
+    Ctx& c = db->ctx;
+    double lf = (load_factor > 0.0 && load_factor < 1.0) ? load_factor : 0.5;
+    uint64_t eg = expected_groups ? expected_groups : (nrows ? nrows : 1);
+    uint64_t cap = 1024;
+    while ((double)cap * lf < (double)eg) cap <<= 1;
+    const size_t need_b = cap * 40 + (16u << 20);
+    CallScope s(db, std::max(default_scratch(c), need_b));
+    op_group_by_i64(s.c, *key, *value, nrows, prog, nterms, pred_cols, npred_cols, expected_groups, lf,
+                    d_groups, capacity, d_ngroups);
+  });
+}
+
+int fdb_join_build(fdb_db* db, const fdb_dev_column* key, const fdb_dev_column* payload, uint64_t nrows,
+                   double load_factor, fdb_hash** out) {
+  if (out) *out = nullptr;
+  if (!db || !key || !out) return set_error(FDB_E_ARG, "fdb_join_build: bad arguments");
+  return guarded([&] {
+    CallScope s(db, default_scratch(db->ctx));
+    fdb_dev_column none;
+    std::memset(&none, 0, sizeof(none));
+    HashTable* h = op_join_build(s.c, *key, payload ? *payload : none, nrows, load_factor);
+    fdb_hash* fh = new fdb_hash();
+    fh->h = h;
+    fh->db = db;
+    *out = fh;
+  });
+}
+
+void fdb_join_free(fdb_hash* h) {
+  if (!h) return;
+  {
+    std::lock_guard<std::recursive_mutex> lk(h->db->ctx.mu);
+    cudaSetDevice(h->db->ctx.device);
+    cudaStreamSynchronize(h->db->ctx.stream);
+    join_free(h->h);
+  }
+  delete h;
+}
+
+uint64_t fdb_join_capacity(const fdb_hash* h) { return h ? join_capacity(h->h) : 0; }
+
+int fdb_join_probe_agg(fdb_db* db, const fdb_hash* h, const fdb_dev_column* probe_key, const fdb_dev_column* value,
+                       uint64_t nrows, int32_t join_type, fdb_join_agg* d_out) {
+  if (!db || !h || !probe_key || !d_out) return set_error(FDB_E_ARG, "fdb_join_probe_agg: bad arguments");
+  if (h->db != db) return set_error(FDB_E_ARG, "fdb_join_probe_agg: hash table belongs to another context");
+  return guarded([&] {
+    CallScope s(db, default_scratch(db->ctx));
+    op_join_probe_agg(s.c, *h->h, *probe_key, value, nrows, join_type, d_out);
+  });
+}
+
+int fdb_join_probe_pairs(fdb_db* db, const fdb_hash* h, const fdb_dev_column* probe_key, uint64_t nrows,
+                         int32_t join_type, uint32_t* d_left, uint32_t* d_right, uint64_t capacity,
+                         uint64_t* d_count) {
+  if (!db || !h || !probe_key || !d_count || (capacity && !d_left))
+    return set_error(FDB_E_ARG, "fdb_join_probe_pairs: bad arguments");
+  if (h->db != db) return set_error(FDB_E_ARG, "fdb_join_probe_pairs: hash table belongs to another context");
+  return guarded([&] {
+    CallScope s(db, default_scratch(db->ctx));
+    op_join_probe_pairs(s.c, *h->h, *probe_key, nrows, join_type, d_left, d_right, capacity, d_count);
+  });
+}
+
+int fdb_topk(fdb_db* db, const fdb_dev_column* col, uint64_t nrows, uint32_t k, int32_t desc, int32_t nulls_last,
+             uint32_t* d_rows, uint64_t* d_count) {
+  if (!db || !col || !d_rows || !d_count) return set_error(FDB_E_ARG, "fdb_topk: bad arguments");
+  return guarded([&] {
+    CallScope s(db, default_scratch(db->ctx));
+    op_topk(s.c, *col, nrows, k, desc != 0, nulls_last != 0, d_rows, d_count);
+  });
+}
+
+}  // extern "C"

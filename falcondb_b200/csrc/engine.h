@@ -1,0 +1,157 @@
+// Host-side internals of the engine: the execution context (device, stream,
+// scratch arena, deferred device errors), resident tables, and the operator
+// launchers that the C ABI and the SQL planner call.
+#pragma once
+#include <cuda_runtime.h>
+
+#include <atomic>
+#include <cstdint>
+#include <map>
+#include <memory>
+#include <mutex>
+#include <stdexcept>
+#include <string>
+#include <vector>
+
+#include "../../include/falcondb_b200.h"
+
+namespace fdb {
+
+// Codes a kernel writes to the context's device error word (read back by
+// fdb_synchronize and turned into FDB_E_TIMEOUT / FDB_E_CAPACITY).
+constexpr int kDevErrTimeout = 1;
+constexpr int kDevErrCapacity = 2;
+
+// Error carried from the engine to the C ABI, which turns it into a return code
+// plus the thread-local message.
+struct Error : std::runtime_error {
+  int code;
+  Error(int c, const std::string& m) : std::runtime_error(m), code(c) {}
+};
+[[noreturn]] void fail(int code, const std::string& msg);
+void cuda_check(cudaError_t e, const char* what);
+#define FDB_CUDA(x) ::fdb::cuda_check((x), #x)
+
+// One device allocation accounted against the context's budget.
+struct DevBuf {
+  void* ptr = nullptr;
+  size_t bytes = 0;
+};
+
+struct Ctx;
+
+// A resident column: dense values in HBM, optional validity words, and for
+// FDB_UTF8 the host dictionary (codes are indices into it).
+struct Column {
+  std::string name;
+  int32_t dtype = 0;
+  DevBuf values;
+  DevBuf validity;              // empty when the column has no NULLs
+  std::vector<std::string> dict;
+  cudaEvent_t ready = nullptr;  // recorded on the upload stream after the copy
+};
+
+struct Table {
+  std::string name;
+  uint64_t nrows = 0;
+  std::vector<Column> cols;
+  int find(const std::string& n) const;
+};
+
+// Per-kernel launch configuration chosen by the autotuner (or its defaults).
+struct LaunchCfg {
+  int grid = 0;        // CTAs (persistent grid)
+  int threads = 0;     // threads per CTA
+};
+
+struct Ctx {
+  int device = 0;
+  int sm_count = 0;
+  size_t budget = 0;
+  std::atomic<size_t> in_use{0};
+  cudaStream_t stream = nullptr;         // operator stream
+  cudaStream_t upload = nullptr;         // host->device copies
+  std::recursive_mutex mu;               // serialises calls on this context
+
+  // Scratch arena: a device buffer carved per operator call.  The first
+  // kTicketBytes hold zeroed counters that kernels reset before they exit.
+  static constexpr size_t kTicketBytes = 256;
+  DevBuf scratch;
+  size_t scratch_top = kTicketBytes;
+  int* d_err = nullptr;                  // deferred device error word (in scratch head)
+  unsigned int* d_ticket = nullptr;      // last-CTA ticket (in scratch head)
+
+  std::map<std::string, std::shared_ptr<Table>> tables;
+  cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+  double last_kernel_ms = 0.0;
+
+  ~Ctx();
+  void* dev_alloc(size_t bytes);                 // budgeted cudaMalloc
+  void dev_free(void* p, size_t bytes);
+  DevBuf alloc_buf(size_t bytes);
+  void free_buf(DevBuf& b);
+  // Scratch for the current operator call (16-byte aligned, grows on demand by
+  // synchronising the stream first).  Reset with scratch_reset().
+  void* scratch_take(size_t bytes);
+  void scratch_reset() { scratch_top = kTicketBytes; }
+  void ensure_scratch(size_t bytes);
+  int check_device_error();                      // reads and clears d_err (syncs)
+};
+
+// Converts the C view to the kernel view.
+struct DevColV {
+  int32_t dtype;
+  const void* values;
+  const uint64_t* validity;
+  uint64_t voff;
+};
+inline DevColV to_v(const fdb_dev_column& c) {
+  return DevColV{c.dtype, c.values, c.validity, c.validity_offset};
+}
+int dtype_size(int32_t dtype);
+
+// ---------------------------------------------------------------------------
+// Operator launchers (asynchronous on ctx.stream). Implemented in the .cu files.
+// ---------------------------------------------------------------------------
+void op_filter_mask(Ctx& c, const fdb_dev_column* cols, int ncols, uint64_t n,
+                    const fdb_pred_term* prog, int nterms, uint64_t* d_mask);
+void op_filter_count(Ctx& c, const fdb_dev_column* cols, int ncols, uint64_t n,
+                     const fdb_pred_term* prog, int nterms, uint64_t* d_count);
+void op_compact_mask(Ctx& c, const uint64_t* d_mask, uint64_t n, uint32_t* d_rows,
+                     uint64_t capacity, uint64_t* d_count);
+void op_gather(Ctx& c, const fdb_dev_column& col, const uint32_t* d_rows, uint64_t n,
+               void* d_out, uint64_t* d_out_validity);
+// Gather where a row number of FDB_NO_ROW yields NULL (the right side of an
+// unmatched LEFT JOIN row); always writes validity words.
+void op_gather_opt(Ctx& c, const fdb_dev_column& col, const uint32_t* d_rows, uint64_t n,
+                   void* d_out, uint64_t* d_out_validity);
+void op_aggregate(Ctx& c, const fdb_dev_column* cols, int ncols, uint64_t n,
+                  const fdb_pred_term* prog, int nterms, const fdb_agg_spec* aggs, int naggs,
+                  fdb_agg_value* d_out);
+void op_distinct_codes(Ctx& c, const fdb_dev_column* cols, int ncols, uint64_t n,
+                       const fdb_pred_term* prog, int nterms, int code_col, uint32_t dict_len,
+                       uint64_t* d_bitmap);
+void op_group_by_codes(Ctx& c, const fdb_dev_column* cols, int ncols, uint64_t n,
+                       const fdb_pred_term* prog, int nterms, int key_col, uint32_t dict_len,
+                       const fdb_agg_spec* aggs, int naggs, fdb_agg_value* d_out,
+                       int64_t* d_group_rows);
+void op_group_by_i64(Ctx& c, const fdb_dev_column& key, const fdb_dev_column& value, uint64_t n,
+                     const fdb_pred_term* prog, int nterms, const fdb_dev_column* pred_cols,
+                     int npred, uint64_t expected_groups, double load_factor,
+                     fdb_group_i64* d_groups, uint64_t capacity, uint64_t* d_ngroups);
+void op_topk(Ctx& c, const fdb_dev_column& col, uint64_t n, uint32_t k, bool desc,
+             bool nulls_last, uint32_t* d_rows, uint64_t* d_count);
+
+struct HashTable;  // join build side (k_join.cu)
+HashTable* op_join_build(Ctx& c, const fdb_dev_column& key, const fdb_dev_column& payload,
+                         uint64_t n, double load_factor);
+void join_free(HashTable* h);
+uint64_t join_capacity(const HashTable* h);
+void op_join_probe_agg(Ctx& c, const HashTable& h, const fdb_dev_column& key,
+                       const fdb_dev_column* value, uint64_t n, int join_type,
+                       fdb_join_agg* d_out);
+void op_join_probe_pairs(Ctx& c, const HashTable& h, const fdb_dev_column& key, uint64_t n,
+                         int join_type, uint32_t* d_left, uint32_t* d_right, uint64_t capacity,
+                         uint64_t* d_count);
+
+}  // namespace fdb

@@ -1,0 +1,578 @@
+// GROUP BY kernels.
+//
+// 1. Dictionary-code GROUP BY (fast_utf8_gb, FalconDB src/query/aggregate.rs:619-836,
+//    accumulate_batch 916-1169, merge_state_entry 1351-1390).  The group id of a
+//    row is its dictionary code (value semantics: one dictionary per column, so
+//    the multi-batch dictionary hazard of the reference cannot arise).  Rows are
+//    combined inside a warp first: __match_any_sync groups the lanes that share a
+//    code, the lowest lane of each group folds its peers' contributions in lane
+//    order and updates the warp's private table in shared memory.  Warp tables,
+//    CTA partials and the final merge are combined in fixed order, so FP64 sums
+//    are repeatable for a given grid.
+//
+// 2. int64-key hash GROUP BY (fast_i64_gb, aggregate.rs:840-912) with COUNT(*),
+//    SUM, MIN, MAX of one value column.  Each CTA keeps an open-addressing table
+//    in shared memory that absorbs the frequent keys (Zipf heavy hitters); rows
+//    whose key finds no room there go straight to a global open-addressing table
+//    with atomics; the CTA table is flushed to the global one at the end.  Keys
+//    are stored XOR 2^63 so that an all-zero slot is empty (cudaMemset clears the
+//    table); MIN is kept as the bitwise NOT of the order key so both MIN and MAX
+//    are atomicMax from a zero identity.  SUM is FP64 atomicAdd (order varies run
+//    to run; tests hold it to 1e-12 relative).
+#include <cstring>
+
+#include "common.cuh"
+#include "engine.h"
+#include "stream.cuh"
+
+namespace fdb {
+
+// ===========================================================================
+// 1. Dictionary-code GROUP BY
+// ===========================================================================
+enum SlotKind : int32_t { kAddU64 = 0, kAddF64 = 1, kMaxU64 = 2 };
+constexpr int kMaxSlots = 9;            // rows + 4 aggregates x (value, count)
+constexpr int kGbWarpTableEntries = 512;  // (groups) x (slots) per warp
+
+struct GbCodesParams {
+  PredProg prog;
+  DevCol cols[4];
+  int32_t key_col;
+  uint32_t ngroups;        // dict_len + 1 (last = NULL key)
+  int32_t nslots;
+  int32_t naggs;
+  int32_t func[4];
+  int32_t acol[4];
+  int32_t vslot[4];        // value slot of each aggregate (-1: none)
+  int32_t cslot[4];        // count slot of each aggregate (-1: uses the row slot)
+  int32_t kind[kMaxSlots];
+  uint64_t* partials;      // [grid][ngroups][nslots]
+  unsigned int* ticket;
+  fdb_agg_value* out;      // [ngroups][naggs]
+  int64_t* group_rows;     // [ngroups]
+};
+
+__device__ __forceinline__ uint64_t slot_combine(int kind, uint64_t a, uint64_t b) {
+  if (kind == kAddF64)
+    return (uint64_t)__double_as_longlong(__longlong_as_double((long long)a) +
+                                          __longlong_as_double((long long)b));
+  if (kind == kMaxU64) return a > b ? a : b;
+  return a + b;
+}
+
+template <class Acc>
+struct GbGetter {
+  const DevCol* cols;
+  const Acc& acc;
+  uint32_t i;
+  uint64_t row;
+  __device__ __forceinline__ int operator()(int c, int64_t& iv, double& fv, uint32_t& code,
+                                            bool& valid) const {
+    const DevCol& col = cols[c];
+    const int dt = col.dtype;
+    if (dt == FDB_FLOAT64)
+      fv = acc.template get<double>(c, i);
+    else if (dt == FDB_INT64)
+      iv = acc.template get<int64_t>(c, i);
+    else
+      code = acc.template get<uint32_t>(c, i);
+    valid = col.validity ? col_valid(col, row) : true;
+    return dt;
+  }
+};
+
+struct GbCodesOp {
+  using Params = GbCodesParams;
+  struct Local {};
+  // smem: per-warp tables [NW][kGbWarpTableEntries] + staging [NW][32][kMaxSlots] + flag
+  static constexpr int kNW = 8;
+  static constexpr size_t kSmem =
+      (size_t)kNW * kGbWarpTableEntries * 8 + (size_t)kNW * 32 * kMaxSlots * 8 + 16;
+
+  static __device__ void init(Local&, const Params& p, unsigned char* sm, int ctid, int nct) {
+    uint64_t* tab = reinterpret_cast<uint64_t*>(sm);
+    for (int i = ctid; i < kNW * kGbWarpTableEntries; i += nct) tab[i] = 0;
+  }
+
+  template <class Acc>
+  static __device__ void step(Local&, const Params& p, unsigned char* sm, const Acc& acc,
+                              uint32_t rows, int ctid, int nct) {
+    const int warp = ctid >> 5, lane = ctid & 31;
+    uint64_t* tab = reinterpret_cast<uint64_t*>(sm) + (size_t)warp * kGbWarpTableEntries;
+    uint64_t* stage = reinterpret_cast<uint64_t*>(sm) + (size_t)kNW * kGbWarpTableEntries +
+                      (size_t)warp * 32 * kMaxSlots;
+    const int ns = p.nslots;
+    for (uint32_t b = 0; b < rows; b += nct) {
+      const uint32_t i = b + ctid;
+      uint32_t gid = 0xFFFFFFFFu;
+      uint64_t v[kMaxSlots];
+#pragma unroll
+      for (int s = 0; s < kMaxSlots; ++s) v[s] = 0;
+      if (i < rows) {
+        const uint64_t row = acc.row(i);
+        GbGetter<Acc> get{p.cols, acc, i, row};
+        if (eval_prog(p.prog, get)) {
+          int64_t iv;
+          double fv;
+          uint32_t code;
+          bool valid;
+          get(p.key_col, iv, fv, code, valid);
+          gid = (!valid || code == kNullCode || code >= p.ngroups - 1) ? p.ngroups - 1 : code;
+          v[0] = 1;
+#pragma unroll
+          for (int a = 0; a < 4; ++a) {
+            if (a >= p.naggs) break;
+            const int f = p.func[a];
+            if (f == FDB_AGG_COUNT_STAR) continue;
+            const int dt = get(p.acol[a], iv, fv, code, valid);
+            if (!valid) continue;
+            if (f == FDB_AGG_MIN || f == FDB_AGG_MAX) {
+              if (dt == FDB_FLOAT64 && isnan(fv)) continue;
+            }
+            const int cs = p.cslot[a];
+            const int vs = p.vslot[a];
+#pragma unroll
+            for (int s = 1; s < kMaxSlots; ++s)
+              if (s == cs) v[s] = 1;
+            uint64_t x = 0;
+            if (f == FDB_AGG_SUM || f == FDB_AGG_AVG) {
+              x = dt == FDB_FLOAT64 ? (uint64_t)__double_as_longlong(fv) : (uint64_t)iv;
+            } else if (f == FDB_AGG_MIN) {
+              x = ~(dt == FDB_FLOAT64 ? f64_ord_key(fv) : i64_ord_key(iv));
+            } else if (f == FDB_AGG_MAX) {
+              x = dt == FDB_FLOAT64 ? f64_ord_key(fv) : i64_ord_key(iv);
+            }
+#pragma unroll
+            for (int s = 1; s < kMaxSlots; ++s)
+              if (s == vs) v[s] = x;
+          }
+        }
+      }
+      // Warp-level combine of the lanes that share a group.
+      const unsigned peers = __match_any_sync(0xffffffffu, gid);
+      const int leader = __ffs(peers) - 1;
+#pragma unroll
+      for (int s = 0; s < kMaxSlots; ++s)
+        if (s < ns) stage[lane * kMaxSlots + s] = v[s];
+      __syncwarp();
+      if (lane == leader && gid != 0xFFFFFFFFu) {
+        unsigned rest = peers & ~(1u << lane);
+        while (rest) {
+          const int q = __ffs(rest) - 1;
+          rest &= rest - 1;
+#pragma unroll
+          for (int s = 0; s < kMaxSlots; ++s)
+            if (s < ns) v[s] = slot_combine(p.kind[s], v[s], stage[q * kMaxSlots + s]);
+        }
+        uint64_t* t = tab + (size_t)gid * ns;
+#pragma unroll
+        for (int s = 0; s < kMaxSlots; ++s)
+          if (s < ns) t[s] = slot_combine(p.kind[s], t[s], v[s]);
+      }
+      __syncwarp();
+    }
+  }
+
+  static __device__ void finish(Local&, const Params& p, unsigned char* sm, int ctid, int nct) {
+    uint64_t* tab = reinterpret_cast<uint64_t*>(sm);
+    unsigned int* s_last = reinterpret_cast<unsigned int*>(
+        sm + (size_t)kNW * kGbWarpTableEntries * 8 + (size_t)kNW * 32 * kMaxSlots * 8);
+    const int ns = p.nslots;
+    const uint32_t entries = p.ngroups * ns;
+    consumer_bar(nct);
+    // Fold warp tables in warp order into the CTA partial.
+    for (uint32_t e = ctid; e < entries; e += nct) {
+      const int kind = p.kind[e % ns];
+      uint64_t acc = tab[e];
+      for (int w = 1; w < kNW; ++w) acc = slot_combine(kind, acc, tab[(size_t)w * kGbWarpTableEntries + e]);
+      p.partials[(size_t)blockIdx.x * entries + e] = acc;
+    }
+    __threadfence();
+    consumer_bar(nct);
+    if (ctid == 0) {
+      const unsigned int t = atomicAdd(p.ticket, 1u);
+      *s_last = (t == gridDim.x - 1) ? 1u : 0u;
+    }
+    consumer_bar(nct);
+    if (*s_last == 0) return;
+    __threadfence();
+    // Last CTA: fold CTA partials in CTA order, one thread per table entry,
+    // into warp 0's table (reused as the final table).
+    for (uint32_t e = ctid; e < entries; e += nct) {
+      const int kind = p.kind[e % ns];
+      uint64_t acc = __ldcg(&p.partials[e]);
+      for (uint32_t b = 1; b < gridDim.x; ++b)
+        acc = slot_combine(kind, acc, __ldcg(&p.partials[(size_t)b * entries + e]));
+      tab[e] = acc;
+    }
+    consumer_bar(nct);
+    for (uint32_t g = ctid; g < p.ngroups; g += nct) {
+      const uint64_t* t = tab + (size_t)g * ns;
+      p.group_rows[g] = (int64_t)t[0];
+      for (int a = 0; a < p.naggs; ++a) {
+        const int f = p.func[a];
+        const int dt = f == FDB_AGG_COUNT_STAR ? FDB_INT64 : p.cols[p.acol[a]].dtype;
+        const uint64_t cnt = p.cslot[a] >= 0 ? t[p.cslot[a]] : t[0];
+        fdb_agg_value v;
+        v.f = 0.0;
+        v.i = 0;
+        v.n = (int64_t)cnt;
+        v.is_int = 0;
+        v.valid = cnt > 0;
+        if (f == FDB_AGG_COUNT_STAR || f == FDB_AGG_COUNT) {
+          v.is_int = 1;
+          v.i = (int64_t)cnt;
+          v.valid = 1;
+        } else if (f == FDB_AGG_SUM || f == FDB_AGG_AVG) {
+          const uint64_t x = t[p.vslot[a]];
+          const double s = dt == FDB_FLOAT64 ? __longlong_as_double((long long)x) : (double)(int64_t)x;
+          v.f = (f == FDB_AGG_AVG && cnt) ? s / (double)cnt : s;
+        } else if (cnt) {
+          uint64_t key = t[p.vslot[a]];
+          if (f == FDB_AGG_MIN) key = ~key;
+          v.f = dt == FDB_FLOAT64 ? f64_from_ord_key(key) : (double)(int64_t)(key ^ (1ull << 63));
+        }
+        p.out[(size_t)g * p.naggs + a] = v;
+      }
+    }
+    if (ctid == 0) *p.ticket = 0u;
+  }
+};
+
+// ===========================================================================
+// 2. int64-key hash GROUP BY
+// ===========================================================================
+struct GSlot {          // 40 bytes; all-zero = empty
+  uint64_t key;         // key ^ 2^63
+  unsigned long long count;
+  double sum;
+  unsigned long long nmin;  // ~order key of MIN (atomicMax)
+  unsigned long long max;   // order key of MAX
+};
+
+constexpr uint32_t kSmemSlots = 1024;      // CTA table slots (power of two)
+constexpr uint32_t kSmemProbe = 16;        // probes before a row spills to global
+constexpr uint32_t kGlobalProbeLimit = 1u << 16;
+
+struct GbHashParams {
+  PredProg prog;
+  DevCol cols[4];          // 0 = key, 1 = value, 2.. = predicate columns
+  GSlot* table;            // global, capacity pow2, zeroed
+  uint64_t mask;           // capacity - 1
+  GSlot* null_slot;        // accumulator of the NULL key group (zeroed)
+  int* err;
+};
+
+__device__ __forceinline__ void gslot_accum(GSlot* s, double v, bool has_v) {
+  atomicAdd(&s->count, 1ull);
+  if (has_v) {
+    atomicAdd(&s->sum, v);
+    if (!isnan(v)) {
+      const uint64_t k = f64_ord_key(v);
+      atomicMax(&s->nmin, (unsigned long long)~k);
+      atomicMax(&s->max, (unsigned long long)k);
+    }
+  }
+}
+
+__device__ __forceinline__ void gslot_merge(GSlot* s, const GSlot& v) {
+  atomicAdd(&s->count, v.count);
+  atomicAdd(&s->sum, v.sum);
+  atomicMax(&s->nmin, v.nmin);
+  atomicMax(&s->max, v.max);
+}
+
+// Find or claim the slot of `skey` (key ^ 2^63, nonzero) in a global table.
+// A table that is too small (more groups than slots) fails fast: the probe is
+// capped, the error word is set, and every later insert sees the error word
+// and gives up at once, so the kernel still ends promptly.
+__device__ __forceinline__ GSlot* gtable_slot(const GbHashParams& p, uint64_t skey) {
+  if (*reinterpret_cast<volatile int*>(p.err) != 0) return nullptr;
+  uint64_t h = mix64(skey) & p.mask;
+  const uint64_t limit = umin64(p.mask + 1, kGlobalProbeLimit);
+  for (uint64_t probe = 0; probe < limit; ++probe) {
+    GSlot* s = p.table + h;
+    uint64_t cur = *reinterpret_cast<volatile uint64_t*>(&s->key);
+    if (cur == skey) return s;
+    if (cur == 0) {
+      const uint64_t prev = atomicCAS(reinterpret_cast<unsigned long long*>(&s->key), 0ull,
+                                      (unsigned long long)skey);
+      if (prev == 0 || prev == skey) return s;
+    }
+    h = (h + 1) & p.mask;
+  }
+  atomicExch(p.err, kErrCapacity);
+  return nullptr;
+}
+
+struct GbHashOp {
+  using Params = GbHashParams;
+  struct Local {};
+  static constexpr size_t kSmem = (size_t)kSmemSlots * sizeof(GSlot) + sizeof(GSlot) + 16;
+
+  static __device__ void init(Local&, const Params&, unsigned char* sm, int ctid, int nct) {
+    uint64_t* w = reinterpret_cast<uint64_t*>(sm);
+    const size_t words = ((size_t)kSmemSlots + 1) * sizeof(GSlot) / 8;
+    for (size_t i = ctid; i < words; i += nct) w[i] = 0;
+  }
+
+  template <class Acc>
+  static __device__ void step(Local&, const Params& p, unsigned char* sm, const Acc& acc,
+                              uint32_t rows, int ctid, int nct) {
+    GSlot* tab = reinterpret_cast<GSlot*>(sm);
+    GSlot* snull = tab + kSmemSlots;
+    for (uint32_t i = ctid; i < rows; i += nct) {
+      const uint64_t row = acc.row(i);
+      if (p.prog.n) {
+        GbGetter<Acc> get{p.cols, acc, i, row};
+        if (!eval_prog(p.prog, get)) continue;
+      }
+      const int64_t key = acc.template get<int64_t>(0, i);
+      const bool kvalid = p.cols[0].validity ? col_valid(p.cols[0], row) : true;
+      bool has_v = p.cols[1].validity ? col_valid(p.cols[1], row) : true;
+      double v = 0.0;
+      if (has_v)
+        v = p.cols[1].dtype == FDB_FLOAT64 ? acc.template get<double>(1, i)
+                                           : (double)acc.template get<int64_t>(1, i);
+      if (!kvalid || key == INT64_MIN) {  // NULL group (i64::MIN reads as NULL)
+        gslot_accum(snull, v, has_v);
+        continue;
+      }
+      const uint64_t skey = (uint64_t)key ^ (1ull << 63);
+      uint32_t h = (uint32_t)mix64(skey) & (kSmemSlots - 1);
+      GSlot* dst = nullptr;
+      for (uint32_t probe = 0; probe < kSmemProbe; ++probe) {
+        GSlot* s = tab + h;
+        const uint64_t cur = *reinterpret_cast<volatile uint64_t*>(&s->key);
+        if (cur == skey) { dst = s; break; }
+        if (cur == 0) {
+          const uint64_t prev = atomicCAS(reinterpret_cast<unsigned long long*>(&s->key), 0ull,
+                                          (unsigned long long)skey);
+          if (prev == 0 || prev == skey) { dst = s; break; }
+        }
+        h = (h + 1) & (kSmemSlots - 1);
+      }
+      if (dst == nullptr) dst = gtable_slot(p, skey);
+      if (dst) gslot_accum(dst, v, has_v);
+    }
+  }
+
+  static __device__ void finish(Local&, const Params& p, unsigned char* sm, int ctid, int nct) {
+    GSlot* tab = reinterpret_cast<GSlot*>(sm);
+    consumer_bar(nct);
+    for (uint32_t i = ctid; i < kSmemSlots; i += nct) {
+      const GSlot s = tab[i];
+      if (s.key == 0) continue;
+      GSlot* g = gtable_slot(p, s.key);
+      if (g) gslot_merge(g, s);
+    }
+    if (ctid == 0) {
+      const GSlot s = tab[kSmemSlots];
+      if (s.count) gslot_merge(p.null_slot, s);
+    }
+  }
+};
+
+__global__ void gb_hash_compact_kernel(const GSlot* __restrict__ table, uint64_t capacity,
+                                       const GSlot* null_slot, fdb_group_i64* out, uint64_t cap_out,
+                                       unsigned long long* counter, int* err) {
+  const int lane = threadIdx.x & 31;
+  for (uint64_t i0 = blockIdx.x * (uint64_t)blockDim.x; i0 < capacity + 32;
+       i0 += (uint64_t)gridDim.x * blockDim.x) {
+    const uint64_t i = i0 + threadIdx.x;
+    GSlot s;
+    bool live = false;
+    if (i < capacity) {
+      s = table[i];
+      live = s.key != 0;
+    } else if (i == capacity && null_slot->count) {
+      s = *null_slot;
+      s.key = 0;  // key INT64_MIN after the XOR below
+      live = true;
+    }
+    const unsigned m = __ballot_sync(0xffffffffu, live);
+    if (!m) continue;
+    unsigned long long base = 0;
+    const int leader = __ffs(m) - 1;
+    if (lane == leader) base = atomicAdd(counter, (unsigned long long)__popc(m));
+    base = __shfl_sync(0xffffffffu, base, leader);
+    if (live) {
+      const uint64_t pos = base + __popc(m & ((1u << lane) - 1u));
+      if (pos < cap_out) {
+        fdb_group_i64 g;
+        g.key = (int64_t)(s.key ^ (1ull << 63));
+        g.count = (int64_t)s.count;
+        g.sum = s.sum;
+        g.min = s.nmin ? f64_from_ord_key(~s.nmin) : __longlong_as_double(0x7ff8000000000000ll);
+        g.max = s.max ? f64_from_ord_key(s.max) : __longlong_as_double(0x7ff8000000000000ll);
+        out[pos] = g;
+      } else {
+        atomicExch(err, kErrCapacity);
+      }
+    }
+  }
+}
+
+// ===========================================================================
+// Launchers
+// ===========================================================================
+template <class Op, int NC, int TR, int STAGES, int NCW>
+static void launch_stream_gb(Ctx& c, const fdb_dev_column* cols, uint64_t n,
+                             const typename Op::Params& p, size_t op_smem) {
+  StreamSrc<NC> src;
+  const void* bases[NC];
+  for (int i = 0; i < NC; ++i) {
+    src.base[i] = static_cast<const unsigned char*>(cols[i].values);
+    src.esize[i] = dtype_size(cols[i].dtype);
+    bases[i] = cols[i].values;
+  }
+  src.n = n;
+  src.m_end = stream_m_end(bases, NC, n);
+  const int op_off = (int)stream_smem_bytes<NC, TR, STAGES>();
+  const size_t smem = op_off + op_smem;
+  auto kern = stream_kernel<Op, NC, TR, STAGES, NCW>;
+  static bool attr = false;
+  if (!attr) {
+    FDB_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, 220 * 1024));
+    attr = true;
+  }
+  int per_sm = 0;
+  FDB_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, (NCW + 1) * 32, smem));
+  if (per_sm < 1) per_sm = 1;
+  if (per_sm > 4) per_sm = 4;
+  const uint64_t ntiles = (src.m_end + TR - 1) / TR;
+  uint64_t want = ntiles ? ntiles : (n + NCW * 32 * 8 - 1) / (NCW * 32 * 8);
+  if (want < 1) want = 1;
+  const int grid = (int)umin64(want, (uint64_t)c.sm_count * per_sm);
+  kern<<<grid, (NCW + 1) * 32, smem, c.stream>>>(src, p, c.d_err, op_off);
+  FDB_CUDA(cudaGetLastError());
+}
+
+static void gb_fill_prog(PredProg& pp, const fdb_pred_term* prog, int nterms, int ncols, int col_shift) {
+  if (nterms < 0 || nterms > FDB_MAX_TERMS) fail(FDB_E_ARG, "predicate has too many terms");
+  std::memset(&pp, 0, sizeof(pp));
+  pp.n = nterms;
+  int depth = 0;
+  for (int i = 0; i < nterms; ++i) {
+    pp.t[i] = prog[i];
+    const int k = prog[i].kind;
+    if (k == FDB_TERM_AND || k == FDB_TERM_OR) {
+      if (depth < 2) fail(FDB_E_ARG, "malformed predicate program");
+      --depth;
+    } else if (k == FDB_TERM_CMP || k == FDB_TERM_IS_NULL || k == FDB_TERM_IS_NOT_NULL ||
+               k == FDB_TERM_CODE_SET) {
+      if (prog[i].col < 0 || prog[i].col >= ncols) fail(FDB_E_ARG, "predicate column out of range");
+      if (k == FDB_TERM_CODE_SET && !prog[i].code_set) fail(FDB_E_ARG, "CODE_SET without a set");
+      pp.t[i].col += col_shift;
+      ++depth;
+    } else {
+      fail(FDB_E_ARG, "unknown predicate term kind");
+    }
+  }
+  if (nterms > 0 && depth != 1) fail(FDB_E_ARG, "malformed predicate program");
+}
+
+void op_group_by_codes(Ctx& c, const fdb_dev_column* cols, int ncols, uint64_t n,
+                       const fdb_pred_term* prog, int nterms, int key_col, uint32_t dict_len,
+                       const fdb_agg_spec* aggs, int naggs, fdb_agg_value* d_out,
+                       int64_t* d_group_rows) {
+  if (ncols < 1 || ncols > 4) fail(FDB_E_ARG, "between 1 and 4 input columns per GROUP BY scan");
+  if (naggs < 1 || naggs > 4) fail(FDB_E_ARG, "between 1 and 4 aggregates per GROUP BY");
+  if (key_col < 0 || key_col >= ncols || cols[key_col].dtype != FDB_UTF8)
+    fail(FDB_E_TYPE, "dictionary GROUP BY needs a Utf8 key column");
+  GbCodesParams p;
+  std::memset(&p, 0, sizeof(p));
+  for (int i = 0; i < ncols; ++i) {
+    if (!cols[i].values) fail(FDB_E_ARG, "column without values");
+    p.cols[i] = DevCol{cols[i].dtype, cols[i].values, cols[i].validity, cols[i].validity_offset};
+  }
+  gb_fill_prog(p.prog, prog, nterms, ncols, 0);
+  p.key_col = key_col;
+  p.ngroups = dict_len + 1;
+  p.naggs = naggs;
+  int ns = 1;
+  p.kind[0] = kAddU64;
+  for (int a = 0; a < naggs; ++a) {
+    const int f = aggs[a].func;
+    p.func[a] = f;
+    p.acol[a] = aggs[a].col;
+    p.vslot[a] = -1;
+    p.cslot[a] = -1;
+    if (f == FDB_AGG_COUNT_STAR) continue;
+    if (f < FDB_AGG_COUNT || f > FDB_AGG_MAX) fail(FDB_E_ARG, "aggregate not supported in GROUP BY");
+    if (aggs[a].col < 0 || aggs[a].col >= ncols) fail(FDB_E_ARG, "aggregate column out of range");
+    const int dt = cols[aggs[a].col].dtype;
+    if (f != FDB_AGG_COUNT && dt == FDB_UTF8) fail(FDB_E_TYPE, "SUM/AVG/MIN/MAX need a numeric column");
+    p.cslot[a] = ns;
+    p.kind[ns++] = kAddU64;
+    if (f == FDB_AGG_COUNT) continue;
+    p.vslot[a] = ns;
+    p.kind[ns++] = (f == FDB_AGG_SUM || f == FDB_AGG_AVG) ? (dt == FDB_FLOAT64 ? kAddF64 : kAddU64)
+                                                          : kMaxU64;
+  }
+  p.nslots = ns;
+  if ((uint64_t)p.ngroups * ns > kGbWarpTableEntries)
+    fail(FDB_E_ARG, "dictionary too large for the code GROUP BY ((dict_len+1) x slots > 512)");
+  const int max_grid = c.sm_count * 4;
+  p.partials = static_cast<uint64_t*>(c.scratch_take((size_t)max_grid * p.ngroups * ns * 8));
+  p.ticket = c.d_ticket;
+  p.out = d_out;
+  p.group_rows = d_group_rows;
+  switch (ncols) {
+    case 1: launch_stream_gb<GbCodesOp, 1, 2048, 4, 8>(c, cols, n, p, GbCodesOp::kSmem); break;
+    case 2: launch_stream_gb<GbCodesOp, 2, 1024, 4, 8>(c, cols, n, p, GbCodesOp::kSmem); break;
+    case 3: launch_stream_gb<GbCodesOp, 3, 1024, 3, 8>(c, cols, n, p, GbCodesOp::kSmem); break;
+    default: launch_stream_gb<GbCodesOp, 4, 1024, 3, 8>(c, cols, n, p, GbCodesOp::kSmem); break;
+  }
+}
+
+void op_group_by_i64(Ctx& c, const fdb_dev_column& key, const fdb_dev_column& value, uint64_t n,
+                     const fdb_pred_term* prog, int nterms, const fdb_dev_column* pred_cols,
+                     int npred, uint64_t expected_groups, double load_factor,
+                     fdb_group_i64* d_groups, uint64_t capacity, uint64_t* d_ngroups) {
+  if (key.dtype != FDB_INT64) fail(FDB_E_TYPE, "hash GROUP BY needs an INT64 key");
+  if (value.dtype != FDB_FLOAT64 && value.dtype != FDB_INT64)
+    fail(FDB_E_TYPE, "hash GROUP BY value must be FLOAT64 or INT64");
+  if (npred < 0 || npred > 2) fail(FDB_E_ARG, "at most 2 predicate columns");
+  if (load_factor <= 0.0 || load_factor >= 1.0) load_factor = 0.5;
+  if (expected_groups == 0) expected_groups = n ? n : 1;
+  uint64_t cap = 1024;
+  while ((double)cap * load_factor < (double)expected_groups) cap <<= 1;
+  const size_t tbytes = cap * sizeof(GSlot);
+  GSlot* table = static_cast<GSlot*>(c.scratch_take(tbytes + sizeof(GSlot)));
+  GSlot* null_slot = table + cap;
+  FDB_CUDA(cudaMemsetAsync(table, 0, tbytes + sizeof(GSlot), c.stream));
+  unsigned long long* counter = static_cast<unsigned long long*>(c.scratch_take(8));
+  FDB_CUDA(cudaMemsetAsync(counter, 0, 8, c.stream));
+
+  GbHashParams p;
+  std::memset(&p, 0, sizeof(p));
+  fdb_dev_column all[4];
+  all[0] = key;
+  all[1] = value;
+  for (int i = 0; i < npred; ++i) all[2 + i] = pred_cols[i];
+  const int nc = 2 + npred;
+  for (int i = 0; i < nc; ++i) {
+    if (!all[i].values) fail(FDB_E_ARG, "column without values");
+    p.cols[i] = DevCol{all[i].dtype, all[i].values, all[i].validity, all[i].validity_offset};
+  }
+  gb_fill_prog(p.prog, prog, nterms, npred, 2);
+  p.table = table;
+  p.mask = cap - 1;
+  p.null_slot = null_slot;
+  p.err = c.d_err;
+  if (n > 0) {
+    switch (nc) {
+      case 2: launch_stream_gb<GbHashOp, 2, 1024, 3, 8>(c, all, n, p, GbHashOp::kSmem); break;
+      case 3: launch_stream_gb<GbHashOp, 3, 1024, 2, 8>(c, all, n, p, GbHashOp::kSmem); break;
+      default: launch_stream_gb<GbHashOp, 4, 512, 3, 8>(c, all, n, p, GbHashOp::kSmem); break;
+    }
+  }
+  const unsigned blocks = (unsigned)umin64((cap + 255) / 256 + 1, (uint64_t)c.sm_count * 8);
+  gb_hash_compact_kernel<<<blocks, 256, 0, c.stream>>>(table, cap, null_slot, d_groups, capacity,
+                                                       counter, c.d_err);
+  FDB_CUDA(cudaGetLastError());
+  FDB_CUDA(cudaMemcpyAsync(d_ngroups, counter, 8, cudaMemcpyDeviceToDevice, c.stream));
+}
+
+}  // namespace fdb

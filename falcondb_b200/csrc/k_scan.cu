@@ -1,0 +1,880 @@
+// Scan kernels: WHERE mask, COUNT(*) WHERE, no-key aggregates, dictionary-code
+// presence (COUNT DISTINCT), selection compaction and gather.
+//
+// Reference routines replaced (FalconDB, src/):
+//   eval_mask_bits / fast_cmp_mask / cmp_f64_avx2 ........ query/expr.rs:635-1175
+//   COUNT(*)+WHERE popcount ............................... db.rs:1439-1476
+//   execute_agg_only / accumulate_typed / sum_lanes ....... query/aggregate.rs:1394-1590, 3121-3386
+//   present_codes (COUNT DISTINCT over a dictionary) ...... query/aggregate.rs:3167-3200
+//   gather_by_bitmask / filter_by_bitmask_cols ............ storage/column.rs:1077-1123, table.rs:148-189
+#include <cstring>
+
+#include "common.cuh"
+#include "engine.h"
+#include "stream.cuh"
+
+namespace fdb {
+
+// ---------------------------------------------------------------------------
+// Shared: predicate + column getter used by the scan ops.
+// ---------------------------------------------------------------------------
+struct ScanCols {
+  DevCol cols[4];
+};
+
+template <class Acc>
+struct RowGetter {
+  const ScanCols& sc;
+  const Acc& acc;
+  uint32_t i;
+  uint64_t row;
+  __device__ __forceinline__ int operator()(int c, int64_t& iv, double& fv, uint32_t& code,
+                                            bool& valid) const {
+    const DevCol& col = sc.cols[c];
+    const int dt = col.dtype;
+    if (dt == FDB_FLOAT64)
+      fv = acc.template get<double>(c, i);
+    else if (dt == FDB_INT64)
+      iv = acc.template get<int64_t>(c, i);
+    else
+      code = acc.template get<uint32_t>(c, i);
+    valid = col.validity ? col_valid(col, row) : true;
+    return dt;
+  }
+};
+
+// ---------------------------------------------------------------------------
+// No-key aggregate op (execute_agg_only).  Per-thread accumulators, a fixed
+// block tree, per-CTA partials, and a last-CTA final pass in CTA order: the
+// FP64 reduction order depends only on the grid, so results are repeatable.
+// ---------------------------------------------------------------------------
+struct AggAcc {
+  double f;      // FP64 sum
+  uint64_t slo;  // exact int sum, low 64 bits (two's complement, 128-bit)
+  int64_t shi;   // high 64 bits
+  uint64_t n;    // rows / values counted
+  uint64_t m;    // MIN / MAX order key
+};
+
+__device__ __forceinline__ void i128_add(uint64_t& lo, int64_t& hi, uint64_t blo, int64_t bhi) {
+  uint64_t r = lo + blo;
+  hi = hi + bhi + (r < lo ? 1 : 0);
+  lo = r;
+}
+
+__device__ __forceinline__ void agg_combine(AggAcc& a, const AggAcc& b, int func) {
+  a.f += b.f;
+  i128_add(a.slo, a.shi, b.slo, b.shi);
+  a.n += b.n;
+  if (func == FDB_AGG_MIN) a.m = b.m < a.m ? b.m : a.m;
+  if (func == FDB_AGG_MAX) a.m = b.m > a.m ? b.m : a.m;
+}
+
+__device__ __forceinline__ AggAcc agg_identity(int func) {
+  AggAcc a;
+  a.f = 0.0;
+  a.slo = 0;
+  a.shi = 0;
+  a.n = 0;
+  a.m = func == FDB_AGG_MIN ? ~0ull : 0ull;
+  return a;
+}
+
+__device__ __forceinline__ AggAcc warp_agg(AggAcc a, int func) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) {
+    AggAcc b;
+    b.f = __shfl_xor_sync(0xffffffffu, a.f, o);
+    b.slo = __shfl_xor_sync(0xffffffffu, a.slo, o);
+    b.shi = __shfl_xor_sync(0xffffffffu, a.shi, o);
+    b.n = __shfl_xor_sync(0xffffffffu, a.n, o);
+    b.m = __shfl_xor_sync(0xffffffffu, a.m, o);
+    agg_combine(a, b, func);
+  }
+  return a;
+}
+
+__device__ double i128_to_f64(uint64_t lo, int64_t hi) {
+  if ((hi == 0 && (int64_t)lo >= 0) || (hi == -1 && (int64_t)lo < 0)) return (double)(int64_t)lo;
+  return (double)hi * 18446744073709551616.0 + (double)lo;
+}
+
+struct ScanAggParams {
+  PredProg prog;
+  ScanCols sc;
+  int32_t naggs;
+  int32_t func[4];
+  int32_t acol[4];
+  AggAcc* partials;       // [gridDim.x * 4]
+  unsigned int* ticket;   // zero on entry; reset by the last CTA
+  fdb_agg_value* out;     // [naggs] or nullptr
+  uint64_t* out_count;    // receives agg 0's count (COUNT(*) WHERE) or nullptr
+};
+
+struct ScanAggOp {
+  using Params = ScanAggParams;
+  struct Local {
+    AggAcc a[4];
+  };
+  static constexpr int kSmem = 32 * 4 * sizeof(AggAcc) + 16;
+
+  static __device__ void init(Local& st, const Params& p, unsigned char*, int, int) {
+#pragma unroll
+    for (int a = 0; a < 4; ++a) st.a[a] = agg_identity(a < p.naggs ? p.func[a] : FDB_AGG_COUNT);
+  }
+
+  template <class Acc>
+  static __device__ __forceinline__ void one_row(Local& st, const Params& p, const Acc& acc,
+                                                 uint32_t i) {
+    const uint64_t row = acc.row(i);
+    RowGetter<Acc> get{p.sc, acc, i, row};
+    if (!eval_prog(p.prog, get)) return;
+#pragma unroll
+    for (int a = 0; a < 4; ++a) {
+      if (a >= p.naggs) break;
+      const int f = p.func[a];
+      if (f == FDB_AGG_COUNT_STAR) {
+        st.a[a].n++;
+        continue;
+      }
+      int64_t iv = 0;
+      double fv = 0.0;
+      uint32_t code = 0;
+      bool valid = true;
+      const int dt = get(p.acol[a], iv, fv, code, valid);
+      if (!valid) continue;
+      if (f == FDB_AGG_COUNT) {
+        st.a[a].n++;
+      } else if (f == FDB_AGG_SUM || f == FDB_AGG_AVG) {
+        if (dt == FDB_FLOAT64)
+          st.a[a].f += fv;
+        else
+          i128_add(st.a[a].slo, st.a[a].shi, (uint64_t)iv, iv < 0 ? -1 : 0);
+        st.a[a].n++;
+      } else if (f == FDB_AGG_MIN || f == FDB_AGG_MAX) {
+        uint64_t k;
+        if (dt == FDB_FLOAT64) {
+          if (isnan(fv)) continue;  // f64::min / f64::max skip NaN
+          k = f64_ord_key(fv);
+        } else {
+          k = i64_ord_key(iv);
+        }
+        if (f == FDB_AGG_MIN)
+          st.a[a].m = k < st.a[a].m ? k : st.a[a].m;
+        else
+          st.a[a].m = k > st.a[a].m ? k : st.a[a].m;
+        st.a[a].n++;
+      }
+    }
+  }
+
+  template <class Acc>
+  static __device__ void step(Local& st, const Params& p, unsigned char*, const Acc& acc,
+                              uint32_t rows, int ctid, int nct) {
+    for (uint32_t i = ctid; i < rows; i += nct) one_row(st, p, acc, i);
+  }
+
+  // Block-reduce `st` into op_smem slot 0 (returned by thread 0).
+  static __device__ void block_reduce(Local& st, const Params& p, AggAcc* sm, int ctid, int nct) {
+    const int warp = ctid >> 5, lane = ctid & 31, nw = nct >> 5;
+#pragma unroll
+    for (int a = 0; a < 4; ++a) {
+      if (a >= p.naggs) break;
+      AggAcc w = warp_agg(st.a[a], p.func[a]);
+      if (lane == 0) sm[warp * 4 + a] = w;
+    }
+    consumer_bar(nct);
+    if (ctid == 0) {
+#pragma unroll
+      for (int a = 0; a < 4; ++a) {
+        if (a >= p.naggs) break;
+        AggAcc t = sm[a];
+        for (int w = 1; w < nw; ++w) agg_combine(t, sm[w * 4 + a], p.func[a]);
+        st.a[a] = t;
+      }
+    }
+  }
+
+  static __device__ void finish(Local& st, const Params& p, unsigned char* op_smem, int ctid,
+                                int nct) {
+    AggAcc* sm = reinterpret_cast<AggAcc*>(op_smem);
+    unsigned int* s_last = reinterpret_cast<unsigned int*>(op_smem + 32 * 4 * sizeof(AggAcc));
+    block_reduce(st, p, sm, ctid, nct);
+    if (ctid == 0) {
+#pragma unroll
+      for (int a = 0; a < 4; ++a)
+        if (a < p.naggs) p.partials[blockIdx.x * 4 + a] = st.a[a];
+      __threadfence();
+      unsigned int t = atomicAdd(p.ticket, 1u);
+      *s_last = (t == gridDim.x - 1) ? 1u : 0u;
+    }
+    consumer_bar(nct);
+    if (*s_last == 0) return;
+    __threadfence();
+    // Last CTA: combine the per-CTA partials in CTA order.
+#pragma unroll
+    for (int a = 0; a < 4; ++a) {
+      if (a >= p.naggs) break;
+      AggAcc t = agg_identity(p.func[a]);
+      for (int b = ctid; b < (int)gridDim.x; b += nct) {
+        const AggAcc* src = p.partials + b * 4 + a;
+        AggAcc v;
+        v.f = __ldcg(&src->f);
+        v.slo = __ldcg(&src->slo);
+        v.shi = __ldcg(&src->shi);
+        v.n = __ldcg(&src->n);
+        v.m = __ldcg(&src->m);
+        agg_combine(t, v, p.func[a]);
+      }
+      st.a[a] = t;
+    }
+    consumer_bar(nct);
+    block_reduce(st, p, sm, ctid, nct);
+    if (ctid == 0) {
+#pragma unroll
+      for (int a = 0; a < 4; ++a) {
+        if (a >= p.naggs) break;
+        const AggAcc& t = st.a[a];
+        const int f = p.func[a];
+        const int dt = f == FDB_AGG_COUNT_STAR ? FDB_INT64 : p.sc.cols[p.acol[a]].dtype;
+        fdb_agg_value v;
+        v.f = 0.0;
+        v.i = 0;
+        v.n = (int64_t)t.n;
+        v.is_int = 0;
+        v.valid = t.n > 0;
+        if (f == FDB_AGG_COUNT_STAR || f == FDB_AGG_COUNT) {
+          v.is_int = 1;
+          v.i = (int64_t)t.n;
+          v.valid = 1;
+        } else if (f == FDB_AGG_SUM || f == FDB_AGG_AVG) {
+          double s = dt == FDB_FLOAT64 ? t.f : i128_to_f64(t.slo, t.shi);
+          v.f = (f == FDB_AGG_AVG && t.n > 0) ? s / (double)t.n : s;
+        } else if (f == FDB_AGG_MIN || f == FDB_AGG_MAX) {
+          if (t.n > 0)
+            v.f = dt == FDB_FLOAT64 ? f64_from_ord_key(t.m) : (double)(int64_t)(t.m ^ (1ull << 63));
+        }
+        if (p.out) p.out[a] = v;
+        if (a == 0 && p.out_count) *p.out_count = t.n;
+      }
+      *p.ticket = 0u;
+    }
+  }
+};
+
+// ---------------------------------------------------------------------------
+// Specialised scans for the two shapes that dominate analytical scans: an
+// aggregate over one NULL-free column with no WHERE (SUM(score)), and COUNT(*)
+// WHERE `col op literal` over one NULL-free column (the popcount fast path of
+// db.rs:1439-1476).  Same partials / final pass as ScanAggOp; the comparison
+// and the value type are template parameters so nothing is decided per row.
+// ---------------------------------------------------------------------------
+template <typename T>
+__device__ __forceinline__ void fold_value(AggAcc& a, int f, T v) {
+  if (f == FDB_AGG_SUM || f == FDB_AGG_AVG) {
+    if constexpr (sizeof(T) == 8 && T(0.5) != T(0))
+      a.f += v;
+    else
+      i128_add(a.slo, a.shi, (uint64_t)v, v < 0 ? -1 : 0);
+  } else if (f == FDB_AGG_MIN || f == FDB_AGG_MAX) {
+    uint64_t k;
+    if constexpr (T(0.5) != T(0)) {
+      if (isnan(v)) return;
+      k = f64_ord_key(v);
+    } else {
+      k = i64_ord_key(v);
+    }
+    if (f == FDB_AGG_MIN)
+      a.m = k < a.m ? k : a.m;
+    else
+      a.m = k > a.m ? k : a.m;
+  }
+  a.n++;
+}
+
+// Aggregates over column 0 only, no predicate, no NULLs.
+template <typename T>
+struct ColAggOp : ScanAggOp {
+  template <class Acc>
+  static __device__ void step(Local& st, const Params& p, unsigned char*, const Acc& acc,
+                              uint32_t rows, int ctid, int nct) {
+    uint32_t i = ctid;
+    for (; i + nct < rows; i += 2 * nct) {
+      const T v0 = acc.template get<T>(0, i);
+      const T v1 = acc.template get<T>(0, i + nct);
+#pragma unroll
+      for (int a = 0; a < 4; ++a) {
+        if (a >= p.naggs) break;
+        fold_value<T>(st.a[a], p.func[a], v0);
+        fold_value<T>(st.a[a], p.func[a], v1);
+      }
+    }
+    for (; i < rows; i += nct) {
+      const T v = acc.template get<T>(0, i);
+#pragma unroll
+      for (int a = 0; a < 4; ++a) {
+        if (a >= p.naggs) break;
+        fold_value<T>(st.a[a], p.func[a], v);
+      }
+    }
+  }
+};
+
+template <int OP, typename T>
+__device__ __forceinline__ bool cmp_fixed(T a, T b) {
+  if constexpr (OP == FDB_EQ) return a == b;
+  else if constexpr (OP == FDB_NE) return a != b;
+  else if constexpr (OP == FDB_LT) return a < b;
+  else if constexpr (OP == FDB_LE) return a <= b;
+  else if constexpr (OP == FDB_GT) return a > b;
+  else return a >= b;
+}
+
+// COUNT(*) WHERE col OP literal; T is the comparison type (double for a
+// FLOAT64 column or a widened INT64 one), S the stored type.
+template <typename S, typename T, int OP>
+struct CmpCountOp : ScanAggOp {
+  template <class Acc>
+  static __device__ void step(Local& st, const Params& p, unsigned char*, const Acc& acc,
+                              uint32_t rows, int ctid, int nct) {
+    const T lit = sizeof(T) == 8 && T(0.5) != T(0)
+                      ? (T)(p.prog.t[0].lit_type == FDB_FLOAT64 ? p.prog.t[0].lit_f : (double)p.prog.t[0].lit_i)
+                      : (T)p.prog.t[0].lit_i;
+    uint32_t cnt = 0;
+    uint32_t i = ctid;
+    for (; i + 3 * nct < rows; i += 4 * nct) {
+      cnt += cmp_fixed<OP, T>((T)acc.template get<S>(0, i), lit);
+      cnt += cmp_fixed<OP, T>((T)acc.template get<S>(0, i + nct), lit);
+      cnt += cmp_fixed<OP, T>((T)acc.template get<S>(0, i + 2 * nct), lit);
+      cnt += cmp_fixed<OP, T>((T)acc.template get<S>(0, i + 3 * nct), lit);
+    }
+    for (; i < rows; i += nct) cnt += cmp_fixed<OP, T>((T)acc.template get<S>(0, i), lit);
+    st.a[0].n += cnt;
+  }
+};
+
+// ---------------------------------------------------------------------------
+// Dictionary-code presence (COUNT DISTINCT over a Utf8 column).
+// ---------------------------------------------------------------------------
+struct DistinctParams {
+  PredProg prog;
+  ScanCols sc;
+  int32_t code_col;
+  uint32_t dict_len;
+  uint64_t* bitmap;  // global, zeroed before launch
+};
+
+struct DistinctOp {
+  using Params = DistinctParams;
+  struct Local {
+    uint64_t bits;   // dict_len <= 64: codes seen by this thread
+  };
+  static constexpr int kSmemMaxCodes = 32768;
+  static constexpr int kSmem = kSmemMaxCodes / 8;
+
+  static __device__ void init(Local& st, const Params& p, unsigned char* sm, int ctid, int nct) {
+    st.bits = 0;
+    if (p.dict_len > 64 && p.dict_len <= kSmemMaxCodes) {
+      uint32_t* w = reinterpret_cast<uint32_t*>(sm);
+      for (int i = ctid; i < kSmemMaxCodes / 32; i += nct) w[i] = 0;
+    }
+  }
+  template <class Acc>
+  static __device__ void step(Local& st, const Params& p, unsigned char* sm, const Acc& acc,
+                              uint32_t rows, int ctid, int nct) {
+    const bool small = p.dict_len <= 64;
+    const bool in_smem = !small && p.dict_len <= kSmemMaxCodes;
+    uint32_t* w = reinterpret_cast<uint32_t*>(sm);
+    for (uint32_t i = ctid; i < rows; i += nct) {
+      const uint64_t row = acc.row(i);
+      if (p.prog.n) {
+        RowGetter<Acc> get{p.sc, acc, i, row};
+        if (!eval_prog(p.prog, get)) continue;
+      }
+      const uint32_t code = acc.template get<uint32_t>(p.code_col, i);
+      if (code == kNullCode || code >= p.dict_len) continue;
+      const DevCol& c = p.sc.cols[p.code_col];
+      if (c.validity && !col_valid(c, row)) continue;
+      if (small) {
+        st.bits |= 1ull << code;
+      } else if (in_smem) {
+        const uint32_t m = 1u << (code & 31);
+        if (!(w[code >> 5] & m)) atomicOr(&w[code >> 5], m);
+      } else {
+        const unsigned long long m = 1ull << (code & 63);
+        if (!(p.bitmap[code >> 6] & m)) atomicOr((unsigned long long*)&p.bitmap[code >> 6], m);
+      }
+    }
+  }
+  static __device__ void finish(Local& st, const Params& p, unsigned char* sm, int ctid, int nct) {
+    if (p.dict_len <= 64) {
+      uint64_t b = st.bits;
+#pragma unroll
+      for (int o = 16; o > 0; o >>= 1) b |= __shfl_xor_sync(0xffffffffu, b, o);
+      if ((ctid & 31) == 0 && b) atomicOr((unsigned long long*)&p.bitmap[0], (unsigned long long)b);
+      return;
+    }
+    if (p.dict_len <= kSmemMaxCodes) {
+      consumer_bar(nct);
+      const uint32_t* w = reinterpret_cast<const uint32_t*>(sm);
+      const uint32_t nw = (p.dict_len + 31) / 32;
+      for (uint32_t i = ctid; i < nw; i += nct)
+        if (w[i]) atomicOr((unsigned int*)p.bitmap + i, w[i]);  // little-endian u64 halves
+    }
+  }
+};
+
+// ---------------------------------------------------------------------------
+// Launch helpers for the streamer.
+// ---------------------------------------------------------------------------
+// Tile rows per column and ring depth: ~64 KB of staging per CTA so that three
+// CTAs (24 consumer warps) fit on one SM.
+template <int NC>
+struct TileShape {
+  static constexpr int TR = NC == 1 ? 2048 : 1024;
+  static constexpr int STAGES = NC <= 2 ? 4 : 3;
+  static constexpr int NCW = 8;
+};
+
+template <class Op, int NC>
+static void launch_stream(Ctx& c, const fdb_dev_column* cols, uint64_t n, const typename Op::Params& p,
+                          size_t op_smem_bytes) {
+  using S = TileShape<NC>;
+  StreamSrc<NC> src;
+  const void* bases[NC];
+  for (int i = 0; i < NC; ++i) {
+    src.base[i] = static_cast<const unsigned char*>(cols[i].values);
+    src.esize[i] = dtype_size(cols[i].dtype);
+    bases[i] = cols[i].values;
+  }
+  src.n = n;
+  src.m_end = stream_m_end(bases, NC, n);
+  const int op_off = (int)stream_smem_bytes<NC, S::TR, S::STAGES>();
+  const size_t smem = op_off + op_smem_bytes;
+  auto kern = stream_kernel<Op, NC, S::TR, S::STAGES, S::NCW>;
+  static bool attr_done = false;  // per instantiation
+  if (!attr_done) {
+    FDB_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024));
+    attr_done = true;
+  }
+  int per_sm = 0;
+  FDB_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, (S::NCW + 1) * 32, smem));
+  if (per_sm < 1) per_sm = 1;
+  if (per_sm > 4) per_sm = 4;  // per-CTA partials are sized for 4 CTAs per SM
+  const uint64_t ntiles = (src.m_end + S::TR - 1) / S::TR;
+  uint64_t want = ntiles ? ntiles : (n + S::NCW * 32 * 8 - 1) / (S::NCW * 32 * 8);
+  if (want < 1) want = 1;
+  const int grid = (int)umin64(want, (uint64_t)c.sm_count * per_sm);
+  kern<<<grid, (S::NCW + 1) * 32, smem, c.stream>>>(src, p, c.d_err, op_off);
+  FDB_CUDA(cudaGetLastError());
+}
+
+template <class Op>
+static void launch_stream_nc(Ctx& c, const fdb_dev_column* cols, int ncols, uint64_t n,
+                             const typename Op::Params& p, size_t op_smem) {
+  switch (ncols) {
+    case 1: launch_stream<Op, 1>(c, cols, n, p, op_smem); break;
+    case 2: launch_stream<Op, 2>(c, cols, n, p, op_smem); break;
+    case 3: launch_stream<Op, 3>(c, cols, n, p, op_smem); break;
+    case 4: launch_stream<Op, 4>(c, cols, n, p, op_smem); break;
+    default: fail(FDB_E_ARG, "between 1 and 4 input columns are supported per scan");
+  }
+}
+
+// Grid upper bound used to size per-CTA partials.
+static int max_stream_grid(Ctx& c) { return c.sm_count * 4; }
+
+static void fill_prog(PredProg& pp, const fdb_pred_term* prog, int nterms, int ncols) {
+  if (nterms < 0 || nterms > FDB_MAX_TERMS) fail(FDB_E_ARG, "predicate has too many terms");
+  std::memset(&pp, 0, sizeof(pp));
+  pp.n = nterms;
+  int depth = 0;
+  for (int i = 0; i < nterms; ++i) {
+    pp.t[i] = prog[i];
+    const int k = prog[i].kind;
+    if (k == FDB_TERM_AND || k == FDB_TERM_OR) {
+      if (depth < 2) fail(FDB_E_ARG, "malformed predicate program (AND/OR needs two operands)");
+      depth -= 1;
+    } else if (k == FDB_TERM_CMP || k == FDB_TERM_IS_NULL || k == FDB_TERM_IS_NOT_NULL ||
+               k == FDB_TERM_CODE_SET) {
+      if (prog[i].col < 0 || prog[i].col >= ncols) fail(FDB_E_ARG, "predicate column out of range");
+      if (k == FDB_TERM_CMP && (prog[i].op < FDB_EQ || prog[i].op > FDB_GE))
+        fail(FDB_E_ARG, "bad comparison operator");
+      if (k == FDB_TERM_CODE_SET && prog[i].code_set == nullptr)
+        fail(FDB_E_ARG, "CODE_SET term without a code set");
+      depth += 1;
+    } else {
+      fail(FDB_E_ARG, "unknown predicate term kind");
+    }
+  }
+  if (nterms > 0 && depth != 1) fail(FDB_E_ARG, "malformed predicate program");
+}
+
+static void fill_cols(ScanCols& sc, const fdb_dev_column* cols, int ncols) {
+  if (ncols < 1 || ncols > 4) fail(FDB_E_ARG, "between 1 and 4 input columns are supported per scan");
+  std::memset(&sc, 0, sizeof(sc));
+  for (int i = 0; i < ncols; ++i) {
+    if (cols[i].values == nullptr) fail(FDB_E_ARG, "column without values");
+    if (cols[i].dtype != FDB_INT64 && cols[i].dtype != FDB_FLOAT64 && cols[i].dtype != FDB_UTF8)
+      fail(FDB_E_TYPE, "unsupported column type");
+    sc.cols[i] = DevCol{cols[i].dtype, cols[i].values, cols[i].validity, cols[i].validity_offset};
+  }
+}
+
+void op_aggregate(Ctx& c, const fdb_dev_column* cols, int ncols, uint64_t n,
+                  const fdb_pred_term* prog, int nterms, const fdb_agg_spec* aggs, int naggs,
+                  fdb_agg_value* d_out) {
+  if (naggs < 1 || naggs > 4) fail(FDB_E_ARG, "between 1 and 4 aggregates per scan");
+  ScanAggParams p;
+  std::memset(&p, 0, sizeof(p));
+  fill_cols(p.sc, cols, ncols);
+  fill_prog(p.prog, prog, nterms, ncols);
+  p.naggs = naggs;
+  for (int a = 0; a < naggs; ++a) {
+    const int f = aggs[a].func;
+    if (f < FDB_AGG_COUNT_STAR || f > FDB_AGG_MAX)
+      fail(FDB_E_ARG, "aggregate not supported by fdb_aggregate (COUNT DISTINCT: fdb_distinct_codes)");
+    if (f != FDB_AGG_COUNT_STAR) {
+      if (aggs[a].col < 0 || aggs[a].col >= ncols) fail(FDB_E_ARG, "aggregate column out of range");
+      if (f != FDB_AGG_COUNT && cols[aggs[a].col].dtype == FDB_UTF8)
+        fail(FDB_E_TYPE, "SUM/AVG/MIN/MAX need a numeric column");
+    }
+    p.func[a] = f;
+    p.acol[a] = aggs[a].col;
+  }
+  p.partials = static_cast<AggAcc*>(c.scratch_take(sizeof(AggAcc) * 4 * max_stream_grid(c)));
+  p.ticket = c.d_ticket;
+  p.out = d_out;
+  p.out_count = nullptr;
+  // One NULL-free numeric column, no WHERE, every aggregate over it.
+  bool single = ncols == 1 && nterms == 0 && cols[0].validity == nullptr && cols[0].dtype != FDB_UTF8;
+  for (int a = 0; a < naggs && single; ++a)
+    single = aggs[a].func == FDB_AGG_COUNT_STAR || aggs[a].col == 0;
+  if (single) {
+    if (cols[0].dtype == FDB_FLOAT64)
+      launch_stream<ColAggOp<double>, 1>(c, cols, n, p, ScanAggOp::kSmem);
+    else
+      launch_stream<ColAggOp<int64_t>, 1>(c, cols, n, p, ScanAggOp::kSmem);
+    return;
+  }
+  launch_stream_nc<ScanAggOp>(c, cols, ncols, n, p, ScanAggOp::kSmem);
+}
+
+template <typename S, typename T>
+static void launch_cmp_count(Ctx& c, const fdb_dev_column* cols, uint64_t n, const ScanAggParams& p, int op) {
+  switch (op) {
+    case FDB_EQ: launch_stream<CmpCountOp<S, T, FDB_EQ>, 1>(c, cols, n, p, ScanAggOp::kSmem); break;
+    case FDB_NE: launch_stream<CmpCountOp<S, T, FDB_NE>, 1>(c, cols, n, p, ScanAggOp::kSmem); break;
+    case FDB_LT: launch_stream<CmpCountOp<S, T, FDB_LT>, 1>(c, cols, n, p, ScanAggOp::kSmem); break;
+    case FDB_LE: launch_stream<CmpCountOp<S, T, FDB_LE>, 1>(c, cols, n, p, ScanAggOp::kSmem); break;
+    case FDB_GT: launch_stream<CmpCountOp<S, T, FDB_GT>, 1>(c, cols, n, p, ScanAggOp::kSmem); break;
+    default: launch_stream<CmpCountOp<S, T, FDB_GE>, 1>(c, cols, n, p, ScanAggOp::kSmem); break;
+  }
+}
+
+void op_filter_count(Ctx& c, const fdb_dev_column* cols, int ncols, uint64_t n,
+                     const fdb_pred_term* prog, int nterms, uint64_t* d_count) {
+  ScanAggParams p;
+  std::memset(&p, 0, sizeof(p));
+  fill_cols(p.sc, cols, ncols);
+  fill_prog(p.prog, prog, nterms, ncols);
+  p.naggs = 1;
+  p.func[0] = FDB_AGG_COUNT_STAR;
+  p.acol[0] = 0;
+  p.partials = static_cast<AggAcc*>(c.scratch_take(sizeof(AggAcc) * 4 * max_stream_grid(c)));
+  p.ticket = c.d_ticket;
+  p.out = nullptr;
+  p.out_count = d_count;
+  // `col op literal` over one NULL-free numeric column.
+  if (ncols == 1 && nterms == 1 && prog[0].kind == FDB_TERM_CMP && prog[0].col == 0 &&
+      cols[0].validity == nullptr && cols[0].dtype != FDB_UTF8) {
+    if (cols[0].dtype == FDB_FLOAT64)
+      launch_cmp_count<double, double>(c, cols, n, p, prog[0].op);
+    else if (prog[0].lit_type == FDB_FLOAT64)
+      launch_cmp_count<int64_t, double>(c, cols, n, p, prog[0].op);  // widened (expr.rs:1122-1132)
+    else
+      launch_cmp_count<int64_t, int64_t>(c, cols, n, p, prog[0].op);
+    return;
+  }
+  launch_stream_nc<ScanAggOp>(c, cols, ncols, n, p, ScanAggOp::kSmem);
+}
+
+void op_distinct_codes(Ctx& c, const fdb_dev_column* cols, int ncols, uint64_t n,
+                       const fdb_pred_term* prog, int nterms, int code_col, uint32_t dict_len,
+                       uint64_t* d_bitmap) {
+  DistinctParams p;
+  std::memset(&p, 0, sizeof(p));
+  fill_cols(p.sc, cols, ncols);
+  fill_prog(p.prog, prog, nterms, ncols);
+  if (code_col < 0 || code_col >= ncols || cols[code_col].dtype != FDB_UTF8)
+    fail(FDB_E_TYPE, "COUNT DISTINCT over codes needs a Utf8 column");
+  p.code_col = code_col;
+  p.dict_len = dict_len;
+  p.bitmap = d_bitmap;
+  const size_t words = (dict_len + 63) / 64;
+  if (words) FDB_CUDA(cudaMemsetAsync(d_bitmap, 0, words * 8, c.stream));
+  if (n == 0 || dict_len == 0) return;
+  launch_stream_nc<DistinctOp>(c, cols, ncols, n, p, DistinctOp::kSmem);
+}
+
+// ---------------------------------------------------------------------------
+// WHERE mask: one warp per 64-row word, two ballots per word; padding bits zero.
+// ---------------------------------------------------------------------------
+struct MaskParams {
+  PredProg prog;
+  ScanCols sc;
+};
+
+__device__ __forceinline__ bool row_passes(const MaskParams& p, uint64_t row) {
+  auto get = [&](int c, int64_t& iv, double& fv, uint32_t& code, bool& valid) -> int {
+    const DevCol& col = p.sc.cols[c];
+    const int dt = col.dtype;
+    if (dt == FDB_FLOAT64)
+      fv = static_cast<const double*>(col.values)[row];
+    else if (dt == FDB_INT64)
+      iv = static_cast<const int64_t*>(col.values)[row];
+    else
+      code = static_cast<const uint32_t*>(col.values)[row];
+    valid = col.validity ? col_valid(col, row) : true;
+    return dt;
+  };
+  return eval_prog(p.prog, get);
+}
+
+__global__ void filter_mask_kernel(MaskParams p, uint64_t n, uint64_t* mask) {
+  const uint64_t nwords = (n + 63) / 64;
+  const int lane = threadIdx.x & 31;
+  const uint64_t gw = (blockIdx.x * (uint64_t)blockDim.x + threadIdx.x) >> 5;
+  const uint64_t nwarps = ((uint64_t)gridDim.x * blockDim.x) >> 5;
+  for (uint64_t w = gw; w < nwords; w += nwarps) {
+    const uint64_t r0 = w * 64 + lane, r1 = r0 + 32;
+    const bool a = r0 < n && row_passes(p, r0);
+    const bool b = r1 < n && row_passes(p, r1);
+    const uint32_t lo = __ballot_sync(0xffffffffu, a);
+    const uint32_t hi = __ballot_sync(0xffffffffu, b);
+    if (lane == 0) mask[w] = (uint64_t)lo | ((uint64_t)hi << 32);
+  }
+}
+
+void op_filter_mask(Ctx& c, const fdb_dev_column* cols, int ncols, uint64_t n,
+                    const fdb_pred_term* prog, int nterms, uint64_t* d_mask) {
+  MaskParams p;
+  std::memset(&p, 0, sizeof(p));
+  fill_cols(p.sc, cols, ncols);
+  fill_prog(p.prog, prog, nterms, ncols);
+  const uint64_t nwords = (n + 63) / 64;
+  if (nwords == 0) return;
+  const int threads = 256;
+  const uint64_t blocks = umin64((nwords + 7) / 8, (uint64_t)c.sm_count * 8);
+  filter_mask_kernel<<<(unsigned)blocks, threads, 0, c.stream>>>(p, n, d_mask);
+  FDB_CUDA(cudaGetLastError());
+}
+
+// ---------------------------------------------------------------------------
+// Stable compaction of a mask into row numbers: chunk popcounts, one-block
+// exclusive scan of the chunk counts, then each chunk writes its rows.
+// ---------------------------------------------------------------------------
+constexpr int kCompactThreads = 256;
+constexpr int kWordsPerThread = 8;
+constexpr int kChunkWords = kCompactThreads * kWordsPerThread;  // 2048 words = 131072 rows
+
+template <typename T>
+__device__ T block_exclusive_scan(T v, T* sm_warp, T* total) {
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+  T x = v;
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    T y = __shfl_up_sync(0xffffffffu, x, o);
+    if (lane >= o) x += y;
+  }
+  if (lane == 31) sm_warp[warp] = x;
+  __syncthreads();
+  if (warp == 0) {
+    T s = lane < nw ? sm_warp[lane] : T(0);
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      T y = __shfl_up_sync(0xffffffffu, s, o);
+      if (lane >= o) s += y;
+    }
+    if (lane < nw) sm_warp[lane] = s;  // inclusive prefix of warp totals
+  }
+  __syncthreads();
+  T warp_base = warp ? sm_warp[warp - 1] : T(0);
+  if (total) *total = sm_warp[nw - 1];
+  __syncthreads();
+  return warp_base + x - v;
+}
+
+__global__ void compact_count_kernel(const uint64_t* mask, uint64_t nwords, uint64_t* counts) {
+  __shared__ uint64_t sm[32];
+  const uint64_t w0 = (uint64_t)blockIdx.x * kChunkWords + threadIdx.x * kWordsPerThread;
+  uint64_t cnt = 0;
+#pragma unroll
+  for (int j = 0; j < kWordsPerThread; ++j)
+    if (w0 + j < nwords) cnt += __popcll(mask[w0 + j]);
+  uint64_t total;
+  block_exclusive_scan<uint64_t>(cnt, sm, &total);
+  if (threadIdx.x == 0) counts[blockIdx.x] = total;
+}
+
+__global__ void compact_scan_kernel(uint64_t* counts, uint64_t nchunks, uint64_t* d_count,
+                                    uint64_t capacity, int* err) {
+  __shared__ uint64_t sm[32];
+  // Each thread owns a contiguous run of chunks.
+  const uint64_t per = (nchunks + blockDim.x - 1) / blockDim.x;
+  const uint64_t b0 = threadIdx.x * per;
+  uint64_t local = 0;
+  for (uint64_t i = b0; i < b0 + per && i < nchunks; ++i) local += counts[i];
+  uint64_t total;
+  uint64_t base = block_exclusive_scan<uint64_t>(local, sm, &total);
+  for (uint64_t i = b0; i < b0 + per && i < nchunks; ++i) {
+    uint64_t v = counts[i];
+    counts[i] = base;
+    base += v;
+  }
+  if (threadIdx.x == 0) {
+    *d_count = total;
+    if (total > capacity) atomicExch(err, kErrCapacity);
+  }
+}
+
+__global__ void compact_write_kernel(const uint64_t* mask, uint64_t nwords, const uint64_t* offsets,
+                                     uint32_t* rows, uint64_t capacity) {
+  __shared__ uint64_t sm[32];
+  const uint64_t w0 = (uint64_t)blockIdx.x * kChunkWords + threadIdx.x * kWordsPerThread;
+  uint64_t words[kWordsPerThread];
+  uint64_t cnt = 0;
+#pragma unroll
+  for (int j = 0; j < kWordsPerThread; ++j) {
+    words[j] = (w0 + j < nwords) ? mask[w0 + j] : 0ull;
+    cnt += __popcll(words[j]);
+  }
+  uint64_t off = offsets[blockIdx.x] + block_exclusive_scan<uint64_t>(cnt, sm, nullptr);
+#pragma unroll
+  for (int j = 0; j < kWordsPerThread; ++j) {
+    uint64_t w = words[j];
+    while (w) {
+      const int b = __ffsll((long long)w) - 1;
+      w &= w - 1;
+      if (off < capacity) rows[off] = (uint32_t)((w0 + j) * 64 + b);
+      ++off;
+    }
+  }
+}
+
+void op_compact_mask(Ctx& c, const uint64_t* d_mask, uint64_t n, uint32_t* d_rows,
+                     uint64_t capacity, uint64_t* d_count) {
+  const uint64_t nwords = (n + 63) / 64;
+  if (nwords == 0) {
+    FDB_CUDA(cudaMemsetAsync(d_count, 0, sizeof(uint64_t), c.stream));
+    return;
+  }
+  const uint64_t nchunks = (nwords + kChunkWords - 1) / kChunkWords;
+  uint64_t* counts = static_cast<uint64_t*>(c.scratch_take(nchunks * sizeof(uint64_t)));
+  compact_count_kernel<<<(unsigned)nchunks, kCompactThreads, 0, c.stream>>>(d_mask, nwords, counts);
+  compact_scan_kernel<<<1, 1024, 0, c.stream>>>(counts, nchunks, d_count, capacity, c.d_err);
+  compact_write_kernel<<<(unsigned)nchunks, kCompactThreads, 0, c.stream>>>(d_mask, nwords, counts,
+                                                                            d_rows, capacity);
+  FDB_CUDA(cudaGetLastError());
+}
+
+// ---------------------------------------------------------------------------
+// Gather rows of one column.
+// ---------------------------------------------------------------------------
+template <typename T>
+__global__ void gather_kernel(const T* __restrict__ in, const uint32_t* __restrict__ rows, uint64_t n,
+                              T* __restrict__ out) {
+  for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n;
+       i += (uint64_t)gridDim.x * blockDim.x)
+    out[i] = in[rows[i]];
+}
+
+__global__ void gather_validity_kernel(const uint64_t* __restrict__ validity, uint64_t voff,
+                                       const uint32_t* __restrict__ rows, uint64_t n,
+                                       uint64_t* __restrict__ out) {
+  const uint64_t nwords = (n + 63) / 64;
+  const int lane = threadIdx.x & 31;
+  const uint64_t gw = (blockIdx.x * (uint64_t)blockDim.x + threadIdx.x) >> 5;
+  const uint64_t nwarps = ((uint64_t)gridDim.x * blockDim.x) >> 5;
+  for (uint64_t w = gw; w < nwords; w += nwarps) {
+    bool a = false, b = false;
+    const uint64_t i0 = w * 64 + lane, i1 = i0 + 32;
+    if (i0 < n) {
+      const uint64_t bit = voff + rows[i0];
+      a = (validity[bit >> 6] >> (bit & 63)) & 1ull;
+    }
+    if (i1 < n) {
+      const uint64_t bit = voff + rows[i1];
+      b = (validity[bit >> 6] >> (bit & 63)) & 1ull;
+    }
+    const uint32_t lo = __ballot_sync(0xffffffffu, a), hi = __ballot_sync(0xffffffffu, b);
+    if (lane == 0) out[w] = (uint64_t)lo | ((uint64_t)hi << 32);
+  }
+}
+
+template <typename T>
+__global__ void gather_opt_kernel(const T* __restrict__ in, const uint64_t* validity, uint64_t voff,
+                                  const uint32_t* __restrict__ rows, uint64_t n, T* __restrict__ out,
+                                  uint64_t* __restrict__ out_valid) {
+  const int lane = threadIdx.x & 31;
+  const uint64_t nw = (n + 31) / 32;
+  const uint64_t gw = (blockIdx.x * (uint64_t)blockDim.x + threadIdx.x) >> 5;
+  const uint64_t nwarps = ((uint64_t)gridDim.x * blockDim.x) >> 5;
+  for (uint64_t w = gw; w < nw; w += nwarps) {  // 32 outputs per warp step
+    const uint64_t i = w * 32 + lane;
+    bool ok = false;
+    if (i < n) {
+      const uint32_t r = rows[i];
+      if (r != FDB_NO_ROW) {
+        ok = true;
+        if (validity) {
+          const uint64_t b = voff + r;
+          ok = (validity[b >> 6] >> (b & 63)) & 1ull;
+        }
+        out[i] = in[r];
+      } else {
+        out[i] = T(0);
+      }
+    }
+    const uint32_t m = __ballot_sync(0xffffffffu, ok);
+    if (lane == 0) reinterpret_cast<uint32_t*>(out_valid)[w] = m;
+  }
+}
+
+void op_gather_opt(Ctx& c, const fdb_dev_column& col, const uint32_t* d_rows, uint64_t n, void* d_out,
+                   uint64_t* d_out_validity) {
+  if (n == 0) return;
+  FDB_CUDA(cudaMemsetAsync(d_out_validity, 0, ((n + 63) / 64) * 8, c.stream));
+  const unsigned blocks = (unsigned)umin64((n + 255) / 256, (uint64_t)c.sm_count * 16);
+  if (dtype_size(col.dtype) == 8)
+    gather_opt_kernel<uint64_t><<<blocks, 256, 0, c.stream>>>(
+        static_cast<const uint64_t*>(col.values), col.validity, col.validity_offset, d_rows, n,
+        static_cast<uint64_t*>(d_out), d_out_validity);
+  else
+    gather_opt_kernel<uint32_t><<<blocks, 256, 0, c.stream>>>(
+        static_cast<const uint32_t*>(col.values), col.validity, col.validity_offset, d_rows, n,
+        static_cast<uint32_t*>(d_out), d_out_validity);
+  FDB_CUDA(cudaGetLastError());
+}
+
+void op_gather(Ctx& c, const fdb_dev_column& col, const uint32_t* d_rows, uint64_t n, void* d_out,
+               uint64_t* d_out_validity) {
+  if (n == 0) return;
+  const int threads = 256;
+  const unsigned blocks = (unsigned)umin64((n + threads - 1) / threads, (uint64_t)c.sm_count * 16);
+  if (dtype_size(col.dtype) == 8)
+    gather_kernel<uint64_t><<<blocks, threads, 0, c.stream>>>(
+        static_cast<const uint64_t*>(col.values), d_rows, n, static_cast<uint64_t*>(d_out));
+  else
+    gather_kernel<uint32_t><<<blocks, threads, 0, c.stream>>>(
+        static_cast<const uint32_t*>(col.values), d_rows, n, static_cast<uint32_t*>(d_out));
+  if (col.validity && d_out_validity) {
+    const uint64_t nwords = (n + 63) / 64;
+    const unsigned vb = (unsigned)umin64((nwords + 7) / 8, (uint64_t)c.sm_count * 8);
+    gather_validity_kernel<<<vb, 256, 0, c.stream>>>(col.validity, col.validity_offset, d_rows, n,
+                                                     d_out_validity);
+  }
+  FDB_CUDA(cudaGetLastError());
+}
+
+}  // namespace fdb

@@ -1,0 +1,349 @@
+/*
+ * falcondb_b200.h — C ABI of the B200 execution engine for FalconDB's relational
+ * hot path: scan, filter, aggregate, GROUP BY, hash join and ORDER BY ... LIMIT.
+ *
+ * Two layers, both plain C (opaque handles, pointers and sizes; no C++ or torch
+ * types cross this boundary):
+ *
+ *  1. Database layer — mirrors FalconDB's C FFI (src/api/c_ffi.rs:27-144) and its
+ *     `Database::sql` entry point (src/db.rs:242).  Tables are copied from host
+ *     columns into HBM once and stay resident; `fdb_sql` plans and runs a query on
+ *     the GPU and returns a host-side result owned by the library.
+ *
+ *  2. Operator layer — one entry point per CPU physical operator routine that
+ *     FalconDB's planner calls (src/db.rs:1439-1717), taking DEVICE pointers and
+ *     writing DEVICE results on the context's CUDA stream without a host sync, so
+ *     a GPU operator is a drop-in for the matching CPU plan node.
+ *
+ * Conventions (kept from c_ffi.rs): 0 = success; a negative FDB_E* code on error
+ * (-1 is the generic error, as in c_ffi.rs); a thread-local message is returned by
+ * fdb_last_error().  Results are owned by the library until *_free.  No C++
+ * exception crosses the ABI.  A context (fdb_db) owns one CUDA stream and its
+ * scratch memory; calls on one context are serialised by the library, so several
+ * host threads may share it, and independent contexts run concurrently.
+ *
+ * Row numbers on the operator layer are uint32 (as FalconDB's typed paths use
+ * u32 row ids, src/query/join.rs:1394-1415, sort.rs:209-215); a single call
+ * covers fewer than 2^32 rows.
+ */
+#ifndef FALCONDB_B200_H
+#define FALCONDB_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ------------------------------------------------------------------------- */
+/* Error codes                                                                */
+/* ------------------------------------------------------------------------- */
+#define FDB_OK            0
+#define FDB_E_GENERIC    -1   /* c_ffi.rs returns -1 / NULL on every error     */
+#define FDB_E_ARG        -2   /* invalid argument (NULL handle, bad enum, ...) */
+#define FDB_E_CUDA       -3   /* CUDA runtime error                           */
+#define FDB_E_OOM        -4   /* device memory budget or allocation exceeded  */
+#define FDB_E_SQL        -5   /* SQL text outside the supported shapes        */
+#define FDB_E_NOTFOUND   -6   /* unknown table / column                       */
+#define FDB_E_TYPE       -7   /* type mismatch (e.g. join keys of two types)  */
+#define FDB_E_TIMEOUT    -8   /* a bounded device-side wait gave up           */
+#define FDB_E_CAPACITY   -9   /* an output buffer was too small               */
+
+/* Column physical types (src/storage/column.rs:8-21).  FDB_UTF8 columns are
+ * dictionary encoded: uint32 codes per row, a host dictionary of strings, and
+ * code 0xFFFFFFFF meaning NULL (column.rs:1257-1277). */
+#define FDB_INT64    1
+#define FDB_FLOAT64  2
+#define FDB_UTF8     3
+
+/* Comparison operators of `col op literal` (src/query/expr.rs:1076-1175).
+ * Floating comparisons are IEEE ordered (NaN fails) except NE, which is
+ * unordered (NaN passes), as cmp_f64_avx2 (expr.rs:894-899) does. */
+#define FDB_EQ 0
+#define FDB_NE 1
+#define FDB_LT 2
+#define FDB_LE 3
+#define FDB_GT 4
+#define FDB_GE 5
+
+/* Aggregate functions (src/query/aggregate.rs:33-47). Result types follow
+ * build_agg_col (aggregate.rs:3390-3420): COUNT* -> int64, others -> float64. */
+#define FDB_AGG_COUNT_STAR      0   /* COUNT(*): rows that pass the filter     */
+#define FDB_AGG_COUNT           1   /* COUNT(col): non-NULL values             */
+#define FDB_AGG_SUM             2
+#define FDB_AGG_AVG             3
+#define FDB_AGG_MIN             4   /* NaN ignored, as f64::min does            */
+#define FDB_AGG_MAX             5
+#define FDB_AGG_COUNT_DISTINCT  6   /* FDB_UTF8 columns on the operator layer   */
+
+/* Join types (src/query/join.rs:29-41). SEMI/ANTI return left columns only
+ * (join.rs:45-48). */
+#define FDB_JOIN_INNER 0
+#define FDB_JOIN_LEFT  1
+#define FDB_JOIN_SEMI  2
+#define FDB_JOIN_ANTI  3
+
+/* "No matching build row" marker in emitted join pairs (join.rs NO_ROW). */
+#define FDB_NO_ROW 0xFFFFFFFFu
+
+/* ------------------------------------------------------------------------- */
+/* Opaque handles                                                             */
+/* ------------------------------------------------------------------------- */
+typedef struct fdb_db     fdb_db;      /* context: device, stream, scratch, catalog */
+typedef struct fdb_result fdb_result;  /* host-side query result                    */
+typedef struct fdb_hash   fdb_hash;    /* resident join build side (IntHashTable)   */
+
+/* Host column handed to fdb_table_from_columns (copied into HBM). */
+typedef struct fdb_column {
+    const char*        name;
+    int32_t            dtype;      /* FDB_INT64 | FDB_FLOAT64 | FDB_UTF8            */
+    const void*        values;     /* int64[n] | double[n] | uint32 codes[n]        */
+    const uint64_t*    validity;   /* LSB-first bit per row, 1 = valid; may be NULL */
+    const char* const* dict;       /* FDB_UTF8 only: dict_len strings               */
+    uint32_t           dict_len;
+} fdb_column;
+
+/* Device column view used by the operator layer.  `values` points at row 0 of
+ * the view; validity bit i of the view is bit (validity_offset + i). */
+typedef struct fdb_dev_column {
+    int32_t         dtype;
+    int32_t         _pad;
+    const void*     values;            /* device pointer                          */
+    const uint64_t* validity;          /* device pointer or NULL                  */
+    uint64_t        validity_offset;
+} fdb_dev_column;
+
+/* One term of a WHERE predicate, in postfix order (expr.rs:635-808).
+ * A program of CMP/IS_NULL/IS_NOT_NULL/CODE_SET leaves and AND/OR nodes; an
+ * empty program selects every row. NULL values fail every leaf except IS_NULL. */
+#define FDB_TERM_CMP          0  /* cols[col] op literal                           */
+#define FDB_TERM_IS_NULL      1  /* validity bit clear, or the Utf8 NULL code       */
+#define FDB_TERM_IS_NOT_NULL  2
+#define FDB_TERM_CODE_SET     3  /* FDB_UTF8: code < lit_i (the dictionary length)
+                                    and bit `code` of code_set (device) is set;
+                                    how Utf8 comparisons, IN and LIKE are decided
+                                    once per dictionary entry (expr.rs:1143-1171) */
+#define FDB_TERM_AND          4
+#define FDB_TERM_OR           5
+#define FDB_MAX_TERMS        16
+
+typedef struct fdb_pred_term {
+    int32_t         kind;
+    int32_t         col;
+    int32_t         op;        /* FDB_EQ..FDB_GE for FDB_TERM_CMP                 */
+    int32_t         lit_type;  /* FDB_INT64 | FDB_FLOAT64                         */
+    int64_t         lit_i;
+    double          lit_f;
+    const uint64_t* code_set;  /* device bitmap over dictionary codes             */
+} fdb_pred_term;
+
+typedef struct fdb_agg_spec {
+    int32_t func;              /* FDB_AGG_*                                       */
+    int32_t col;               /* input column index; ignored for COUNT(*)        */
+} fdb_agg_spec;
+
+/* One aggregate result, written to device memory by the operator layer.
+ * int64 results (COUNT*) are in `i`; float64 results in `f`; `valid` = 0 means
+ * SQL NULL (SUM/AVG/MIN/MAX over no non-NULL rows, aggregate.rs:420-440). */
+typedef struct fdb_agg_value {
+    double  f;
+    int64_t i;
+    int64_t n;                 /* rows that contributed                            */
+    int32_t is_int;            /* 1: result is int64 (`i`), 0: float64 (`f`)       */
+    int32_t valid;
+} fdb_agg_value;
+
+/* Join aggregate result (device): COUNT(*) and SUM(payload) for INNER/LEFT;
+ * COUNT(*) and SUM(value) of the kept left rows for SEMI/ANTI. */
+typedef struct fdb_join_agg {
+    int64_t count;
+    int64_t sum_payload;       /* exact int64 sum of matched non-NULL payloads     */
+    double  sum_value;         /* FP64 sum of the left `value` column (SEMI/ANTI)  */
+    int64_t payload_rows;      /* non-NULL payloads summed (SUM NULL when 0)        */
+} fdb_join_agg;
+
+/* One output group of the int64-key hash GROUP BY (aggregate.rs:840-912). */
+typedef struct fdb_group_i64 {
+    int64_t key;
+    int64_t count;
+    double  sum;
+    double  min;
+    double  max;
+} fdb_group_i64;
+
+/* ------------------------------------------------------------------------- */
+/* 1. Database layer  (c_ffi.rs:27-144, db.rs:242)                            */
+/* ------------------------------------------------------------------------- */
+
+/* Open a context on CUDA device `device`.  mem_budget_bytes caps the device
+ * memory the context may hold (tables, hash tables, scratch); 0 = 90% of free.
+ * Replaces falcondb_open (c_ffi.rs:27-30). */
+int  fdb_open(int device, uint64_t mem_budget_bytes, fdb_db** out);
+
+/* Replaces falcondb_close (c_ffi.rs:32-37). Frees every device allocation. */
+void fdb_close(fdb_db* db);
+
+/* Thread-local message of the last failed call on this thread ("" if none).
+ * c_ffi.rs exports no message; this adds one without changing return codes. */
+const char* fdb_last_error(void);
+
+/* Create (or replace) table `name` from host columns; the values are copied to
+ * HBM (asynchronously on an upload stream when `host` buffers are pinned) and the
+ * library owns the device copy.  Replaces the loaders falcondb_load_csv /
+ * falcondb_load_fdb (c_ffi.rs:41-79) and Database::create_table_from_batches
+ * (db.rs:180-204) for in-memory columns. Returns rows loaded or a negative code. */
+int64_t fdb_table_from_columns(fdb_db* db, const char* name, const fdb_column* cols,
+                               int32_t ncols, uint64_t nrows);
+
+/* Rows of table `name`, or 0 if absent (falcondb_table_row_count, c_ffi.rs:131-144). */
+uint64_t fdb_table_row_count(const fdb_db* db, const char* name);
+
+/* Drop table `name` and free its device memory. */
+int  fdb_table_drop(fdb_db* db, const char* name);
+
+/* Device view of a resident column, for the operator layer. */
+int  fdb_table_column(const fdb_db* db, const char* table, const char* column,
+                      fdb_dev_column* out, uint64_t* nrows);
+
+/* Execute SQL (falcondb_sql, c_ffi.rs:86-99 -> Database::sql, db.rs:242-316).
+ * *out is NULL on error. Supported shapes: see DESIGN.md of the package. */
+int  fdb_sql(fdb_db* db, const char* sql, fdb_result** out);
+
+/* Result accessors (c_ffi.rs:103-127). */
+uint64_t    fdb_result_row_count(const fdb_result* r);
+int32_t     fdb_result_num_columns(const fdb_result* r);
+const char* fdb_result_column_name(const fdb_result* r, int32_t col);
+int32_t     fdb_result_column_dtype(const fdb_result* r, int32_t col);
+/* int64[rows] / double[rows] / const char*[rows] (FDB_UTF8); valid until free. */
+const void* fdb_result_column_values(const fdb_result* r, int32_t col);
+/* uint8 per row, 1 = NULL; NULL pointer when the column has no NULLs. */
+const uint8_t* fdb_result_column_nulls(const fdb_result* r, int32_t col);
+/* Pretty-printed table, valid until the result is freed (c_ffi.rs:108-121). */
+const char* fdb_result_display(fdb_result* r);
+void        fdb_result_free(fdb_result* r);
+
+/* Device time of the kernels of the last fdb_sql on this context, in ms. */
+double      fdb_last_kernel_ms(const fdb_db* db);
+
+/* ------------------------------------------------------------------------- */
+/* 2. Operator layer (device pointers; asynchronous on the context's stream) */
+/* ------------------------------------------------------------------------- */
+
+/* The context's CUDA stream (a cudaStream_t), for events and synchronisation. */
+void* fdb_stream(fdb_db* db);
+/* Block until every operator queued on the context has finished; returns the
+ * first deferred device-side error (e.g. FDB_E_TIMEOUT) if one was recorded. */
+int   fdb_synchronize(fdb_db* db);
+
+/* WHERE mask: packed uint64 words, bit i of word i/64 = row i passes; bits past
+ * nrows are zero.  Replaces Expr::eval_mask_bits / fast_cmp_mask
+ * (expr.rs:635-652, 1076-1175) and clear_null_bits / mask_off_padding
+ * (expr.rs:961-986). d_mask holds ceil(nrows/64) words. */
+int fdb_filter_mask(fdb_db* db, const fdb_dev_column* cols, int32_t ncols,
+                    uint64_t nrows, const fdb_pred_term* prog, int32_t nterms,
+                    uint64_t* d_mask);
+
+/* COUNT(*) WHERE pred without materialising the mask: replaces the popcount fast
+ * path of execute_plan (db.rs:1439-1476). */
+int fdb_filter_count(fdb_db* db, const fdb_dev_column* cols, int32_t ncols,
+                     uint64_t nrows, const fdb_pred_term* prog, int32_t nterms,
+                     uint64_t* d_count);
+
+/* Stable selection compaction: the row numbers of the set bits of d_mask in
+ * ascending order, and their count.  Replaces gather_by_bitmask's row walk
+ * (column.rs:1077-1123, table.rs:148-189). d_rows holds `capacity` entries;
+ * FDB_E_CAPACITY (deferred to fdb_synchronize) if more rows pass. */
+int fdb_compact_mask(fdb_db* db, const uint64_t* d_mask, uint64_t nrows,
+                     uint32_t* d_rows, uint64_t capacity, uint64_t* d_count);
+
+/* Gather rows `d_rows[0..n)` of a column (values and validity) into a dense
+ * device column (Column::gather_u32, column.rs:1502-1520). d_out_validity may be
+ * NULL when the input has no validity. */
+int fdb_gather(fdb_db* db, const fdb_dev_column* col, const uint32_t* d_rows,
+               uint64_t n, void* d_out_values, uint64_t* d_out_validity);
+
+/* No-key aggregates over the rows that pass `prog` (execute_agg_only +
+ * accumulate_typed, aggregate.rs:1394-1528, 3121-3386).  FLOAT64 SUM/AVG are
+ * FP64 with a fixed reduction tree (deterministic for a given device); INT64 SUM
+ * is exact.  COUNT_DISTINCT is answered by fdb_distinct_codes. */
+int fdb_aggregate(fdb_db* db, const fdb_dev_column* cols, int32_t ncols,
+                  uint64_t nrows, const fdb_pred_term* prog, int32_t nterms,
+                  const fdb_agg_spec* aggs, int32_t naggs, fdb_agg_value* d_out);
+
+/* Presence bitmap of the dictionary codes that occur among rows passing `prog`
+ * (present_codes, aggregate.rs:3167-3200): d_bitmap holds ceil(dict_len/64)
+ * words.  COUNT(DISTINCT) is the number of distinct strings whose code is set. */
+int fdb_distinct_codes(fdb_db* db, const fdb_dev_column* cols, int32_t ncols,
+                       uint64_t nrows, const fdb_pred_term* prog, int32_t nterms,
+                       int32_t code_col, uint32_t dict_len, uint64_t* d_bitmap);
+
+/* Dictionary-code GROUP BY (fast_utf8_gb, aggregate.rs:619-836), with value
+ * semantics: group g is dictionary code g, group dict_len is the NULL key.
+ * d_out[g*naggs + a] is aggregate a of group g; d_group_rows[g] counts the rows
+ * of group g that passed the filter (0 = group absent).  Both arrays hold
+ * (dict_len+1) groups.  Requires (dict_len+1) * slots <= 2048, where an
+ * aggregate takes 2 slots for AVG and 1 otherwise, plus 1 for the row count. */
+int fdb_group_by_codes(fdb_db* db, const fdb_dev_column* cols, int32_t ncols,
+                       uint64_t nrows, const fdb_pred_term* prog, int32_t nterms,
+                       int32_t key_col, uint32_t dict_len,
+                       const fdb_agg_spec* aggs, int32_t naggs,
+                       fdb_agg_value* d_out, int64_t* d_group_rows);
+
+/* int64-key hash GROUP BY with COUNT(*), SUM, MIN and MAX of one float64 or
+ * int64 value column (fast_i64_gb, aggregate.rs:840-912).  NULL keys (and
+ * i64::MIN, which fast_i64_gb reads as NULL, aggregate.rs:867) form one group
+ * reported with key INT64_MIN.  Groups are written to d_groups (order
+ * unspecified) and their number to d_ngroups; `capacity` bounds d_groups
+ * (FDB_E_CAPACITY, deferred, if exceeded).  expected_groups sizes the table
+ * (0 = nrows); load_factor in (0,1) (0 = autotuned). */
+int fdb_group_by_i64(fdb_db* db, const fdb_dev_column* key, const fdb_dev_column* value,
+                     uint64_t nrows, const fdb_pred_term* prog, int32_t nterms,
+                     const fdb_dev_column* pred_cols, int32_t npred_cols,
+                     uint64_t expected_groups, double load_factor,
+                     fdb_group_i64* d_groups, uint64_t capacity, uint64_t* d_ngroups);
+
+/* Build side of an int64 equi-join (build_hash_table + IntHashTable,
+ * join.rs:607-645, 1054-1351): open addressing with linear probing over
+ * next_pow2(rows / load_factor) slots (load_factor 0 = autotuned).  NULL keys
+ * are never inserted (they match nothing, join.rs:637).  The table keeps
+ * device pointers to `payload`, which must stay alive while it is used. */
+int fdb_join_build(fdb_db* db, const fdb_dev_column* key, const fdb_dev_column* payload,
+                   uint64_t nrows, double load_factor, fdb_hash** out);
+void fdb_join_free(fdb_hash* h);
+uint64_t fdb_join_capacity(const fdb_hash* h);
+
+/* Probe with aggregation fused in (probe_in_place / probe_one + execute_agg_only,
+ * join.rs:297-375, 657-723; execute_hash_semi_anti_join, join.rs:49-132):
+ *   INNER: count = matched pairs, sum_payload = SUM(payload) over them;
+ *   LEFT : count = matched pairs + unmatched left rows, sum_payload as INNER;
+ *   SEMI : count = left rows with a match, sum_value = SUM(value) over them;
+ *   ANTI : count = left rows without a match (NULL keys included),
+ *          sum_value = SUM(value) over them.
+ * `value` may be NULL (sum_value is then 0). */
+int fdb_join_probe_agg(fdb_db* db, const fdb_hash* h, const fdb_dev_column* probe_key,
+                       const fdb_dev_column* value, uint64_t nrows, int32_t join_type,
+                       fdb_join_agg* d_out);
+
+/* Probe emitting the joined row pairs (left row, build row); build row is
+ * FDB_NO_ROW for LEFT's unmatched rows; SEMI/ANTI emit left rows only
+ * (d_right untouched).  Pair order is unspecified. */
+int fdb_join_probe_pairs(fdb_db* db, const fdb_hash* h, const fdb_dev_column* probe_key,
+                         uint64_t nrows, int32_t join_type, uint32_t* d_left,
+                         uint32_t* d_right, uint64_t capacity, uint64_t* d_count);
+
+/* ORDER BY col [DESC] LIMIT k over one FLOAT64 / INT64 column
+ * (execute_sort_limit + top_k_ascending + assemble, sort.rs:59-115, 564-620,
+ * 773-791): the k best row numbers, in order, ties broken by row ascending;
+ * NULL rows first or last as `nulls_last` says.  1 <= k <= 4096.  d_rows holds
+ * k entries; d_count receives min(k, nrows). */
+int fdb_topk(fdb_db* db, const fdb_dev_column* col, uint64_t nrows, uint32_t k,
+             int32_t desc, int32_t nulls_last, uint32_t* d_rows, uint64_t* d_count);
+
+/* Library version string. */
+const char* fdb_version(void);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* FALCONDB_B200_H */

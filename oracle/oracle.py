@@ -1,0 +1,260 @@
+"""ORACLE — test infrastructure only.
+
+ctypes front end of ``oracle/liboracle.so``: the serial CPU restatement of
+FalconDB's operators (oracle.cpp) and the reference-shaped multi-threaded CPU
+engine (refengine.cpp).  Only tests/, ``__graft_entry__.smoke()`` and bench.py's
+CPU-baseline leg may import it; the product never does.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import subprocess
+from pathlib import Path
+from typing import Optional, Tuple
+
+import numpy as np
+
+HERE = Path(__file__).resolve().parent
+LIB = HERE / "liboracle.so"
+_lib: Optional[C.CDLL] = None
+
+P = C.c_void_p
+U64 = C.c_uint64
+_SIGS = {
+    "orc_cmp_mask": (None, [C.c_int, P, P, U64, C.c_int, C.c_int, C.c_int64, C.c_double, P]),
+    "orc_code_mask": (None, [P, P, U64, P, C.c_uint32, P]),
+    "orc_popcount": (U64, [P, U64]),
+    "orc_mask_rows": (U64, [P, U64, P]),
+    "orc_sum_lanes_f64": (C.c_double, [P, U64]),
+    "orc_sum_serial_f64": (C.c_double, [P, U64]),
+    "orc_checked_sum_i64": (C.c_int, [P, U64, P]),
+    "orc_agg": (C.c_int, [C.c_int, C.c_int, P, P, P, U64, P, P]),
+    "orc_sum_i64_masked": (C.c_int, [P, P, P, U64, P]),
+    "orc_present_codes": (None, [P, P, P, U64, C.c_uint32, P]),
+    "orc_group_codes": (None, [P, P, P, U64, C.c_uint32, P, P, P, P, P, P, P, P, P, P, P]),
+    "orc_group_i64": (U64, [P, P, P, P, U64, P, P, P, P, P]),
+    "orc_join_agg": (None, [P, P, P, P, U64, P, P, P, P, U64, C.c_int, P, P, P, P]),
+    "orc_join_pairs": (U64, [P, P, U64, P, P, U64, C.c_int, P, P, U64]),
+    "orc_topk": (U64, [C.c_int, P, P, U64, C.c_uint32, C.c_int, C.c_int, P]),
+    "ref_hardware_threads": (C.c_int, []),
+    "ref_sum_f64": (C.c_double, [P, U64, C.c_int]),
+    "ref_count_cmp_f64": (U64, [P, U64, C.c_int, C.c_double]),
+    "ref_present_codes": (None, [P, U64, C.c_uint32, C.c_int, P]),
+    "ref_topk": (U64, [C.c_int, P, U64, C.c_uint32, C.c_int, P]),
+    "ref_filter_group_codes": (None, [P, P, P, U64, C.c_uint32, C.c_int, C.c_double, C.c_int, P, P, P]),
+    "ref_join_agg": (None, [P, P, U64, P, P, U64, C.c_int, C.c_int, P, P, P]),
+    "ref_group_i64": (U64, [P, P, U64, C.c_int]),
+}
+
+
+def build() -> Path:
+    """Compile liboracle.so with the committed Makefile (gcc)."""
+    subprocess.run(["make", "-s", "-C", str(HERE)], check=True)
+    return LIB
+
+
+def lib() -> C.CDLL:
+    global _lib
+    if _lib is None:
+        if not LIB.exists():
+            build()
+        L = C.CDLL(str(LIB))
+        for name, (res, args) in _SIGS.items():
+            f = getattr(L, name)
+            f.restype = res
+            f.argtypes = args
+        _lib = L
+    return _lib
+
+
+def _p(a: Optional[np.ndarray]):
+    return None if a is None else a.ctypes.data
+
+
+def _c(a, dtype):
+    return None if a is None else np.ascontiguousarray(a, dtype=dtype)
+
+
+# ---------------------------------------------------------------------------- serial oracle
+def cmp_mask(values: np.ndarray, op: int, literal, validity: Optional[np.ndarray] = None) -> np.ndarray:
+    v = np.ascontiguousarray(values)
+    dtype = 2 if v.dtype.kind == "f" else 1
+    v = v.astype(np.float64 if dtype == 2 else np.int64, copy=False)
+    out = np.zeros(max(1, (len(v) + 63) // 64), dtype=np.uint64)
+    lit_type = 2 if isinstance(literal, (float, np.floating)) else 1
+    lib().orc_cmp_mask(dtype, _p(v), _p(_c(validity, np.uint64)), len(v), op, lit_type,
+                       int(literal) if lit_type == 1 else 0, float(literal) if lit_type == 2 else 0.0, _p(out))
+    return out
+
+
+def code_mask(codes: np.ndarray, passing, validity=None) -> np.ndarray:
+    c = _c(codes, np.uint32)
+    pas = np.asarray(passing, dtype=np.uint8)
+    out = np.zeros(max(1, (len(c) + 63) // 64), dtype=np.uint64)
+    lib().orc_code_mask(_p(c), _p(_c(validity, np.uint64)), len(c), _p(pas), len(pas), _p(out))
+    return out
+
+
+def popcount(words: np.ndarray) -> int:
+    w = _c(words, np.uint64)
+    return int(lib().orc_popcount(_p(w), len(w)))
+
+
+def mask_rows(words: np.ndarray, n: int) -> np.ndarray:
+    w = _c(words, np.uint64)
+    out = np.zeros(max(1, n), dtype=np.uint32)
+    k = lib().orc_mask_rows(_p(w), n, _p(out))
+    return out[:k]
+
+
+def sum_lanes(v: np.ndarray) -> float:
+    v = _c(v, np.float64)
+    return float(lib().orc_sum_lanes_f64(_p(v), len(v)))
+
+
+def sum_serial(v: np.ndarray) -> float:
+    v = _c(v, np.float64)
+    return float(lib().orc_sum_serial_f64(_p(v), len(v)))
+
+
+def checked_sum_i64(v: np.ndarray) -> Optional[int]:
+    v = _c(v, np.int64)
+    out = np.zeros(1, dtype=np.int64)
+    return int(out[0]) if lib().orc_checked_sum_i64(_p(v), len(v), _p(out)) else None
+
+
+def agg(func: int, values: np.ndarray, mask=None, validity=None) -> Tuple[Optional[float], int]:
+    """(value or None for SQL NULL, contributing count) of COUNT/SUM/AVG/MIN/MAX."""
+    v = np.ascontiguousarray(values)
+    dtype = 2 if v.dtype.kind == "f" else 1
+    v = v.astype(np.float64 if dtype == 2 else np.int64, copy=False)
+    val = np.zeros(1, dtype=np.float64)
+    cnt = np.zeros(1, dtype=np.int64)
+    ok = lib().orc_agg(func, dtype, _p(v), _p(_c(validity, np.uint64)), _p(_c(mask, np.uint64)), len(v),
+                       _p(val), _p(cnt))
+    return (float(val[0]) if ok else None), int(cnt[0])
+
+
+def sum_i64_exact(values, mask=None, validity=None) -> Optional[int]:
+    v = _c(values, np.int64)
+    out = np.zeros(1, dtype=np.int64)
+    ok = lib().orc_sum_i64_masked(_p(v), _p(_c(validity, np.uint64)), _p(_c(mask, np.uint64)), len(v), _p(out))
+    return int(out[0]) if ok else None
+
+
+def present_codes(codes, dict_len, mask=None, validity=None) -> np.ndarray:
+    c = _c(codes, np.uint32)
+    out = np.zeros(max(1, dict_len), dtype=np.uint8)
+    lib().orc_present_codes(_p(c), _p(_c(validity, np.uint64)), _p(_c(mask, np.uint64)), len(c), dict_len, _p(out))
+    return out[:dict_len]
+
+
+def group_codes(codes, dict_len, mask=None, fvals=None, ivals=None, kvalid=None, fvalid=None, ivalid=None):
+    """Per-group dict over groups 0..dict_len (dict_len = NULL key)."""
+    c = _c(codes, np.uint32)
+    ng = dict_len + 1
+    arrs = {k: np.zeros(ng, dtype=dt) for k, dt in
+            [("rows", np.int64), ("fsum", np.float64), ("fcnt", np.int64), ("isum", np.float64),
+             ("icnt", np.int64), ("fmin", np.float64), ("fmax", np.float64)]}
+    fv = _c(fvals, np.float64)
+    iv = _c(ivals, np.int64)
+    lib().orc_group_codes(_p(c), _p(_c(kvalid, np.uint64)), _p(_c(mask, np.uint64)), len(c), dict_len, _p(fv),
+                          _p(_c(fvalid, np.uint64)), _p(iv), _p(_c(ivalid, np.uint64)), _p(arrs["rows"]),
+                          _p(arrs["fsum"]), _p(arrs["fcnt"]), _p(arrs["isum"]), _p(arrs["icnt"]),
+                          _p(arrs["fmin"]), _p(arrs["fmax"]))
+    return arrs
+
+
+def group_i64(keys, vals, mask=None, kvalid=None):
+    k = _c(keys, np.int64)
+    v = _c(vals, np.float64)
+    n = len(k)
+    out = {"key": np.zeros(n + 1, np.int64), "count": np.zeros(n + 1, np.int64), "sum": np.zeros(n + 1),
+           "min": np.zeros(n + 1), "max": np.zeros(n + 1)}
+    g = lib().orc_group_i64(_p(k), _p(_c(kvalid, np.uint64)), _p(v), _p(_c(mask, np.uint64)), n, _p(out["key"]),
+                            _p(out["count"]), _p(out["sum"]), _p(out["min"]), _p(out["max"]))
+    return {kk: vv[:g] for kk, vv in out.items()}
+
+
+def join_agg(bkeys, bpay, pkeys, pval, join_type, bvalid=None, bpvalid=None, pvalid=None, pvvalid=None):
+    bk, bp, pk, pv = _c(bkeys, np.int64), _c(bpay, np.int64), _c(pkeys, np.int64), _c(pval, np.float64)
+    o = [np.zeros(1, np.int64), np.zeros(1, np.int64), np.zeros(1, np.int64), np.zeros(1, np.float64)]
+    lib().orc_join_agg(_p(bk), _p(_c(bvalid, np.uint64)), _p(bp), _p(_c(bpvalid, np.uint64)), len(bk), _p(pk),
+                       _p(_c(pvalid, np.uint64)), _p(pv), _p(_c(pvvalid, np.uint64)), len(pk), join_type,
+                       *[_p(x) for x in o])
+    return {"count": int(o[0][0]), "sum_payload": int(o[1][0]), "payload_rows": int(o[2][0]),
+            "sum_value": float(o[3][0])}
+
+
+def join_pairs(bkeys, pkeys, join_type, bvalid=None, pvalid=None):
+    bk, pk = _c(bkeys, np.int64), _c(pkeys, np.int64)
+    cap = 0
+    n = lib().orc_join_pairs(_p(bk), _p(_c(bvalid, np.uint64)), len(bk), _p(pk), _p(_c(pvalid, np.uint64)), len(pk),
+                             join_type, None, None, 0)
+    left = np.zeros(max(1, n), np.uint32)
+    right = np.zeros(max(1, n), np.uint32)
+    lib().orc_join_pairs(_p(bk), _p(_c(bvalid, np.uint64)), len(bk), _p(pk), _p(_c(pvalid, np.uint64)), len(pk),
+                         join_type, _p(left), _p(right), n)
+    return left[:n], right[:n]
+
+
+def topk(values, k, desc, nulls_last=None, validity=None) -> np.ndarray:
+    v = np.ascontiguousarray(values)
+    dtype = 2 if v.dtype.kind == "f" else 1
+    v = v.astype(np.float64 if dtype == 2 else np.int64, copy=False)
+    if nulls_last is None:
+        nulls_last = desc
+    out = np.zeros(max(1, k), dtype=np.uint32)
+    m = lib().orc_topk(dtype, _p(v), _p(_c(validity, np.uint64)), len(v), k, int(desc), int(nulls_last), _p(out))
+    return out[:m]
+
+
+# ---------------------------------------------------------------------------- reference-shaped engine
+def hardware_threads() -> int:
+    return int(lib().ref_hardware_threads())
+
+
+def ref_sum_f64(v, threads):
+    v = _c(v, np.float64)
+    return float(lib().ref_sum_f64(_p(v), len(v), threads))
+
+
+def ref_count_cmp_f64(v, op, lit):
+    v = _c(v, np.float64)
+    return int(lib().ref_count_cmp_f64(_p(v), len(v), op, float(lit)))
+
+
+def ref_present_codes(codes, dict_len, threads):
+    c = _c(codes, np.uint32)
+    out = np.zeros(max(1, dict_len), np.uint8)
+    lib().ref_present_codes(_p(c), len(c), dict_len, threads, _p(out))
+    return out[:dict_len]
+
+
+def ref_topk(values, k, desc):
+    v = np.ascontiguousarray(values)
+    dtype = 2 if v.dtype.kind == "f" else 1
+    out = np.zeros(max(1, k), np.uint32)
+    m = lib().ref_topk(dtype, _p(v), len(v), k, int(desc), _p(out))
+    return out[:m]
+
+
+def ref_filter_group_codes(codes, score, salary, dict_len, op, lit, threads):
+    c, s, sa = _c(codes, np.uint32), _c(score, np.float64), _c(salary, np.int64)
+    rows, fs, is_ = np.zeros(dict_len, np.int64), np.zeros(dict_len), np.zeros(dict_len)
+    lib().ref_filter_group_codes(_p(c), _p(s), _p(sa), len(c), dict_len, op, float(lit), threads, _p(rows), _p(fs),
+                                 _p(is_))
+    return rows, fs, is_
+
+
+def ref_join_agg(bkeys, bpay, pkeys, pval, join_type, threads):
+    bk, bp, pk = _c(bkeys, np.int64), _c(bpay, np.int64), _c(pkeys, np.int64)
+    pv = _c(pval, np.float64)
+    o = [np.zeros(1, np.int64), np.zeros(1, np.int64), np.zeros(1, np.float64)]
+    lib().ref_join_agg(_p(bk), _p(bp), len(bk), _p(pk), _p(pv), len(pk), join_type, threads, *[_p(x) for x in o])
+    return int(o[0][0]), int(o[1][0]), float(o[2][0])
+
+
+def ref_group_i64(keys, vals, threads):
+    k, v = _c(keys, np.int64), _c(vals, np.float64)
+    return int(lib().ref_group_i64(_p(k), _p(v), len(k), threads))

@@ -1,0 +1,133 @@
+"""GPU parity of GROUP BY: dictionary-code groups (fast_utf8_gb) and int64 hash
+groups (fast_i64_gb) against the oracle.  Counts and integer sums bit-exact;
+FP64 sums within 1e-12 relative; MIN/MAX exact."""
+import numpy as np
+import pytest
+import torch
+
+import falcondb_b200 as F
+from falcondb_b200 import ops, workloads as W
+from oracle import oracle as O
+
+pytestmark = pytest.mark.gpu
+RTOL = 1e-12
+
+
+def dev(a):
+    return torch.from_numpy(np.ascontiguousarray(a)).cuda()
+
+
+def close(a, b):
+    return abs(a - b) <= RTOL * max(abs(a), abs(b), 1e-300)
+
+
+@pytest.mark.parametrize("n", [1, 65, 4096, 1_000_000, 3_000_017])
+def test_filter_group_by_dept(db, n):
+    """The config-0 query shape: WHERE score > 50 GROUP BY dept with COUNT(*),
+    SUM(score), AVG(salary)."""
+    t = W.table_t(n, seed=n)
+    codes, score, salary = t["dept"].codes, t["score"], t["salary"]
+    cols = [dev(codes.view(np.int32)), dev(score), dev(salary)]
+    out, rows = ops.group_by_codes(db, cols, n, [ops.cmp(1, F.GT, 50)], 0, 12,
+                                   [(F.AGG_COUNT_STAR, 0), (F.AGG_SUM, 1), (F.AGG_AVG, 2), (F.AGG_MIN, 1)])
+    rec = ops.to_records(out, F.AGG_VALUE_DTYPE).reshape(13, 4)[:13]
+    grows = rows.cpu().numpy()
+    mask = O.cmp_mask(score, F.GT, 50)
+    g = O.group_codes(codes, 12, mask=mask, fvals=score, ivals=salary)
+    assert list(grows) == list(g["rows"])
+    for d in range(12):
+        if g["rows"][d] == 0:
+            continue
+        assert rec[d, 0]["i"] == g["rows"][d]
+        assert close(rec[d, 1]["f"], g["fsum"][d])
+        assert rec[d, 2]["f"] == g["isum"][d] / g["icnt"][d]  # bit-exact: integer partial sums
+        assert rec[d, 3]["f"] == g["fmin"][d]
+
+
+def test_group_by_codes_nulls_and_empty_groups(db):
+    n = 50_000
+    r = np.random.default_rng(3)
+    codes = r.integers(0, 7, n).astype(np.uint32)
+    codes[::13] = 0xFFFFFFFF
+    vals = r.integers(-100, 100, n)
+    valid = r.random(n) > 0.3
+    vw = F.validity_words(valid)
+    cols = [dev(codes.view(np.int32)), (dev(vals), dev(vw.view(np.int64)))]
+    out, rows = ops.group_by_codes(db, cols, n, [], 0, 10, [(F.AGG_COUNT, 1), (F.AGG_SUM, 1), (F.AGG_MAX, 1)])
+    rec = ops.to_records(out, F.AGG_VALUE_DTYPE).reshape(11, 3)
+    grows = rows.cpu().numpy()
+    g = O.group_codes(codes, 10, ivals=vals, ivalid=vw)
+    assert list(grows) == list(g["rows"])
+    for d in range(11):
+        if g["rows"][d] == 0:
+            continue
+        assert rec[d, 0]["i"] == g["icnt"][d]
+        assert rec[d, 1]["f"] == g["isum"][d]
+        sel = (np.where(codes == 0xFFFFFFFF, 10, codes) == d) & valid
+        if sel.any():
+            assert rec[d, 2]["f"] == float(vals[sel].max())
+        else:
+            assert rec[d, 2]["valid"] == 0
+
+
+def test_group_by_codes_is_repeatable(db):
+    n = 2_000_000
+    t = W.table_t(n, seed=5)
+    cols = [dev(t["dept"].codes.view(np.int32)), dev(t["score"])]
+    outs = [ops.to_records(ops.group_by_codes(db, cols, n, [], 0, 12, [(F.AGG_SUM, 1)])[0], F.AGG_VALUE_DTYPE)
+            for _ in range(3)]
+    assert np.array_equal(outs[0]["f"], outs[1]["f"]) and np.array_equal(outs[1]["f"], outs[2]["f"])
+
+
+def _hash_groups(db, keys, vals, **kw):
+    n = len(keys)
+    out, ng = ops.group_by_i64(db, dev(keys), dev(vals), n, **kw)
+    g = int(ng.item())
+    rec = ops.to_records(out, F.GROUP_I64_DTYPE, g)
+    return rec[np.argsort(rec["key"], kind="stable")]
+
+
+@pytest.mark.parametrize("n,distinct", [(1, 10), (1000, 50), (200_000, 100_000), (2_000_000, 1_000_000)])
+def test_hash_group_by_zipf(db, n, distinct):
+    t = W.groupby_table(n, distinct=distinct, seed=n)
+    rec = _hash_groups(db, t["key"], t["v"])
+    want = O.group_i64(t["key"], t["v"])
+    assert np.array_equal(rec["key"], want["key"])
+    assert np.array_equal(rec["count"], want["count"])
+    assert np.array_equal(rec["min"], want["min"]) and np.array_equal(rec["max"], want["max"])
+    rel = np.abs(rec["sum"] - want["sum"]) / np.maximum(np.abs(want["sum"]), 1e-300)
+    assert rel.max() <= RTOL
+
+
+def test_hash_group_by_null_keys_and_int_values(db):
+    n = 100_000
+    r = np.random.default_rng(8)
+    keys = r.integers(-50, 50, n)
+    keys[::17] = np.iinfo(np.int64).min  # reads as NULL (aggregate.rs:867)
+    vals = r.integers(0, 1000, n)
+    rec = _hash_groups(db, keys, vals)
+    want = O.group_i64(keys, vals.astype(np.float64))
+    assert np.array_equal(rec["key"], want["key"])
+    assert np.array_equal(rec["count"], want["count"])
+    assert np.array_equal(rec["sum"], want["sum"])  # integer-valued f64 sums are exact
+
+
+def test_hash_group_by_all_distinct_and_load_factor(db):
+    n = 500_000
+    keys = np.random.default_rng(9).permutation(n).astype(np.int64) * 7 - 3
+    vals = np.random.default_rng(10).random(n)
+    for lf in (0.25, 0.5, 0.7):
+        rec = _hash_groups(db, keys, vals, load_factor=lf, expected_groups=n)
+        assert len(rec) == n
+        order = np.argsort(keys)
+        assert np.array_equal(rec["key"], keys[order]) and np.array_equal(rec["sum"], vals[order])
+
+
+def test_hash_group_by_with_filter(db):
+    n = 300_000
+    t = W.groupby_table(n, distinct=20_000, seed=12)
+    sel = np.random.default_rng(13).random(n) * 100
+    rec = _hash_groups(db, t["key"], t["v"], prog=[ops.cmp(0, F.LT, 25.0)], pred_cols=[dev(sel)])
+    mask = O.cmp_mask(sel, F.LT, 25.0)
+    want = O.group_i64(t["key"], t["v"], mask=mask)
+    assert np.array_equal(rec["key"], want["key"]) and np.array_equal(rec["count"], want["count"])

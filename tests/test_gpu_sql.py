@@ -1,0 +1,114 @@
+"""Database.sql on the GPU: every known answer of the reference's own tests
+(tests/golden/known_answers.json) and the headline query shapes against the
+oracle."""
+import numpy as np
+import pytest
+
+import falcondb_b200 as F
+from falcondb_b200 import workloads as W
+from oracle import oracle as O
+from tests.known_answers import build_table, cases, check_result
+
+pytestmark = pytest.mark.gpu
+RTOL = 1e-12
+
+
+def load(db, tables):
+    for name, spec in tables.items():
+        db.create_table(name, build_table(spec))
+
+
+@pytest.mark.parametrize("case", cases(), ids=lambda c: c["name"])
+def test_known_answer(db, case):
+    load(db, case["tables"])
+    res = db.sql(case["sql"])
+    check_result(case, res)
+
+
+def test_config0_query(db):
+    n = 1_000_000
+    t = W.table_t(n, seed=1)
+    db.create_table("t", t)
+    res = db.sql("SELECT dept, COUNT(*), SUM(score), AVG(salary) FROM t WHERE score > 50 GROUP BY dept ORDER BY dept")
+    mask = O.cmp_mask(t["score"], F.GT, 50)
+    g = O.group_codes(t["dept"].codes, 12, mask=mask, fvals=t["score"], ivals=t["salary"])
+    assert res.row_count() == 12
+    assert res.column(0) == W.DEPTS  # ORDER BY dept
+    for i in range(12):
+        assert res.column(1)[i] == g["rows"][i]
+        assert abs(res.column(2)[i] - g["fsum"][i]) <= RTOL * g["fsum"][i]
+        assert res.column(3)[i] == g["isum"][i] / g["icnt"][i]
+
+
+def test_config1_queries(db):
+    n = 2_000_003
+    t = W.table_t(n, seed=2)
+    db.create_table("t", t)
+    s = db.sql("SELECT SUM(score) FROM t").column(0)[0]
+    want = O.sum_serial(t["score"])
+    assert abs(s - want) <= RTOL * want
+    assert db.sql("SELECT COUNT(*) FROM t WHERE score > 50").column(0)[0] == O.popcount(
+        O.cmp_mask(t["score"], F.GT, 50))
+    assert db.sql("SELECT COUNT(DISTINCT dept) FROM t").column(0)[0] == 12
+    top = db.sql("SELECT id, score FROM t ORDER BY score DESC LIMIT 10")
+    rows = O.topk(t["score"], 10, True)
+    assert list(top.column(0)) == list(t["id"][rows])
+    assert list(top.column(1)) == list(t["score"][rows])
+    top2 = db.sql("SELECT id FROM t ORDER BY id DESC LIMIT 10")
+    assert list(top2.column(0)) == list(range(n - 1, n - 11, -1))
+
+
+def test_config2_join_queries(db):
+    b, p = W.join_tables(100_000, 1_000_003, seed=5)
+    db.create_table("b", b)
+    db.create_table("p", p)
+    for sql, jt in [("SELECT COUNT(*), SUM(b.payload) FROM p JOIN b ON p.key = b.key", F.JOIN_INNER),
+                    ("SELECT COUNT(*), SUM(b.payload) FROM p LEFT JOIN b ON p.key = b.key", F.JOIN_LEFT)]:
+        r = db.sql(sql)
+        want = O.join_agg(b["key"], b["payload"], p["key"], p["value"], jt)
+        assert r.column(0)[0] == want["count"] and r.column(1)[0] == float(want["sum_payload"])
+    for sql, jt in [("SELECT COUNT(*), SUM(value) FROM p WHERE EXISTS (SELECT 1 FROM b WHERE b.key = p.key)",
+                     F.JOIN_SEMI),
+                    ("SELECT COUNT(*), SUM(value) FROM p WHERE NOT EXISTS (SELECT 1 FROM b WHERE b.key = p.key)",
+                     F.JOIN_ANTI)]:
+        r = db.sql(sql)
+        want = O.join_agg(b["key"], b["payload"], p["key"], p["value"], jt)
+        assert r.column(0)[0] == want["count"]
+        assert abs(r.column(1)[0] - want["sum_value"]) <= RTOL * want["sum_value"]
+
+
+def test_config3_group_by(db):
+    n = 1_000_000
+    g = W.groupby_table(n, distinct=200_000, seed=4)
+    db.create_table("g", g)
+    r = db.sql("SELECT key, COUNT(*), SUM(v), MIN(v), MAX(v) FROM g GROUP BY key ORDER BY key")
+    want = O.group_i64(g["key"], g["v"])
+    assert np.array_equal(np.asarray(r.column(0)), want["key"])
+    assert np.array_equal(np.asarray(r.column(1)), want["count"])
+    rel = np.abs(np.asarray(r.column(2)) - want["sum"]) / np.abs(want["sum"])
+    assert rel.max() <= RTOL
+    assert np.array_equal(np.asarray(r.column(3)), want["min"])
+
+
+def test_where_with_projection_and_limit(db):
+    t = W.table_t(100_000, seed=9)
+    db.create_table("t", t)
+    r = db.sql("SELECT id, score FROM t WHERE score > 99.9 AND dept = 'd03' ORDER BY score DESC LIMIT 5")
+    sel = np.flatnonzero((t["score"] > 99.9) & (t["dept"].codes == 3))
+    order = sel[np.lexsort((sel, -t["score"][sel]))][:5]
+    assert list(r.column(0)) == list(order)
+    r2 = db.sql("SELECT COUNT(*) FROM t WHERE dept IN ('d01', 'd02') OR salary < 31000")
+    want = int(((t["dept"].codes == 1) | (t["dept"].codes == 2) | (t["salary"] < 31000)).sum())
+    assert r2.column(0)[0] == want
+
+
+def test_errors_are_reported(db):
+    db.create_table("t", {"x": np.arange(10, dtype=np.int64)})
+    with pytest.raises(F.FalconError) as e:
+        db.sql("SELECT y FROM t")
+    assert e.value.code == -6
+    with pytest.raises(F.FalconError) as e:
+        db.sql("SELEKT x FROM t")
+    assert e.value.code == -5
+    with pytest.raises(F.FalconError):
+        db.sql("SELECT x FROM nope")
