@@ -483,7 +483,7 @@ void op_group_by_codes(Ctx& c, const fdb_dev_column* cols, int ncols, uint64_t n
   GbCodesParams p;
   std::memset(&p, 0, sizeof(p));
   for (int i = 0; i < ncols; ++i) {
-    if (!cols[i].values) fail(FDB_E_ARG, "column without values");
+    if (!cols[i].values && n > 0) fail(FDB_E_ARG, "column without values");
     p.cols[i] = DevCol{cols[i].dtype, cols[i].values, cols[i].validity, cols[i].validity_offset};
   }
   gb_fill_prog(p.prog, prog, nterms, ncols, 0);
@@ -553,7 +553,7 @@ void op_group_by_i64(Ctx& c, const fdb_dev_column& key, const fdb_dev_column& va
   for (int i = 0; i < npred; ++i) all[2 + i] = pred_cols[i];
   const int nc = 2 + npred;
   for (int i = 0; i < nc; ++i) {
-    if (!all[i].values) fail(FDB_E_ARG, "column without values");
+    if (!all[i].values && n > 0) fail(FDB_E_ARG, "column without values");
     p.cols[i] = DevCol{all[i].dtype, all[i].values, all[i].validity, all[i].validity_offset};
   }
   gb_fill_prog(p.prog, prog, nterms, npred, 2);

@@ -510,11 +510,11 @@ static void fill_prog(PredProg& pp, const fdb_pred_term* prog, int nterms, int n
   if (nterms > 0 && depth != 1) fail(FDB_E_ARG, "malformed predicate program");
 }
 
-static void fill_cols(ScanCols& sc, const fdb_dev_column* cols, int ncols) {
+static void fill_cols(ScanCols& sc, const fdb_dev_column* cols, int ncols, uint64_t n) {
   if (ncols < 1 || ncols > 4) fail(FDB_E_ARG, "between 1 and 4 input columns are supported per scan");
   std::memset(&sc, 0, sizeof(sc));
   for (int i = 0; i < ncols; ++i) {
-    if (cols[i].values == nullptr) fail(FDB_E_ARG, "column without values");
+    if (cols[i].values == nullptr && n > 0) fail(FDB_E_ARG, "column without values");
     if (cols[i].dtype != FDB_INT64 && cols[i].dtype != FDB_FLOAT64 && cols[i].dtype != FDB_UTF8)
       fail(FDB_E_TYPE, "unsupported column type");
     sc.cols[i] = DevCol{cols[i].dtype, cols[i].values, cols[i].validity, cols[i].validity_offset};
@@ -527,7 +527,7 @@ void op_aggregate(Ctx& c, const fdb_dev_column* cols, int ncols, uint64_t n,
   if (naggs < 1 || naggs > 4) fail(FDB_E_ARG, "between 1 and 4 aggregates per scan");
   ScanAggParams p;
   std::memset(&p, 0, sizeof(p));
-  fill_cols(p.sc, cols, ncols);
+  fill_cols(p.sc, cols, ncols, n);
   fill_prog(p.prog, prog, nterms, ncols);
   p.naggs = naggs;
   for (int a = 0; a < naggs; ++a) {
@@ -576,7 +576,7 @@ void op_filter_count(Ctx& c, const fdb_dev_column* cols, int ncols, uint64_t n,
                      const fdb_pred_term* prog, int nterms, uint64_t* d_count) {
   ScanAggParams p;
   std::memset(&p, 0, sizeof(p));
-  fill_cols(p.sc, cols, ncols);
+  fill_cols(p.sc, cols, ncols, n);
   fill_prog(p.prog, prog, nterms, ncols);
   p.naggs = 1;
   p.func[0] = FDB_AGG_COUNT_STAR;
@@ -604,7 +604,7 @@ void op_distinct_codes(Ctx& c, const fdb_dev_column* cols, int ncols, uint64_t n
                        uint64_t* d_bitmap) {
   DistinctParams p;
   std::memset(&p, 0, sizeof(p));
-  fill_cols(p.sc, cols, ncols);
+  fill_cols(p.sc, cols, ncols, n);
   fill_prog(p.prog, prog, nterms, ncols);
   if (code_col < 0 || code_col >= ncols || cols[code_col].dtype != FDB_UTF8)
     fail(FDB_E_TYPE, "COUNT DISTINCT over codes needs a Utf8 column");
@@ -660,7 +660,7 @@ void op_filter_mask(Ctx& c, const fdb_dev_column* cols, int ncols, uint64_t n,
                     const fdb_pred_term* prog, int nterms, uint64_t* d_mask) {
   MaskParams p;
   std::memset(&p, 0, sizeof(p));
-  fill_cols(p.sc, cols, ncols);
+  fill_cols(p.sc, cols, ncols, n);
   fill_prog(p.prog, prog, nterms, ncols);
   const uint64_t nwords = (n + 63) / 64;
   if (nwords == 0) return;
