@@ -29,9 +29,7 @@ import argparse
 import json
 import os
 import statistics
-import subprocess
 import sys
-import tempfile
 import time
 from pathlib import Path
 
@@ -73,57 +71,75 @@ def traffic_from_profiles(kernel: str):
 
 
 class Clocks:
-    """nvidia-smi sampling of SM clocks and throttle reasons during a region."""
+    """SM clock and clock-event (throttle) reasons sampled through NVML every
+    millisecond while the timed region runs (the region is tens of ms, too short
+    for nvidia-smi's sampling period).  Reads only; changes no GPU setting."""
 
-    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
-              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
-              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+    REASONS = {0x4: "sw_power_cap", 0x8: "hw_slowdown", 0x20: "sw_thermal_slowdown",
+               0x40: "hw_thermal_slowdown", 0x80: "hw_power_brake_slowdown"}
 
     def __init__(self, device: int):
         self.device = device
-        self.proc = None
-        self.path = None
+        self.samples = []
+        self.reasons = set()
+        self.max_mhz = None
+        self._stop = None
+        self._thread = None
+        self._nvml = None
+
+    def _handle(self):
+        import pynvml
+
+        pynvml.nvmlInit()
+        try:
+            from cuda import cudart
+
+            err, bus = cudart.cudaDeviceGetPCIBusId(64, self.device)
+            bus = bus.decode() if isinstance(bus, bytes) else bus
+            return pynvml, pynvml.nvmlDeviceGetHandleByPciBusId(bus.strip("\x00"))
+        except Exception:
+            return pynvml, pynvml.nvmlDeviceGetHandleByIndex(self.device)
 
     def __enter__(self):
-        fd, self.path = tempfile.mkstemp(suffix=".csv")
-        os.close(fd)
+        import threading
+
         try:
-            self.proc = subprocess.Popen(
-                ["nvidia-smi", f"--id={self.device}", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
-                 "-lms", "200"], stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
-        except FileNotFoundError:
-            self.proc = None
+            nv, h = self._handle()
+        except Exception:
+            return self
+        self._nvml = nv
+        self.max_mhz = nv.nvmlDeviceGetMaxClockInfo(h, nv.NVML_CLOCK_SM)
+        get_reasons = getattr(nv, "nvmlDeviceGetCurrentClocksEventReasons", None) or \
+            nv.nvmlDeviceGetCurrentClocksThrottleReasons
+        self._stop = threading.Event()
+
+        def run():
+            while not self._stop.is_set():
+                try:
+                    self.samples.append(nv.nvmlDeviceGetClockInfo(h, nv.NVML_CLOCK_SM))
+                    r = get_reasons(h)
+                    for bit, name in self.REASONS.items():
+                        if r & bit:
+                            self.reasons.add(name)
+                except Exception:
+                    pass
+                time.sleep(0.001)
+
+        self._thread = threading.Thread(target=run, daemon=True)
+        self._thread.start()
+        time.sleep(0.003)
         return self
 
     def __exit__(self, *a):
-        if self.proc is not None:
-            self.proc.terminate()
-            try:
-                self.proc.wait(timeout=5)
-            except subprocess.TimeoutExpired:
-                self.proc.kill()
+        if self._thread is not None:
+            self._stop.set()
+            self._thread.join(timeout=2)
 
     def summary(self):
-        if not self.path or not os.path.exists(self.path):
+        if not self.samples:
             return None
-        sm, mx, reasons = [], [], set()
-        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        for line in open(self.path):
-            parts = [x.strip() for x in line.split(",")]
-            if len(parts) < 9:
-                continue
-            try:
-                sm.append(float(parts[1]))
-                mx.append(float(parts[2]))
-            except ValueError:
-                continue
-            for nm, flag in zip(names, parts[5:9]):
-                if flag.lower() == "active":
-                    reasons.add(nm)
-        os.unlink(self.path)
-        if not sm:
-            return None
-        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": max(mx), "reasons": sorted(reasons), "samples": len(sm)}
+        return {"sm_mhz": statistics.median(self.samples), "sm_max_mhz": self.max_mhz,
+                "reasons": sorted(self.reasons), "samples": len(self.samples), "source": "NVML, 1 ms polling"}
 
 
 def make_table(n: int, seed: int):
@@ -376,6 +392,121 @@ def cpu_baseline(t, n, threads):
             "seconds": round(el, 3)}
 
 
+# ----------------------------------------------------------------------------- secondary workloads
+def _time_steps(fn, K, W, stream, torch):
+    """CUDA-event time of K calls of fn() on `stream` after W warm-ups."""
+    for _ in range(W):
+        fn()
+    torch.cuda.synchronize()
+    s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    s.record(stream)
+    for _ in range(K):
+        fn()
+    e.record(stream)
+    torch.cuda.synchronize()
+    return s.elapsed_time(e) / K
+
+
+def run_secondary(args):
+    """Per-operator lines for the other hot-path rows (not the headline):
+    filter_groupby (fused WHERE -> GROUP BY dept, 20 B/row), join (1M build x
+    100M probe, INNER/LEFT/SEMI/ANTI), groupby (100M Zipf keys, 16 B/row + 40 B
+    per group)."""
+    import torch
+
+    import falcondb_b200 as F
+    from falcondb_b200 import ops, workloads as W
+    from oracle import oracle as O
+
+    dev = torch.device("cuda", 0)
+    db = F.Database(0)
+    stream = ops.lib_stream(db)
+    peak, peak_kind = peaks()
+    out = []
+    n = args.rows
+    K, Wm = args.steps, args.warmup
+
+    def line(name, ms, nbytes, extra):
+        gbs = nbytes / (ms / 1e3) / 1e9
+        d = {"metric": METRIC, "workload": name, "value": round(gbs, 1), "unit": "GB/s", "ms": round(ms, 4),
+             "frac_of_measured_hbm": round(gbs / peak, 4), "frac_vs_8TBs": round(gbs / 8000, 4),
+             "algorithmic_bytes": nbytes, "steps": K, "warmup": Wm}
+        d.update(extra)
+        out.append(d)
+
+    if args.workload in ("filter_groupby", "all"):
+        for rows in sorted({1_000_000, n}):
+            t = W.table_t(rows, seed=1)
+            db.create_table("t", t)
+            cols = [db.column("t", c) for c in ("dept", "score", "salary")]
+            prog = [ops.cmp(1, F.GT, 50)]
+            aggs = [(F.AGG_COUNT_STAR, 0), (F.AGG_SUM, 1), (F.AGG_AVG, 2)]
+            res = ops._bytes(F.AGG_VALUE_DTYPE.itemsize * 13 * 3, db)
+            grows = torch.empty(13, dtype=torch.int64, device=dev)
+            L = F.lib()
+            ca, nc = ops._cols(cols)
+            pa, npr = ops._prog(prog)
+            aa, na = ops._aggs(aggs)
+
+            def q():
+                F.check(L.fdb_group_by_codes(db.handle, ca, nc, rows, pa, npr, 0, 12, aa, na, res.data_ptr(),
+                                             grows.data_ptr()))
+            ms = _time_steps(q, K, Wm, stream, torch)
+            g = O.group_codes(t["dept"].codes, 12, mask=O.cmp_mask(t["score"], F.GT, 50), fvals=t["score"],
+                              ivals=t["salary"])
+            assert list(grows.cpu().numpy()[:12]) == list(g["rows"][:12])
+            line("filter_groupby", ms, 20 * rows, {"rows": rows, "query": "SELECT dept, COUNT(*), SUM(score), "
+                                                   "AVG(salary) FROM t WHERE score > 50 GROUP BY dept"})
+            db.drop_table("t")
+
+    if args.workload in ("join", "all"):
+        nb, npb = 1_000_000, n
+        b, p = W.join_tables(nb, npb, seed=7)
+        db.create_table("b", b)
+        db.create_table("p", p)
+        bk, bp = db.column("b", "key"), db.column("b", "payload")
+        pk, pv = db.column("p", "key"), db.column("p", "value")
+        res = ops._bytes(F.JOIN_AGG_DTYPE.itemsize, db)
+        ms_build = _time_steps(lambda: ops.HashTable(db, bk, bp, nb).free(), max(3, K // 5), 2, stream, torch)
+        h = ops.HashTable(db, bk, bp, nb)
+        for jt, name in [(F.JOIN_INNER, "inner"), (F.JOIN_LEFT, "left"), (F.JOIN_SEMI, "semi"), (F.JOIN_ANTI, "anti")]:
+            val = pv if jt >= F.JOIN_SEMI else None
+            ms = _time_steps(lambda: h.probe_agg(pk, npb, jt, value=val, out=res), K, Wm, stream, torch)
+            got = ops.to_records(res, F.JOIN_AGG_DTYPE, 1)[0]
+            nbytes = 8 * npb + (8 * npb if jt >= F.JOIN_SEMI else 0)
+            line(f"join_probe_{name}", ms, nbytes, {"build_rows": nb, "probe_rows": npb, "count": int(got["count"]),
+                                                   "build_ms": round(ms_build, 4),
+                                                   "query_ms_build_plus_probe": round(ms + ms_build, 4),
+                                                   "query_GBps": round((nbytes + 16 * nb) / ((ms + ms_build) / 1e3)
+                                                                       / 1e9, 1)})
+        want = O.join_agg(b["key"], b["payload"], p["key"], p["value"], F.JOIN_INNER)
+        got = ops.to_records(h.probe_agg(pk, npb, F.JOIN_INNER, out=res), F.JOIN_AGG_DTYPE, 1)[0]
+        assert int(got["count"]) == want["count"] and int(got["sum_payload"]) == want["sum_payload"]
+        h.free()
+        db.drop_table("b")
+        db.drop_table("p")
+
+    if args.workload in ("groupby", "all"):
+        g = W.groupby_table(n, distinct=10_000_000, seed=11)
+        db.create_table("g", g)
+        gk, gv = db.column("g", "key"), db.column("g", "v")
+        cap = 12_000_000
+        outb = ops._bytes(F.GROUP_I64_DTYPE.itemsize * cap, db)
+        ng = torch.empty(1, dtype=torch.int64, device=dev)
+        lf = args.load_factor
+
+        def q():
+            ops.group_by_i64(db, gk, gv, n, expected_groups=10_000_000, load_factor=lf, capacity=cap, out=outb,
+                             ngroups=ng)
+        ms = _time_steps(q, K, Wm, stream, torch)
+        groups = int(ng.item())
+        line("groupby_zipf", ms, 16 * n + 40 * groups, {"rows": n, "groups": groups, "distinct_domain": 10_000_000,
+                                                        "zipf_s": 1.1, "load_factor": lf})
+        db.drop_table("g")
+    db.close()
+    return out
+
+
 def run_reference(args):
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
@@ -408,7 +539,7 @@ def run_reference(args):
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--steps", type=int, default=50)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="engine", choices=["engine", "reference"])
     ap.add_argument("--rows", type=int, default=N_ROWS)
@@ -416,9 +547,17 @@ def main():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--cpu-threads", type=int, default=0)
+    ap.add_argument("--workload", default="scan",
+                    choices=["scan", "filter_groupby", "join", "groupby", "all"],
+                    help="scan = the headline line; the others print per-operator lines")
+    ap.add_argument("--load-factor", type=float, default=0.5)
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
+    if args.workload != "scan" and args.impl != "reference":
+        for line in run_secondary(args):
+            print(json.dumps(line), flush=True)
+        return
     res = run_reference(args) if args.impl == "reference" else run_gpu(args)
     if res is not None:
         print(json.dumps(res), flush=True)

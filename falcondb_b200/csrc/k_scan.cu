@@ -298,6 +298,21 @@ struct ColAggOp : ScanAggOp {
   template <class Acc>
   static __device__ void step(Local& st, const Params& p, unsigned char*, const Acc& acc,
                               uint32_t rows, int ctid, int nct) {
+    if constexpr (Acc::kSmemTile && T(0.5) != T(0)) {
+      // SUM alone over a FLOAT64 tile: two rows per 16-byte load, two chains.
+      if (p.naggs == 1 && p.func[0] == FDB_AGG_SUM && (rows & 1u) == 0) {
+        const double2* v = reinterpret_cast<const double2*>(acc.template col_ptr<double>(0));
+        double s0 = 0.0, s1 = 0.0;
+        for (uint32_t i = ctid; i < (rows >> 1); i += nct) {
+          const double2 x = v[i];
+          s0 += x.x;
+          s1 += x.y;
+        }
+        st.a[0].f += s0 + s1;
+        st.a[0].n += rows / nct + ((uint32_t)ctid < rows % nct ? 1 : 0);
+        return;
+      }
+    }
     uint32_t i = ctid;
     for (; i + nct < rows; i += 2 * nct) {
       const T v0 = acc.template get<T>(0, i);
@@ -382,6 +397,22 @@ struct DistinctOp {
   template <class Acc>
   static __device__ void step(Local& st, const Params& p, unsigned char* sm, const Acc& acc,
                               uint32_t rows, int ctid, int nct) {
+    if constexpr (Acc::kSmemTile) {
+      // Fast path: one code column, no WHERE, no NULLs, <= 64 codes: four
+      // codes per 16-byte shared-memory load into a register bitmask.
+      if (p.prog.n == 0 && p.dict_len <= 64 && p.sc.cols[p.code_col].validity == nullptr && (rows & 3u) == 0) {
+        const uint4* v = reinterpret_cast<const uint4*>(acc.template col_ptr<uint32_t>(p.code_col));
+        uint64_t bits = 0;
+        const uint32_t dl = p.dict_len;
+        for (uint32_t i = ctid; i < (rows >> 2); i += nct) {
+          const uint4 c = v[i];
+          bits |= (c.x < dl ? 1ull << c.x : 0ull) | (c.y < dl ? 1ull << c.y : 0ull) |
+                  (c.z < dl ? 1ull << c.z : 0ull) | (c.w < dl ? 1ull << c.w : 0ull);
+        }
+        st.bits |= bits;
+        return;
+      }
+    }
     const bool small = p.dict_len <= 64;
     const bool in_smem = !small && p.dict_len <= kSmemMaxCodes;
     uint32_t* w = reinterpret_cast<uint32_t*>(sm);
@@ -435,23 +466,32 @@ struct TileShape {
   static constexpr int STAGES = NC <= 2 ? 4 : 3;
   static constexpr int NCW = 8;
 };
+template <int NC, int TRo>
+struct TileShapeO {
+  static constexpr int TR = TRo ? TRo : TileShape<NC>::TR;
+  static constexpr int STAGES = TileShape<NC>::STAGES;
+  static constexpr int NCW = TileShape<NC>::NCW;
+};
 
-template <class Op, int NC>
+// TRo / CBo override the tile rows and the bytes reserved per row per column
+// (a scan of one 4-byte column uses 4096-row, 16 KB tiles).
+template <class Op, int NC, int TRo = 0, int CBo = 8>
 static void launch_stream(Ctx& c, const fdb_dev_column* cols, uint64_t n, const typename Op::Params& p,
                           size_t op_smem_bytes) {
-  using S = TileShape<NC>;
+  using S = TileShapeO<NC, TRo>;
   StreamSrc<NC> src;
   const void* bases[NC];
   for (int i = 0; i < NC; ++i) {
     src.base[i] = static_cast<const unsigned char*>(cols[i].values);
     src.esize[i] = dtype_size(cols[i].dtype);
+    if (src.esize[i] > CBo) fail(FDB_E_ARG, "column wider than the tile layout");
     bases[i] = cols[i].values;
   }
   src.n = n;
   src.m_end = stream_m_end(bases, NC, n);
-  const int op_off = (int)stream_smem_bytes<NC, S::TR, S::STAGES>();
+  const int op_off = (int)stream_smem_bytes<NC, S::TR, S::STAGES, CBo>();
   const size_t smem = op_off + op_smem_bytes;
-  auto kern = stream_kernel<Op, NC, S::TR, S::STAGES, S::NCW>;
+  auto kern = stream_kernel<Op, NC, S::TR, S::STAGES, S::NCW, CBo>;
   static bool attr_done = false;  // per instantiation
   if (!attr_done) {
     FDB_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024));
@@ -614,7 +654,10 @@ void op_distinct_codes(Ctx& c, const fdb_dev_column* cols, int ncols, uint64_t n
   const size_t words = (dict_len + 63) / 64;
   if (words) FDB_CUDA(cudaMemsetAsync(d_bitmap, 0, words * 8, c.stream));
   if (n == 0 || dict_len == 0) return;
-  launch_stream_nc<DistinctOp>(c, cols, ncols, n, p, DistinctOp::kSmem);
+  if (ncols == 1)
+    launch_stream<DistinctOp, 1, 4096, 4>(c, cols, n, p, DistinctOp::kSmem);
+  else
+    launch_stream_nc<DistinctOp>(c, cols, ncols, n, p, DistinctOp::kSmem);
 }
 
 // ---------------------------------------------------------------------------

@@ -25,14 +25,19 @@ struct StreamSrc {
 };
 
 // Rows staged in shared memory: column c of the current stage starts at
-// stage + c * TR * 8.
-template <int TR>
+// stage + c * TR * CB (CB = bytes reserved per row per column, 8 or 4).
+template <int TR, int CB = 8>
 struct TileAcc {
+  static constexpr bool kSmemTile = true;
   const unsigned char* stage;
   uint64_t row0;
   template <typename T>
+  __device__ __forceinline__ const T* col_ptr(int c) const {
+    return reinterpret_cast<const T*>(stage + (size_t)c * TR * CB);
+  }
+  template <typename T>
   __device__ __forceinline__ T get(int c, uint32_t i) const {
-    return reinterpret_cast<const T*>(stage + (size_t)c * TR * 8)[i];
+    return reinterpret_cast<const T*>(stage + (size_t)c * TR * CB)[i];
   }
   __device__ __forceinline__ uint64_t row(uint32_t i) const { return row0 + i; }
 };
@@ -40,6 +45,11 @@ struct TileAcc {
 // Rows read straight from global memory.
 template <int NC>
 struct GlobAcc {
+  static constexpr bool kSmemTile = false;
+  template <typename T>
+  __device__ __forceinline__ const T* col_ptr(int) const {
+    return nullptr;
+  }
   const unsigned char* base[NC];
   int esize[NC];
   uint64_t row0;
@@ -60,9 +70,9 @@ __device__ __forceinline__ void consumer_bar(int nthreads) {
 
 constexpr int kBarBytes = 128;  // mbarrier block at the start of dynamic smem
 
-template <int NC, int TR, int STAGES>
+template <int NC, int TR, int STAGES, int CB = 8>
 constexpr size_t stream_smem_bytes() {
-  return kBarBytes + (size_t)STAGES * NC * TR * 8;
+  return kBarBytes + (size_t)STAGES * NC * TR * CB;
 }
 
 // Host helper: the TMA-staged prefix of the row range.  Every column base must
@@ -82,7 +92,7 @@ inline uint64_t stream_m_end(const void* const* bases, int nc, uint64_t n) {
 //   static __device__ void finish(Local&, const Params&, unsigned char* op_smem, int ctid, int nct);
 // step() and finish() are executed by all consumer threads; block-wide syncs
 // inside them must use consumer_bar(nct).
-template <class Op, int NC, int TR, int STAGES, int NCW>
+template <class Op, int NC, int TR, int STAGES, int NCW, int CB = 8>
 __global__ void __launch_bounds__((NCW + 1) * 32)
     stream_kernel(StreamSrc<NC> src, typename Op::Params p, int* err, int op_smem_off) {
   extern __shared__ __align__(128) unsigned char smem[];
@@ -120,7 +130,7 @@ __global__ void __launch_bounds__((NCW + 1) * 32)
         mbar_arrive_expect_tx(&full[s], bytes);
 #pragma unroll
         for (int c = 0; c < NC; ++c)
-          bulk_g2s(tiles + ((size_t)s * NC + c) * TR * 8, src.base[c] + r0 * src.esize[c],
+          bulk_g2s(tiles + ((size_t)s * NC + c) * TR * CB, src.base[c] + r0 * src.esize[c],
                    rows * src.esize[c], &full[s]);
       }
     }
@@ -147,7 +157,7 @@ __global__ void __launch_bounds__((NCW + 1) * 32)
     if (!dead && !mbar_wait(&full[s], ph, err)) dead = true;
     const uint64_t r0 = t * TR;
     const uint32_t rows = (uint32_t)umin64(TR, src.m_end - r0);
-    TileAcc<TR> acc{tiles + (size_t)s * NC * TR * 8, r0};
+    TileAcc<TR, CB> acc{tiles + (size_t)s * NC * TR * CB, r0};
     Op::step(st, p, op_smem, acc, rows, ctid, NCT);
     __syncwarp();
     if (lane == 0) mbar_arrive(&empty[s]);
