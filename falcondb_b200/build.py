@@ -23,6 +23,8 @@ NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 COMMON = ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC", "-I", str(ROOT / "include")]
+# Extra nvcc flags (e.g. -D overrides of launch-shape constants for tuning sweeps).
+COMMON += os.environ.get("FDB_NVCC_FLAGS", "").split()
 
 
 def _headers() -> list[Path]:

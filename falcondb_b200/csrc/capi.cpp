@@ -52,23 +52,26 @@ Ctx::~Ctx() {
   if (upload) cudaStreamDestroy(upload);
 }
 
+// Device memory comes from the device's stream-ordered pool (cudaMallocAsync on
+// the context stream, release threshold raised at open): allocating and freeing
+// per query costs no device synchronisation and reuses cached blocks.
 void* Ctx::dev_alloc(size_t bytes) {
   if (bytes == 0) bytes = 16;
   if (in_use.load() + bytes > budget)
     fail(FDB_E_OOM, "device memory budget exceeded: " + std::to_string(in_use.load() + bytes) + " > " +
                         std::to_string(budget) + " bytes");
   void* p = nullptr;
-  cudaError_t e = cudaMalloc(&p, bytes);
+  cudaError_t e = cudaMallocAsync(&p, bytes, stream);
   if (e != cudaSuccess) {
     cudaGetLastError();
-    fail(FDB_E_OOM, std::string("cudaMalloc failed: ") + cudaGetErrorString(e));
+    fail(FDB_E_OOM, std::string("cudaMallocAsync failed: ") + cudaGetErrorString(e));
   }
   in_use += bytes;
   return p;
 }
 void Ctx::dev_free(void* p, size_t bytes) {
   if (!p) return;
-  cudaFree(p);
+  cudaFreeAsync(p, stream);  // ordered after every operator already queued
   in_use -= bytes ? bytes : 16;
 }
 DevBuf Ctx::alloc_buf(size_t bytes) {
@@ -85,8 +88,7 @@ void Ctx::free_buf(DevBuf& b) {
 
 void Ctx::ensure_scratch(size_t bytes) {
   if (scratch.bytes >= bytes) return;
-  // Work already queued may use the old arena: drain the stream first.
-  FDB_CUDA(cudaStreamSynchronize(stream));
+  // The old arena is released in stream order (after the work that uses it).
   size_t want = std::max(bytes, scratch.bytes * 2);
   want = (want + (1u << 20) - 1) & ~size_t((1u << 20) - 1);
   if (scratch.ptr) free_buf(scratch);
@@ -188,10 +190,17 @@ int fdb_open(int device, uint64_t mem_budget_bytes, fdb_db** out) {
     c.budget = mem_budget_bytes ? (size_t)mem_budget_bytes : (size_t)(free_b * 0.9);
     FDB_CUDA(cudaStreamCreateWithFlags(&c.stream, cudaStreamNonBlocking));
     FDB_CUDA(cudaStreamCreateWithFlags(&c.upload, cudaStreamNonBlocking));
+    // Keep freed pool blocks cached in this process (the pool belongs to this
+    // process's context; nothing outlives it).
+    cudaMemPool_t pool;
+    FDB_CUDA(cudaDeviceGetDefaultMemPool(&pool, device));
+    uint64_t threshold = UINT64_MAX;
+    FDB_CUDA(cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &threshold));
     FDB_CUDA(cudaEventCreate(&c.ev0));
     FDB_CUDA(cudaEventCreate(&c.ev1));
     c.d_err = static_cast<int*>(c.dev_alloc(Ctx::kTicketBytes));
-    FDB_CUDA(cudaMemset(c.d_err, 0, Ctx::kTicketBytes));
+    FDB_CUDA(cudaMemsetAsync(c.d_err, 0, Ctx::kTicketBytes, c.stream));
+    FDB_CUDA(cudaStreamSynchronize(c.stream));
     c.d_ticket = reinterpret_cast<unsigned int*>(reinterpret_cast<char*>(c.d_err) + 64);
     c.ensure_scratch(default_scratch(c));
   });
@@ -277,19 +286,21 @@ int64_t fdb_table_from_columns(fdb_db* db, const char* name, const fdb_column* c
         col.name = hc.name;
         col.dtype = hc.dtype;
         const size_t vbytes = nrows * dtype_size(hc.dtype);
+        const size_t wbytes = ((nrows + 63) / 64) * 8;
         col.values = c.alloc_buf(vbytes);
+        if (hc.validity) col.validity = c.alloc_buf(wbytes);
+        // The buffers come from the pool in the context stream's order; the
+        // upload stream waits for that before copying into them.
+        FDB_CUDA(cudaEventCreateWithFlags(&col.ready, cudaEventDisableTiming));
+        FDB_CUDA(cudaEventRecord(col.ready, c.stream));
+        FDB_CUDA(cudaStreamWaitEvent(c.upload, col.ready, 0));
         if (vbytes) FDB_CUDA(cudaMemcpyAsync(col.values.ptr, hc.values, vbytes, cudaMemcpyHostToDevice, c.upload));
-        if (hc.validity) {
-          const size_t wbytes = ((nrows + 63) / 64) * 8;
-          col.validity = c.alloc_buf(wbytes);
-          if (wbytes)
-            FDB_CUDA(cudaMemcpyAsync(col.validity.ptr, hc.validity, wbytes, cudaMemcpyHostToDevice, c.upload));
-        }
+        if (hc.validity && wbytes)
+          FDB_CUDA(cudaMemcpyAsync(col.validity.ptr, hc.validity, wbytes, cudaMemcpyHostToDevice, c.upload));
         if (hc.dtype == FDB_UTF8) {
           need(hc.dict != nullptr || hc.dict_len == 0, "Utf8 column without a dictionary");
           for (uint32_t d = 0; d < hc.dict_len; ++d) col.dict.emplace_back(hc.dict[d] ? hc.dict[d] : "");
         }
-        FDB_CUDA(cudaEventCreateWithFlags(&col.ready, cudaEventDisableTiming));
         FDB_CUDA(cudaEventRecord(col.ready, c.upload));
         t->cols.push_back(std::move(col));
       }
@@ -503,9 +514,7 @@ int fdb_group_by_i64(fdb_db* db, const fdb_dev_column* key, const fdb_dev_column
     Ctx& c = db->ctx;
     double lf = (load_factor > 0.0 && load_factor < 1.0) ? load_factor : 0.5;
     uint64_t eg = expected_groups ? expected_groups : (nrows ? nrows : 1);
-    uint64_t cap = 1024;
-    while ((double)cap * lf < (double)eg) cap <<= 1;
-    const size_t need_b = cap * 40 + (16u << 20);
+    const size_t need_b = group_by_i64_scratch(eg, lf) + (16u << 20);
     CallScope s(db, std::max(default_scratch(c), need_b));
     op_group_by_i64(s.c, *key, *value, nrows, prog, nterms, pred_cols, npred_cols, expected_groups, lf,
                     d_groups, capacity, d_ngroups);

@@ -204,13 +204,40 @@ __device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity, int* e
   if (err) atomicExch(err, kErrTimeout);
   return false;
 }
-// 1-D bulk copy global -> shared through the TMA unit, completing on `bar`.
-// dst/src 16-byte aligned, bytes a multiple of 16.
-__device__ __forceinline__ void bulk_g2s(void* dst, const void* src, uint32_t bytes, uint64_t* bar) {
+// Bounded wait with back-off, for the single producer lane of a streaming
+// kernel: between polls the lane sleeps `ns` nanoseconds, so that while the
+// ring is full it does not take issue slots from the consumer warps of its
+// SM sub-partition.  Same limit and error reporting as mbar_wait (the bound is
+// kSpinLimit polls, i.e. at most kSpinLimit * ns of sleep plus the polls).
+__device__ __forceinline__ bool mbar_wait_backoff(uint64_t* bar, uint32_t parity, int* err, unsigned ns) {
+  for (uint32_t i = 0; i < kSpinLimit; ++i) {
+    if (mbar_try_wait(bar, parity)) return true;
+    __nanosleep(ns);
+  }
+  if (err) atomicExch(err, kErrTimeout);
+  return false;
+}
+// L2 policy for data that is streamed once: evict it first, so that it does
+// not push out what is reused (hash tables probed at random, partials).
+__device__ __forceinline__ uint64_t l2_evict_first_policy() {
+  uint64_t pol;
+  asm volatile("createpolicy.fractional.L2::evict_first.b64 %0, 1.0;" : "=l"(pol));
+  return pol;
+}
+// L2 policy for data that is reused at random (hash tables): evict it last.
+__device__ __forceinline__ uint64_t l2_evict_last_policy() {
+  uint64_t pol;
+  asm volatile("createpolicy.fractional.L2::evict_last.b64 %0, 1.0;" : "=l"(pol));
+  return pol;
+}
+// 1-D bulk copy global -> shared through the TMA unit, completing on `bar`,
+// with an L2 cache-hint policy.  dst/src 16-byte aligned, bytes a multiple of 16.
+__device__ __forceinline__ void bulk_g2s(void* dst, const void* src, uint32_t bytes, uint64_t* bar,
+                                         uint64_t policy) {
   asm volatile(
-      "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
-          smem_u32(dst)),
-      "l"(src), "r"(bytes), "r"(smem_u32(bar))
+      "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes.L2::cache_hint [%0], [%1], %2, [%3], "
+      "%4;" ::"r"(smem_u32(dst)),
+      "l"(src), "r"(bytes), "r"(smem_u32(bar)), "l"(policy)
       : "memory");
 }
 

@@ -135,6 +135,8 @@ void op_group_by_codes(Ctx& c, const fdb_dev_column* cols, int ncols, uint64_t n
                        const fdb_pred_term* prog, int nterms, int key_col, uint32_t dict_len,
                        const fdb_agg_spec* aggs, int naggs, fdb_agg_value* d_out,
                        int64_t* d_group_rows);
+// Scratch bytes op_group_by_i64 takes for `expected_groups` at `load_factor`.
+size_t group_by_i64_scratch(uint64_t expected_groups, double load_factor);
 void op_group_by_i64(Ctx& c, const fdb_dev_column& key, const fdb_dev_column& value, uint64_t n,
                      const fdb_pred_term* prog, int nterms, const fdb_dev_column* pred_cols,
                      int npred, uint64_t expected_groups, double load_factor,

@@ -81,6 +81,54 @@ struct GbGetter {
   }
 };
 
+// Row i of `acc`: false when it fails the WHERE program; otherwise its group
+// id (dictionary code; ngroups-1 for the NULL key) and the value each table
+// slot adds (slot 0: the row count).
+template <class Acc>
+__device__ __forceinline__ bool gb_row_values(const GbCodesParams& p, const Acc& acc, uint32_t i, uint32_t& gid,
+                                              uint64_t (&v)[kMaxSlots]) {
+#pragma unroll
+  for (int s = 0; s < kMaxSlots; ++s) v[s] = 0;
+  const uint64_t row = acc.row(i);
+  GbGetter<Acc> get{p.cols, acc, i, row};
+  if (!eval_prog(p.prog, get)) return false;
+  int64_t iv;
+  double fv;
+  uint32_t code;
+  bool valid;
+  get(p.key_col, iv, fv, code, valid);
+  gid = (!valid || code == kNullCode || code >= p.ngroups - 1) ? p.ngroups - 1 : code;
+  v[0] = 1;
+#pragma unroll
+  for (int a = 0; a < 4; ++a) {
+    if (a >= p.naggs) break;
+    const int f = p.func[a];
+    if (f == FDB_AGG_COUNT_STAR) continue;
+    const int dt = get(p.acol[a], iv, fv, code, valid);
+    if (!valid) continue;
+    if ((f == FDB_AGG_MIN || f == FDB_AGG_MAX) && dt == FDB_FLOAT64 && isnan(fv)) continue;
+    const int cs = p.cslot[a];
+    const int vs = p.vslot[a];
+#pragma unroll
+    for (int s = 1; s < kMaxSlots; ++s)
+      if (s == cs) v[s] = 1;
+    uint64_t x = 0;
+    if (f == FDB_AGG_SUM || f == FDB_AGG_AVG) {
+      x = dt == FDB_FLOAT64 ? (uint64_t)__double_as_longlong(fv) : (uint64_t)iv;
+    } else if (f == FDB_AGG_MIN) {
+      x = ~(dt == FDB_FLOAT64 ? f64_ord_key(fv) : i64_ord_key(iv));
+    } else if (f == FDB_AGG_MAX) {
+      x = dt == FDB_FLOAT64 ? f64_ord_key(fv) : i64_ord_key(iv);
+    }
+#pragma unroll
+    for (int s = 1; s < kMaxSlots; ++s)
+      if (s == vs) v[s] = x;
+  }
+  return true;
+}
+
+__device__ void gb_codes_merge(const GbCodesParams& p, uint64_t* tab, unsigned int* s_last, int ctid, int nct);
+
 struct GbCodesOp {
   using Params = GbCodesParams;
   struct Local {};
@@ -106,47 +154,10 @@ struct GbCodesOp {
       const uint32_t i = b + ctid;
       uint32_t gid = 0xFFFFFFFFu;
       uint64_t v[kMaxSlots];
+      if (!(i < rows && gb_row_values(p, acc, i, gid, v))) {
+        gid = 0xFFFFFFFFu;
 #pragma unroll
-      for (int s = 0; s < kMaxSlots; ++s) v[s] = 0;
-      if (i < rows) {
-        const uint64_t row = acc.row(i);
-        GbGetter<Acc> get{p.cols, acc, i, row};
-        if (eval_prog(p.prog, get)) {
-          int64_t iv;
-          double fv;
-          uint32_t code;
-          bool valid;
-          get(p.key_col, iv, fv, code, valid);
-          gid = (!valid || code == kNullCode || code >= p.ngroups - 1) ? p.ngroups - 1 : code;
-          v[0] = 1;
-#pragma unroll
-          for (int a = 0; a < 4; ++a) {
-            if (a >= p.naggs) break;
-            const int f = p.func[a];
-            if (f == FDB_AGG_COUNT_STAR) continue;
-            const int dt = get(p.acol[a], iv, fv, code, valid);
-            if (!valid) continue;
-            if (f == FDB_AGG_MIN || f == FDB_AGG_MAX) {
-              if (dt == FDB_FLOAT64 && isnan(fv)) continue;
-            }
-            const int cs = p.cslot[a];
-            const int vs = p.vslot[a];
-#pragma unroll
-            for (int s = 1; s < kMaxSlots; ++s)
-              if (s == cs) v[s] = 1;
-            uint64_t x = 0;
-            if (f == FDB_AGG_SUM || f == FDB_AGG_AVG) {
-              x = dt == FDB_FLOAT64 ? (uint64_t)__double_as_longlong(fv) : (uint64_t)iv;
-            } else if (f == FDB_AGG_MIN) {
-              x = ~(dt == FDB_FLOAT64 ? f64_ord_key(fv) : i64_ord_key(iv));
-            } else if (f == FDB_AGG_MAX) {
-              x = dt == FDB_FLOAT64 ? f64_ord_key(fv) : i64_ord_key(iv);
-            }
-#pragma unroll
-            for (int s = 1; s < kMaxSlots; ++s)
-              if (s == vs) v[s] = x;
-          }
-        }
+        for (int s = 0; s < kMaxSlots; ++s) v[s] = 0;
       }
       // Warp-level combine of the lanes that share a group.
       const unsigned peers = __match_any_sync(0xffffffffu, gid);
@@ -187,6 +198,16 @@ struct GbCodesOp {
       for (int w = 1; w < kNW; ++w) acc = slot_combine(kind, acc, tab[(size_t)w * kGbWarpTableEntries + e]);
       p.partials[(size_t)blockIdx.x * entries + e] = acc;
     }
+    gb_codes_merge(p, tab, s_last, ctid, nct);
+  }
+};
+
+// Publish this CTA's partial (already in p.partials) and, in the last CTA,
+// fold all partials in CTA order and write the per-group results.  `tab` is
+// shared memory of at least ngroups * nslots words.
+__device__ void gb_codes_merge(const GbCodesParams& p, uint64_t* tab, unsigned int* s_last, int ctid, int nct) {
+    const int ns = p.nslots;
+    const uint32_t entries = p.ngroups * ns;
     __threadfence();
     consumer_bar(nct);
     if (ctid == 0) {
@@ -196,8 +217,7 @@ struct GbCodesOp {
     consumer_bar(nct);
     if (*s_last == 0) return;
     __threadfence();
-    // Last CTA: fold CTA partials in CTA order, one thread per table entry,
-    // into warp 0's table (reused as the final table).
+    // Last CTA: fold CTA partials in CTA order, one thread per table entry.
     for (uint32_t e = ctid; e < entries; e += nct) {
       const int kind = p.kind[e % ns];
       uint64_t acc = __ldcg(&p.partials[e]);
@@ -236,6 +256,148 @@ struct GbCodesOp {
       }
     }
     if (ctid == 0) *p.ticket = 0u;
+}
+
+// Lane-private variant for small tables ((groups x slots) <= kLaneEntries):
+// every consumer thread owns one column of a shared-memory table laid out
+// [entry][thread], so a row updates its thread's own words — no atomics, no
+// warp combine, bank-conflict free (a warp's 32 threads touch 32 consecutive
+// 8-byte words whatever groups they hit).  Each thread folds its rows in row
+// order; the CTA then folds the 256 columns in thread order: FP64 sums are
+// repeatable for a given grid.
+constexpr int kLaneEntries = 48;
+
+struct GbLaneOp {
+  using Params = GbCodesParams;
+  struct Local {};
+
+  static __device__ void init(Local&, const Params& p, unsigned char* sm, int ctid, int nct) {
+    uint64_t* tab = reinterpret_cast<uint64_t*>(sm);
+    const uint32_t entries = p.ngroups * p.nslots;
+    for (uint32_t e = 0; e < entries; ++e) tab[(size_t)e * nct + ctid] = 0;  // every kind's identity is 0
+  }
+
+  // Column-at-a-time inside the tile: first the WHERE result and group id of
+  // this thread's (up to kR) rows, then one tight loop per aggregate whose
+  // (function, type) dispatch is decided once per tile, not per row.
+  static constexpr int kR = 8;
+
+  template <class Acc>
+  static __device__ void step(Local&, const Params& p, unsigned char* sm, const Acc& acc, uint32_t rows,
+                              int ctid, int nct) {
+    uint64_t* tab = reinterpret_cast<uint64_t*>(sm);
+    const int ns = p.nslots;
+    for (uint32_t b = 0; b < rows; b += kR * nct) {
+      uint32_t off[kR];  // table word offset of (group, slot 0) for this thread
+      uint32_t pm = 0;
+      // Phase 1: WHERE + group id.
+      const bool one_cmp = p.prog.n == 1 && p.prog.t[0].kind == FDB_TERM_CMP &&
+                           p.cols[p.prog.t[0].col].dtype == FDB_FLOAT64 && !p.cols[p.prog.t[0].col].validity;
+      const int pc = p.prog.t[0].col, pop = p.prog.t[0].op;
+      const double plit = p.prog.t[0].lit_type == FDB_FLOAT64 ? p.prog.t[0].lit_f : (double)p.prog.t[0].lit_i;
+      const DevCol& kc = p.cols[p.key_col];
+#pragma unroll
+      for (int j = 0; j < kR; ++j) {
+        const uint32_t i = b + j * nct + ctid;
+        off[j] = 0;
+        if (i >= rows) continue;
+        bool pass;
+        if (p.prog.n == 0) {
+          pass = true;
+        } else if (one_cmp) {
+          pass = cmp_op<double>(pop, acc.template get<double>(pc, i), plit);
+        } else {
+          GbGetter<Acc> get{p.cols, acc, i, acc.row(i)};
+          pass = eval_prog(p.prog, get);
+        }
+        if (!pass) continue;
+        const uint32_t code = acc.template get<uint32_t>(p.key_col, i);
+        const bool kvalid = !kc.validity || col_valid(kc, acc.row(i));
+        const uint32_t gid = (!kvalid || code >= p.ngroups - 1) ? p.ngroups - 1 : code;
+        off[j] = gid * ns * nct + ctid;
+        pm |= 1u << j;
+      }
+      if (pm == 0) continue;
+      // Phase 2: the row count (slot 0).
+#pragma unroll
+      for (int j = 0; j < kR; ++j)
+        if ((pm >> j) & 1u) tab[off[j]] += 1;
+      // Phase 3: one loop per aggregate.
+      for (int a = 0; a < p.naggs; ++a) {
+        const int f = p.func[a];
+        if (f == FDB_AGG_COUNT_STAR) continue;
+        const int c = p.acol[a];
+        const DevCol& col = p.cols[c];
+        const int dt = col.dtype;
+        const uint32_t cs = p.cslot[a] >= 0 ? (uint32_t)p.cslot[a] * nct : 0xFFFFFFFFu;
+        const uint32_t vs = p.vslot[a] >= 0 ? (uint32_t)p.vslot[a] * nct : 0u;
+        const bool sum = f == FDB_AGG_SUM || f == FDB_AGG_AVG;
+        if (sum && dt == FDB_FLOAT64 && !col.validity && cs == 0xFFFFFFFFu) {
+#pragma unroll
+          for (int j = 0; j < kR; ++j)
+            if ((pm >> j) & 1u) {
+              double* w = reinterpret_cast<double*>(tab + off[j] + vs);
+              *w += acc.template get<double>(c, b + j * nct + ctid);
+            }
+        } else if (sum && dt == FDB_INT64 && !col.validity && cs == 0xFFFFFFFFu) {
+#pragma unroll
+          for (int j = 0; j < kR; ++j)
+            if ((pm >> j) & 1u) tab[off[j] + vs] += (uint64_t)acc.template get<int64_t>(c, b + j * nct + ctid);
+        } else {
+          // General: validity, counts, MIN / MAX.
+#pragma unroll
+          for (int j = 0; j < kR; ++j) {
+            if (!((pm >> j) & 1u)) continue;
+            const uint32_t i = b + j * nct + ctid;
+            if (col.validity && !col_valid(col, acc.row(i))) continue;
+            uint64_t x = 0;
+            double fv = 0.0;
+            int64_t iv = 0;
+            if (dt == FDB_FLOAT64)
+              fv = acc.template get<double>(c, i);
+            else if (dt == FDB_INT64)
+              iv = acc.template get<int64_t>(c, i);
+            if ((f == FDB_AGG_MIN || f == FDB_AGG_MAX) && dt == FDB_FLOAT64 && isnan(fv)) continue;
+            if (cs != 0xFFFFFFFFu) tab[off[j] + cs] += 1;
+            if (f == FDB_AGG_COUNT) continue;
+            if (sum) {
+              if (dt == FDB_FLOAT64) {
+                double* w = reinterpret_cast<double*>(tab + off[j] + vs);
+                *w += fv;
+              } else {
+                tab[off[j] + vs] += (uint64_t)iv;
+              }
+              continue;
+            }
+            const uint64_t k = dt == FDB_FLOAT64 ? f64_ord_key(fv) : i64_ord_key(iv);
+            x = f == FDB_AGG_MIN ? ~k : k;
+            uint64_t& w = tab[off[j] + vs];
+            w = x > w ? x : w;
+          }
+        }
+      }
+    }
+  }
+
+  static __device__ void finish(Local&, const Params& p, unsigned char* sm, int ctid, int nct) {
+    uint64_t* tab = reinterpret_cast<uint64_t*>(sm);
+    const int ns = p.nslots;
+    const uint32_t entries = p.ngroups * ns;
+    unsigned int* s_last = reinterpret_cast<unsigned int*>(sm + (size_t)entries * nct * 8);
+    const int warp = ctid >> 5, lane = ctid & 31, nw = nct >> 5;
+    consumer_bar(nct);
+    // Fold each entry's thread columns: lanes read 32 consecutive words per
+    // step, then a fixed shuffle tree.
+    for (uint32_t e = warp; e < entries; e += nw) {
+      const int kind = p.kind[e % ns];
+      uint64_t a = tab[(size_t)e * nct + lane];
+      for (int j = lane + 32; j < nct; j += 32) a = slot_combine(kind, a, tab[(size_t)e * nct + j]);
+#pragma unroll
+      for (int o = 16; o > 0; o >>= 1) a = slot_combine(kind, a, __shfl_xor_sync(0xffffffffu, a, o));
+      if (lane == 0) p.partials[(size_t)blockIdx.x * entries + e] = a;
+    }
+    consumer_bar(nct);
+    gb_codes_merge(p, tab, s_last, ctid, nct);
   }
 };
 
@@ -251,7 +413,10 @@ struct GSlot {          // 40 bytes; all-zero = empty
 };
 
 constexpr uint32_t kSmemSlots = 1024;      // CTA table slots (power of two)
-constexpr uint32_t kSmemProbe = 16;        // probes before a row spills to global
+#ifndef FDB_GB_SMEM_PROBE
+#define FDB_GB_SMEM_PROBE 4
+#endif
+constexpr uint32_t kSmemProbe = FDB_GB_SMEM_PROBE;  // probes before a row spills to global
 constexpr uint32_t kGlobalProbeLimit = 1u << 16;
 
 struct GbHashParams {
@@ -503,8 +668,14 @@ void op_group_by_codes(Ctx& c, const fdb_dev_column* cols, int ncols, uint64_t n
     if (aggs[a].col < 0 || aggs[a].col >= ncols) fail(FDB_E_ARG, "aggregate column out of range");
     const int dt = cols[aggs[a].col].dtype;
     if (f != FDB_AGG_COUNT && dt == FDB_UTF8) fail(FDB_E_TYPE, "SUM/AVG/MIN/MAX need a numeric column");
-    p.cslot[a] = ns;
-    p.kind[ns++] = kAddU64;
+    // A value count equals the group's row count when the column has no NULLs
+    // (and, for MIN/MAX, no NaN to skip: integers), so it needs no slot.
+    const bool own_count = cols[aggs[a].col].validity != nullptr || f == FDB_AGG_COUNT ||
+                           ((f == FDB_AGG_MIN || f == FDB_AGG_MAX) && dt == FDB_FLOAT64);
+    if (own_count) {
+      p.cslot[a] = ns;
+      p.kind[ns++] = kAddU64;
+    }
     if (f == FDB_AGG_COUNT) continue;
     p.vslot[a] = ns;
     p.kind[ns++] = (f == FDB_AGG_SUM || f == FDB_AGG_AVG) ? (dt == FDB_FLOAT64 ? kAddF64 : kAddU64)
@@ -518,12 +689,35 @@ void op_group_by_codes(Ctx& c, const fdb_dev_column* cols, int ncols, uint64_t n
   p.ticket = c.d_ticket;
   p.out = d_out;
   p.group_rows = d_group_rows;
+  if ((uint64_t)p.ngroups * ns <= kLaneEntries) {
+    // Lane-private tables: 4 consumer warps per CTA, 512-row tiles.
+    const size_t sm = (size_t)p.ngroups * ns * 128 * 8 + 16;
+    switch (ncols) {
+      case 1: launch_stream_gb<GbLaneOp, 1, 2048, 3, 4>(c, cols, n, p, sm); break;
+      case 2: launch_stream_gb<GbLaneOp, 2, 1024, 3, 4>(c, cols, n, p, sm); break;
+      case 3: launch_stream_gb<GbLaneOp, 3, 1024, 3, 4>(c, cols, n, p, sm); break;
+      default: launch_stream_gb<GbLaneOp, 4, 1024, 2, 4>(c, cols, n, p, sm); break;
+    }
+    return;
+  }
   switch (ncols) {
     case 1: launch_stream_gb<GbCodesOp, 1, 2048, 4, 8>(c, cols, n, p, GbCodesOp::kSmem); break;
     case 2: launch_stream_gb<GbCodesOp, 2, 1024, 4, 8>(c, cols, n, p, GbCodesOp::kSmem); break;
     case 3: launch_stream_gb<GbCodesOp, 3, 1024, 3, 8>(c, cols, n, p, GbCodesOp::kSmem); break;
     default: launch_stream_gb<GbCodesOp, 4, 1024, 3, 8>(c, cols, n, p, GbCodesOp::kSmem); break;
   }
+}
+
+static uint64_t gb_table_capacity(uint64_t expected_groups, double load_factor) {
+  uint64_t cap = 1024;
+  while ((double)cap * load_factor < (double)expected_groups) cap <<= 1;
+  return cap;
+}
+
+size_t group_by_i64_scratch(uint64_t expected_groups, double load_factor) {
+  if (load_factor <= 0.0 || load_factor >= 1.0) load_factor = 0.5;
+  const uint64_t cap = gb_table_capacity(expected_groups ? expected_groups : 1, load_factor);
+  return (cap + 1) * sizeof(GSlot) + 2 * 256;  // each scratch_take rounds up to 256 bytes
 }
 
 void op_group_by_i64(Ctx& c, const fdb_dev_column& key, const fdb_dev_column& value, uint64_t n,
@@ -536,8 +730,7 @@ void op_group_by_i64(Ctx& c, const fdb_dev_column& key, const fdb_dev_column& va
   if (npred < 0 || npred > 2) fail(FDB_E_ARG, "at most 2 predicate columns");
   if (load_factor <= 0.0 || load_factor >= 1.0) load_factor = 0.5;
   if (expected_groups == 0) expected_groups = n ? n : 1;
-  uint64_t cap = 1024;
-  while ((double)cap * load_factor < (double)expected_groups) cap <<= 1;
+  const uint64_t cap = gb_table_capacity(expected_groups, load_factor);
   const size_t tbytes = cap * sizeof(GSlot);
   GSlot* table = static_cast<GSlot*>(c.scratch_take(tbytes + sizeof(GSlot)));
   GSlot* null_slot = table + cap;

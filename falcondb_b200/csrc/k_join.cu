@@ -300,6 +300,21 @@ struct ProbeParams {
   fdb_join_agg* out;
 };
 
+// Probe launch shape: rows in flight per thread, ring stages, tile rows (one
+// column), and resident CTAs per SM the register budget is sized for.
+#ifndef FDB_PROBE_PR
+#define FDB_PROBE_PR 1
+#endif
+#ifndef FDB_PROBE_STAGES
+#define FDB_PROBE_STAGES 2
+#endif
+#ifndef FDB_PROBE_TR
+#define FDB_PROBE_TR 2048
+#endif
+#ifndef FDB_PROBE_MINB
+#define FDB_PROBE_MINB 4
+#endif
+
 struct ProbeOp {
   using Params = ProbeParams;
   struct Local {
@@ -314,22 +329,91 @@ struct ProbeOp {
     st.a.vsum = 0.0;
   }
 
+  // Software-pipelined probe: each thread advances kPR rows together.  Every
+  // round issues one 32-byte load per unfinished row — the aligned pair of
+  // slots holding its current probe position — so up to kPR independent L2
+  // reads are in flight per thread, and a pair resolves two probe steps.
+  static constexpr int kPR = FDB_PROBE_PR;
+
+  // Both slots of an aligned pair (32 bytes, one L2 sector) in one 256-bit load.
+  static __device__ __forceinline__ void load_pair(const JSlot* pair, uint64_t pol, JSlot& a, JSlot& b) {
+    asm volatile("ld.global.L2::cache_hint.v4.u64 {%0, %1, %2, %3}, [%4], %5;"
+                 : "=l"(a.key), "=l"(a.psum), "=l"(b.key), "=l"(b.psum)
+                 : "l"(pair), "l"(pol));
+  }
+
   template <class Acc>
-  static __device__ __forceinline__ void one_row(Local& st, const Params& p, const Acc& acc, uint32_t i) {
-    const uint64_t row = acc.row(i);
-    const int64_t k = acc.template get<int64_t>(0, i);
-    const bool kvalid = p.key.validity ? col_valid(p.key, row) : true;
-    unsigned long long matches = 0, prows = 0;
-    long long psum = 0;
-    if (kvalid) {
-      JSlot s;
-      const uint32_t at = join_find(p.slots, p.cnt, p.cap, k, &s);
-      if (at != kNoSlot) {
-        matches = p.unique ? 1ull : (unsigned long long)p.cnt[at];
-        psum = (long long)s.psum;
-        prows = p.payload_nulls ? (unsigned long long)p.pcnt[at] : matches;
+  static __device__ void step(Local& st, const Params& p, unsigned char*, const Acc& acc, uint32_t rows,
+                              int ctid, int nct) {
+    const uint64_t mask = p.cap - 1;
+    const uint64_t pol = l2_evict_last_policy();  // keep the table resident against the streamed keys
+    for (uint32_t b = 0; b < rows; b += kPR * nct) {
+      uint64_t sk[kPR], h[kPR], ps[kPR];
+      uint32_t at[kPR];
+      uint32_t todo = 0, live = 0;
+#pragma unroll
+      for (int j = 0; j < kPR; ++j) {
+        const uint32_t i = b + j * nct + ctid;
+        at[j] = kNoSlot;
+        sk[j] = 0;
+        h[j] = 0;
+        ps[j] = 0;
+        if (i >= rows) continue;
+        live |= 1u << j;
+        if (p.key.validity && !col_valid(p.key, acc.row(i))) continue;  // NULL key: no match
+        const int64_t k = acc.template get<int64_t>(0, i);
+        if (k == INT64_MIN) {
+          if (p.cnt[p.cap] != 0u) {
+            at[j] = (uint32_t)p.cap;
+            ps[j] = p.slots[p.cap].psum;
+          }
+          continue;
+        }
+        sk[j] = (unsigned long long)k ^ (1ull << 63);
+        h[j] = mix64(sk[j]) & mask;
+        todo |= 1u << j;
+      }
+      for (uint32_t round = 0; todo && round <= mask; ++round) {
+        JSlot s0[kPR], s1[kPR];
+#pragma unroll
+        for (int j = 0; j < kPR; ++j) {
+          if ((todo >> j) & 1u) load_pair(p.slots + (h[j] & ~1ull), pol, s0[j], s1[j]);
+        }
+#pragma unroll
+        for (int j = 0; j < kPR; ++j) {
+          if (!((todo >> j) & 1u)) continue;
+          const bool odd = h[j] & 1ull;
+          const uint64_t base = h[j] & ~1ull;
+          // Slots in probe order: the pair's second slot only when h is odd.
+          if (!odd) {
+            if (s0[j].key == sk[j]) { at[j] = (uint32_t)base; ps[j] = s0[j].psum; todo &= ~(1u << j); continue; }
+            if (s0[j].key == 0ull) { todo &= ~(1u << j); continue; }
+          }
+          if (s1[j].key == sk[j]) { at[j] = (uint32_t)(base + 1); ps[j] = s1[j].psum; todo &= ~(1u << j); continue; }
+          if (s1[j].key == 0ull) { todo &= ~(1u << j); continue; }
+          h[j] = (base + 2) & mask;
+        }
+      }
+#pragma unroll
+      for (int j = 0; j < kPR; ++j) {
+        if (!((live >> j) & 1u)) continue;
+        const uint32_t i = b + j * nct + ctid;
+        unsigned long long matches = 0, prows = 0;
+        long long psum = 0;
+        if (at[j] != kNoSlot) {
+          matches = p.unique ? 1ull : (unsigned long long)p.cnt[at[j]];
+          psum = (long long)ps[j];
+          prows = p.payload_nulls ? (unsigned long long)p.pcnt[at[j]] : matches;
+        }
+        accumulate(st, p, acc, i, matches, psum, prows);
       }
     }
+  }
+
+  template <class Acc>
+  static __device__ __forceinline__ void accumulate(Local& st, const Params& p, const Acc& acc, uint32_t i,
+                                                    unsigned long long matches, long long psum,
+                                                    unsigned long long prows) {
     switch (p.join_type) {
       case FDB_JOIN_INNER:
         st.a.count += matches;
@@ -346,7 +430,7 @@ struct ProbeOp {
         if (keep) {
           st.a.count += 1;
           if (p.has_value) {
-            const bool vv = p.value.validity ? col_valid(p.value, row) : true;
+            const bool vv = p.value.validity ? col_valid(p.value, acc.row(i)) : true;
             if (vv) {
               st.a.vsum += acc.template get<double>(1, i);
               st.a.prows += 1;
@@ -355,17 +439,6 @@ struct ProbeOp {
         }
       }
     }
-  }
-
-  template <class Acc>
-  static __device__ void step(Local& st, const Params& p, unsigned char*, const Acc& acc, uint32_t rows,
-                              int ctid, int nct) {
-    uint32_t i = ctid;
-    for (; i + nct < rows; i += 2 * nct) {
-      one_row(st, p, acc, i);
-      one_row(st, p, acc, i + nct);
-    }
-    for (; i < rows; i += nct) one_row(st, p, acc, i);
   }
 
   static __device__ JoinAggAcc warp_red(JoinAggAcc a) {
@@ -435,9 +508,11 @@ struct ProbeOp {
   }
 };
 
+constexpr int kProbeMaxPerSm = 8;  // partials are sized for this many CTAs per SM
+
 template <int NC>
 static void launch_probe(Ctx& c, const fdb_dev_column* cols, uint64_t n, const ProbeParams& p) {
-  constexpr int TR = NC == 1 ? 2048 : 1024, STAGES = 4, NCW = 8;
+  constexpr int TR = NC == 1 ? FDB_PROBE_TR : FDB_PROBE_TR / 2, STAGES = FDB_PROBE_STAGES, NCW = 8;
   StreamSrc<NC> src;
   const void* bases[NC];
   for (int i = 0; i < NC; ++i) {
@@ -449,7 +524,7 @@ static void launch_probe(Ctx& c, const fdb_dev_column* cols, uint64_t n, const P
   src.m_end = stream_m_end(bases, NC, n);
   const int op_off = (int)stream_smem_bytes<NC, TR, STAGES>();
   const size_t smem = op_off + ProbeOp::kSmem;
-  auto kern = stream_kernel<ProbeOp, NC, TR, STAGES, NCW>;
+  auto kern = stream_kernel<ProbeOp, NC, TR, STAGES, NCW, 8, FDB_PROBE_MINB>;
   static bool attr = false;
   if (!attr) {
     FDB_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024));
@@ -458,7 +533,7 @@ static void launch_probe(Ctx& c, const fdb_dev_column* cols, uint64_t n, const P
   int per_sm = 0;
   FDB_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, (NCW + 1) * 32, smem));
   if (per_sm < 1) per_sm = 1;
-  if (per_sm > 4) per_sm = 4;
+  if (per_sm > kProbeMaxPerSm) per_sm = kProbeMaxPerSm;
   const uint64_t ntiles = (src.m_end + TR - 1) / TR;
   uint64_t want = ntiles ? ntiles : (n + NCW * 32 * 8 - 1) / (NCW * 32 * 8);
   if (want < 1) want = 1;
@@ -485,7 +560,7 @@ void op_join_probe_agg(Ctx& c, const HashTable& h, const fdb_dev_column& key, co
   p.payload_nulls = h.payload_nulls ? 1 : 0;
   p.join_type = join_type;
   p.has_value = (has_value && (join_type == FDB_JOIN_SEMI || join_type == FDB_JOIN_ANTI)) ? 1 : 0;
-  p.partials = static_cast<JoinAggAcc*>(c.scratch_take(sizeof(JoinAggAcc) * c.sm_count * 4));
+  p.partials = static_cast<JoinAggAcc*>(c.scratch_take(sizeof(JoinAggAcc) * c.sm_count * kProbeMaxPerSm));
   p.ticket = c.d_ticket;
   p.out = d_out;
   if (n == 0) {

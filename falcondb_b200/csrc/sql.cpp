@@ -1008,10 +1008,8 @@ static void run_aggregates(Plan& plan, const Rel& rel, const Query& q, fdb_resul
       const uint64_t cap = rel.nrows + 1;
       fdb_group_i64* d = plan.dev<fdb_group_i64>(cap);
       uint64_t* dn = plan.dev<uint64_t>(1);
-      uint64_t tcap = 1024;
-      while ((double)tcap * 0.5 < (double)rel.nrows) tcap <<= 1;
       plan.c.scratch_reset();
-      plan.c.ensure_scratch(tcap * 40 + (16u << 20));
+      plan.c.ensure_scratch(group_by_i64_scratch(rel.nrows, 0.5) + (16u << 20));
       op_group_by_i64(plan.c, col.dev, col.dev, rel.nrows, prog.data(), (int)prog.size(), pcols.data(),
                       (int)pcols.size(), rel.nrows, 0.5, d, cap, dn);
       plan.check();
@@ -1157,9 +1155,7 @@ static void run_group_by(Plan& plan, const Rel& rel, const Query& q, fdb_result*
     uint64_t* dn = plan.dev<uint64_t>(1);
     std::vector<fdb_group_i64> groups;
     if (rel.nrows > 0) {
-      uint64_t tcap = 1024;
-      while ((double)tcap * 0.5 < (double)rel.nrows) tcap <<= 1;
-      plan.c.ensure_scratch(tcap * 40 + (16u << 20));
+      plan.c.ensure_scratch(group_by_i64_scratch(rel.nrows, 0.5) + (16u << 20));
       op_group_by_i64(plan.c, key.dev, rel.cols[vc].dev, rel.nrows, prog.data(), (int)prog.size(), pcols.data(),
                       (int)pcols.size(), rel.nrows, 0.5, d, cap, dn);
       plan.check();

@@ -92,8 +92,9 @@ inline uint64_t stream_m_end(const void* const* bases, int nc, uint64_t n) {
 //   static __device__ void finish(Local&, const Params&, unsigned char* op_smem, int ctid, int nct);
 // step() and finish() are executed by all consumer threads; block-wide syncs
 // inside them must use consumer_bar(nct).
-template <class Op, int NC, int TR, int STAGES, int NCW, int CB = 8>
-__global__ void __launch_bounds__((NCW + 1) * 32)
+// MINB: resident CTAs per SM the register allocation must allow.
+template <class Op, int NC, int TR, int STAGES, int NCW, int CB = 8, int MINB = 1>
+__global__ void __launch_bounds__((NCW + 1) * 32, MINB)
     stream_kernel(StreamSrc<NC> src, typename Op::Params p, int* err, int op_smem_off) {
   extern __shared__ __align__(128) unsigned char smem[];
   uint64_t* full = reinterpret_cast<uint64_t*>(smem);
@@ -117,11 +118,12 @@ __global__ void __launch_bounds__((NCW + 1) * 32)
   if (warp == NCW) {
     // ---------------- producer warp ----------------
     if (lane == 0) {
+      const uint64_t policy = l2_evict_first_policy();  // columns are read once
       uint32_t it = 0;
       for (uint64_t t = blockIdx.x; t < ntiles; t += gridDim.x, ++it) {
         const int s = it % STAGES;
         const uint32_t ph = (it / STAGES) & 1u;
-        if (it >= STAGES && !mbar_wait(&empty[s], ph ^ 1u, err)) break;
+        if (it >= STAGES && !mbar_wait_backoff(&empty[s], ph ^ 1u, err, 64)) break;
         const uint64_t r0 = t * TR;
         const uint32_t rows = (uint32_t)umin64(TR, src.m_end - r0);
         uint32_t bytes = 0;
@@ -131,7 +133,7 @@ __global__ void __launch_bounds__((NCW + 1) * 32)
 #pragma unroll
         for (int c = 0; c < NC; ++c)
           bulk_g2s(tiles + ((size_t)s * NC + c) * TR * CB, src.base[c] + r0 * src.esize[c],
-                   rows * src.esize[c], &full[s]);
+                   rows * src.esize[c], &full[s], policy);
       }
     }
     return;  // consumers sync among themselves with named barrier 1
