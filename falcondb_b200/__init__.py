@@ -124,6 +124,9 @@ _SIGS = {
     "fdb_aggregate": (C.c_int, [C.c_void_p, C.POINTER(fdb_dev_column), C.c_int32, C.c_uint64,
                                 C.POINTER(fdb_pred_term), C.c_int32, C.POINTER(fdb_agg_spec), C.c_int32,
                                 C.c_void_p]),
+    "fdb_aggregate_noalloc": (C.c_int, [C.c_void_p, C.POINTER(fdb_dev_column), C.c_int32, C.c_uint64,
+                                        C.POINTER(fdb_pred_term), C.c_int32, C.POINTER(fdb_agg_spec), C.c_int32,
+                                        C.c_void_p]),
     "fdb_distinct_codes": (C.c_int, [C.c_void_p, C.POINTER(fdb_dev_column), C.c_int32, C.c_uint64,
                                      C.POINTER(fdb_pred_term), C.c_int32, C.c_int32, C.c_uint32, C.c_void_p]),
     "fdb_group_by_codes": (C.c_int, [C.c_void_p, C.POINTER(fdb_dev_column), C.c_int32, C.c_uint64,

@@ -480,6 +480,19 @@ int fdb_aggregate(fdb_db* db, const fdb_dev_column* cols, int32_t ncols, uint64_
   });
 }
 
+int fdb_aggregate_noalloc(fdb_db* db, const fdb_dev_column* cols, int32_t ncols, uint64_t nrows,
+                          const fdb_pred_term* prog, int32_t nterms, const fdb_agg_spec* aggs, int32_t naggs,
+                          fdb_agg_value* d_out) {
+  if (!db || !cols || !aggs || !d_out || (nterms && !prog))
+    return set_error(FDB_E_ARG, "fdb_aggregate_noalloc: bad arguments");
+  return guarded([&] {
+    // No CallScope: it resets and may grow the scratch arena.
+    std::lock_guard<std::recursive_mutex> lk(db->ctx.mu);
+    FDB_CUDA(cudaSetDevice(db->ctx.device));
+    op_aggregate_noalloc(db->ctx, cols, ncols, nrows, prog, nterms, aggs, naggs, d_out);
+  });
+}
+
 int fdb_distinct_codes(fdb_db* db, const fdb_dev_column* cols, int32_t ncols, uint64_t nrows,
                        const fdb_pred_term* prog, int32_t nterms, int32_t code_col, uint32_t dict_len,
                        uint64_t* d_bitmap) {

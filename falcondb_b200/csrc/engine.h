@@ -128,6 +128,11 @@ void op_gather_opt(Ctx& c, const fdb_dev_column& col, const uint32_t* d_rows, ui
 void op_aggregate(Ctx& c, const fdb_dev_column* cols, int ncols, uint64_t n,
                   const fdb_pred_term* prog, int nterms, const fdb_agg_spec* aggs, int naggs,
                   fdb_agg_value* d_out);
+// op_aggregate's interpreted scan with its partials and ticket in a fixed
+// device array instead of the scratch arena: allocates nothing.
+void op_aggregate_noalloc(Ctx& c, const fdb_dev_column* cols, int ncols, uint64_t n,
+                          const fdb_pred_term* prog, int nterms, const fdb_agg_spec* aggs, int naggs,
+                          fdb_agg_value* d_out);
 void op_distinct_codes(Ctx& c, const fdb_dev_column* cols, int ncols, uint64_t n,
                        const fdb_pred_term* prog, int nterms, int code_col, uint32_t dict_len,
                        uint64_t* d_bitmap);

@@ -8,6 +8,8 @@
 //   present_codes (COUNT DISTINCT over a dictionary) ...... query/aggregate.rs:3167-3200
 //   gather_by_bitmask / filter_by_bitmask_cols ............ storage/column.rs:1077-1123, table.rs:148-189
 #include <cstring>
+#include <mutex>
+#include <string>
 
 #include "common.cuh"
 #include "engine.h"
@@ -597,6 +599,73 @@ void op_aggregate(Ctx& c, const fdb_dev_column* cols, int ncols, uint64_t n,
       launch_stream<ColAggOp<int64_t>, 1>(c, cols, n, p, ScanAggOp::kSmem);
     return;
   }
+  launch_stream_nc<ScanAggOp>(c, cols, ncols, n, p, ScanAggOp::kSmem);
+}
+
+// ---------------------------------------------------------------------------
+// Aggregate scan that allocates nothing: its per-CTA partials and its ticket
+// live in a fixed module-scope device array instead of the context's scratch
+// arena (which may grow, i.e. allocate, on any call).  The array's device
+// address is looked up once per device with cudaGetSymbolAddress, by the first
+// call made on that device.  All calls on one device share the array, so two
+// calls whose kernels overlap in time race on it.
+// ---------------------------------------------------------------------------
+constexpr size_t kNoAllocScratchBytes = 128 * 1024;  // ticket (256 B) + partials
+constexpr int kNoAllocMaxDevices = 64;
+
+static __device__ __align__(256) unsigned char g_noalloc_scratch[kNoAllocScratchBytes];
+
+static std::mutex g_noalloc_mu;
+static void* g_noalloc_ptr[kNoAllocMaxDevices];
+
+// Device address of g_noalloc_scratch on the current device (c.device).
+static unsigned char* noalloc_scratch(Ctx& c) {
+  if (c.device < 0 || c.device >= kNoAllocMaxDevices) fail(FDB_E_ARG, "device ordinal out of range");
+  std::lock_guard<std::mutex> lk(g_noalloc_mu);
+  if (g_noalloc_ptr[c.device] == nullptr) {
+    void* ptr = nullptr;
+    const cudaError_t e = cudaGetSymbolAddress(&ptr, g_noalloc_scratch);
+    if (e != cudaSuccess || ptr == nullptr)
+      fail(FDB_E_CUDA, std::string("cudaGetSymbolAddress of the fixed aggregate scratch failed: ") +
+                           cudaGetErrorString(e));
+    g_noalloc_ptr[c.device] = ptr;
+  }
+  return static_cast<unsigned char*>(g_noalloc_ptr[c.device]);
+}
+
+void op_aggregate_noalloc(Ctx& c, const fdb_dev_column* cols, int ncols, uint64_t n,
+                          const fdb_pred_term* prog, int nterms, const fdb_agg_spec* aggs, int naggs,
+                          fdb_agg_value* d_out) {
+  if (naggs < 1 || naggs > 4) fail(FDB_E_ARG, "between 1 and 4 aggregates per scan");
+  const size_t need = 256 + sizeof(AggAcc) * 4 * (size_t)max_stream_grid(c);
+  if (need > kNoAllocScratchBytes)
+    fail(FDB_E_CAPACITY, "fdb_aggregate_noalloc: this device needs " + std::to_string(need) +
+                             " bytes of partials, above the fixed " + std::to_string(kNoAllocScratchBytes));
+  ScanAggParams p;
+  std::memset(&p, 0, sizeof(p));
+  fill_cols(p.sc, cols, ncols, n);
+  fill_prog(p.prog, prog, nterms, ncols);
+  p.naggs = naggs;
+  for (int a = 0; a < naggs; ++a) {
+    const int f = aggs[a].func;
+    if (f < FDB_AGG_COUNT_STAR || f > FDB_AGG_MAX)
+      fail(FDB_E_ARG, "aggregate not supported by fdb_aggregate_noalloc");
+    if (f != FDB_AGG_COUNT_STAR) {
+      if (aggs[a].col < 0 || aggs[a].col >= ncols) fail(FDB_E_ARG, "aggregate column out of range");
+      if (f != FDB_AGG_COUNT && cols[aggs[a].col].dtype == FDB_UTF8)
+        fail(FDB_E_TYPE, "SUM/AVG/MIN/MAX need a numeric column");
+    }
+    p.func[a] = f;
+    p.acol[a] = aggs[a].col;
+  }
+  unsigned char* scratch = noalloc_scratch(c);
+  p.ticket = reinterpret_cast<unsigned int*>(scratch);
+  p.partials = reinterpret_cast<AggAcc*>(scratch + 256);
+  p.out = d_out;
+  p.out_count = nullptr;
+  // The ticket must start at zero (the last CTA resets it, but a launch that
+  // timed out may have left it set).  The partials are written before read.
+  FDB_CUDA(cudaMemsetAsync(p.ticket, 0, sizeof(unsigned int), c.stream));
   launch_stream_nc<ScanAggOp>(c, cols, ncols, n, p, ScanAggOp::kSmem);
 }
 

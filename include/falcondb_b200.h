@@ -271,6 +271,22 @@ int fdb_aggregate(fdb_db* db, const fdb_dev_column* cols, int32_t ncols,
                   uint64_t nrows, const fdb_pred_term* prog, int32_t nterms,
                   const fdb_agg_spec* aggs, int32_t naggs, fdb_agg_value* d_out);
 
+/* fdb_aggregate for callers that must not allocate device memory.  No
+ * counterpart in the reference: FalconDB's CPU aggregates allocate freely.
+ * Same arguments, semantics and results as fdb_aggregate (always through its
+ * general interpreted kernel), but the per-CTA partials and the completion
+ * ticket live in a fixed 128 KB module-scope device array rather than in the
+ * context's scratch arena, and the call makes no cudaMalloc / cudaFree /
+ * pool allocation.  Returns FDB_E_CAPACITY if the device's SM count needs
+ * more partials than the array holds.  The first call on each device looks the
+ * array's address up (cudaGetSymbolAddress); make that first call before any
+ * stream capture.  Every call on one device uses the same array: calls whose
+ * kernels can overlap in time (other streams, other contexts on the device,
+ * other threads) race and must be serialised by the caller. */
+int fdb_aggregate_noalloc(fdb_db* db, const fdb_dev_column* cols, int32_t ncols,
+                          uint64_t nrows, const fdb_pred_term* prog, int32_t nterms,
+                          const fdb_agg_spec* aggs, int32_t naggs, fdb_agg_value* d_out);
+
 /* Presence bitmap of the dictionary codes that occur among rows passing `prog`
  * (present_codes, aggregate.rs:3167-3200): d_bitmap holds ceil(dict_len/64)
  * words.  COUNT(DISTINCT) is the number of distinct strings whose code is set. */
