@@ -17,6 +17,7 @@
 //     CTA writes its k best; the last CTA to finish merges them the same way.
 // On random data T0 admits about k*kSampleStride rows in total; on an ascending
 // column read DESC (the reference's slow case, FINDINGS.md) it admits the same.
+#include <algorithm>
 #include <cstring>
 
 #include "common.cuh"
@@ -642,6 +643,13 @@ __global__ void __launch_bounds__(256) wt_sample_kernel(TopkParams p, uint64_t n
 // CTA merges the partials that are <= the final global bound.
 // ===========================================================================
 constexpr uint32_t kRegMaxK = 32;
+constexpr uint64_t kRegSamples = 32768;  // sample budget of the register top-k's bound
+// Tiles between exchanges of a CTA's bound with the global one (0: never
+// during the scan; the CTAs' final bounds still meet in gbound).
+#ifndef FDB_TOPK_GLOBAL_EVERY
+#define FDB_TOPK_GLOBAL_EVERY 0
+#endif
+constexpr uint32_t kRtGlobalEvery = FDB_TOPK_GLOBAL_EVERY;
 
 struct RTParams {
   DevCol col;
@@ -687,11 +695,84 @@ __device__ __forceinline__ void rt_insert(RTLocal& s, uint32_t k, uint64_t ck, u
   }
 }
 
+// One compare-exchange of a bitonic network across lanes: this lane keeps the
+// smaller (key,row) of itself and lane ^ stride when keep_min, else the larger.
+__device__ __forceinline__ void rt_cx(uint64_t& k, uint32_t& r, int stride, bool keep_min) {
+  const uint64_t ok = __shfl_xor_sync(0xffffffffu, k, stride);
+  const uint32_t orow = __shfl_xor_sync(0xffffffffu, r, stride);
+  if (keep_min == kr_gt(k, r, ok, orow)) {
+    k = ok;
+    r = orow;
+  }
+}
+
+// Merge a sorted list held across the warp (lane i: i-th smallest, sentinel
+// ~0 past its end) into the warp list: the k best of the two are
+// min(list[i], other[31-i]), put in order by a bitonic merge.
+__device__ __forceinline__ void rt_merge_sorted(RTLocal& s, uint32_t k, uint64_t ok, uint32_t orow, int lane) {
+  const uint64_t rk = __shfl_sync(0xffffffffu, ok, 31 - lane);
+  const uint32_t rr = __shfl_sync(0xffffffffu, orow, 31 - lane);
+  uint64_t lk = (uint32_t)lane < k ? s.lk : ~0ull;
+  uint32_t lr = (uint32_t)lane < k ? s.lr : 0xFFFFFFFFu;
+  if (kr_gt(lk, lr, rk, rr)) {
+    lk = rk;
+    lr = rr;
+  }
+#pragma unroll
+  for (int stride = 16; stride > 0; stride >>= 1) rt_cx(lk, lr, stride, (lane & stride) == 0);
+  s.lk = lk;
+  s.lr = lr;
+  const uint64_t kk = __shfl_sync(0xffffffffu, lk, k - 1);
+  const uint32_t kr = __shfl_sync(0xffffffffu, lr, k - 1);
+  if (!(kk == ~0ull && kr == 0xFFFFFFFFu) && kr_le(kk, kr, s.tk, s.tr)) {
+    s.tk = kk;
+    s.tr = kr;
+  }
+}
+
+// Batched insertion: one candidate per lane (sentinel ~0 where none) is
+// bitonic-sorted across the warp, then merged with the list.  ~20 exchange
+// steps for 32 candidates, against one ballot/shuffle round per candidate in
+// rt_insert; used when many lanes hold candidates at once (rows in key order,
+// e.g. ORDER BY id DESC over ascending ids).
+__device__ __forceinline__ void rt_insert32(RTLocal& s, uint32_t k, uint64_t ck, uint32_t cr, int lane) {
+#pragma unroll
+  for (int size = 2; size <= 32; size <<= 1) {
+    const bool up = (lane & size) == 0 || size == 32;
+#pragma unroll
+    for (int stride = size >> 1; stride > 0; stride >>= 1) rt_cx(ck, cr, stride, ((lane & stride) == 0) == up);
+  }
+  rt_merge_sorted(s, k, ck, cr, lane);
+}
+
+constexpr int kRtBulkLanes = 8;  // lanes with candidates from which rt_insert32 pays
+
 // Insert this lane's masked candidates (m: bit j set = key[j]/row[j]) into the
 // warp list, re-testing each against the threshold as it tightens.
 template <int R>
 __device__ __forceinline__ void rt_offer(RTLocal& s, uint32_t k, const uint64_t (&key)[R], const uint32_t (&row)[R],
                                          uint32_t m, int lane) {
+  for (;;) {
+    const unsigned lanes = __ballot_sync(0xffffffffu, m != 0u);
+    if (__popc(lanes) < kRtBulkLanes) break;
+    const int j = m ? __ffs(m) - 1 : 0;
+    uint64_t ck = ~0ull;
+    uint32_t cr = 0xFFFFFFFFu;
+    if (m) {
+#pragma unroll
+      for (int jj = 0; jj < R; ++jj)
+        if (jj == j) {
+          ck = key[jj];
+          cr = row[jj];
+        }
+      m &= m - 1u;
+    }
+    rt_insert32(s, k, ck, cr, lane);
+    // Drop what the tightened threshold now excludes.
+#pragma unroll
+    for (int jj = 0; jj < R; ++jj)
+      if (((m >> jj) & 1u) && !kr_le(key[jj], row[jj], s.tk, s.tr)) m &= ~(1u << jj);
+  }
   for (;;) {
     const unsigned lanes = __ballot_sync(0xffffffffu, m != 0u);
     if (!lanes) break;
@@ -755,23 +836,18 @@ __device__ __forceinline__ void rt_share(RTSmem& sm, RTLocal& s, const RTParams&
   rt_bound(s, __shfl_sync(0xffffffffu, nb, 0));
 }
 
-// Merge the warps' lists into warp 0 (consumer threads only).
+// Merge the warps' lists into warp 0 (consumer threads only): log2(warps)
+// levels, each a sorted-list merge of the upper half's lists into the lower's.
 __device__ void rt_tree_merge(RTSmem& sm, RTLocal& s, uint32_t k, int warp, int lane, int nct) {
   for (int half = (nct >> 5) / 2; half >= 1; half >>= 1) {
     consumer_bar(nct);
     if (warp >= half && warp < 2 * half) {
-      sm.keys[warp][lane] = s.lk;
-      sm.rows[warp][lane] = s.lr;
+      const bool in = (uint32_t)lane < k;
+      sm.keys[warp][lane] = in ? s.lk : ~0ull;
+      sm.rows[warp][lane] = in ? s.lr : 0xFFFFFFFFu;
     }
     consumer_bar(nct);
-    if (warp < half) {
-      for (uint32_t i = 0; i < k; ++i) {
-        const uint64_t ck = sm.keys[warp + half][i];
-        const uint32_t cr = sm.rows[warp + half][i];
-        if (ck == ~0ull && cr == 0xFFFFFFFFu) break;  // lists are sorted: the rest are empty
-        if (kr_le(ck, cr, s.tk, s.tr)) rt_insert(s, k, ck, cr, lane);
-      }
-    }
+    if (warp < half) rt_merge_sorted(s, k, sm.keys[warp + half][lane], sm.rows[warp + half][lane], lane);
   }
   consumer_bar(nct);
 }
@@ -834,22 +910,37 @@ struct RegTopkOp {
           }
         }
       }
-      // Prefilter on the order key alone (key <= T's key); the row tie-break
-      // is only consulted for rows that pass.
-      uint64_t key[8];
+      // Prefilter in the value domain against the threshold's value: a row is
+      // dropped only when its value is strictly worse (an ordered compare, so a
+      // NaN on either side passes on to the exact test; so does -0.0 against
+      // +0.0).  Every dropped row has an order key above T's key.  Order keys
+      // and the row tie-break are only computed for rows that pass.
       uint32_t pm = 0;
+      const uint64_t tkey = DESC ? ~s.tk : s.tk;
+      if constexpr (DT == FDB_FLOAT64) {
+        const double tv = f64_from_ord_key(tkey);
 #pragma unroll
-      for (int j = 0; j < 8; ++j) {
-        key[j] = wt_key<DT, DESC>(v[j]);
-        if (key[j] <= s.tk) pm |= 1u << j;
+        for (int j = 0; j < 8; ++j) {
+          const double x = __longlong_as_double((long long)v[j]);
+          if (!(DESC ? x < tv : x > tv)) pm |= 1u << j;
+        }
+      } else {
+        const int64_t tv = (int64_t)(tkey ^ (1ull << 63));
+#pragma unroll
+        for (int j = 0; j < 8; ++j) {
+          const int64_t x = (int64_t)v[j];
+          if (DESC ? x >= tv : x <= tv) pm |= 1u << j;
+        }
       }
       pm &= vm;
       if (!__any_sync(0xffffffffu, pm != 0u)) continue;
+      uint64_t key[8];
       uint32_t row[8];
       uint32_t m = 0;
 #pragma unroll
       for (int j = 0; j < 8; ++j) {
         const uint32_t i = base + (j >> 1) * 64 + 2 * lane + (j & 1);
+        key[j] = wt_key<DT, DESC>(v[j]);
         row[j] = (uint32_t)acc.row(i);
         if (((pm >> j) & 1u) && kr_le(key[j], row[j], s.tk, s.tr)) m |= 1u << j;
       }
@@ -864,7 +955,8 @@ struct RegTopkOp {
     // tiles warp 0 also exchanges it with the global bound.
     ++s.steps;
     if ((s.steps & 3u) == 0u)
-      rt_share(*reinterpret_cast<RTSmem*>(smraw), s, p, warp, lane, (s.steps & 15u) == 0u);
+      rt_share(*reinterpret_cast<RTSmem*>(smraw), s, p, warp, lane,
+               kRtGlobalEvery != 0u && (s.steps % kRtGlobalEvery) == 0u);
   }
 
   static __device__ void finish(Local& s, const Params& p, unsigned char* smraw, int ctid, int nct) {
@@ -891,23 +983,45 @@ struct RegTopkOp {
     const uint64_t gb = *reinterpret_cast<volatile unsigned long long*>(p.gbound);
     rt_bound(s, gb);
     if (warp != 0) rt_clear(s);
-    const uint32_t total = gridDim.x * k;
-    for (uint32_t b = warp * 256; b < total; b += 256 * (nct / 32)) {
-      uint64_t key[8];
-      uint32_t row[8];
-      uint32_t m = 0;
+    // One thread per CTA list: each list is sorted, so only a prefix of it can
+    // be at or under the bound, and most lists stop at their first entry.
+    // Up to 8 entries per list per pass; a list with more qualifying entries
+    // (possible only while the bound is loose) is walked in further passes.
+    for (uint32_t c0 = 0; c0 < gridDim.x; c0 += nct) {
+      const uint32_t c = c0 + ctid;
+      uint32_t from = 0;
+      for (;;) {
+        uint64_t key[8];
+        uint32_t row[8];
+        uint32_t m = 0;
+        bool more = false;
+        if (c < gridDim.x && c != blockIdx.x) {
+          const uint64_t* lk = p.partials_k + (size_t)c * k;
+          const uint32_t* lr = p.partials_r + (size_t)c * k;
 #pragma unroll
-      for (int j = 0; j < 8; ++j) {
-        const uint32_t i = b + j * 32 + lane;
-        key[j] = ~0ull;
-        row[j] = 0xFFFFFFFFu;
-        if (i < total && i / k != blockIdx.x) {
-          key[j] = __ldcg(&p.partials_k[i]);
-          row[j] = __ldcg(&p.partials_r[i]);
-          if (!(key[j] == ~0ull && row[j] == 0xFFFFFFFFu) && kr_le(key[j], row[j], s.tk, s.tr)) m |= 1u << j;
+          for (int j = 0; j < 8; ++j) {  // independent loads: one L2 round trip per pass
+            key[j] = ~0ull;
+            row[j] = 0xFFFFFFFFu;
+            if (from + j < k) {
+              key[j] = __ldcg(lk + from + j);
+              row[j] = __ldcg(lr + from + j);
+            }
+          }
+#pragma unroll
+          for (int j = 0; j < 8; ++j)
+            if (!(key[j] == ~0ull && row[j] == 0xFFFFFFFFu) && kr_le(key[j], row[j], s.tk, s.tr)) m |= 1u << j;
+          more = ((m >> 7) & 1u) && from + 8 < k;
+        } else {
+#pragma unroll
+          for (int j = 0; j < 8; ++j) {
+            key[j] = ~0ull;
+            row[j] = 0xFFFFFFFFu;
+          }
         }
+        if (__any_sync(0xffffffffu, m != 0u)) rt_offer<8>(s, k, key, row, m, lane);
+        if (!__any_sync(0xffffffffu, more)) break;
+        from = more ? from + 8 : k;  // a finished list offers nothing on later passes
       }
-      if (__any_sync(0xffffffffu, m != 0u)) rt_offer<8>(s, k, key, row, m, lane);
     }
     rt_tree_merge(sm, s, k, warp, lane, nct);
     if (warp == 0) {
@@ -1008,12 +1122,20 @@ static void launch_reg_topk(Ctx& c, const fdb_dev_column& col, uint64_t n, uint3
   p.n = n;
   p.k = k;
   p.tile_rows = TR;
-  p.gbound = static_cast<unsigned long long*>(c.scratch_take(8));
-  FDB_CUDA(cudaMemsetAsync(p.gbound, 0xFF, 8, c.stream));
-  const uint64_t nsamples = (n + kSampleStride - 1) / kSampleStride;
+  // gbound (8 bytes, ~0 = no bound yet) and the dynamic tile counter (4 bytes,
+  // 0xFFFFFFFF on entry) share one memset.
+  p.gbound = static_cast<unsigned long long*>(c.scratch_take(16));
+  FDB_CUDA(cudaMemsetAsync(p.gbound, 0xFF, 16, c.stream));
+  src.tile_ctr = reinterpret_cast<unsigned int*>(p.gbound + 1);
+  if ((src.m_end + TR - 1) / TR >= 0xFFFFFFFFull) fail(FDB_E_ARG, "too many tiles for the tile counter");
+  // At most kRegSamples samples: their loads are scattered (one DRAM burst
+  // each), and the batched insertion absorbs the k * stride rows a coarser
+  // bound admits.
+  const uint64_t stride = std::max<uint64_t>(kSampleStride, n / kRegSamples);
+  const uint64_t nsamples = (n + stride - 1) / stride;
   if (nsamples >= 2ull * k) {
     const unsigned sgrid = (unsigned)umin64((nsamples + 2047) / 2048, (uint64_t)c.sm_count * 8);
-    rt_sample_kernel<DT, DESC><<<sgrid, 256, 0, c.stream>>>(p, nsamples, kSampleStride);
+    rt_sample_kernel<DT, DESC><<<sgrid, 256, 0, c.stream>>>(p, nsamples, stride);
     FDB_CUDA(cudaGetLastError());
   }
   p.partials_k = partials_k;
@@ -1023,7 +1145,7 @@ static void launch_reg_topk(Ctx& c, const fdb_dev_column& col, uint64_t n, uint3
   p.out_count = out_count;
   const int op_off = (int)stream_smem_bytes<1, TR, STAGES>();
   const size_t smem = op_off + sizeof(RTSmem);
-  auto kern = stream_kernel<RegTopkOp<DT, DESC>, 1, TR, STAGES, NCW>;
+  auto kern = stream_kernel<RegTopkOp<DT, DESC>, 1, TR, STAGES, NCW, 8, 3, true>;  // 3 CTAs per SM, dynamic tiles
   static bool attr = false;
   if (!attr) {
     FDB_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));

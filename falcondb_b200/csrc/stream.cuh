@@ -22,6 +22,7 @@ struct StreamSrc {
   int esize[NC];                  // bytes per value (4 or 8)
   uint64_t n;                     // rows
   uint64_t m_end;                 // rows [0, m_end) are staged by TMA
+  unsigned int* tile_ctr;         // dynamic tile order only: 0xFFFFFFFF on entry
 };
 
 // Rows staged in shared memory: column c of the current stage starts at
@@ -93,12 +94,19 @@ inline uint64_t stream_m_end(const void* const* bases, int nc, uint64_t n) {
 // step() and finish() are executed by all consumer threads; block-wide syncs
 // inside them must use consumer_bar(nct).
 // MINB: resident CTAs per SM the register allocation must allow.
-template <class Op, int NC, int TR, int STAGES, int NCW, int CB = 8, int MINB = 1>
+// DYN: tiles are handed out by an atomic counter (src.tile_ctr) instead of
+// round-robin, so CTAs that run faster take more tiles and all finish
+// together.  The tile order then varies run to run, so DYN is only for ops
+// whose result does not depend on it (top-k, counts), and for ops whose step
+// has no CTA-wide barrier: on a time-out a warp leaves the tile loop at once.
+template <class Op, int NC, int TR, int STAGES, int NCW, int CB = 8, int MINB = 1, bool DYN = false>
 __global__ void __launch_bounds__((NCW + 1) * 32, MINB)
     stream_kernel(StreamSrc<NC> src, typename Op::Params p, int* err, int op_smem_off) {
+  static_assert((DYN ? 20 : 16) * STAGES <= kBarBytes, "mbarriers (and DYN tile ids) fit the barrier block");
   extern __shared__ __align__(128) unsigned char smem[];
   uint64_t* full = reinterpret_cast<uint64_t*>(smem);
   uint64_t* empty = full + STAGES;
+  uint32_t* tile_id = reinterpret_cast<uint32_t*>(empty + STAGES);  // [STAGES], DYN only
   unsigned char* tiles = smem + kBarBytes;
   unsigned char* op_smem = smem + op_smem_off;
   constexpr int NCT = NCW * 32;
@@ -120,10 +128,21 @@ __global__ void __launch_bounds__((NCW + 1) * 32, MINB)
     if (lane == 0) {
       const uint64_t policy = l2_evict_first_policy();  // columns are read once
       uint32_t it = 0;
-      for (uint64_t t = blockIdx.x; t < ntiles; t += gridDim.x, ++it) {
+      for (uint64_t t = blockIdx.x; t < ntiles || DYN; t += gridDim.x, ++it) {
         const int s = it % STAGES;
         const uint32_t ph = (it / STAGES) & 1u;
         if (it >= STAGES && !mbar_wait_backoff(&empty[s], ph ^ 1u, err, 64)) break;
+        if constexpr (DYN) {
+          // First tile: blockIdx.x; then gridDim.x + 0, 1, 2, ... in claim order
+          // (the counter starts at 0xFFFFFFFF, so its first value wraps to 0).
+          if (it > 0) t = (uint64_t)gridDim.x + (uint32_t)(atomicAdd(src.tile_ctr, 1u) + 1u);
+          if (t >= ntiles) {
+            tile_id[s] = 0xFFFFFFFFu;
+            mbar_arrive(&full[s]);  // completes the phase with no bytes: the end mark
+            break;
+          }
+          tile_id[s] = (uint32_t)t;
+        }
         const uint64_t r0 = t * TR;
         const uint32_t rows = (uint32_t)umin64(TR, src.m_end - r0);
         uint32_t bytes = 0;
@@ -153,10 +172,19 @@ __global__ void __launch_bounds__((NCW + 1) * 32, MINB)
   // always ends.
   uint32_t it = 0;
   bool dead = false;
-  for (uint64_t t = blockIdx.x; t < ntiles; t += gridDim.x, ++it) {
+  for (uint64_t t = blockIdx.x; t < ntiles || DYN; t += gridDim.x, ++it) {
     const int s = it % STAGES;
     const uint32_t ph = (it / STAGES) & 1u;
-    if (!dead && !mbar_wait(&full[s], ph, err)) dead = true;
+    if constexpr (DYN) {
+      // The wait's outcome is made warp-uniform so that the warp collectives
+      // inside Op::step stay converged; a warp that timed out stops here.
+      if (!__all_sync(0xffffffffu, mbar_wait(&full[s], ph, err))) break;
+      const uint32_t tid = tile_id[s];
+      if (tid == 0xFFFFFFFFu) break;
+      t = tid;
+    } else {
+      if (!dead && !mbar_wait(&full[s], ph, err)) dead = true;
+    }
     const uint64_t r0 = t * TR;
     const uint32_t rows = (uint32_t)umin64(TR, src.m_end - r0);
     TileAcc<TR, CB> acc{tiles + (size_t)s * NC * TR * CB, r0};

@@ -47,6 +47,19 @@ def test_topk_ascending_id_desc(db, n):
     assert np.array_equal(run(db, dev(v), n, 10, False), O.topk(v, 10, False))
 
 
+@pytest.mark.parametrize("k", [1, 17, 32])
+def test_topk_candidate_floods_with_ties(db, k):
+    """Inputs where whole warps hold candidates at once (the batched bitonic
+    insertion): ascending runs of equal keys, and a sawtooth whose every tile
+    beats the running bound; ties must still break on row ascending."""
+    n = 3_000_001
+    v = (np.arange(n) // 3).astype(np.int64)
+    w = (np.arange(n) % 65_536).astype(np.float64)
+    for col in (v, w):
+        for desc in (True, False):
+            assert np.array_equal(run(db, dev(col), n, k, desc), O.topk(col, k, desc)), (k, desc, col.dtype)
+
+
 def test_topk_all_equal_ties_on_row(db):
     n = 2_000_000
     v = np.full(n, 42.5)
@@ -78,6 +91,26 @@ def test_topk_nan_and_inf(db):
     v[[11]] = -np.inf
     for desc in (True, False):
         assert np.array_equal(run(db, dev(v), n, 10, desc), O.topk(v, 10, desc))
+
+
+def test_topk_signed_zero_and_negative_nan(db):
+    """-0.0 orders below +0.0 and a NaN with the sign bit set below -inf
+    (f64_ord_key, sort.rs:451-454); the value-domain prefilter must pass all
+    of them on to the exact key test."""
+    n = 200_003
+    v = np.random.default_rng(8).random(n) - 0.5
+    v[::5] = 0.0
+    v[1::5] = -0.0
+    neg_nan = np.array([0xFFF8000000000001], dtype=np.uint64).view(np.float64)[0]
+    v[[7, 70_000]] = neg_nan
+    v[9] = np.nan
+    v[11] = -np.inf
+    for k in (1, 10, 32):
+        for desc in (True, False):
+            assert np.array_equal(run(db, dev(v), n, k, desc), O.topk(v, k, desc)), (k, desc)
+    z = np.where(np.arange(n) % 2 == 0, 0.0, -0.0)  # only signed zeros: ties on the key, then row
+    for desc in (True, False):
+        assert np.array_equal(run(db, dev(z), n, 10, desc), O.topk(z, 10, desc)), desc
 
 
 @pytest.mark.parametrize("nulls_last", [True, False])
