@@ -33,6 +33,17 @@ struct JSlot {
 
 constexpr uint32_t kNoSlot = 0xFFFFFFFFu;
 
+// Home slot of a stored key in a table of 2^(64-shift) slots: multiplicative
+// (Fibonacci) hashing, the top bits of key * 2^64/phi.  One 64-bit multiply
+// and a shift; consecutive keys land far apart, so linear probing stays
+// short on the dense integer keys joins usually have.  The choice of hash is
+// not observable in any result (the reference mixes with int_key_hash,
+// join.rs:1368-1374).
+__host__ __device__ __forceinline__ uint64_t join_hash(uint64_t sk, int shift) {
+  return (sk * 0x9E3779B97F4A7C15ull) >> shift;
+}
+__device__ __forceinline__ int join_shift(uint64_t cap) { return __clzll((long long)cap) + 1; }  // cap = 2^b
+
 struct HashTable {
   Ctx* ctx = nullptr;
   DevBuf slots, cnt, pcnt, off, rows;
@@ -65,7 +76,7 @@ __global__ void join_insert_kernel(const int64_t* __restrict__ keys, const uint6
       s = cap;
     } else {
       const unsigned long long sk = (unsigned long long)k ^ (1ull << 63);
-      uint64_t h = mix64(sk) & mask;
+      uint64_t h = join_hash(sk, join_shift(cap));
       for (uint64_t probe = 0; probe <= mask; ++probe) {  // cap > distinct keys: always ends
         const unsigned long long cur = *reinterpret_cast<volatile unsigned long long*>(&slots[h].key);
         if (cur == sk) { s = h; break; }
@@ -261,7 +272,7 @@ __device__ __forceinline__ uint32_t join_find(const JSlot* __restrict__ slots, c
   }
   const unsigned long long sk = (unsigned long long)k ^ (1ull << 63);
   const uint64_t mask = cap - 1;
-  uint64_t h = mix64(sk) & mask;
+  uint64_t h = join_hash(sk, join_shift(cap));
   for (uint64_t probe = 0; probe <= mask; ++probe) {
     const JSlot s = slots[h];
     if (s.key == sk) {
@@ -293,18 +304,15 @@ struct ProbeParams {
   uint64_t cap;
   int32_t unique;
   int32_t payload_nulls;
-  int32_t join_type;
   int32_t has_value;
+  int32_t _pad;
   JoinAggAcc* partials;   // [grid]
   unsigned int* ticket;
   fdb_join_agg* out;
 };
 
-// Probe launch shape: rows in flight per thread, ring stages, tile rows (one
-// column), and resident CTAs per SM the register budget is sized for.
-#ifndef FDB_PROBE_PR
-#define FDB_PROBE_PR 1
-#endif
+// Probe launch shape: ring stages, tile rows (one column), and resident CTAs
+// per SM the register budget is sized for.
 #ifndef FDB_PROBE_STAGES
 #define FDB_PROBE_STAGES 2
 #endif
@@ -312,9 +320,11 @@ struct ProbeParams {
 #define FDB_PROBE_TR 2048
 #endif
 #ifndef FDB_PROBE_MINB
-#define FDB_PROBE_MINB 4
+#define FDB_PROBE_MINB 5
 #endif
 
+// JT: the join type (FDB_JOIN_*), fixed per instantiation.
+template <int JT>
 struct ProbeOp {
   using Params = ProbeParams;
   struct Local {
@@ -329,12 +339,6 @@ struct ProbeOp {
     st.a.vsum = 0.0;
   }
 
-  // Software-pipelined probe: each thread advances kPR rows together.  Every
-  // round issues one 32-byte load per unfinished row — the aligned pair of
-  // slots holding its current probe position — so up to kPR independent L2
-  // reads are in flight per thread, and a pair resolves two probe steps.
-  static constexpr int kPR = FDB_PROBE_PR;
-
   // Both slots of an aligned pair (32 bytes, one L2 sector) in one 256-bit load.
   static __device__ __forceinline__ void load_pair(const JSlot* pair, uint64_t pol, JSlot& a, JSlot& b) {
     asm volatile("ld.global.L2::cache_hint.v4.u64 {%0, %1, %2, %3}, [%4], %5;"
@@ -342,99 +346,63 @@ struct ProbeOp {
                  : "l"(pair), "l"(pol));
   }
 
+  // One row per thread per pass.  Each probe round reads the aligned pair of
+  // slots around the current position and resolves both in probe order
+  // without branches: the first slot counts only when the position is even;
+  // the walk ends at the key or at the first empty slot.
   template <class Acc>
   static __device__ void step(Local& st, const Params& p, unsigned char*, const Acc& acc, uint32_t rows,
                               int ctid, int nct) {
     const uint64_t mask = p.cap - 1;
+    const int shift = join_shift(p.cap);
     const uint64_t pol = l2_evict_last_policy();  // keep the table resident against the streamed keys
-    for (uint32_t b = 0; b < rows; b += kPR * nct) {
-      uint64_t sk[kPR], h[kPR], ps[kPR];
-      uint32_t at[kPR];
-      uint32_t todo = 0, live = 0;
-#pragma unroll
-      for (int j = 0; j < kPR; ++j) {
-        const uint32_t i = b + j * nct + ctid;
-        at[j] = kNoSlot;
-        sk[j] = 0;
-        h[j] = 0;
-        ps[j] = 0;
-        if (i >= rows) continue;
-        live |= 1u << j;
-        if (p.key.validity && !col_valid(p.key, acc.row(i))) continue;  // NULL key: no match
+    for (uint32_t i = ctid; i < rows; i += nct) {
+      uint32_t at = kNoSlot;
+      uint64_t ps = 0;
+      if (!p.key.validity || col_valid(p.key, acc.row(i))) {  // a NULL key matches nothing
         const int64_t k = acc.template get<int64_t>(0, i);
         if (k == INT64_MIN) {
           if (p.cnt[p.cap] != 0u) {
-            at[j] = (uint32_t)p.cap;
-            ps[j] = p.slots[p.cap].psum;
+            at = (uint32_t)p.cap;
+            ps = p.slots[p.cap].psum;
           }
-          continue;
-        }
-        sk[j] = (unsigned long long)k ^ (1ull << 63);
-        h[j] = mix64(sk[j]) & mask;
-        todo |= 1u << j;
-      }
-      for (uint32_t round = 0; todo && round <= mask; ++round) {
-        JSlot s0[kPR], s1[kPR];
-#pragma unroll
-        for (int j = 0; j < kPR; ++j) {
-          if ((todo >> j) & 1u) load_pair(p.slots + (h[j] & ~1ull), pol, s0[j], s1[j]);
-        }
-#pragma unroll
-        for (int j = 0; j < kPR; ++j) {
-          if (!((todo >> j) & 1u)) continue;
-          const bool odd = h[j] & 1ull;
-          const uint64_t base = h[j] & ~1ull;
-          // Slots in probe order: the pair's second slot only when h is odd.
-          if (!odd) {
-            if (s0[j].key == sk[j]) { at[j] = (uint32_t)base; ps[j] = s0[j].psum; todo &= ~(1u << j); continue; }
-            if (s0[j].key == 0ull) { todo &= ~(1u << j); continue; }
+        } else {
+          const uint64_t sk = (uint64_t)k ^ (1ull << 63);
+          uint64_t h = join_hash(sk, shift);
+          for (uint64_t round = 0; round <= mask; ++round) {
+            const uint64_t base = h & ~1ull;
+            JSlot a, b;
+            load_pair(p.slots + base, pol, a, b);
+            const bool even = (h & 1ull) == 0;
+            const bool hit0 = even && a.key == sk;
+            const bool stop0 = even && (a.key == sk || a.key == 0ull);
+            const bool hit1 = !stop0 && b.key == sk;
+            if (hit0 || hit1) {
+              at = (uint32_t)(base + (hit1 ? 1 : 0));
+              ps = hit1 ? b.psum : a.psum;
+              break;
+            }
+            if (stop0 || b.key == 0ull) break;
+            h = (base + 2) & mask;
           }
-          if (s1[j].key == sk[j]) { at[j] = (uint32_t)(base + 1); ps[j] = s1[j].psum; todo &= ~(1u << j); continue; }
-          if (s1[j].key == 0ull) { todo &= ~(1u << j); continue; }
-          h[j] = (base + 2) & mask;
         }
       }
-#pragma unroll
-      for (int j = 0; j < kPR; ++j) {
-        if (!((live >> j) & 1u)) continue;
-        const uint32_t i = b + j * nct + ctid;
-        unsigned long long matches = 0, prows = 0;
-        long long psum = 0;
-        if (at[j] != kNoSlot) {
-          matches = p.unique ? 1ull : (unsigned long long)p.cnt[at[j]];
-          psum = (long long)ps[j];
-          prows = p.payload_nulls ? (unsigned long long)p.pcnt[at[j]] : matches;
-        }
-        accumulate(st, p, acc, i, matches, psum, prows);
+      unsigned long long matches = 0, prows = 0;
+      if (at != kNoSlot) {
+        matches = p.unique ? 1ull : (unsigned long long)p.cnt[at];
+        prows = p.payload_nulls ? (unsigned long long)p.pcnt[at] : matches;
       }
-    }
-  }
-
-  template <class Acc>
-  static __device__ __forceinline__ void accumulate(Local& st, const Params& p, const Acc& acc, uint32_t i,
-                                                    unsigned long long matches, long long psum,
-                                                    unsigned long long prows) {
-    switch (p.join_type) {
-      case FDB_JOIN_INNER:
-        st.a.count += matches;
-        st.a.psum += psum;
+      if constexpr (JT == FDB_JOIN_INNER || JT == FDB_JOIN_LEFT) {
+        st.a.count += (JT == FDB_JOIN_LEFT && matches == 0) ? 1ull : matches;
+        st.a.psum += (long long)ps;
         st.a.prows += prows;
-        break;
-      case FDB_JOIN_LEFT:
-        st.a.count += matches ? matches : 1ull;
-        st.a.psum += psum;
-        st.a.prows += prows;
-        break;
-      default: {
-        const bool keep = (p.join_type == FDB_JOIN_SEMI) ? (matches != 0) : (matches == 0);
+      } else {
+        const bool keep = (JT == FDB_JOIN_SEMI) ? (matches != 0) : (matches == 0);
         if (keep) {
           st.a.count += 1;
-          if (p.has_value) {
-            const bool vv = p.value.validity ? col_valid(p.value, acc.row(i)) : true;
-            if (vv) {
-              st.a.vsum += acc.template get<double>(1, i);
-              st.a.prows += 1;
-            }
+          if (p.has_value && (!p.value.validity || col_valid(p.value, acc.row(i)))) {
+            st.a.vsum += acc.template get<double>(1, i);
+            st.a.prows += 1;
           }
         }
       }
@@ -510,7 +478,7 @@ struct ProbeOp {
 
 constexpr int kProbeMaxPerSm = 8;  // partials are sized for this many CTAs per SM
 
-template <int NC>
+template <int NC, int JT>
 static void launch_probe(Ctx& c, const fdb_dev_column* cols, uint64_t n, const ProbeParams& p) {
   constexpr int TR = NC == 1 ? FDB_PROBE_TR : FDB_PROBE_TR / 2, STAGES = FDB_PROBE_STAGES, NCW = 8;
   StreamSrc<NC> src;
@@ -523,8 +491,8 @@ static void launch_probe(Ctx& c, const fdb_dev_column* cols, uint64_t n, const P
   src.n = n;
   src.m_end = stream_m_end(bases, NC, n);
   const int op_off = (int)stream_smem_bytes<NC, TR, STAGES>();
-  const size_t smem = op_off + ProbeOp::kSmem;
-  auto kern = stream_kernel<ProbeOp, NC, TR, STAGES, NCW, 8, FDB_PROBE_MINB>;
+  const size_t smem = op_off + ProbeOp<JT>::kSmem;
+  auto kern = stream_kernel<ProbeOp<JT>, NC, TR, STAGES, NCW, 8, FDB_PROBE_MINB>;
   static bool attr = false;
   if (!attr) {
     FDB_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024));
@@ -558,7 +526,6 @@ void op_join_probe_agg(Ctx& c, const HashTable& h, const fdb_dev_column& key, co
   p.cap = h.cap;
   p.unique = h.unique ? 1 : 0;
   p.payload_nulls = h.payload_nulls ? 1 : 0;
-  p.join_type = join_type;
   p.has_value = (has_value && (join_type == FDB_JOIN_SEMI || join_type == FDB_JOIN_ANTI)) ? 1 : 0;
   p.partials = static_cast<JoinAggAcc*>(c.scratch_take(sizeof(JoinAggAcc) * c.sm_count * kProbeMaxPerSm));
   p.ticket = c.d_ticket;
@@ -568,10 +535,17 @@ void op_join_probe_agg(Ctx& c, const HashTable& h, const fdb_dev_column& key, co
     return;
   }
   fdb_dev_column cols[2] = {key, has_value ? *value : key};
-  if (p.has_value)
-    launch_probe<2>(c, cols, n, p);
-  else
-    launch_probe<1>(c, cols, n, p);
+  switch (join_type) {
+    case FDB_JOIN_INNER: launch_probe<1, FDB_JOIN_INNER>(c, cols, n, p); break;
+    case FDB_JOIN_LEFT: launch_probe<1, FDB_JOIN_LEFT>(c, cols, n, p); break;
+    case FDB_JOIN_SEMI:
+      if (p.has_value) launch_probe<2, FDB_JOIN_SEMI>(c, cols, n, p);
+      else launch_probe<1, FDB_JOIN_SEMI>(c, cols, n, p);
+      break;
+    default:
+      if (p.has_value) launch_probe<2, FDB_JOIN_ANTI>(c, cols, n, p);
+      else launch_probe<1, FDB_JOIN_ANTI>(c, cols, n, p);
+  }
 }
 
 // ---------------------------------------------------------------------------
