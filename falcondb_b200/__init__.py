@@ -393,7 +393,18 @@ class Database:
         check(rc)
         # Keep host buffers referenced until the upload is known complete.
         self._keep[name] = keep
+        self._dicts = getattr(self, "_dicts", {})
+        for cname, col in columns.items():
+            if isinstance(col, Utf8):
+                self._dicts[(name, cname)] = list(col.dictionary)
         return int(rc)
+
+    def dictionary(self, table: str, column: str) -> List[str]:
+        """The dictionary of a Utf8 column created through :meth:`create_table`."""
+        try:
+            return self._dicts[(table, column)]
+        except (AttributeError, KeyError):
+            raise FalconError(-6, f"no dictionary for {table}.{column}") from None
 
     def create_table_from_pointers(self, name: str, specs: List[Tuple[str, int, int]], nrows: int) -> int:
         """Create a table from raw host pointers: ``specs`` = [(name, dtype, ptr)]

@@ -131,3 +131,38 @@ def test_hash_group_by_with_filter(db):
     mask = O.cmp_mask(sel, F.LT, 25.0)
     want = O.group_i64(t["key"], t["v"], mask=mask)
     assert np.array_equal(rec["key"], want["key"]) and np.array_equal(rec["count"], want["count"])
+
+
+def _pandas_groups(keys, vals, vvalid=None):
+    """COUNT(*), SUM/MIN/MAX over the non-NULL values, per key (NULL values as NaN)."""
+    import pandas as pd
+
+    v = vals.astype(np.float64) if vvalid is None else np.where(vvalid, vals.astype(np.float64), np.nan)
+    g = pd.DataFrame({"k": keys, "v": v}).groupby("k", sort=True)["v"]
+    return {"key": g.size().index.to_numpy(), "count": g.size().to_numpy(), "sum": g.sum().to_numpy(),
+            "min": g.min().to_numpy(), "max": g.max().to_numpy()}
+
+
+def _same_groups(rec, want):
+    assert np.array_equal(rec["key"], want["key"]) and np.array_equal(rec["count"], want["count"])
+    assert np.array_equal(rec["min"], want["min"], equal_nan=True)
+    assert np.array_equal(rec["max"], want["max"], equal_nan=True)
+    rel = np.abs(rec["sum"] - want["sum"]) / np.maximum(np.abs(want["sum"]), 1e-300)
+    assert rel.max() <= RTOL
+
+
+def test_hash_group_by_large_with_null_values_and_keys(db):
+    """850k groups (a table far larger than the CTA tables) with NULL values
+    (SUM/MIN/MAX skip them, COUNT(*) counts the row) and a NULL key group."""
+    n = 1_500_000
+    r = np.random.default_rng(21)
+    keys = r.integers(0, 1_200_000, n)
+    keys[::100] = np.iinfo(np.int64).min  # the NULL group
+    vals = r.random(n)
+    vvalid = r.random(n) > 0.1
+    vw = F.validity_words(vvalid)
+    out, ng = ops.group_by_i64(db, dev(keys), (dev(vals), dev(vw.view(np.int64))), n)
+    g = int(ng.item())
+    rec = ops.to_records(out, F.GROUP_I64_DTYPE, g)
+    rec = rec[np.argsort(rec["key"], kind="stable")]
+    _same_groups(rec, _pandas_groups(keys, vals, vvalid))
