@@ -503,6 +503,42 @@ def run_secondary(args):
         line("groupby_zipf", ms, 16 * n + 40 * groups, {"rows": n, "groups": groups, "distinct_domain": 10_000_000,
                                                         "zipf_s": 1.1, "load_factor": lf})
         db.drop_table("g")
+
+    if args.workload in ("batch", "all"):
+        # 64 GROUP BY key queries over slices of the 100M-row Zipf table, sizes
+        # log-uniform in [10k, 10M] rows, offsets uniform: one captured graph
+        # (the autotuner's tuning) against the same queries run one by one.
+        g = W.groupby_table(n, distinct=10_000_000, seed=11)
+        db.create_table("g", g)
+        kt = torch.from_numpy(g["key"]).to(dev)
+        vt = torch.from_numpy(g["v"]).to(dev)
+        rng = np.random.default_rng(64)
+        sizes = np.minimum(np.floor(10 ** (4 + 3 * rng.random(64))).astype(np.int64), n)
+        offs = [int(rng.integers(0, n - s + 1)) for s in sizes]
+        qs = [(kt[o:o + int(s)], vt[o:o + int(s)], int(s)) for o, s in zip(offs, sizes)]
+        rows_total = int(sizes.sum())
+        tuning, tuned_ms = ops.GroupByBatch.autotune(db, qs, reps=2)
+        b = ops.GroupByBatch(db, qs, tuning=tuning)
+        ms_batch = _time_steps(b.run, K, Wm, stream, torch)
+        groups = [int(b.outs[i][1].item()) for i in range(len(qs))]
+        outs = [(ops._bytes(F.GROUP_I64_DTYPE.itemsize * (gq + 1), db), torch.empty(1, dtype=torch.int64, device=dev))
+                for gq in groups]
+
+        def serial():
+            for (kk, vv, s), gq, (ob, nb) in zip(qs, groups, outs):
+                ops.group_by_i64(db, kk, vv, s, expected_groups=max(gq, 1), capacity=gq + 1, out=ob, ngroups=nb)
+        ms_serial = _time_steps(serial, K, Wm, stream, torch)
+        assert [int(nb.item()) for _, nb in outs] == groups
+        b.free()
+        nbytes = 16 * rows_total + 40 * sum(groups)
+        line("groupby_batched", ms_batch, nbytes, {
+            "queries": len(qs), "rows_total": rows_total, "groups_total": sum(groups),
+            "qps_batched": round(len(qs) / (ms_batch / 1e3), 1), "ms_serial": round(ms_serial, 4),
+            "qps_serial": round(len(qs) / (ms_serial / 1e3), 1), "speedup_vs_serial": round(ms_serial / ms_batch, 2),
+            "tuning": {"load_factor": tuning[0], "ctas_per_sm": tuning[1], "tile_rows": tuning[2]},
+            "serial": "the same 64 queries as fdb_group_by_i64 calls in sequence, tables sized to the exact "
+                      "group counts"})
+        db.drop_table("g")
     db.close()
     return out
 
@@ -548,7 +584,7 @@ def main():
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--cpu-threads", type=int, default=0)
     ap.add_argument("--workload", default="scan",
-                    choices=["scan", "filter_groupby", "join", "groupby", "all"],
+                    choices=["scan", "filter_groupby", "join", "groupby", "batch", "all"],
                     help="scan = the headline line; the others print per-operator lines")
     ap.add_argument("--load-factor", type=float, default=0.5)
     args = ap.parse_args()

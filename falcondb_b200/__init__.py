@@ -84,6 +84,16 @@ class fdb_group_i64(C.Structure):
                 ("max", C.c_double)]
 
 
+class fdb_gb_query(C.Structure):
+    _fields_ = [("key", fdb_dev_column), ("value", fdb_dev_column), ("nrows", C.c_uint64),
+                ("expected_groups", C.c_uint64), ("d_groups", C.c_void_p), ("capacity", C.c_uint64),
+                ("d_ngroups", C.c_void_p)]
+
+
+class fdb_batch_tuning(C.Structure):
+    _fields_ = [("load_factor", C.c_double), ("ctas_per_sm", C.c_int32), ("tile_rows", C.c_int32)]
+
+
 AGG_VALUE_DTYPE = np.dtype([("f", "<f8"), ("i", "<i8"), ("n", "<i8"), ("is_int", "<i4"), ("valid", "<i4")])
 JOIN_AGG_DTYPE = np.dtype([("count", "<i8"), ("sum_payload", "<i8"), ("sum_value", "<f8"),
                            ("payload_rows", "<i8")])
@@ -145,6 +155,12 @@ _SIGS = {
                                        C.c_void_p, C.c_void_p, C.c_uint64, C.c_void_p]),
     "fdb_topk": (C.c_int, [C.c_void_p, C.POINTER(fdb_dev_column), C.c_uint64, C.c_uint32, C.c_int32, C.c_int32,
                            C.c_void_p, C.c_void_p]),
+    "fdb_gb_batch_prepare": (C.c_int, [C.c_void_p, C.POINTER(fdb_gb_query), C.c_int32, C.POINTER(fdb_batch_tuning),
+                                       C.POINTER(C.c_void_p)]),
+    "fdb_gb_batch_run": (C.c_int, [C.c_void_p]),
+    "fdb_gb_batch_free": (None, [C.c_void_p]),
+    "fdb_gb_batch_autotune": (C.c_int, [C.c_void_p, C.POINTER(fdb_gb_query), C.c_int32, C.c_int32,
+                                        C.POINTER(fdb_batch_tuning), C.POINTER(C.c_double)]),
 }
 
 EXPORTED = tuple(_SIGS)

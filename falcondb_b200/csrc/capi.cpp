@@ -20,6 +20,10 @@ struct fdb_hash {
   fdb::HashTable* h = nullptr;
   fdb_db* db = nullptr;
 };
+struct fdb_batch {
+  fdb::BatchPlan* plan = nullptr;
+  fdb_db* db = nullptr;
+};
 
 namespace fdb {
 
@@ -591,6 +595,48 @@ int fdb_topk(fdb_db* db, const fdb_dev_column* col, uint64_t nrows, uint32_t k, 
   return guarded([&] {
     CallScope s(db, default_scratch(db->ctx));
     op_topk(s.c, *col, nrows, k, desc != 0, nulls_last != 0, d_rows, d_count);
+  });
+}
+
+int fdb_gb_batch_prepare(fdb_db* db, const fdb_gb_query* queries, int32_t nqueries, const fdb_batch_tuning* tuning,
+                         fdb_batch** out) {
+  if (out) *out = nullptr;
+  if (!db || !queries || !out) return set_error(FDB_E_ARG, "fdb_gb_batch_prepare: bad arguments");
+  return guarded([&] {
+    CallScope s(db, default_scratch(db->ctx));
+    std::unique_ptr<fdb_batch> b(new fdb_batch());
+    b->db = db;
+    b->plan = op_gb_batch_prepare(s.c, queries, nqueries, tuning);
+    *out = b.release();
+  });
+}
+
+int fdb_gb_batch_run(fdb_batch* b) {
+  if (!b || !b->plan) return set_error(FDB_E_ARG, "fdb_gb_batch_run: bad batch");
+  return guarded([&] {
+    std::lock_guard<std::recursive_mutex> lk(b->db->ctx.mu);
+    FDB_CUDA(cudaSetDevice(b->db->ctx.device));
+    op_gb_batch_run(b->plan);
+  });
+}
+
+void fdb_gb_batch_free(fdb_batch* b) {
+  if (!b) return;
+  guarded([&] {
+    std::lock_guard<std::recursive_mutex> lk(b->db->ctx.mu);
+    FDB_CUDA(cudaSetDevice(b->db->ctx.device));
+    op_gb_batch_free(b->plan);
+  });
+  delete b;
+}
+
+int fdb_gb_batch_autotune(fdb_db* db, const fdb_gb_query* queries, int32_t nqueries, int32_t reps,
+                          fdb_batch_tuning* best, double* best_ms) {
+  if (!db || !queries || !best) return set_error(FDB_E_ARG, "fdb_gb_batch_autotune: bad arguments");
+  return guarded([&] {
+    CallScope s(db, default_scratch(db->ctx));
+    const double ms = op_gb_batch_autotune(s.c, queries, nqueries, reps, best);
+    if (best_ms) *best_ms = ms;
   });
 }
 

@@ -146,6 +146,11 @@ void op_group_by_i64(Ctx& c, const fdb_dev_column& key, const fdb_dev_column& va
                      const fdb_pred_term* prog, int nterms, const fdb_dev_column* pred_cols,
                      int npred, uint64_t expected_groups, double load_factor,
                      fdb_group_i64* d_groups, uint64_t capacity, uint64_t* d_ngroups);
+struct BatchPlan;
+BatchPlan* op_gb_batch_prepare(Ctx& c, const fdb_gb_query* qs, int nq, const fdb_batch_tuning* t);
+void op_gb_batch_run(BatchPlan* p);
+void op_gb_batch_free(BatchPlan* p);
+double op_gb_batch_autotune(Ctx& c, const fdb_gb_query* qs, int nq, int reps, fdb_batch_tuning* best);
 void op_topk(Ctx& c, const fdb_dev_column& col, uint64_t n, uint32_t k, bool desc,
              bool nulls_last, uint32_t* d_rows, uint64_t* d_count);
 

@@ -23,6 +23,7 @@
 
 #include "common.cuh"
 #include "engine.h"
+#include "gtable.cuh"
 #include "stream.cuh"
 
 namespace fdb {
@@ -404,21 +405,6 @@ struct GbLaneOp {
 // ===========================================================================
 // 2. int64-key hash GROUP BY
 // ===========================================================================
-struct GSlot {          // 40 bytes; all-zero = empty
-  uint64_t key;         // key ^ 2^63
-  unsigned long long count;
-  double sum;
-  unsigned long long nmin;  // ~order key of MIN (atomicMax)
-  unsigned long long max;   // order key of MAX
-};
-
-constexpr uint32_t kSmemSlots = 1024;      // CTA table slots (power of two)
-#ifndef FDB_GB_SMEM_PROBE
-#define FDB_GB_SMEM_PROBE 4
-#endif
-constexpr uint32_t kSmemProbe = FDB_GB_SMEM_PROBE;  // probes before a row spills to global
-constexpr uint32_t kGlobalProbeLimit = 1u << 16;
-
 struct GbHashParams {
   PredProg prog;
   DevCol cols[4];          // 0 = key, 1 = value, 2.. = predicate columns
@@ -428,46 +414,9 @@ struct GbHashParams {
   int* err;
 };
 
-__device__ __forceinline__ void gslot_accum(GSlot* s, double v, bool has_v) {
-  atomicAdd(&s->count, 1ull);
-  if (has_v) {
-    atomicAdd(&s->sum, v);
-    if (!isnan(v)) {
-      const uint64_t k = f64_ord_key(v);
-      atomicMax(&s->nmin, (unsigned long long)~k);
-      atomicMax(&s->max, (unsigned long long)k);
-    }
-  }
-}
-
-__device__ __forceinline__ void gslot_merge(GSlot* s, const GSlot& v) {
-  atomicAdd(&s->count, v.count);
-  atomicAdd(&s->sum, v.sum);
-  atomicMax(&s->nmin, v.nmin);
-  atomicMax(&s->max, v.max);
-}
-
-// Find or claim the slot of `skey` (key ^ 2^63, nonzero) in a global table.
-// A table that is too small (more groups than slots) fails fast: the probe is
-// capped, the error word is set, and every later insert sees the error word
-// and gives up at once, so the kernel still ends promptly.
+// Find or claim the slot of `skey` (key ^ 2^63, nonzero) in the global table.
 __device__ __forceinline__ GSlot* gtable_slot(const GbHashParams& p, uint64_t skey) {
-  if (*reinterpret_cast<volatile int*>(p.err) != 0) return nullptr;
-  uint64_t h = mix64(skey) & p.mask;
-  const uint64_t limit = umin64(p.mask + 1, kGlobalProbeLimit);
-  for (uint64_t probe = 0; probe < limit; ++probe) {
-    GSlot* s = p.table + h;
-    uint64_t cur = *reinterpret_cast<volatile uint64_t*>(&s->key);
-    if (cur == skey) return s;
-    if (cur == 0) {
-      const uint64_t prev = atomicCAS(reinterpret_cast<unsigned long long*>(&s->key), 0ull,
-                                      (unsigned long long)skey);
-      if (prev == 0 || prev == skey) return s;
-    }
-    h = (h + 1) & p.mask;
-  }
-  atomicExch(p.err, kErrCapacity);
-  return nullptr;
+  return gtable_find(p.table, p.mask, skey, p.err);
 }
 
 struct GbHashOp {
@@ -504,19 +453,7 @@ struct GbHashOp {
         continue;
       }
       const uint64_t skey = (uint64_t)key ^ (1ull << 63);
-      uint32_t h = (uint32_t)mix64(skey) & (kSmemSlots - 1);
-      GSlot* dst = nullptr;
-      for (uint32_t probe = 0; probe < kSmemProbe; ++probe) {
-        GSlot* s = tab + h;
-        const uint64_t cur = *reinterpret_cast<volatile uint64_t*>(&s->key);
-        if (cur == skey) { dst = s; break; }
-        if (cur == 0) {
-          const uint64_t prev = atomicCAS(reinterpret_cast<unsigned long long*>(&s->key), 0ull,
-                                          (unsigned long long)skey);
-          if (prev == 0 || prev == skey) { dst = s; break; }
-        }
-        h = (h + 1) & (kSmemSlots - 1);
-      }
+      GSlot* dst = smem_table_slot(tab, skey);
       if (dst == nullptr) dst = gtable_slot(p, skey);
       if (dst) gslot_accum(dst, v, has_v);
     }
@@ -564,13 +501,7 @@ __global__ void gb_hash_compact_kernel(const GSlot* __restrict__ table, uint64_t
     if (live) {
       const uint64_t pos = base + __popc(m & ((1u << lane) - 1u));
       if (pos < cap_out) {
-        fdb_group_i64 g;
-        g.key = (int64_t)(s.key ^ (1ull << 63));
-        g.count = (int64_t)s.count;
-        g.sum = s.sum;
-        g.min = s.nmin ? f64_from_ord_key(~s.nmin) : __longlong_as_double(0x7ff8000000000000ll);
-        g.max = s.max ? f64_from_ord_key(s.max) : __longlong_as_double(0x7ff8000000000000ll);
-        out[pos] = g;
+        out[pos] = gslot_group(s.key, s);
       } else {
         atomicExch(err, kErrCapacity);
       }

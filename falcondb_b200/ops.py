@@ -344,5 +344,89 @@ def topk(db: Database, col: ColArg, nrows: int, k: int, desc: bool, nulls_last: 
     return rows, count
 
 
+class GroupByBatch:
+    """Many int64-key GROUP BY queries (COUNT(*), SUM, MIN, MAX of a value
+    column) captured as one CUDA graph: fdb_gb_batch_prepare / _run / _free.
+    ``queries`` = [(key, value, nrows)] with key / value column arguments (a
+    slice of a table is a tensor view); outputs are allocated here, one
+    (groups, count) pair per query, ``capacity`` groups each (default nrows)."""
+
+    def __init__(self, db: Database, queries: Sequence[Tuple[ColArg, ColArg, int]],
+                 tuning: Optional[Tuple[float, int, int]] = None, expected_groups: Optional[Sequence[int]] = None,
+                 capacity: Optional[Sequence[int]] = None):
+        from . import fdb_batch_tuning, fdb_gb_query
+        self.db = db
+        nq = len(queries)
+        arr = (fdb_gb_query * max(1, nq))()
+        dev = _dev(db)
+        self.outs: List[Tuple[torch.Tensor, torch.Tensor]] = []
+        self._keep = list(queries)
+        for i, (k, v, n) in enumerate(queries):
+            cap = int(capacity[i]) if capacity is not None else max(1, int(n) + 1)
+            groups = _bytes(GROUP_I64_DTYPE.itemsize * cap, db)
+            count = torch.zeros(1, dtype=torch.int64, device=dev)
+            self.outs.append((groups, count))
+            arr[i].key = dev_column(k)
+            arr[i].value = dev_column(v)
+            arr[i].nrows = int(n)
+            arr[i].expected_groups = int(expected_groups[i]) if expected_groups is not None else 0
+            arr[i].d_groups = groups.data_ptr()
+            arr[i].capacity = cap
+            arr[i].d_ngroups = count.data_ptr()
+        self._arr, self._nq = arr, nq
+        t = fdb_batch_tuning(*(tuning or (0.0, 0, 0)))
+        h = C.c_void_p()
+        with _Fenced(db):
+            check(lib().fdb_gb_batch_prepare(db.handle, arr, nq, C.byref(t), C.byref(h)))
+        self._h = h
+
+    def run(self) -> None:
+        """Replay the batch on the context stream (asynchronous)."""
+        with _Fenced(self.db):
+            check(lib().fdb_gb_batch_run(self._h))
+
+    def results(self, i: int) -> np.ndarray:
+        """Query i's groups as a record array (GROUP_I64_DTYPE), unordered."""
+        groups, count = self.outs[i]
+        return to_records(groups, GROUP_I64_DTYPE, int(count.item()))
+
+    def free(self) -> None:
+        if getattr(self, "_h", None) is not None and self._h.value:
+            lib().fdb_gb_batch_free(self._h)
+        self._h = None
+
+    def __del__(self):
+        try:
+            self.free()
+        except Exception:
+            pass
+
+    @staticmethod
+    def autotune(db: Database, queries: Sequence[Tuple[ColArg, ColArg, int]], reps: int = 3,
+                 expected_groups: Optional[Sequence[int]] = None) -> Tuple[Tuple[float, int, int], float]:
+        """The fastest (load_factor, ctas_per_sm, tile_rows) for these queries and its ms per run."""
+        from . import fdb_batch_tuning, fdb_gb_query
+        nq = len(queries)
+        arr = (fdb_gb_query * max(1, nq))()
+        dev = _dev(db)
+        keep = []
+        for i, (k, v, n) in enumerate(queries):
+            groups = _bytes(GROUP_I64_DTYPE.itemsize * (int(n) + 1), db)
+            count = torch.zeros(1, dtype=torch.int64, device=dev)
+            keep += [groups, count]
+            arr[i].key = dev_column(k)
+            arr[i].value = dev_column(v)
+            arr[i].nrows = int(n)
+            arr[i].expected_groups = int(expected_groups[i]) if expected_groups is not None else 0
+            arr[i].d_groups = groups.data_ptr()
+            arr[i].capacity = int(n) + 1
+            arr[i].d_ngroups = count.data_ptr()
+        best = fdb_batch_tuning()
+        ms = C.c_double()
+        with _Fenced(db):
+            check(lib().fdb_gb_batch_autotune(db.handle, arr, nq, reps, C.byref(best), C.byref(ms)))
+        return (best.load_factor, best.ctas_per_sm, best.tile_rows), ms.value
+
+
 def synchronize(db: Database) -> None:
     db.synchronize()

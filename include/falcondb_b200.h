@@ -356,6 +356,47 @@ int fdb_join_probe_pairs(fdb_db* db, const fdb_hash* h, const fdb_dev_column* pr
 int fdb_topk(fdb_db* db, const fdb_dev_column* col, uint64_t nrows, uint32_t k,
              int32_t desc, int32_t nulls_last, uint32_t* d_rows, uint64_t* d_count);
 
+/* ---- Batched GROUP BY -------------------------------------------------------
+ * Many independent `GROUP BY key` queries (COUNT(*), SUM, MIN, MAX of one
+ * value column, each over its own rows, e.g. slices of one table) run as one
+ * persistent kernel plus one compaction kernel, captured into a CUDA graph at
+ * prepare time and replayed by each run.  The reference answers each query
+ * with its own GroupByExec::execute (fast_i64_gb, aggregate.rs:840-912); each
+ * query's result equals fdb_group_by_i64 on its rows (groups unordered). */
+typedef struct fdb_gb_query {
+    fdb_dev_column key;        /* FDB_INT64; values point at the query's first row */
+    fdb_dev_column value;      /* FDB_FLOAT64 or FDB_INT64, same rows              */
+    uint64_t       nrows;
+    uint64_t       expected_groups;  /* 0: estimated by a HyperLogLog pass      */
+    fdb_group_i64* d_groups;   /* output groups (device), `capacity` entries     */
+    uint64_t       capacity;
+    uint64_t*      d_ngroups;  /* output group count (device)                     */
+} fdb_gb_query;
+
+/* Launch shape and table sizing of a batch; zero fields take defaults
+ * (load factor 0.5, 2 CTAs per SM, 8192-row tiles). */
+typedef struct fdb_batch_tuning {
+    double  load_factor;       /* table slots = 2 x expected groups / load_factor, pow2 */
+    int32_t ctas_per_sm;       /* persistent CTAs per SM (capped by occupancy)    */
+    int32_t tile_rows;         /* rows per claimed work unit (>= 256)             */
+} fdb_batch_tuning;
+
+typedef struct fdb_batch fdb_batch;
+
+/* Size the queries' tables (one device arena), upload their descriptors and
+ * capture the batch into a CUDA graph.  Inputs and outputs must stay valid
+ * while the batch exists. */
+int fdb_gb_batch_prepare(fdb_db* db, const fdb_gb_query* queries, int32_t nqueries,
+                         const fdb_batch_tuning* tuning, fdb_batch** out);
+/* Replay the batch on the context stream (asynchronous). */
+int fdb_gb_batch_run(fdb_batch* b);
+void fdb_gb_batch_free(fdb_batch* b);
+/* Autotuner (replaces the reference's fixed parallel cut-offs, tuning.rs:39-53):
+ * times every (load factor, CTAs per SM, tile rows) candidate on these queries
+ * and returns the fastest in *best and its time per run in *best_ms. */
+int fdb_gb_batch_autotune(fdb_db* db, const fdb_gb_query* queries, int32_t nqueries, int32_t reps,
+                          fdb_batch_tuning* best, double* best_ms);
+
 /* Library version string. */
 const char* fdb_version(void);
 
