@@ -94,6 +94,34 @@ class fdb_batch_tuning(C.Structure):
     _fields_ = [("load_factor", C.c_double), ("ctas_per_sm", C.c_int32), ("tile_rows", C.c_int32)]
 
 
+class fdb_serve_query(C.Structure):
+    _fields_ = [("kind", C.c_int32), ("k", C.c_int32), ("nrows", C.c_uint64), ("threshold", C.c_double),
+                ("c0", C.c_void_p), ("c1", C.c_void_p), ("c2", C.c_void_p), ("dict_len", C.c_uint32),
+                ("_pad", C.c_uint32), ("table", C.c_void_p), ("arrival_s", C.c_double)]
+
+
+SERVE_MAX_GROUPS, SERVE_MAX_K = 16, 32
+SERVE_COUNT, SERVE_GROUP, SERVE_JOIN, SERVE_TOPK = range(4)
+
+
+class fdb_serve_result(C.Structure):
+    _fields_ = [("count", C.c_int64), ("sum_payload", C.c_int64),
+                ("group_count", C.c_int64 * SERVE_MAX_GROUPS), ("group_sum0", C.c_double * SERVE_MAX_GROUPS),
+                ("group_sum2", C.c_int64 * SERVE_MAX_GROUPS), ("rows", C.c_uint32 * SERVE_MAX_K),
+                ("arrival_s", C.c_double), ("start_s", C.c_double), ("done_s", C.c_double),
+                ("batch_size", C.c_int32), ("status", C.c_int32)]
+
+
+class fdb_serve_config(C.Structure):
+    _fields_ = [("max_batch", C.c_int32), ("slots", C.c_int32), ("mem_budget", C.c_uint64)]
+
+
+class fdb_serve_stats(C.Structure):
+    _fields_ = [("wall_s", C.c_double), ("qps", C.c_double), ("p50_ms", C.c_double), ("p99_ms", C.c_double),
+                ("max_ms", C.c_double), ("mean_batch", C.c_double), ("batches", C.c_int64),
+                ("peak_reserved", C.c_uint64), ("resident_bytes", C.c_uint64)]
+
+
 AGG_VALUE_DTYPE = np.dtype([("f", "<f8"), ("i", "<i8"), ("n", "<i8"), ("is_int", "<i4"), ("valid", "<i4")])
 JOIN_AGG_DTYPE = np.dtype([("count", "<i8"), ("sum_payload", "<i8"), ("sum_value", "<f8"),
                            ("payload_rows", "<i8")])
@@ -161,6 +189,12 @@ _SIGS = {
     "fdb_gb_batch_free": (None, [C.c_void_p]),
     "fdb_gb_batch_autotune": (C.c_int, [C.c_void_p, C.POINTER(fdb_gb_query), C.c_int32, C.c_int32,
                                         C.POINTER(fdb_batch_tuning), C.POINTER(C.c_double)]),
+    "fdb_server_start": (C.c_int, [C.c_void_p, C.POINTER(fdb_serve_config), C.POINTER(C.c_void_p)]),
+    "fdb_server_submit": (C.c_int, [C.c_void_p, C.POINTER(fdb_serve_query), C.POINTER(C.c_uint64)]),
+    "fdb_server_wait": (C.c_int, [C.c_void_p, C.c_uint64, C.c_int64, C.POINTER(fdb_serve_result)]),
+    "fdb_server_stop": (C.c_int, [C.c_void_p, C.POINTER(fdb_serve_stats)]),
+    "fdb_serve_trace": (C.c_int, [C.c_void_p, C.POINTER(fdb_serve_query), C.c_int32, C.POINTER(fdb_serve_config),
+                                  C.POINTER(fdb_serve_result), C.POINTER(fdb_serve_stats)]),
 }
 
 EXPORTED = tuple(_SIGS)

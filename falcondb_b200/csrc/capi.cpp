@@ -20,12 +20,20 @@ struct fdb_hash {
   fdb::HashTable* h = nullptr;
   fdb_db* db = nullptr;
 };
+struct fdb_server {
+  fdb::Server* s = nullptr;
+  fdb_db* db = nullptr;
+};
 struct fdb_batch {
   fdb::BatchPlan* plan = nullptr;
   fdb_db* db = nullptr;
 };
 
 namespace fdb {
+HashTable* hash_of(const fdb_hash* h) {
+  if (!h || !h->h) fail(FDB_E_ARG, "null join table");
+  return h->h;
+}
 
 static thread_local std::string g_last_error;
 
@@ -637,6 +645,52 @@ int fdb_gb_batch_autotune(fdb_db* db, const fdb_gb_query* queries, int32_t nquer
     CallScope s(db, default_scratch(db->ctx));
     const double ms = op_gb_batch_autotune(s.c, queries, nqueries, reps, best);
     if (best_ms) *best_ms = ms;
+  });
+}
+
+int fdb_server_start(fdb_db* db, const fdb_serve_config* cfg, fdb_server** out) {
+  if (out) *out = nullptr;
+  if (!db || !out) return set_error(FDB_E_ARG, "fdb_server_start: bad arguments");
+  return guarded([&] {
+    std::lock_guard<std::recursive_mutex> lk(db->ctx.mu);
+    FDB_CUDA(cudaSetDevice(db->ctx.device));
+    std::unique_ptr<fdb_server> h(new fdb_server());
+    h->db = db;
+    h->s = server_start(db, db->ctx, cfg);
+    *out = h.release();
+  });
+}
+
+int fdb_server_submit(fdb_server* s, const fdb_serve_query* q, uint64_t* ticket) {
+  if (!s || !q || !ticket) return set_error(FDB_E_ARG, "fdb_server_submit: bad arguments");
+  return guarded([&] { *ticket = server_submit(*s->s, *q, -1.0); });
+}
+
+int fdb_server_wait(fdb_server* s, uint64_t ticket, int64_t timeout_ns, fdb_serve_result* out) {
+  if (!s) return set_error(FDB_E_ARG, "fdb_server_wait: bad arguments");
+  bool ok = false;
+  const int rc = guarded([&] { ok = server_wait(*s->s, ticket, timeout_ns, out); });
+  if (rc < 0) return rc;
+  return ok ? FDB_OK : set_error(FDB_E_TIMEOUT, "fdb_server_wait: not answered yet");
+}
+
+int fdb_server_stop(fdb_server* s, fdb_serve_stats* stats) {
+  if (!s) return set_error(FDB_E_ARG, "fdb_server_stop: bad arguments");
+  const int rc = guarded([&] { server_stop(s->s, stats); });
+  delete s;
+  return rc;
+}
+
+int fdb_serve_trace(fdb_db* db, const fdb_serve_query* queries, int32_t nqueries, const fdb_serve_config* cfg,
+                    fdb_serve_result* out, fdb_serve_stats* stats) {
+  if (!db || (nqueries && !queries)) return set_error(FDB_E_ARG, "fdb_serve_trace: bad arguments");
+  return guarded([&] {
+    {
+      std::lock_guard<std::recursive_mutex> lk(db->ctx.mu);
+      FDB_CUDA(cudaSetDevice(db->ctx.device));
+      FDB_CUDA(cudaStreamSynchronize(db->ctx.stream));  // tables and hash tables are built
+    }
+    serve_trace(db, db->ctx, queries, nqueries, cfg, out, stats);
   });
 }
 

@@ -146,6 +146,28 @@ void op_group_by_i64(Ctx& c, const fdb_dev_column& key, const fdb_dev_column& va
                      const fdb_pred_term* prog, int nterms, const fdb_dev_column* pred_cols,
                      int npred, uint64_t expected_groups, double load_factor,
                      fdb_group_i64* d_groups, uint64_t capacity, uint64_t* d_ngroups);
+struct HashTable;  // join build side (k_join.cu)
+// Device pointers of a join build table for kernels outside k_join.cu.
+struct JoinView {
+  const void* slots;         // JSlot[cap + 1]
+  const unsigned int* cnt;   // build rows per slot
+  uint64_t cap;
+  int32_t unique;
+  int32_t _pad;
+};
+JoinView join_view(const HashTable* h);
+
+HashTable* hash_of(const fdb_hash* h);  // the build side behind a C handle
+
+// Serving loop (serve.cu).
+struct Server;
+Server* server_start(fdb_db* db, Ctx& c, const fdb_serve_config* cfg);
+uint64_t server_submit(Server& s, const fdb_serve_query& q, double arrival_s);  // arrival_s < 0: now
+bool server_wait(Server& s, uint64_t ticket, int64_t timeout_ns, fdb_serve_result* out);  // false: timed out
+void server_stop(Server* s, fdb_serve_stats* st);
+void serve_trace(fdb_db* db, Ctx& c, const fdb_serve_query* qs, int nq, const fdb_serve_config* cfg,
+                 fdb_serve_result* out, fdb_serve_stats* st);
+
 struct BatchPlan;
 BatchPlan* op_gb_batch_prepare(Ctx& c, const fdb_gb_query* qs, int nq, const fdb_batch_tuning* t);
 void op_gb_batch_run(BatchPlan* p);

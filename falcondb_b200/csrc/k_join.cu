@@ -22,27 +22,10 @@
 
 #include "common.cuh"
 #include "engine.h"
+#include "join_table.cuh"
 #include "stream.cuh"
 
 namespace fdb {
-
-struct JSlot {
-  unsigned long long key;   // key ^ 2^63; 0 = empty
-  unsigned long long psum;  // SUM of non-NULL payloads (two's complement)
-};
-
-constexpr uint32_t kNoSlot = 0xFFFFFFFFu;
-
-// Home slot of a stored key in a table of 2^(64-shift) slots: multiplicative
-// (Fibonacci) hashing, the top bits of key * 2^64/phi.  One 64-bit multiply
-// and a shift; consecutive keys land far apart, so linear probing stays
-// short on the dense integer keys joins usually have.  The choice of hash is
-// not observable in any result (the reference mixes with int_key_hash,
-// join.rs:1368-1374).
-__host__ __device__ __forceinline__ uint64_t join_hash(uint64_t sk, int shift) {
-  return (sk * 0x9E3779B97F4A7C15ull) >> shift;
-}
-__device__ __forceinline__ int join_shift(uint64_t cap) { return __clzll((long long)cap) + 1; }  // cap = 2^b
 
 struct HashTable {
   Ctx* ctx = nullptr;
@@ -262,27 +245,13 @@ void join_free(HashTable* h) {
 }
 uint64_t join_capacity(const HashTable* h) { return h ? h->cap : 0; }
 
-// Slot of probe key k, or kNoSlot.
-__device__ __forceinline__ uint32_t join_find(const JSlot* __restrict__ slots, const unsigned int* cnt,
-                                              uint64_t cap, int64_t k, JSlot* out) {
-  if (k == INT64_MIN) {
-    if (cnt[cap] == 0u) return kNoSlot;
-    *out = slots[cap];
-    return (uint32_t)cap;
-  }
-  const unsigned long long sk = (unsigned long long)k ^ (1ull << 63);
-  const uint64_t mask = cap - 1;
-  uint64_t h = join_hash(sk, join_shift(cap));
-  for (uint64_t probe = 0; probe <= mask; ++probe) {
-    const JSlot s = slots[h];
-    if (s.key == sk) {
-      *out = s;
-      return (uint32_t)h;
-    }
-    if (s.key == 0ull) return kNoSlot;
-    h = (h + 1) & mask;
-  }
-  return kNoSlot;
+JoinView join_view(const HashTable* h) {
+  JoinView v;
+  v.slots = h->slots.ptr;
+  v.cnt = static_cast<const unsigned int*>(h->cnt.ptr);
+  v.cap = h->cap;
+  v.unique = h->unique ? 1 : 0;
+  return v;
 }
 
 // ---------------------------------------------------------------------------

@@ -1,0 +1,721 @@
+// Serving loop: continuous batching of queries over device-resident tables.
+//
+// A scheduler thread owns `slots` launch slots.  Each slot has a stream, a
+// pinned input buffer (a batch header and one descriptor per query), a pinned
+// output buffer (one result per query) and a CUDA graph captured once:
+//   H2D descriptors -> zero results -> serve_kernel -> serve_finish_kernel ->
+//   D2H results (+ the slot's error word).
+// Whenever a slot is free and queries are waiting, the scheduler admits them
+// in arrival order while the device-memory budget allows (resident tables plus
+// what admitted queries hold) up to max_batch, writes their descriptors and
+// replays the slot's graph; batches on different slots overlap on the GPU.  A
+// slot's results are handed out when its completion event fires.
+//
+// serve_kernel is persistent: the batch's rows are cut into kServeTile-row
+// tiles, numbered query by query, and CTAs claim tile numbers from an atomic
+// counter.  A CTA keeps per-query state (counts in registers, GROUP BY tables
+// per warp in shared memory, a top-k list per warp) while its consecutive
+// tiles belong to one query, and publishes it with atomics when it moves on —
+// so a query touched by G CTAs costs G atomic merges, whatever its size.
+// Top-k queries publish each CTA's k best (below the query's running bound)
+// as candidates; serve_finish_kernel reduces them, one CTA per query.
+#include <algorithm>
+#include <atomic>
+#include <chrono>
+#include <condition_variable>
+#include <cstring>
+#include <deque>
+#include <memory>
+#include <mutex>
+#include <thread>
+#include <unordered_map>
+#include <vector>
+
+#include "common.cuh"
+#include "engine.h"
+#include "join_table.cuh"
+#include "topk_warp.cuh"
+
+namespace fdb {
+
+constexpr int kServeThreads = 256;
+constexpr int kServeWarps = kServeThreads / 32;
+constexpr uint32_t kServeTile = 8192;
+constexpr int kServeMaxBatch = 256;
+constexpr int kServeCtasPerSm = 2;
+
+struct ServeQ {            // device descriptor of one query
+  int32_t kind, k;
+  uint64_t n, tile0;
+  double thr;
+  const void* c0;
+  const void* c1;
+  const void* c2;
+  uint32_t dict_len, _pad;
+  const JSlot* slots;
+  const unsigned int* cnt;
+  uint64_t cap;
+  int32_t unique, _pad2;
+};
+
+struct ServeRes {          // device result of one query (and its host copy)
+  unsigned long long count;
+  long long sum;
+  unsigned long long nbound;   // TOPK: ~(best published k-th order key); 0 = none
+  unsigned int ncand, _pad;
+  unsigned long long gcount[FDB_SERVE_MAX_GROUPS];
+  double gsum0[FDB_SERVE_MAX_GROUPS];
+  long long gsum2[FDB_SERVE_MAX_GROUPS];
+  uint32_t rows[FDB_SERVE_MAX_K];
+};
+
+struct ServeHeader {
+  int32_t nq, _pad;
+  uint64_t total_tiles;
+};
+
+struct ServeArgs {
+  const ServeHeader* hdr;
+  const ServeQ* q;
+  ServeRes* res;
+  unsigned int* claim;       // zero at launch (after res in the same memset)
+  uint64_t* cand_k;          // [kServeMaxBatch][cand_cap]
+  uint32_t* cand_r;
+  uint32_t cand_cap;
+  int* err;
+};
+
+struct ServeSmem {
+  uint64_t start[kServeMaxBatch + 1];
+  unsigned long long gcount[kServeWarps][FDB_SERVE_MAX_GROUPS];
+  double gsum0[kServeWarps][FDB_SERVE_MAX_GROUPS];
+  long long gsum2[kServeWarps][FDB_SERVE_MAX_GROUPS];
+  uint64_t tkeys[kServeWarps][32];
+  uint32_t trows[kServeWarps][32];
+  unsigned long long red[kServeWarps][2];
+  unsigned int t;
+};
+
+__device__ __forceinline__ int serve_find(const uint64_t* start, int nq, uint64_t t) {
+  int lo = 0, hi = nq;  // start[lo] <= t < start[hi]
+  while (hi - lo > 1) {
+    const int mid = (lo + hi) >> 1;
+    if (start[mid] <= t) lo = mid; else hi = mid;
+  }
+  return lo;
+}
+
+// Merge every warp's list into warp 0 (sorted-list merges, log2(warps) levels).
+__device__ void serve_tree_merge(ServeSmem& sm, RTLocal& s, uint32_t k, int warp, int lane) {
+  for (int half = kServeWarps / 2; half >= 1; half >>= 1) {
+    __syncthreads();
+    if (warp >= half && warp < 2 * half) {
+      const bool in = (uint32_t)lane < k;
+      sm.tkeys[warp][lane] = in ? s.lk : ~0ull;
+      sm.trows[warp][lane] = in ? s.lr : 0xFFFFFFFFu;
+    }
+    __syncthreads();
+    if (warp < half) rt_merge_sorted(s, k, sm.tkeys[warp + half][lane], sm.trows[warp + half][lane], lane);
+  }
+  __syncthreads();
+}
+
+__device__ __forceinline__ void rt_reset(RTLocal& s) {
+  s.lk = ~0ull;
+  s.lr = 0xFFFFFFFFu;
+  s.tk = ~0ull;
+  s.tr = 0xFFFFFFFFu;
+  s.steps = 0;
+}
+
+// Publish this CTA's state for query qi (all threads call; ends with a barrier).
+__device__ void serve_publish(const ServeArgs& a, const ServeQ& q, int qi, ServeSmem& sm, unsigned long long& cnt,
+                              long long& sum, RTLocal& tl) {
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  ServeRes& r = a.res[qi];
+  if (q.kind == FDB_SERVE_COUNT || q.kind == FDB_SERVE_JOIN) {
+    const unsigned long long c = warp_sum_u64(cnt);
+    const unsigned long long sv = warp_sum_u64((unsigned long long)sum);
+    if (lane == 0) {
+      sm.red[warp][0] = c;
+      sm.red[warp][1] = sv;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      unsigned long long tc = 0, ts = 0;
+      for (int w = 0; w < kServeWarps; ++w) {
+        tc += sm.red[w][0];
+        ts += sm.red[w][1];
+      }
+      if (tc) atomicAdd(&r.count, tc);
+      if (ts) atomicAdd(reinterpret_cast<unsigned long long*>(&r.sum), ts);
+    }
+  } else if (q.kind == FDB_SERVE_GROUP) {
+    __syncthreads();
+    const uint32_t g = threadIdx.x;
+    if (g < q.dict_len) {
+      unsigned long long c = 0;
+      double s0 = 0.0;
+      long long s2 = 0;
+      for (int w = 0; w < kServeWarps; ++w) {
+        c += sm.gcount[w][g];
+        s0 += sm.gsum0[w][g];
+        s2 += sm.gsum2[w][g];
+      }
+      if (c) {
+        atomicAdd(&r.gcount[g], c);
+        atomicAdd(&r.gsum0[g], s0);
+        atomicAdd(reinterpret_cast<unsigned long long*>(&r.gsum2[g]), (unsigned long long)s2);
+      }
+    }
+    __syncthreads();
+    for (uint32_t i = threadIdx.x; i < kServeWarps * FDB_SERVE_MAX_GROUPS; i += blockDim.x) {
+      (&sm.gcount[0][0])[i] = 0;
+      (&sm.gsum0[0][0])[i] = 0.0;
+      (&sm.gsum2[0][0])[i] = 0;
+    }
+  } else {  // TOPK
+    const uint32_t k = (uint32_t)q.k;
+    serve_tree_merge(sm, tl, k, warp, lane);
+    if (warp == 0) {
+      const uint64_t kk = __shfl_sync(0xffffffffu, tl.lk, k - 1);
+      const uint32_t kr = __shfl_sync(0xffffffffu, tl.lr, k - 1);
+      if (lane == 0 && !(kk == ~0ull && kr == 0xFFFFFFFFu)) atomicMax(&r.nbound, ~kk);
+      const uint64_t bound = ~*reinterpret_cast<volatile unsigned long long*>(&r.nbound);
+      const bool emit = (uint32_t)lane < k && !(tl.lk == ~0ull && tl.lr == 0xFFFFFFFFu) && tl.lk <= bound;
+      const unsigned m = __ballot_sync(0xffffffffu, emit);
+      if (m) {
+        unsigned int base = 0;
+        if (lane == 0) base = atomicAdd(&r.ncand, (unsigned int)__popc(m));
+        base = __shfl_sync(0xffffffffu, base, 0);
+        if (emit) {
+          const uint32_t pos = base + __popc(m & ((1u << lane) - 1u));
+          if (pos < a.cand_cap) {
+            a.cand_k[(size_t)qi * a.cand_cap + pos] = tl.lk;
+            a.cand_r[(size_t)qi * a.cand_cap + pos] = tl.lr;
+          } else {
+            atomicExch(a.err, kErrCapacity);
+          }
+        }
+      }
+    }
+    rt_reset(tl);
+  }
+  cnt = 0;
+  sum = 0;
+  __syncthreads();
+}
+
+__device__ __forceinline__ void serve_tile(const ServeQ& q, ServeSmem& sm, uint64_t r0, uint64_t r1,
+                                           unsigned long long& cnt, long long& sum, RTLocal& tl) {
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  if (q.kind == FDB_SERVE_COUNT) {
+    const double* c0 = static_cast<const double*>(q.c0);
+    for (uint64_t r = r0 + threadIdx.x; r < r1; r += blockDim.x) cnt += __ldcs(c0 + r) > q.thr;
+  } else if (q.kind == FDB_SERVE_GROUP) {
+    const double* c0 = static_cast<const double*>(q.c0);
+    const uint32_t* c1 = static_cast<const uint32_t*>(q.c1);
+    const int64_t* c2 = static_cast<const int64_t*>(q.c2);
+    for (uint64_t r = r0 + threadIdx.x; r < r1; r += blockDim.x) {
+      const double v = __ldcs(c0 + r);
+      const uint32_t g = __ldcs(c1 + r);
+      if (v > q.thr && g < q.dict_len) {
+        atomicAdd(&sm.gcount[warp][g], 1ull);
+        atomicAdd(&sm.gsum0[warp][g], v);
+        atomicAdd(reinterpret_cast<unsigned long long*>(&sm.gsum2[warp][g]), (unsigned long long)__ldcs(c2 + r));
+      }
+    }
+  } else if (q.kind == FDB_SERVE_JOIN) {
+    const int64_t* c0 = static_cast<const int64_t*>(q.c0);
+    const double* c1 = static_cast<const double*>(q.c1);
+    const double lim = q.thr / 100.0;
+    const int shift = join_shift(q.cap);
+    const uint64_t mask = q.cap - 1;
+    for (uint64_t r = r0 + threadIdx.x; r < r1; r += blockDim.x) {
+      if (!(__ldcs(c1 + r) < lim)) continue;
+      const int64_t k = __ldcs(c0 + r);
+      uint32_t at = kNoSlot;
+      uint64_t ps = 0;
+      if (k == INT64_MIN) {
+        if (q.cnt[q.cap] != 0u) {
+          at = (uint32_t)q.cap;
+          ps = q.slots[q.cap].psum;
+        }
+      } else {
+        const uint64_t sk = (uint64_t)k ^ (1ull << 63);
+        uint64_t h = join_hash(sk, shift);
+        for (uint64_t probe = 0; probe <= mask; ++probe) {
+          const JSlot s = q.slots[h];
+          if (s.key == sk) {
+            at = (uint32_t)h;
+            ps = s.psum;
+            break;
+          }
+          if (s.key == 0ull) break;
+          h = (h + 1) & mask;
+        }
+      }
+      if (at != kNoSlot) {
+        cnt += q.unique ? 1ull : (unsigned long long)q.cnt[at];
+        sum += (long long)ps;
+      }
+    }
+  } else {  // TOPK: WHERE c0 < thr ORDER BY c0 DESC
+    const uint64_t* c0 = static_cast<const uint64_t*>(q.c0);
+    const uint32_t k = (uint32_t)q.k;
+    for (uint64_t b = r0 + (uint64_t)warp * 256; b < r1; b += 256 * kServeWarps) {
+      uint64_t v[8];
+      uint32_t vm = 0;
+#pragma unroll
+      for (int j = 0; j < 8; ++j) {
+        const uint64_t i = b + j * 32 + lane;
+        v[j] = 0;
+        if (i < r1) {
+          v[j] = __ldcs(c0 + i);
+          vm |= 1u << j;
+        }
+      }
+      const double tv = f64_from_ord_key(~tl.tk);  // threshold's value (DESC keys)
+      uint32_t pm = 0;
+#pragma unroll
+      for (int j = 0; j < 8; ++j) {
+        const double x = __longlong_as_double((long long)v[j]);
+        if (x < q.thr && !(x < tv)) pm |= 1u << j;
+      }
+      pm &= vm;
+      if (!__any_sync(0xffffffffu, pm != 0u)) continue;
+      uint64_t key[8];
+      uint32_t row[8];
+      uint32_t m = 0;
+#pragma unroll
+      for (int j = 0; j < 8; ++j) {
+        key[j] = wt_key<FDB_FLOAT64, true>(v[j]);
+        row[j] = (uint32_t)(b + j * 32 + lane);
+        if (((pm >> j) & 1u) && kr_le(key[j], row[j], tl.tk, tl.tr)) m |= 1u << j;
+      }
+      if (__any_sync(0xffffffffu, m != 0u)) rt_offer<8>(tl, k, key, row, m, lane);
+    }
+  }
+}
+
+__global__ void __launch_bounds__(kServeThreads) serve_kernel(ServeArgs a) {
+  __shared__ ServeSmem sm;
+  const int nq = a.hdr->nq;
+  const uint64_t total = a.hdr->total_tiles;
+  for (int i = threadIdx.x; i < nq; i += blockDim.x) sm.start[i] = a.q[i].tile0;
+  if (threadIdx.x == 0) sm.start[nq] = total;
+  for (uint32_t i = threadIdx.x; i < kServeWarps * FDB_SERVE_MAX_GROUPS; i += blockDim.x) {
+    (&sm.gcount[0][0])[i] = 0;
+    (&sm.gsum0[0][0])[i] = 0.0;
+    (&sm.gsum2[0][0])[i] = 0;
+  }
+  __syncthreads();
+  unsigned long long cnt = 0;
+  long long sum = 0;
+  RTLocal tl;
+  rt_reset(tl);
+  int cur = -1;
+  for (;;) {
+    if (threadIdx.x == 0) sm.t = atomicAdd(a.claim, 1u);
+    __syncthreads();
+    const uint64_t t = sm.t;
+    if (t >= total) break;
+    const int qi = serve_find(sm.start, nq, t);
+    if (qi != cur) {
+      if (cur >= 0) serve_publish(a, a.q[cur], cur, sm, cnt, sum, tl);
+      cur = qi;
+    }
+    const ServeQ& q = a.q[qi];
+    if (q.kind == FDB_SERVE_TOPK) {  // start from the query's published bound
+      const uint64_t b = ~*reinterpret_cast<volatile unsigned long long*>(&a.res[qi].nbound);
+      rt_bound(tl, b);
+    }
+    const uint64_t r0 = (t - q.tile0) * kServeTile;
+    serve_tile(q, sm, r0, umin64(r0 + kServeTile, q.n), cnt, sum, tl);
+    __syncthreads();  // the tile is done before sm.t is rewritten
+  }
+  if (cur >= 0) serve_publish(a, a.q[cur], cur, sm, cnt, sum, tl);
+}
+
+// Top-k queries: the k best of the CTAs' candidates, one CTA per query.
+__global__ void __launch_bounds__(kServeThreads) serve_finish_kernel(ServeArgs a) {
+  __shared__ ServeSmem sm;
+  const int qi = blockIdx.x;
+  if (qi >= a.hdr->nq) return;
+  const ServeQ& q = a.q[qi];
+  if (q.kind != FDB_SERVE_TOPK) return;
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const uint32_t k = (uint32_t)q.k;
+  ServeRes& r = a.res[qi];
+  const uint32_t nc = min(r.ncand, a.cand_cap);
+  RTLocal tl;
+  rt_reset(tl);
+  rt_bound(tl, ~r.nbound);
+  const uint64_t* ck = a.cand_k + (size_t)qi * a.cand_cap;
+  const uint32_t* cr = a.cand_r + (size_t)qi * a.cand_cap;
+  for (uint32_t b = warp * 256; b < nc; b += 256 * kServeWarps) {
+    uint64_t key[8];
+    uint32_t row[8];
+    uint32_t m = 0;
+#pragma unroll
+    for (int j = 0; j < 8; ++j) {
+      const uint32_t i = b + j * 32 + lane;
+      key[j] = ~0ull;
+      row[j] = 0xFFFFFFFFu;
+      if (i < nc) {
+        key[j] = ck[i];
+        row[j] = cr[i];
+        if (kr_le(key[j], row[j], tl.tk, tl.tr)) m |= 1u << j;
+      }
+    }
+    if (__any_sync(0xffffffffu, m != 0u)) rt_offer<8>(tl, k, key, row, m, lane);
+  }
+  serve_tree_merge(sm, tl, k, warp, lane);
+  if (warp == 0) {
+    const bool real = (uint32_t)lane < k && !(tl.lk == ~0ull && tl.lr == 0xFFFFFFFFu);
+    const unsigned vb = __ballot_sync(0xffffffffu, real);
+    if (real) r.rows[lane] = tl.lr;
+    if (lane == 0) r.count = (unsigned long long)__popc(vb);
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Host: slots, scheduler, trace driver
+// ---------------------------------------------------------------------------
+using Clock = std::chrono::steady_clock;
+
+struct ServeSlot {
+  cudaStream_t stream = nullptr;
+  cudaEvent_t done = nullptr;
+  unsigned char* h_in = nullptr;   // ServeHeader + ServeQ[kServeMaxBatch] (pinned)
+  ServeRes* h_out = nullptr;       // [kServeMaxBatch] (pinned)
+  int* h_err = nullptr;            // (pinned)
+  DevBuf d_in, d_res, d_cand_k, d_cand_r, d_err;
+  cudaGraph_t graph = nullptr;
+  cudaGraphExec_t exec = nullptr;
+  std::vector<uint64_t> tickets;
+  bool busy = false;
+};
+
+struct ServeJob {
+  fdb_serve_query q;
+  fdb_serve_result r;
+  uint64_t bytes = 0;
+  bool done = false;
+};
+
+struct Server {
+  fdb_db* db = nullptr;
+  Ctx* c = nullptr;
+  fdb_serve_config cfg{};
+  std::vector<ServeSlot> slots;
+  std::thread thr;
+  std::mutex mu;
+  std::condition_variable cv;
+  std::deque<uint64_t> queue;
+  std::unordered_map<uint64_t, ServeJob> jobs;
+  uint64_t next_ticket = 1;
+  bool stopping = false;
+  uint64_t budget = 0, resident = 0, reserved = 0, peak_reserved = 0;
+  int64_t batches = 0, batched_queries = 0;
+  std::vector<double> latencies;
+  double first_arrival = 1e300, last_done = 0.0;
+  Clock::time_point t0;
+  uint32_t cand_cap = 0;
+  int grid = 0;
+  std::string error;
+
+  double now() const { return std::chrono::duration<double>(Clock::now() - t0).count(); }
+};
+
+static constexpr size_t kServeInBytes = sizeof(ServeHeader) + sizeof(ServeQ) * kServeMaxBatch;
+static constexpr size_t kServeResBytes = sizeof(ServeRes) * kServeMaxBatch;
+
+static uint64_t serve_query_bytes(const fdb_serve_query& q, uint32_t cand_cap) {
+  return sizeof(ServeQ) + sizeof(ServeRes) + (q.kind == FDB_SERVE_TOPK ? (uint64_t)cand_cap * 12 : 0);
+}
+
+static void serve_check(const fdb_serve_query& q) {
+  if (q.kind < FDB_SERVE_COUNT || q.kind > FDB_SERVE_TOPK) fail(FDB_E_ARG, "unknown serving template");
+  if (q.nrows >= 0xFFFFFFFFull) fail(FDB_E_ARG, "a served query addresses rows as uint32");
+  if (q.nrows && !q.c0) fail(FDB_E_ARG, "query without its column");
+  if (q.kind == FDB_SERVE_GROUP && (q.dict_len == 0 || q.dict_len > FDB_SERVE_MAX_GROUPS || (q.nrows && (!q.c1 || !q.c2))))
+    fail(FDB_E_ARG, "GROUP needs codes (dict_len 1..16) and an INT64 column");
+  if (q.kind == FDB_SERVE_JOIN && (!q.table || (q.nrows && !q.c1)))
+    fail(FDB_E_ARG, "JOIN needs a build table and a value column");
+  if (q.kind == FDB_SERVE_TOPK && (q.k < 1 || q.k > FDB_SERVE_MAX_K)) fail(FDB_E_ARG, "TOPK needs 1 <= k <= 32");
+}
+
+static void slot_capture(Server& s, ServeSlot& sl) {
+  Ctx& c = *s.c;
+  ServeArgs a;
+  a.hdr = static_cast<const ServeHeader*>(sl.d_in.ptr);
+  a.q = reinterpret_cast<const ServeQ*>(static_cast<unsigned char*>(sl.d_in.ptr) + sizeof(ServeHeader));
+  a.res = static_cast<ServeRes*>(sl.d_res.ptr);
+  a.claim = reinterpret_cast<unsigned int*>(static_cast<unsigned char*>(sl.d_res.ptr) + kServeResBytes);
+  a.cand_k = static_cast<uint64_t*>(sl.d_cand_k.ptr);
+  a.cand_r = static_cast<uint32_t*>(sl.d_cand_r.ptr);
+  a.cand_cap = s.cand_cap;
+  a.err = static_cast<int*>(sl.d_err.ptr);
+  FDB_CUDA(cudaStreamBeginCapture(sl.stream, cudaStreamCaptureModeThreadLocal));
+  cudaMemcpyAsync(sl.d_in.ptr, sl.h_in, kServeInBytes, cudaMemcpyHostToDevice, sl.stream);
+  cudaMemsetAsync(sl.d_res.ptr, 0, kServeResBytes + 256, sl.stream);
+  serve_kernel<<<s.grid, kServeThreads, 0, sl.stream>>>(a);
+  serve_finish_kernel<<<kServeMaxBatch, kServeThreads, 0, sl.stream>>>(a);
+  cudaMemcpyAsync(sl.h_out, sl.d_res.ptr, kServeResBytes, cudaMemcpyDeviceToHost, sl.stream);
+  cudaMemcpyAsync(sl.h_err, sl.d_err.ptr, sizeof(int), cudaMemcpyDeviceToHost, sl.stream);
+  cudaMemsetAsync(sl.d_err.ptr, 0, sizeof(int), sl.stream);
+  FDB_CUDA(cudaStreamEndCapture(sl.stream, &sl.graph));
+  FDB_CUDA(cudaGraphInstantiate(&sl.exec, sl.graph, 0));
+}
+
+static void server_destroy(Server* s) {
+  if (!s) return;
+  for (ServeSlot& sl : s->slots) {
+    if (sl.stream) cudaStreamSynchronize(sl.stream);
+    if (sl.exec) cudaGraphExecDestroy(sl.exec);
+    if (sl.graph) cudaGraphDestroy(sl.graph);
+    if (sl.done) cudaEventDestroy(sl.done);
+    if (sl.stream) cudaStreamDestroy(sl.stream);
+    if (sl.h_in) cudaFreeHost(sl.h_in);
+    if (sl.h_out) cudaFreeHost(sl.h_out);
+    if (sl.h_err) cudaFreeHost(sl.h_err);
+    s->c->free_buf(sl.d_in);
+    s->c->free_buf(sl.d_res);
+    s->c->free_buf(sl.d_cand_k);
+    s->c->free_buf(sl.d_cand_r);
+    s->c->free_buf(sl.d_err);
+  }
+  delete s;
+}
+
+// Hand out a finished slot's results (scheduler thread, s.mu held).
+static void slot_complete(Server& s, ServeSlot& sl) {
+  const double t = s.now();
+  const int err = *sl.h_err;
+  const int n = (int)sl.tickets.size();
+  for (int i = 0; i < n; ++i) {
+    ServeJob& j = s.jobs[sl.tickets[i]];
+    const ServeRes& d = sl.h_out[i];
+    fdb_serve_result& r = j.r;
+    r.count = (int64_t)d.count;
+    r.sum_payload = d.sum;
+    for (int g = 0; g < FDB_SERVE_MAX_GROUPS; ++g) {
+      r.group_count[g] = (int64_t)d.gcount[g];
+      r.group_sum0[g] = d.gsum0[g];
+      r.group_sum2[g] = d.gsum2[g];
+    }
+    std::memcpy(r.rows, d.rows, sizeof(r.rows));
+    r.done_s = t;
+    r.batch_size = n;
+    r.status = err ? (err == kErrCapacity ? FDB_E_CAPACITY : FDB_E_TIMEOUT) : FDB_OK;
+    j.done = true;
+    s.reserved -= j.bytes;
+    s.latencies.push_back(t - r.arrival_s);
+    s.first_arrival = std::min(s.first_arrival, r.arrival_s);
+    s.last_done = std::max(s.last_done, t);
+  }
+  sl.tickets.clear();
+  sl.busy = false;
+}
+
+// Admit queued queries into a free slot and launch it (s.mu held).
+static bool slot_launch(Server& s, ServeSlot& sl) {
+  ServeHeader* hdr = reinterpret_cast<ServeHeader*>(sl.h_in);
+  ServeQ* dq = reinterpret_cast<ServeQ*>(sl.h_in + sizeof(ServeHeader));
+  const uint64_t room = s.budget > s.resident ? s.budget - s.resident : 0;
+  const double t = s.now();
+  uint64_t tiles = 0;
+  int n = 0;
+  while (!s.queue.empty() && n < s.cfg.max_batch) {
+    ServeJob& j = s.jobs[s.queue.front()];
+    if (s.reserved + j.bytes > room && n > 0) break;  // wait for memory (a lone query always runs)
+    const fdb_serve_query& q = j.q;
+    ServeQ& d = dq[n];
+    std::memset(&d, 0, sizeof(d));
+    d.kind = q.kind;
+    d.k = q.k;
+    d.n = q.nrows;
+    d.tile0 = tiles;
+    tiles += (q.nrows + kServeTile - 1) / kServeTile;
+    d.thr = q.threshold;
+    d.c0 = q.c0;
+    d.c1 = q.c1;
+    d.c2 = q.c2;
+    d.dict_len = q.dict_len;
+    if (q.kind == FDB_SERVE_JOIN) {
+      const JoinView v = join_view(hash_of(q.table));
+      d.slots = static_cast<const JSlot*>(v.slots);
+      d.cnt = v.cnt;
+      d.cap = v.cap;
+      d.unique = v.unique;
+    }
+    s.reserved += j.bytes;
+    s.peak_reserved = std::max(s.peak_reserved, s.reserved);
+    j.r.start_s = t;
+    sl.tickets.push_back(s.queue.front());
+    s.queue.pop_front();
+    ++n;
+  }
+  if (n == 0) return false;
+  hdr->nq = n;
+  hdr->total_tiles = tiles;
+  FDB_CUDA(cudaGraphLaunch(sl.exec, sl.stream));
+  FDB_CUDA(cudaEventRecord(sl.done, sl.stream));
+  sl.busy = true;
+  ++s.batches;
+  s.batched_queries += n;
+  return true;
+}
+
+static void server_loop(Server* s) {
+  cudaSetDevice(s->c->device);
+  for (;;) {
+    bool progress = false, idle = true;
+    {
+      std::unique_lock<std::mutex> lk(s->mu);
+      for (ServeSlot& sl : s->slots) {
+        if (!sl.busy) continue;
+        const cudaError_t q = cudaEventQuery(sl.done);
+        if (q == cudaSuccess) {
+          slot_complete(*s, sl);
+          progress = true;
+        } else if (q != cudaErrorNotReady) {
+          s->error = cudaGetErrorString(q);
+          slot_complete(*s, sl);
+          progress = true;
+        }
+      }
+      try {
+        for (ServeSlot& sl : s->slots)
+          if (!sl.busy && !s->queue.empty()) progress |= slot_launch(*s, sl);
+      } catch (const Error& e) {
+        s->error = e.what();
+      }
+      for (ServeSlot& sl : s->slots) idle &= !sl.busy;
+      if (progress) s->cv.notify_all();
+      if (s->stopping && idle && s->queue.empty()) break;
+    }
+    if (!progress) std::this_thread::yield();
+  }
+}
+
+Server* server_start(fdb_db* db, Ctx& c, const fdb_serve_config* cfg) {
+  std::unique_ptr<Server, void (*)(Server*)> s(new Server(), server_destroy);
+  s->db = db;
+  s->c = &c;
+  s->cfg.max_batch = cfg && cfg->max_batch > 0 ? std::min(cfg->max_batch, kServeMaxBatch) : 128;
+  s->cfg.slots = cfg && cfg->slots > 0 ? std::min(cfg->slots, 8) : 4;
+  s->budget = cfg && cfg->mem_budget ? cfg->mem_budget : c.budget;
+  s->cfg.mem_budget = s->budget;
+  s->resident = c.in_use.load();
+  s->grid = c.sm_count * kServeCtasPerSm;
+  s->cand_cap = (uint32_t)s->grid * FDB_SERVE_MAX_K;
+  s->slots.resize(s->cfg.slots);
+  for (ServeSlot& sl : s->slots) {
+    FDB_CUDA(cudaStreamCreateWithFlags(&sl.stream, cudaStreamNonBlocking));
+    FDB_CUDA(cudaEventCreateWithFlags(&sl.done, cudaEventDisableTiming));
+    FDB_CUDA(cudaHostAlloc(reinterpret_cast<void**>(&sl.h_in), kServeInBytes, cudaHostAllocDefault));
+    FDB_CUDA(cudaHostAlloc(reinterpret_cast<void**>(&sl.h_out), kServeResBytes, cudaHostAllocDefault));
+    FDB_CUDA(cudaHostAlloc(reinterpret_cast<void**>(&sl.h_err), sizeof(int), cudaHostAllocDefault));
+    std::memset(sl.h_in, 0, kServeInBytes);
+    *sl.h_err = 0;
+    sl.d_in = c.alloc_buf(kServeInBytes);
+    sl.d_res = c.alloc_buf(kServeResBytes + 256);
+    sl.d_cand_k = c.alloc_buf((size_t)kServeMaxBatch * s->cand_cap * 8);
+    sl.d_cand_r = c.alloc_buf((size_t)kServeMaxBatch * s->cand_cap * 4);
+    sl.d_err = c.alloc_buf(256);
+    FDB_CUDA(cudaMemset(sl.d_err.ptr, 0, 256));
+    slot_capture(*s, sl);
+  }
+  s->t0 = Clock::now();
+  Server* raw = s.release();
+  raw->thr = std::thread(server_loop, raw);
+  return raw;
+}
+
+uint64_t server_submit(Server& s, const fdb_serve_query& q, double arrival_s) {
+  serve_check(q);
+  std::lock_guard<std::mutex> lk(s.mu);
+  if (s.stopping) fail(FDB_E_ARG, "the server is stopping");
+  const uint64_t t = s.next_ticket++;
+  ServeJob& j = s.jobs[t];
+  j.q = q;
+  std::memset(&j.r, 0, sizeof(j.r));
+  j.r.arrival_s = arrival_s >= 0 ? arrival_s : s.now();
+  j.bytes = serve_query_bytes(q, s.cand_cap);
+  s.queue.push_back(t);
+  return t;
+}
+
+bool server_wait(Server& s, uint64_t ticket, int64_t timeout_ns, fdb_serve_result* out) {
+  std::unique_lock<std::mutex> lk(s.mu);
+  auto it = s.jobs.find(ticket);
+  if (it == s.jobs.end()) fail(FDB_E_ARG, "unknown ticket");
+  const auto until = Clock::now() + std::chrono::nanoseconds(timeout_ns < 0 ? 0 : timeout_ns);
+  while (!it->second.done) {
+    if (timeout_ns >= 0 && Clock::now() >= until) return false;
+    if (timeout_ns >= 0)
+      s.cv.wait_until(lk, until);
+    else
+      s.cv.wait(lk);
+  }
+  if (out) *out = it->second.r;
+  s.jobs.erase(it);
+  return true;
+}
+
+double server_now(Server& s) { return s.now(); }
+
+void server_stop(Server* s, fdb_serve_stats* st) {
+  {
+    std::lock_guard<std::mutex> lk(s->mu);
+    s->stopping = true;
+  }
+  if (s->thr.joinable()) s->thr.join();
+  if (st) {
+    std::memset(st, 0, sizeof(*st));
+    std::vector<double> l = s->latencies;
+    std::sort(l.begin(), l.end());
+    auto pct = [&](double p) { return l.empty() ? 0.0 : l[std::min(l.size() - 1, (size_t)(p * (l.size() - 1) + 0.5))]; };
+    st->wall_s = l.empty() ? 0.0 : s->last_done - s->first_arrival;
+    st->qps = st->wall_s > 0 ? (double)l.size() / st->wall_s : 0.0;
+    st->p50_ms = pct(0.50) * 1e3;
+    st->p99_ms = pct(0.99) * 1e3;
+    st->max_ms = l.empty() ? 0.0 : l.back() * 1e3;
+    st->batches = s->batches;
+    st->mean_batch = s->batches ? (double)s->batched_queries / (double)s->batches : 0.0;
+    st->peak_reserved = s->peak_reserved;
+    st->resident_bytes = s->resident;
+  }
+  const std::string err = s->error;
+  server_destroy(s);
+  if (!err.empty()) fail(FDB_E_CUDA, "serving loop: " + err);
+}
+
+// Submit the trace's queries at their arrival times (this thread spins for
+// the last 100 us before each), then collect every result.
+void serve_trace(fdb_db* db, Ctx& c, const fdb_serve_query* qs, int nq, const fdb_serve_config* cfg,
+                 fdb_serve_result* out, fdb_serve_stats* st) {
+  for (int i = 0; i < nq; ++i) serve_check(qs[i]);
+  Server* s = server_start(db, c, cfg);
+  std::vector<uint64_t> tickets(nq);
+  try {
+    for (int i = 0; i < nq; ++i) {
+      const double at = qs[i].arrival_s;
+      for (;;) {
+        const double wait = at - s->now();
+        if (wait <= 0) break;
+        if (wait > 2e-4) std::this_thread::sleep_for(std::chrono::duration<double>(wait - 1e-4));
+      }
+      tickets[i] = server_submit(*s, qs[i], at);
+    }
+    for (int i = 0; i < nq; ++i) server_wait(*s, tickets[i], -1, out ? out + i : nullptr);
+  } catch (...) {
+    server_stop(s, nullptr);
+    throw;
+  }
+  server_stop(s, st);
+}
+
+}  // namespace fdb

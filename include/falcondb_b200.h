@@ -397,6 +397,90 @@ void fdb_gb_batch_free(fdb_batch* b);
 int fdb_gb_batch_autotune(fdb_db* db, const fdb_gb_query* queries, int32_t nqueries, int32_t reps,
                           fdb_batch_tuning* best, double* best_ms);
 
+/* ---- Serving loop ------------------------------------------------------------
+ * A request loop over device-resident tables with continuous batching: queries
+ * are admitted under a device-memory budget as they arrive, and whatever has
+ * been admitted when a launch slot frees up goes to the GPU as one batch, run
+ * by one persistent kernel (plus a top-k finish kernel) replayed from a CUDA
+ * graph; batches on different slots overlap on the device.  No counterpart in
+ * the reference, whose server (src/bin/server.rs:151-169) runs each request
+ * through Database::sql on its own.
+ *
+ * Templates (over rows [0, nrows) of the given columns, literal x):
+ *   FDB_SERVE_COUNT   SELECT COUNT(*) WHERE c0 > x                 (c0 FLOAT64)
+ *   FDB_SERVE_GROUP   SELECT c1, COUNT(*), SUM(c0), SUM(c2) WHERE c0 > x GROUP BY c1
+ *                     (c0 FLOAT64, c1 dictionary codes < dict_len <= 16, c2 INT64;
+ *                      AVG(c2) = SUM / COUNT)
+ *   FDB_SERVE_JOIN    SELECT COUNT(*), SUM(payload) FROM probe JOIN build ON c0 = key
+ *                     WHERE c1 < x / 100                           (c0 INT64 keys,
+ *                      c1 FLOAT64, `table` the resident build side)
+ *   FDB_SERVE_TOPK    SELECT row WHERE c0 < x ORDER BY c0 DESC LIMIT k   (k <= 32;
+ *                      ties by row ascending)
+ * Columns hold no NULLs. */
+#define FDB_SERVE_COUNT 0
+#define FDB_SERVE_GROUP 1
+#define FDB_SERVE_JOIN  2
+#define FDB_SERVE_TOPK  3
+#define FDB_SERVE_MAX_GROUPS 16
+#define FDB_SERVE_MAX_K 32
+
+typedef struct fdb_serve_query {
+    int32_t     kind;          /* FDB_SERVE_*                                    */
+    int32_t     k;             /* TOPK: LIMIT                                    */
+    uint64_t    nrows;
+    double      threshold;     /* the literal x                                  */
+    const void* c0;
+    const void* c1;
+    const void* c2;
+    uint32_t    dict_len;      /* GROUP                                          */
+    uint32_t    _pad;
+    fdb_hash*   table;         /* JOIN                                           */
+    double      arrival_s;     /* fdb_serve_trace: seconds after the trace starts */
+} fdb_serve_query;
+
+typedef struct fdb_serve_result {
+    int64_t  count;            /* COUNT rows / JOIN rows / TOPK rows returned    */
+    int64_t  sum_payload;      /* JOIN                                           */
+    int64_t  group_count[FDB_SERVE_MAX_GROUPS];
+    double   group_sum0[FDB_SERVE_MAX_GROUPS];
+    int64_t  group_sum2[FDB_SERVE_MAX_GROUPS];
+    uint32_t rows[FDB_SERVE_MAX_K];
+    double   arrival_s, start_s, done_s;   /* admitted at start_s, result on host at done_s */
+    int32_t  batch_size;       /* queries in the launch that answered it         */
+    int32_t  status;           /* FDB_OK or an error code                         */
+} fdb_serve_result;
+
+typedef struct fdb_serve_config {
+    int32_t  max_batch;        /* queries per launch (1 = one query at a time)    */
+    int32_t  slots;            /* launches in flight                              */
+    uint64_t mem_budget;       /* bytes resident tables + admitted queries may hold; 0 = the context's budget */
+} fdb_serve_config;
+
+typedef struct fdb_serve_stats {
+    double   wall_s;           /* first arrival to last result                    */
+    double   qps;
+    double   p50_ms, p99_ms, max_ms;   /* latency = done_s - arrival_s              */
+    double   mean_batch;
+    int64_t  batches;
+    uint64_t peak_reserved;    /* peak bytes held by admitted queries             */
+    uint64_t resident_bytes;   /* device bytes of the context when serving started */
+} fdb_serve_stats;
+
+typedef struct fdb_server fdb_server;
+
+/* Start the scheduler thread (it owns `slots` streams and launch graphs). */
+int fdb_server_start(fdb_db* db, const fdb_serve_config* cfg, fdb_server** out);
+/* Queue a query; *ticket identifies it.  Returns at once. */
+int fdb_server_submit(fdb_server* s, const fdb_serve_query* q, uint64_t* ticket);
+/* Wait up to timeout_ns for a ticket's result (FDB_E_TIMEOUT if not ready). */
+int fdb_server_wait(fdb_server* s, uint64_t ticket, int64_t timeout_ns, fdb_serve_result* out);
+/* Drain, stop the thread, free the slots; *stats summarises every answered query. */
+int fdb_server_stop(fdb_server* s, fdb_serve_stats* stats);
+/* Replay an arrival trace: each query is submitted at its arrival_s (in
+ * order), results land in out[i]; returns when all are answered. */
+int fdb_serve_trace(fdb_db* db, const fdb_serve_query* queries, int32_t nqueries,
+                    const fdb_serve_config* cfg, fdb_serve_result* out, fdb_serve_stats* stats);
+
 /* Library version string. */
 const char* fdb_version(void);
 
