@@ -11,14 +11,20 @@
 // replays the slot's graph; batches on different slots overlap on the GPU.  A
 // slot's results are handed out when its completion event fires.
 //
-// serve_kernel is persistent: the batch's rows are cut into kServeTile-row
-// tiles, numbered query by query, and CTAs claim tile numbers from an atomic
-// counter.  A CTA keeps per-query state (counts in registers, GROUP BY tables
-// per warp in shared memory, a top-k list per warp) while its consecutive
-// tiles belong to one query, and publishes it with atomics when it moves on —
-// so a query touched by G CTAs costs G atomic merges, whatever its size.
-// Top-k queries publish each CTA's k best (below the query's running bound)
-// as candidates; serve_finish_kernel reduces them, one CTA per query.
+// serve_kernel is persistent and scans shared: the batch's COUNT, GROUP and
+// JOIN queries are grouped by the table they read, and each group's rows are
+// cut into kShareTile-row units.  A CTA that claims a unit stages the rows'
+// columns in shared memory once (for a join group it also probes every row
+// once: whether a build row matches does not depend on the query) and then
+// evaluates every query of the group that covers the unit from shared memory,
+// each with its own predicate.  HBM therefore sees each table once per batch,
+// not once per query.  Partial results go out with one atomic per warp (COUNT,
+// JOIN) or per group and field (GROUP BY) per query and unit.
+// Top-k queries scan their own rows in kServeTile-row units claimed after the
+// shared ones: a CTA keeps a list per warp while its consecutive units belong
+// to one query and publishes its k best (below the query's running bound) as
+// candidates when it moves on; serve_finish_kernel reduces them, one CTA per
+// query.
 #include <algorithm>
 #include <atomic>
 #include <chrono>
@@ -42,7 +48,10 @@ constexpr int kServeThreads = 256;
 constexpr int kServeWarps = kServeThreads / 32;
 constexpr uint32_t kServeTile = 8192;
 constexpr int kServeMaxBatch = 256;
-constexpr int kServeCtasPerSm = 2;
+constexpr int kServeCtasPerSm = 3;
+constexpr uint32_t kShareTile = 2048;
+// Shared-scan staging: c0 (8 B/row), c1 (<= 8 B/row), c2 (8 B/row), matches (4 B/row).
+constexpr size_t kShareSmem = (size_t)kShareTile * (8 + 8 + 8 + 4);
 
 struct ServeQ {            // device descriptor of one query
   int32_t kind, k;
@@ -69,14 +78,31 @@ struct ServeRes {          // device result of one query (and its host copy)
   uint32_t rows[FDB_SERVE_MAX_K];
 };
 
+struct ServeG {             // a group of queries that read the same table
+  const void* c0;
+  const void* c1;
+  const void* c2;
+  uint32_t q0, nq;          // its queries, by rows descending
+  uint64_t max_n, unit0;
+  int32_t c1_bytes;         // 0 (not read), 4 (dictionary codes) or 8
+  int32_t load_c2;
+  int32_t join;             // c0 holds probe keys for the table below
+  int32_t unique;
+  const JSlot* slots;
+  const unsigned int* cnt;
+  uint64_t cap;
+};
+
 struct ServeHeader {
-  int32_t nq, _pad;
-  uint64_t total_tiles;
+  int32_t nq, ngroups;
+  int32_t topk0, _pad;      // top-k queries are descriptors [topk0, nq)
+  uint64_t shared_units, total_units;
 };
 
 struct ServeArgs {
   const ServeHeader* hdr;
   const ServeQ* q;
+  const ServeG* g;
   ServeRes* res;
   unsigned int* claim;       // zero at launch (after res in the same memset)
   uint64_t* cand_k;          // [kServeMaxBatch][cand_cap]
@@ -86,7 +112,8 @@ struct ServeArgs {
 };
 
 struct ServeSmem {
-  uint64_t start[kServeMaxBatch + 1];
+  uint64_t start[kServeMaxBatch + 1];   // unit0 of each top-k query
+  uint64_t gstart[kServeMaxBatch + 1];  // unit0 of each shared group
   unsigned long long gcount[kServeWarps][FDB_SERVE_MAX_GROUPS];
   double gsum0[kServeWarps][FDB_SERVE_MAX_GROUPS];
   long long gsum2[kServeWarps][FDB_SERVE_MAX_GROUPS];
@@ -128,190 +155,221 @@ __device__ __forceinline__ void rt_reset(RTLocal& s) {
   s.steps = 0;
 }
 
-// Publish this CTA's state for query qi (all threads call; ends with a barrier).
-__device__ void serve_publish(const ServeArgs& a, const ServeQ& q, int qi, ServeSmem& sm, unsigned long long& cnt,
-                              long long& sum, RTLocal& tl) {
+// Publish this CTA's top-k state for query qi (all threads call; ends with a barrier).
+__device__ void serve_publish(const ServeArgs& a, const ServeQ& q, int qi, ServeSmem& sm, RTLocal& tl) {
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   ServeRes& r = a.res[qi];
-  if (q.kind == FDB_SERVE_COUNT || q.kind == FDB_SERVE_JOIN) {
-    const unsigned long long c = warp_sum_u64(cnt);
-    const unsigned long long sv = warp_sum_u64((unsigned long long)sum);
-    if (lane == 0) {
-      sm.red[warp][0] = c;
-      sm.red[warp][1] = sv;
-    }
-    __syncthreads();
-    if (threadIdx.x == 0) {
-      unsigned long long tc = 0, ts = 0;
-      for (int w = 0; w < kServeWarps; ++w) {
-        tc += sm.red[w][0];
-        ts += sm.red[w][1];
-      }
-      if (tc) atomicAdd(&r.count, tc);
-      if (ts) atomicAdd(reinterpret_cast<unsigned long long*>(&r.sum), ts);
-    }
-  } else if (q.kind == FDB_SERVE_GROUP) {
-    __syncthreads();
-    const uint32_t g = threadIdx.x;
-    if (g < q.dict_len) {
-      unsigned long long c = 0;
-      double s0 = 0.0;
-      long long s2 = 0;
-      for (int w = 0; w < kServeWarps; ++w) {
-        c += sm.gcount[w][g];
-        s0 += sm.gsum0[w][g];
-        s2 += sm.gsum2[w][g];
-      }
-      if (c) {
-        atomicAdd(&r.gcount[g], c);
-        atomicAdd(&r.gsum0[g], s0);
-        atomicAdd(reinterpret_cast<unsigned long long*>(&r.gsum2[g]), (unsigned long long)s2);
-      }
-    }
-    __syncthreads();
-    for (uint32_t i = threadIdx.x; i < kServeWarps * FDB_SERVE_MAX_GROUPS; i += blockDim.x) {
-      (&sm.gcount[0][0])[i] = 0;
-      (&sm.gsum0[0][0])[i] = 0.0;
-      (&sm.gsum2[0][0])[i] = 0;
-    }
-  } else {  // TOPK
-    const uint32_t k = (uint32_t)q.k;
-    serve_tree_merge(sm, tl, k, warp, lane);
-    if (warp == 0) {
-      const uint64_t kk = __shfl_sync(0xffffffffu, tl.lk, k - 1);
-      const uint32_t kr = __shfl_sync(0xffffffffu, tl.lr, k - 1);
-      if (lane == 0 && !(kk == ~0ull && kr == 0xFFFFFFFFu)) atomicMax(&r.nbound, ~kk);
-      const uint64_t bound = ~*reinterpret_cast<volatile unsigned long long*>(&r.nbound);
-      const bool emit = (uint32_t)lane < k && !(tl.lk == ~0ull && tl.lr == 0xFFFFFFFFu) && tl.lk <= bound;
-      const unsigned m = __ballot_sync(0xffffffffu, emit);
-      if (m) {
-        unsigned int base = 0;
-        if (lane == 0) base = atomicAdd(&r.ncand, (unsigned int)__popc(m));
-        base = __shfl_sync(0xffffffffu, base, 0);
-        if (emit) {
-          const uint32_t pos = base + __popc(m & ((1u << lane) - 1u));
-          if (pos < a.cand_cap) {
-            a.cand_k[(size_t)qi * a.cand_cap + pos] = tl.lk;
-            a.cand_r[(size_t)qi * a.cand_cap + pos] = tl.lr;
-          } else {
-            atomicExch(a.err, kErrCapacity);
-          }
+  const uint32_t k = (uint32_t)q.k;
+  serve_tree_merge(sm, tl, k, warp, lane);
+  if (warp == 0) {
+    const uint64_t kk = __shfl_sync(0xffffffffu, tl.lk, k - 1);
+    const uint32_t kr = __shfl_sync(0xffffffffu, tl.lr, k - 1);
+    if (lane == 0 && !(kk == ~0ull && kr == 0xFFFFFFFFu)) atomicMax(&r.nbound, ~kk);
+    const uint64_t bound = ~*reinterpret_cast<volatile unsigned long long*>(&r.nbound);
+    const bool emit = (uint32_t)lane < k && !(tl.lk == ~0ull && tl.lr == 0xFFFFFFFFu) && tl.lk <= bound;
+    const unsigned m = __ballot_sync(0xffffffffu, emit);
+    if (m) {
+      unsigned int base = 0;
+      if (lane == 0) base = atomicAdd(&r.ncand, (unsigned int)__popc(m));
+      base = __shfl_sync(0xffffffffu, base, 0);
+      if (emit) {
+        const uint32_t pos = base + __popc(m & ((1u << lane) - 1u));
+        if (pos < a.cand_cap) {
+          a.cand_k[(size_t)qi * a.cand_cap + pos] = tl.lk;
+          a.cand_r[(size_t)qi * a.cand_cap + pos] = tl.lr;
+        } else {
+          atomicExch(a.err, kErrCapacity);
         }
       }
     }
-    rt_reset(tl);
   }
-  cnt = 0;
-  sum = 0;
+  rt_reset(tl);
   __syncthreads();
 }
 
-__device__ __forceinline__ void serve_tile(const ServeQ& q, ServeSmem& sm, uint64_t r0, uint64_t r1,
-                                           unsigned long long& cnt, long long& sum, RTLocal& tl) {
+// Rows [r0, r1) of a top-k query: WHERE c0 < thr ORDER BY c0 DESC into the warp lists.
+__device__ __forceinline__ void serve_topk_tile(const ServeQ& q, uint64_t r0, uint64_t r1, RTLocal& tl) {
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  if (q.kind == FDB_SERVE_COUNT) {
-    const double* c0 = static_cast<const double*>(q.c0);
-    for (uint64_t r = r0 + threadIdx.x; r < r1; r += blockDim.x) cnt += __ldcs(c0 + r) > q.thr;
-  } else if (q.kind == FDB_SERVE_GROUP) {
-    const double* c0 = static_cast<const double*>(q.c0);
-    const uint32_t* c1 = static_cast<const uint32_t*>(q.c1);
-    const int64_t* c2 = static_cast<const int64_t*>(q.c2);
-    for (uint64_t r = r0 + threadIdx.x; r < r1; r += blockDim.x) {
-      const double v = __ldcs(c0 + r);
-      const uint32_t g = __ldcs(c1 + r);
-      if (v > q.thr && g < q.dict_len) {
-        atomicAdd(&sm.gcount[warp][g], 1ull);
-        atomicAdd(&sm.gsum0[warp][g], v);
-        atomicAdd(reinterpret_cast<unsigned long long*>(&sm.gsum2[warp][g]), (unsigned long long)__ldcs(c2 + r));
+  const uint64_t* c0 = static_cast<const uint64_t*>(q.c0);
+  const uint32_t k = (uint32_t)q.k;
+  for (uint64_t b = r0 + (uint64_t)warp * 256; b < r1; b += 256 * kServeWarps) {
+    uint64_t v[8];
+    uint32_t vm = 0;
+#pragma unroll
+    for (int j = 0; j < 8; ++j) {
+      const uint64_t i = b + j * 32 + lane;
+      v[j] = 0;
+      if (i < r1) {
+        v[j] = __ldcs(c0 + i);
+        vm |= 1u << j;
       }
     }
-  } else if (q.kind == FDB_SERVE_JOIN) {
-    const int64_t* c0 = static_cast<const int64_t*>(q.c0);
-    const double* c1 = static_cast<const double*>(q.c1);
-    const double lim = q.thr / 100.0;
-    const int shift = join_shift(q.cap);
-    const uint64_t mask = q.cap - 1;
-    for (uint64_t r = r0 + threadIdx.x; r < r1; r += blockDim.x) {
-      if (!(__ldcs(c1 + r) < lim)) continue;
-      const int64_t k = __ldcs(c0 + r);
+    const double tv = f64_from_ord_key(~tl.tk);  // the threshold's value (DESC keys)
+    uint32_t pm = 0;
+#pragma unroll
+    for (int j = 0; j < 8; ++j) {
+      const double x = __longlong_as_double((long long)v[j]);
+      if (x < q.thr && !(x < tv)) pm |= 1u << j;
+    }
+    pm &= vm;
+    if (!__any_sync(0xffffffffu, pm != 0u)) continue;
+    uint64_t key[8];
+    uint32_t row[8];
+    uint32_t m = 0;
+#pragma unroll
+    for (int j = 0; j < 8; ++j) {
+      key[j] = wt_key<FDB_FLOAT64, true>(v[j]);
+      row[j] = (uint32_t)(b + j * 32 + lane);
+      if (((pm >> j) & 1u) && kr_le(key[j], row[j], tl.tk, tl.tr)) m |= 1u << j;
+    }
+    if (__any_sync(0xffffffffu, m != 0u)) rt_offer<8>(tl, k, key, row, m, lane);
+  }
+}
+
+// Copy rows [r0, r0 + rows) of a column (esize 4 or 8) into shared memory.
+__device__ __forceinline__ void share_load(unsigned char* dst, const void* src, uint64_t r0, uint32_t rows, int esize) {
+  const unsigned char* s = static_cast<const unsigned char*>(src) + r0 * esize;
+  const uint32_t bytes = rows * (uint32_t)esize;
+  uint32_t done = 0;
+  if (((uintptr_t)s & 15u) == 0) {
+    const uint32_t nv = bytes / 16;
+    for (uint32_t i = threadIdx.x; i < nv; i += blockDim.x)
+      reinterpret_cast<uint4*>(dst)[i] = __ldcs(reinterpret_cast<const uint4*>(s) + i);
+    done = nv * 16;
+  }
+  if (esize == 8) {
+    for (uint32_t i = done / 8 + threadIdx.x; i < rows; i += blockDim.x)
+      reinterpret_cast<uint64_t*>(dst)[i] = __ldcs(reinterpret_cast<const unsigned long long*>(s) + i);
+  } else {
+    for (uint32_t i = done / 4 + threadIdx.x; i < rows; i += blockDim.x)
+      reinterpret_cast<uint32_t*>(dst)[i] = __ldcs(reinterpret_cast<const unsigned int*>(s) + i);
+  }
+}
+
+// One shared unit: stage the group's rows, probe them once for a join group,
+// then evaluate every query of the group that reaches this unit.
+__device__ void serve_shared_unit(const ServeArgs& a, const ServeG& g, uint64_t tile, unsigned char* tsm,
+                                  ServeSmem& sm) {
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const uint64_t r0 = tile * kShareTile;
+  const uint32_t rows = (uint32_t)umin64(kShareTile, g.max_n - r0);
+  uint64_t* s0 = reinterpret_cast<uint64_t*>(tsm);
+  unsigned char* s1 = tsm + (size_t)kShareTile * 8;
+  const int64_t* s2 = reinterpret_cast<const int64_t*>(tsm + (size_t)kShareTile * 16);
+  uint32_t* smm = reinterpret_cast<uint32_t*>(tsm + (size_t)kShareTile * 24);
+  share_load(tsm, g.c0, r0, rows, 8);
+  if (g.c1_bytes) share_load(s1, g.c1, r0, rows, g.c1_bytes);
+  if (g.load_c2) share_load(tsm + (size_t)kShareTile * 16, g.c2, r0, rows, 8);
+  __syncthreads();
+  if (g.join) {  // row i's build matches and their payload sum replace its key
+    const int shift = join_shift(g.cap);
+    const uint64_t mask = g.cap - 1;
+    for (uint32_t i = threadIdx.x; i < rows; i += blockDim.x) {
+      const int64_t key = (int64_t)s0[i];
       uint32_t at = kNoSlot;
       uint64_t ps = 0;
-      if (k == INT64_MIN) {
-        if (q.cnt[q.cap] != 0u) {
-          at = (uint32_t)q.cap;
-          ps = q.slots[q.cap].psum;
+      if (key == INT64_MIN) {
+        if (g.cnt[g.cap] != 0u) {
+          at = (uint32_t)g.cap;
+          ps = g.slots[g.cap].psum;
         }
       } else {
-        const uint64_t sk = (uint64_t)k ^ (1ull << 63);
+        const uint64_t sk = (uint64_t)key ^ (1ull << 63);
         uint64_t h = join_hash(sk, shift);
         for (uint64_t probe = 0; probe <= mask; ++probe) {
-          const JSlot s = q.slots[h];
-          if (s.key == sk) {
+          const JSlot sl = g.slots[h];
+          if (sl.key == sk) {
             at = (uint32_t)h;
-            ps = s.psum;
+            ps = sl.psum;
             break;
           }
-          if (s.key == 0ull) break;
+          if (sl.key == 0ull) break;
           h = (h + 1) & mask;
         }
       }
-      if (at != kNoSlot) {
-        cnt += q.unique ? 1ull : (unsigned long long)q.cnt[at];
-        sum += (long long)ps;
-      }
+      smm[i] = at == kNoSlot ? 0u : (g.unique ? 1u : g.cnt[at]);
+      s0[i] = ps;
     }
-  } else {  // TOPK: WHERE c0 < thr ORDER BY c0 DESC
-    const uint64_t* c0 = static_cast<const uint64_t*>(q.c0);
-    const uint32_t k = (uint32_t)q.k;
-    for (uint64_t b = r0 + (uint64_t)warp * 256; b < r1; b += 256 * kServeWarps) {
-      uint64_t v[8];
-      uint32_t vm = 0;
-#pragma unroll
-      for (int j = 0; j < 8; ++j) {
-        const uint64_t i = b + j * 32 + lane;
-        v[j] = 0;
-        if (i < r1) {
-          v[j] = __ldcs(c0 + i);
-          vm |= 1u << j;
+    __syncthreads();
+  }
+  for (uint32_t qi = g.q0; qi < g.q0 + g.nq; ++qi) {
+    const ServeQ& q = a.q[qi];
+    if (q.n <= r0) break;  // queries are by rows descending
+    const uint32_t re = (uint32_t)umin64(rows, q.n - r0);
+    ServeRes& r = a.res[qi];
+    if (q.kind == FDB_SERVE_COUNT) {
+      unsigned long long c = 0;
+      for (uint32_t i = threadIdx.x; i < re; i += blockDim.x) c += __longlong_as_double((long long)s0[i]) > q.thr;
+      c = warp_sum_u64(c);
+      if (lane == 0 && c) atomicAdd(&r.count, c);
+    } else if (q.kind == FDB_SERVE_JOIN) {
+      const double lim = q.thr / 100.0;
+      const double* v = reinterpret_cast<const double*>(s1);
+      unsigned long long c = 0, ps = 0;
+      for (uint32_t i = threadIdx.x; i < re; i += blockDim.x)
+        if (v[i] < lim) {
+          c += smm[i];
+          ps += s0[i];
+        }
+      c = warp_sum_u64(c);
+      ps = warp_sum_u64(ps);
+      if (lane == 0 && c) {
+        atomicAdd(&r.count, c);
+        atomicAdd(reinterpret_cast<unsigned long long*>(&r.sum), ps);
+      }
+    } else {  // GROUP
+      if (lane < FDB_SERVE_MAX_GROUPS) {
+        sm.gcount[warp][lane] = 0;
+        sm.gsum0[warp][lane] = 0.0;
+        sm.gsum2[warp][lane] = 0;
+      }
+      __syncwarp();
+      const uint32_t* codes = reinterpret_cast<const uint32_t*>(s1);
+      for (uint32_t i = threadIdx.x; i < re; i += blockDim.x) {
+        const double v = __longlong_as_double((long long)s0[i]);
+        const uint32_t gc = codes[i];
+        if (v > q.thr && gc < q.dict_len) {
+          atomicAdd(&sm.gcount[warp][gc], 1ull);
+          atomicAdd(&sm.gsum0[warp][gc], v);
+          atomicAdd(reinterpret_cast<unsigned long long*>(&sm.gsum2[warp][gc]), (unsigned long long)s2[i]);
         }
       }
-      const double tv = f64_from_ord_key(~tl.tk);  // threshold's value (DESC keys)
-      uint32_t pm = 0;
-#pragma unroll
-      for (int j = 0; j < 8; ++j) {
-        const double x = __longlong_as_double((long long)v[j]);
-        if (x < q.thr && !(x < tv)) pm |= 1u << j;
+      __syncthreads();
+      if (threadIdx.x < q.dict_len) {
+        const uint32_t gc = threadIdx.x;
+        unsigned long long c = 0;
+        double v0 = 0.0;
+        long long v2 = 0;
+        for (int w = 0; w < kServeWarps; ++w) {
+          c += sm.gcount[w][gc];
+          v0 += sm.gsum0[w][gc];
+          v2 += sm.gsum2[w][gc];
+        }
+        if (c) {
+          atomicAdd(&r.gcount[gc], c);
+          atomicAdd(&r.gsum0[gc], v0);
+          atomicAdd(reinterpret_cast<unsigned long long*>(&r.gsum2[gc]), (unsigned long long)v2);
+        }
       }
-      pm &= vm;
-      if (!__any_sync(0xffffffffu, pm != 0u)) continue;
-      uint64_t key[8];
-      uint32_t row[8];
-      uint32_t m = 0;
-#pragma unroll
-      for (int j = 0; j < 8; ++j) {
-        key[j] = wt_key<FDB_FLOAT64, true>(v[j]);
-        row[j] = (uint32_t)(b + j * 32 + lane);
-        if (((pm >> j) & 1u) && kr_le(key[j], row[j], tl.tk, tl.tr)) m |= 1u << j;
-      }
-      if (__any_sync(0xffffffffu, m != 0u)) rt_offer<8>(tl, k, key, row, m, lane);
+      __syncthreads();
     }
   }
+  __syncthreads();  // before the next unit overwrites the staged rows
 }
 
 __global__ void __launch_bounds__(kServeThreads) serve_kernel(ServeArgs a) {
+  extern __shared__ __align__(16) unsigned char tsm[];
   __shared__ ServeSmem sm;
-  const int nq = a.hdr->nq;
-  const uint64_t total = a.hdr->total_tiles;
-  for (int i = threadIdx.x; i < nq; i += blockDim.x) sm.start[i] = a.q[i].tile0;
-  if (threadIdx.x == 0) sm.start[nq] = total;
-  for (uint32_t i = threadIdx.x; i < kServeWarps * FDB_SERVE_MAX_GROUPS; i += blockDim.x) {
-    (&sm.gcount[0][0])[i] = 0;
-    (&sm.gsum0[0][0])[i] = 0.0;
-    (&sm.gsum2[0][0])[i] = 0;
+  const int nq = a.hdr->nq, ng = a.hdr->ngroups, topk0 = a.hdr->topk0;
+  const int ntopk = nq - topk0;
+  const uint64_t shared = a.hdr->shared_units, total = a.hdr->total_units;
+  for (int i = threadIdx.x; i < ng; i += blockDim.x) sm.gstart[i] = a.g[i].unit0;
+  for (int i = threadIdx.x; i < ntopk; i += blockDim.x) sm.start[i] = a.q[topk0 + i].tile0;
+  if (threadIdx.x == 0) {
+    sm.gstart[ng] = shared;
+    sm.start[ntopk] = total;
   }
   __syncthreads();
-  unsigned long long cnt = 0;
-  long long sum = 0;
   RTLocal tl;
   rt_reset(tl);
   int cur = -1;
@@ -320,21 +378,23 @@ __global__ void __launch_bounds__(kServeThreads) serve_kernel(ServeArgs a) {
     __syncthreads();
     const uint64_t t = sm.t;
     if (t >= total) break;
-    const int qi = serve_find(sm.start, nq, t);
+    if (t < shared) {  // claims only grow, so a CTA is done with shared units before any top-k unit
+      const int gi = serve_find(sm.gstart, ng, t);
+      serve_shared_unit(a, a.g[gi], t - sm.gstart[gi], tsm, sm);
+      continue;
+    }
+    const int qi = topk0 + serve_find(sm.start, ntopk, t);
     if (qi != cur) {
-      if (cur >= 0) serve_publish(a, a.q[cur], cur, sm, cnt, sum, tl);
+      if (cur >= 0) serve_publish(a, a.q[cur], cur, sm, tl);
       cur = qi;
     }
     const ServeQ& q = a.q[qi];
-    if (q.kind == FDB_SERVE_TOPK) {  // start from the query's published bound
-      const uint64_t b = ~*reinterpret_cast<volatile unsigned long long*>(&a.res[qi].nbound);
-      rt_bound(tl, b);
-    }
+    rt_bound(tl, ~*reinterpret_cast<volatile unsigned long long*>(&a.res[qi].nbound));
     const uint64_t r0 = (t - q.tile0) * kServeTile;
-    serve_tile(q, sm, r0, umin64(r0 + kServeTile, q.n), cnt, sum, tl);
-    __syncthreads();  // the tile is done before sm.t is rewritten
+    serve_topk_tile(q, r0, umin64(r0 + kServeTile, q.n), tl);
+    __syncthreads();  // the unit is done before sm.t is rewritten
   }
-  if (cur >= 0) serve_publish(a, a.q[cur], cur, sm, cnt, sum, tl);
+  if (cur >= 0) serve_publish(a, a.q[cur], cur, sm, tl);
 }
 
 // Top-k queries: the k best of the CTAs' candidates, one CTA per query.
@@ -428,7 +488,9 @@ struct Server {
   double now() const { return std::chrono::duration<double>(Clock::now() - t0).count(); }
 };
 
-static constexpr size_t kServeInBytes = sizeof(ServeHeader) + sizeof(ServeQ) * kServeMaxBatch;
+static constexpr size_t kServeQOff = sizeof(ServeHeader);
+static constexpr size_t kServeGOff = kServeQOff + sizeof(ServeQ) * kServeMaxBatch;
+static constexpr size_t kServeInBytes = kServeGOff + sizeof(ServeG) * kServeMaxBatch;
 static constexpr size_t kServeResBytes = sizeof(ServeRes) * kServeMaxBatch;
 
 static uint64_t serve_query_bytes(const fdb_serve_query& q, uint32_t cand_cap) {
@@ -450,7 +512,8 @@ static void slot_capture(Server& s, ServeSlot& sl) {
   Ctx& c = *s.c;
   ServeArgs a;
   a.hdr = static_cast<const ServeHeader*>(sl.d_in.ptr);
-  a.q = reinterpret_cast<const ServeQ*>(static_cast<unsigned char*>(sl.d_in.ptr) + sizeof(ServeHeader));
+  a.q = reinterpret_cast<const ServeQ*>(static_cast<unsigned char*>(sl.d_in.ptr) + kServeQOff);
+  a.g = reinterpret_cast<const ServeG*>(static_cast<unsigned char*>(sl.d_in.ptr) + kServeGOff);
   a.res = static_cast<ServeRes*>(sl.d_res.ptr);
   a.claim = reinterpret_cast<unsigned int*>(static_cast<unsigned char*>(sl.d_res.ptr) + kServeResBytes);
   a.cand_k = static_cast<uint64_t*>(sl.d_cand_k.ptr);
@@ -460,7 +523,7 @@ static void slot_capture(Server& s, ServeSlot& sl) {
   FDB_CUDA(cudaStreamBeginCapture(sl.stream, cudaStreamCaptureModeThreadLocal));
   cudaMemcpyAsync(sl.d_in.ptr, sl.h_in, kServeInBytes, cudaMemcpyHostToDevice, sl.stream);
   cudaMemsetAsync(sl.d_res.ptr, 0, kServeResBytes + 256, sl.stream);
-  serve_kernel<<<s.grid, kServeThreads, 0, sl.stream>>>(a);
+  serve_kernel<<<s.grid, kServeThreads, kShareSmem, sl.stream>>>(a);
   serve_finish_kernel<<<kServeMaxBatch, kServeThreads, 0, sl.stream>>>(a);
   cudaMemcpyAsync(sl.h_out, sl.d_res.ptr, kServeResBytes, cudaMemcpyDeviceToHost, sl.stream);
   cudaMemcpyAsync(sl.h_err, sl.d_err.ptr, sizeof(int), cudaMemcpyDeviceToHost, sl.stream);
@@ -519,52 +582,128 @@ static void slot_complete(Server& s, ServeSlot& sl) {
   sl.busy = false;
 }
 
-// Admit queued queries into a free slot and launch it (s.mu held).
+// Admit queued queries into a free slot and launch it (s.mu held).  The
+// admitted queries are laid out group by group (queries reading the same
+// table, by rows descending), then the top-k queries.
 static bool slot_launch(Server& s, ServeSlot& sl) {
-  ServeHeader* hdr = reinterpret_cast<ServeHeader*>(sl.h_in);
-  ServeQ* dq = reinterpret_cast<ServeQ*>(sl.h_in + sizeof(ServeHeader));
   const uint64_t room = s.budget > s.resident ? s.budget - s.resident : 0;
   const double t = s.now();
-  uint64_t tiles = 0;
-  int n = 0;
-  while (!s.queue.empty() && n < s.cfg.max_batch) {
+  std::vector<uint64_t> admitted;
+  while (!s.queue.empty() && (int)admitted.size() < s.cfg.max_batch) {
     ServeJob& j = s.jobs[s.queue.front()];
-    if (s.reserved + j.bytes > room && n > 0) break;  // wait for memory (a lone query always runs)
-    const fdb_serve_query& q = j.q;
-    ServeQ& d = dq[n];
+    if (s.reserved + j.bytes > room && !admitted.empty()) break;  // wait for memory (a lone query always runs)
+    s.reserved += j.bytes;
+    s.peak_reserved = std::max(s.peak_reserved, s.reserved);
+    j.r.start_s = t;
+    admitted.push_back(s.queue.front());
+    s.queue.pop_front();
+  }
+  if (admitted.empty()) return false;
+
+  // Groups: COUNT joins any non-join group on the same c0; GROUP needs the same
+  // (c0, c1, c2) or a COUNT-only group on c0; JOIN needs the same (c0, c1, table).
+  struct G {
+    const void *c0, *c1, *c2;
+    const fdb_hash* table;
+    bool join, has_group;
+    std::vector<uint64_t> tickets;
+  };
+  std::vector<G> groups;
+  std::vector<uint64_t> topk;
+  for (uint64_t tk : admitted) {
+    const fdb_serve_query& q = s.jobs[tk].q;
+    if (q.kind == FDB_SERVE_TOPK) {
+      topk.push_back(tk);
+      continue;
+    }
+    G* home = nullptr;
+    for (G& g : groups) {
+      if (g.c0 != q.c0) continue;
+      if (q.kind == FDB_SERVE_JOIN) {
+        if (g.join && g.c1 == q.c1 && g.table == q.table) home = &g;
+      } else if (!g.join) {
+        if (q.kind == FDB_SERVE_COUNT) home = &g;
+        else if (!g.has_group || (g.c1 == q.c1 && g.c2 == q.c2)) home = &g;
+      }
+      if (home) break;
+    }
+    if (!home) {
+      groups.push_back(G{q.c0, nullptr, nullptr, nullptr, q.kind == FDB_SERVE_JOIN, false, {}});
+      home = &groups.back();
+      if (home->join) {
+        home->c1 = q.c1;
+        home->table = q.table;
+      }
+    }
+    if (q.kind == FDB_SERVE_GROUP && !home->has_group) {
+      home->has_group = true;
+      home->c1 = q.c1;
+      home->c2 = q.c2;
+    }
+    home->tickets.push_back(tk);
+  }
+
+  ServeHeader* hdr = reinterpret_cast<ServeHeader*>(sl.h_in);
+  ServeQ* dq = reinterpret_cast<ServeQ*>(sl.h_in + kServeQOff);
+  ServeG* dg = reinterpret_cast<ServeG*>(sl.h_in + kServeGOff);
+  sl.tickets.clear();
+  uint64_t units = 0;
+  auto put = [&](uint64_t tk) -> ServeQ& {
+    const fdb_serve_query& q = s.jobs[tk].q;
+    ServeQ& d = dq[sl.tickets.size()];
     std::memset(&d, 0, sizeof(d));
     d.kind = q.kind;
     d.k = q.k;
     d.n = q.nrows;
-    d.tile0 = tiles;
-    tiles += (q.nrows + kServeTile - 1) / kServeTile;
     d.thr = q.threshold;
     d.c0 = q.c0;
     d.c1 = q.c1;
     d.c2 = q.c2;
     d.dict_len = q.dict_len;
-    if (q.kind == FDB_SERVE_JOIN) {
-      const JoinView v = join_view(hash_of(q.table));
+    sl.tickets.push_back(tk);
+    return d;
+  };
+  for (size_t gi = 0; gi < groups.size(); ++gi) {
+    G& g = groups[gi];
+    std::stable_sort(g.tickets.begin(), g.tickets.end(),
+                     [&](uint64_t x, uint64_t y) { return s.jobs[x].q.nrows > s.jobs[y].q.nrows; });
+    ServeG& d = dg[gi];
+    std::memset(&d, 0, sizeof(d));
+    d.c0 = g.c0;
+    d.c1 = g.c1;
+    d.c2 = g.c2;
+    d.q0 = (uint32_t)sl.tickets.size();
+    d.nq = (uint32_t)g.tickets.size();
+    d.max_n = s.jobs[g.tickets.front()].q.nrows;
+    d.unit0 = units;
+    units += (d.max_n + kShareTile - 1) / kShareTile;
+    d.c1_bytes = g.join ? 8 : (g.has_group ? 4 : 0);
+    d.load_c2 = g.has_group ? 1 : 0;
+    d.join = g.join ? 1 : 0;
+    if (g.join) {
+      const JoinView v = join_view(hash_of(g.table));
       d.slots = static_cast<const JSlot*>(v.slots);
       d.cnt = v.cnt;
       d.cap = v.cap;
       d.unique = v.unique;
     }
-    s.reserved += j.bytes;
-    s.peak_reserved = std::max(s.peak_reserved, s.reserved);
-    j.r.start_s = t;
-    sl.tickets.push_back(s.queue.front());
-    s.queue.pop_front();
-    ++n;
+    for (uint64_t tk : g.tickets) put(tk);
   }
-  if (n == 0) return false;
-  hdr->nq = n;
-  hdr->total_tiles = tiles;
+  hdr->nq = (int32_t)admitted.size();
+  hdr->ngroups = (int32_t)groups.size();
+  hdr->topk0 = (int32_t)sl.tickets.size();
+  hdr->shared_units = units;
+  for (uint64_t tk : topk) {
+    ServeQ& d = put(tk);
+    d.tile0 = units;
+    units += (d.n + kServeTile - 1) / kServeTile;
+  }
+  hdr->total_units = units;
   FDB_CUDA(cudaGraphLaunch(sl.exec, sl.stream));
   FDB_CUDA(cudaEventRecord(sl.done, sl.stream));
   sl.busy = true;
   ++s.batches;
-  s.batched_queries += n;
+  s.batched_queries += (int64_t)admitted.size();
   return true;
 }
 
@@ -609,7 +748,10 @@ Server* server_start(fdb_db* db, Ctx& c, const fdb_serve_config* cfg) {
   s->budget = cfg && cfg->mem_budget ? cfg->mem_budget : c.budget;
   s->cfg.mem_budget = s->budget;
   s->resident = c.in_use.load();
-  s->grid = c.sm_count * kServeCtasPerSm;
+  FDB_CUDA(cudaFuncSetAttribute(serve_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kShareSmem));
+  int per_sm = 0;
+  FDB_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, serve_kernel, kServeThreads, kShareSmem));
+  s->grid = c.sm_count * std::max(1, std::min(per_sm, kServeCtasPerSm));
   s->cand_cap = (uint32_t)s->grid * FDB_SERVE_MAX_K;
   s->slots.resize(s->cfg.slots);
   for (ServeSlot& sl : s->slots) {
