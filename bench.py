@@ -590,9 +590,9 @@ def run_serving(args, db, out, peak):
     budget = 40 << 30
     burst = [S.Query(**{**q.__dict__, "arrival_s": 0.0}) for q in qs]
     S.serve_trace(db, burst[:200], max_batch=128, slots=4, mem_budget=budget)  # warm-up
-    res_b, live_b = S.serve_trace(db, qs, max_batch=128, slots=4, mem_budget=budget)
+    res_b, live_b = S.serve_trace(db, qs, max_batch=128, slots=args.serve_slots, mem_budget=budget)
     res_s, live_s = S.serve_trace(db, qs, max_batch=1, slots=1, mem_budget=budget)
-    _, sat_b = S.serve_trace(db, burst, max_batch=128, slots=4, mem_budget=budget)
+    _, sat_b = S.serve_trace(db, burst, max_batch=128, slots=args.serve_slots, mem_budget=budget)
     _, sat_s = S.serve_trace(db, burst, max_batch=1, slots=1, mem_budget=budget)
     same = all(a.status == 0 and b.status == 0 and a.count == b.count and a.sum_payload == b.sum_payload
                and list(a.group_count) == list(b.group_count) and list(a.rows[:a.count]) == list(b.rows[:b.count])
@@ -602,13 +602,25 @@ def run_serving(args, db, out, peak):
     def d(st):
         return {"qps": round(st.qps, 1), "p50_ms": round(st.p50_ms, 4), "p99_ms": round(st.p99_ms, 4),
                 "max_ms": round(st.max_ms, 4), "mean_batch": round(st.mean_batch, 2), "batches": st.batches}
+
+    def by_kind(res):
+        names = {S.SERVE_COUNT: "count", S.SERVE_GROUP: "group", S.SERVE_JOIN: "join", S.SERVE_TOPK: "topk"}
+        outk = {}
+        for kind, name in names.items():
+            lat = sorted((r.done_s - r.arrival_s) * 1e3 for q, r in zip(qs, res) if q.kind == kind)
+            big = sorted((r.done_s - r.arrival_s) * 1e3 for q, r in zip(qs, res) if q.kind == kind and q.nrows >= n // 2)
+            if lat:
+                outk[name] = {"p50_ms": round(lat[len(lat) // 2], 4), "p99_ms": round(lat[int(0.99 * (len(lat) - 1))], 4),
+                              "p50_ms_rows_ge_half": round(big[len(big) // 2], 4) if big else None}
+        return outk
     out.append({"metric": METRIC, "workload": "serving", "value": round(sat_b.qps, 1), "unit": "queries/s",
                 "higher_is_better": True, "queries": nq, "arrival_qps": rate,
                 "templates": "filter-count, filter-group-by, inner join, top-k (uniform)",
                 "table_rows": n, "prefix_rows": "log-uniform [10k, 100M]", "thresholds": "uniform [0, 100)",
-                "mem_budget_bytes": budget, "resident_bytes": live_b.resident_bytes,
+                "mem_budget_bytes": budget, "slots": args.serve_slots, "max_batch": 128, "resident_bytes": live_b.resident_bytes,
                 "peak_reserved_bytes": live_b.peak_reserved,
                 "at_2000qps": {"batched": d(live_b), "serial": d(live_s)},
+                "at_2000qps_by_template": {"batched": by_kind(res_b), "serial": by_kind(res_s)},
                 "saturated": {"batched": d(sat_b), "serial": d(sat_s)},
                 "throughput_speedup": round(sat_b.qps / sat_s.qps, 2) if sat_s.qps else None,
                 "results_identical_batched_vs_serial": same})
@@ -659,6 +671,7 @@ def main():
                     help="scan = the headline line; the others print per-operator lines")
     ap.add_argument("--load-factor", type=float, default=0.5)
     ap.add_argument("--serve-queries", type=int, default=10_000)
+    ap.add_argument("--serve-slots", type=int, default=2)
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3

@@ -114,9 +114,11 @@ struct ServeArgs {
 struct ServeSmem {
   uint64_t start[kServeMaxBatch + 1];   // unit0 of each top-k query
   uint64_t gstart[kServeMaxBatch + 1];  // unit0 of each shared group
-  unsigned long long gcount[kServeWarps][FDB_SERVE_MAX_GROUPS];
-  double gsum0[kServeWarps][FDB_SERVE_MAX_GROUPS];
-  long long gsum2[kServeWarps][FDB_SERVE_MAX_GROUPS];
+  // GROUP BY partials: per warp, two copies (even and odd lanes) to halve
+  // the atomic contention of lanes that hit the same group.
+  unsigned long long gcount[kServeWarps][2][FDB_SERVE_MAX_GROUPS];
+  double gsum0[kServeWarps][2][FDB_SERVE_MAX_GROUPS];
+  long long gsum2[kServeWarps][2][FDB_SERVE_MAX_GROUPS];
   uint64_t tkeys[kServeWarps][32];
   uint32_t trows[kServeWarps][32];
   unsigned long long red[kServeWarps][2];
@@ -246,6 +248,77 @@ __device__ __forceinline__ void share_load(unsigned char* dst, const void* src, 
   }
 }
 
+// Probe every staged row of a join group once: row i's build matches go to
+// m[i] and their payload sum replaces its key in s0[i].  Each thread walks
+// kProbeIlp rows together, one 32-byte slot pair (one L2 sector) per row per
+// round, so their L2 round trips overlap.
+constexpr int kProbeIlp = 4;
+
+__device__ void serve_probe_rows(const ServeG& g, uint64_t* s0, uint32_t* m, uint32_t rows) {
+  const int shift = join_shift(g.cap);
+  const uint64_t mask = g.cap - 1;
+  const uint64_t pol = l2_evict_last_policy();
+  for (uint32_t base = 0; base < rows; base += kProbeIlp * blockDim.x) {
+    uint64_t sk[kProbeIlp], h[kProbeIlp], ps[kProbeIlp];
+    uint32_t at[kProbeIlp];
+    uint32_t todo = 0;
+#pragma unroll
+    for (int j = 0; j < kProbeIlp; ++j) {
+      const uint32_t i = base + j * blockDim.x + threadIdx.x;
+      at[j] = kNoSlot;
+      ps[j] = 0;
+      sk[j] = 0;
+      h[j] = 0;
+      if (i >= rows) continue;
+      const int64_t key = (int64_t)s0[i];
+      if (key == INT64_MIN) {
+        if (g.cnt[g.cap] != 0u) {
+          at[j] = (uint32_t)g.cap;
+          ps[j] = g.slots[g.cap].psum;
+        }
+        continue;
+      }
+      sk[j] = (uint64_t)key ^ (1ull << 63);
+      h[j] = join_hash(sk[j], shift);
+      todo |= 1u << j;
+    }
+    for (uint64_t round = 0; todo && round <= mask; ++round) {
+      JSlot lo[kProbeIlp], hi[kProbeIlp];
+#pragma unroll
+      for (int j = 0; j < kProbeIlp; ++j)
+        if ((todo >> j) & 1u)
+          asm volatile("ld.global.L2::cache_hint.v4.u64 {%0, %1, %2, %3}, [%4], %5;"
+                       : "=l"(lo[j].key), "=l"(lo[j].psum), "=l"(hi[j].key), "=l"(hi[j].psum)
+                       : "l"(g.slots + (h[j] & ~1ull)), "l"(pol));
+#pragma unroll
+      for (int j = 0; j < kProbeIlp; ++j) {
+        if (!((todo >> j) & 1u)) continue;
+        const bool even = (h[j] & 1ull) == 0;
+        const bool hit0 = even && lo[j].key == sk[j];
+        const bool stop0 = even && (lo[j].key == sk[j] || lo[j].key == 0ull);
+        const bool hit1 = !stop0 && hi[j].key == sk[j];
+        if (hit0 || hit1) {
+          at[j] = (uint32_t)((h[j] & ~1ull) + (hit1 ? 1 : 0));
+          ps[j] = hit1 ? hi[j].psum : lo[j].psum;
+          todo &= ~(1u << j);
+        } else if (stop0 || hi[j].key == 0ull) {
+          todo &= ~(1u << j);
+        } else {
+          h[j] = ((h[j] & ~1ull) + 2) & mask;
+        }
+      }
+    }
+#pragma unroll
+    for (int j = 0; j < kProbeIlp; ++j) {
+      const uint32_t i = base + j * blockDim.x + threadIdx.x;
+      if (i >= rows) continue;
+      m[i] = at[j] == kNoSlot ? 0u : (g.unique ? 1u : g.cnt[at[j]]);
+      s0[i] = ps[j];
+    }
+  }
+  __syncthreads();
+}
+
 // One shared unit: stage the group's rows, probe them once for a join group,
 // then evaluate every query of the group that reaches this unit.
 __device__ void serve_shared_unit(const ServeArgs& a, const ServeG& g, uint64_t tile, unsigned char* tsm,
@@ -261,37 +334,7 @@ __device__ void serve_shared_unit(const ServeArgs& a, const ServeG& g, uint64_t 
   if (g.c1_bytes) share_load(s1, g.c1, r0, rows, g.c1_bytes);
   if (g.load_c2) share_load(tsm + (size_t)kShareTile * 16, g.c2, r0, rows, 8);
   __syncthreads();
-  if (g.join) {  // row i's build matches and their payload sum replace its key
-    const int shift = join_shift(g.cap);
-    const uint64_t mask = g.cap - 1;
-    for (uint32_t i = threadIdx.x; i < rows; i += blockDim.x) {
-      const int64_t key = (int64_t)s0[i];
-      uint32_t at = kNoSlot;
-      uint64_t ps = 0;
-      if (key == INT64_MIN) {
-        if (g.cnt[g.cap] != 0u) {
-          at = (uint32_t)g.cap;
-          ps = g.slots[g.cap].psum;
-        }
-      } else {
-        const uint64_t sk = (uint64_t)key ^ (1ull << 63);
-        uint64_t h = join_hash(sk, shift);
-        for (uint64_t probe = 0; probe <= mask; ++probe) {
-          const JSlot sl = g.slots[h];
-          if (sl.key == sk) {
-            at = (uint32_t)h;
-            ps = sl.psum;
-            break;
-          }
-          if (sl.key == 0ull) break;
-          h = (h + 1) & mask;
-        }
-      }
-      smm[i] = at == kNoSlot ? 0u : (g.unique ? 1u : g.cnt[at]);
-      s0[i] = ps;
-    }
-    __syncthreads();
-  }
+  if (g.join) serve_probe_rows(g, s0, smm, rows);
   for (uint32_t qi = g.q0; qi < g.q0 + g.nq; ++qi) {
     const ServeQ& q = a.q[qi];
     if (q.n <= r0) break;  // queries are by rows descending
@@ -318,20 +361,22 @@ __device__ void serve_shared_unit(const ServeArgs& a, const ServeG& g, uint64_t 
         atomicAdd(reinterpret_cast<unsigned long long*>(&r.sum), ps);
       }
     } else {  // GROUP
-      if (lane < FDB_SERVE_MAX_GROUPS) {
-        sm.gcount[warp][lane] = 0;
-        sm.gsum0[warp][lane] = 0.0;
-        sm.gsum2[warp][lane] = 0;
+      {
+        const int cp = lane >> 4, gi = lane & 15;  // 32 lanes clear 2 copies x 16 groups
+        sm.gcount[warp][cp][gi] = 0;
+        sm.gsum0[warp][cp][gi] = 0.0;
+        sm.gsum2[warp][cp][gi] = 0;
       }
       __syncwarp();
+      const int cp = lane & 1;
       const uint32_t* codes = reinterpret_cast<const uint32_t*>(s1);
       for (uint32_t i = threadIdx.x; i < re; i += blockDim.x) {
         const double v = __longlong_as_double((long long)s0[i]);
         const uint32_t gc = codes[i];
         if (v > q.thr && gc < q.dict_len) {
-          atomicAdd(&sm.gcount[warp][gc], 1ull);
-          atomicAdd(&sm.gsum0[warp][gc], v);
-          atomicAdd(reinterpret_cast<unsigned long long*>(&sm.gsum2[warp][gc]), (unsigned long long)s2[i]);
+          atomicAdd(&sm.gcount[warp][cp][gc], 1ull);
+          atomicAdd(&sm.gsum0[warp][cp][gc], v);
+          atomicAdd(reinterpret_cast<unsigned long long*>(&sm.gsum2[warp][cp][gc]), (unsigned long long)s2[i]);
         }
       }
       __syncthreads();
@@ -340,11 +385,12 @@ __device__ void serve_shared_unit(const ServeArgs& a, const ServeG& g, uint64_t 
         unsigned long long c = 0;
         double v0 = 0.0;
         long long v2 = 0;
-        for (int w = 0; w < kServeWarps; ++w) {
-          c += sm.gcount[w][gc];
-          v0 += sm.gsum0[w][gc];
-          v2 += sm.gsum2[w][gc];
-        }
+        for (int w = 0; w < kServeWarps; ++w)
+          for (int c2 = 0; c2 < 2; ++c2) {
+            c += sm.gcount[w][c2][gc];
+            v0 += sm.gsum0[w][c2][gc];
+            v2 += sm.gsum2[w][c2][gc];
+          }
         if (c) {
           atomicAdd(&r.gcount[gc], c);
           atomicAdd(&r.gsum0[gc], v0);
@@ -357,7 +403,7 @@ __device__ void serve_shared_unit(const ServeArgs& a, const ServeG& g, uint64_t 
   __syncthreads();  // before the next unit overwrites the staged rows
 }
 
-__global__ void __launch_bounds__(kServeThreads) serve_kernel(ServeArgs a) {
+__global__ void __launch_bounds__(kServeThreads, kServeCtasPerSm) serve_kernel(ServeArgs a) {
   extern __shared__ __align__(16) unsigned char tsm[];
   __shared__ ServeSmem sm;
   const int nq = a.hdr->nq, ng = a.hdr->ngroups, topk0 = a.hdr->topk0;
@@ -483,6 +529,7 @@ struct Server {
   Clock::time_point t0;
   uint32_t cand_cap = 0;
   int grid = 0;
+  uint64_t split_rows = 1ull << 22;  // size classes of batches: fewer / at least this many rows
   std::string error;
 
   double now() const { return std::chrono::duration<double>(Clock::now() - t0).count(); }
@@ -588,15 +635,23 @@ static void slot_complete(Server& s, ServeSlot& sl) {
 static bool slot_launch(Server& s, ServeSlot& sl) {
   const uint64_t room = s.budget > s.resident ? s.budget - s.resident : 0;
   const double t = s.now();
+  // A batch holds queries of one size class, the class of the oldest waiting
+  // query: a query that reads few rows never waits for a long scan that
+  // happened to be admitted with it.  Within the class, arrival order.
   std::vector<uint64_t> admitted;
-  while (!s.queue.empty() && (int)admitted.size() < s.cfg.max_batch) {
-    ServeJob& j = s.jobs[s.queue.front()];
+  const bool big = s.jobs[s.queue.front()].q.nrows >= s.split_rows;
+  for (auto it = s.queue.begin(); it != s.queue.end() && (int)admitted.size() < s.cfg.max_batch;) {
+    ServeJob& j = s.jobs[*it];
+    if ((j.q.nrows >= s.split_rows) != big) {
+      ++it;
+      continue;
+    }
     if (s.reserved + j.bytes > room && !admitted.empty()) break;  // wait for memory (a lone query always runs)
     s.reserved += j.bytes;
     s.peak_reserved = std::max(s.peak_reserved, s.reserved);
     j.r.start_s = t;
-    admitted.push_back(s.queue.front());
-    s.queue.pop_front();
+    admitted.push_back(*it);
+    it = s.queue.erase(it);
   }
   if (admitted.empty()) return false;
 
