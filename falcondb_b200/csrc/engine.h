@@ -140,6 +140,9 @@ void op_group_by_codes(Ctx& c, const fdb_dev_column* cols, int ncols, uint64_t n
                        const fdb_pred_term* prog, int nterms, int key_col, uint32_t dict_len,
                        const fdb_agg_spec* aggs, int naggs, fdb_agg_value* d_out,
                        int64_t* d_group_rows);
+// Groups to size a hash GROUP BY table for: `expected_groups` when nonzero,
+// else a HyperLogLog estimate of the key column plus headroom (synchronises).
+uint64_t group_by_i64_groups(Ctx& c, const fdb_dev_column& key, uint64_t n, uint64_t expected_groups);
 // Scratch bytes op_group_by_i64 takes for `expected_groups` at `load_factor`.
 size_t group_by_i64_scratch(uint64_t expected_groups, double load_factor);
 void op_group_by_i64(Ctx& c, const fdb_dev_column& key, const fdb_dev_column& value, uint64_t n,
@@ -167,6 +170,10 @@ bool server_wait(Server& s, uint64_t ticket, int64_t timeout_ns, fdb_serve_resul
 void server_stop(Server* s, fdb_serve_stats* st);
 void serve_trace(fdb_db* db, Ctx& c, const fdb_serve_query* qs, int nq, const fdb_serve_config* cfg,
                  fdb_serve_result* out, fdb_serve_stats* st);
+
+// HyperLogLog estimate of the distinct keys among n INT64 values (hll.cu);
+// synchronises the context stream.
+uint64_t estimate_distinct_i64(Ctx& c, const void* keys, uint64_t n);
 
 struct BatchPlan;
 BatchPlan* op_gb_batch_prepare(Ctx& c, const fdb_gb_query* qs, int nq, const fdb_batch_tuning* t);

@@ -19,6 +19,7 @@
 //    table); MIN is kept as the bitwise NOT of the order key so both MIN and MAX
 //    are atomicMax from a zero identity.  SUM is FP64 atomicAdd (order varies run
 //    to run; tests hold it to 1e-12 relative).
+#include <algorithm>
 #include <cstring>
 
 #include "common.cuh"
@@ -643,6 +644,14 @@ static uint64_t gb_table_capacity(uint64_t expected_groups, double load_factor) 
   uint64_t cap = 1024;
   while ((double)cap * load_factor < (double)expected_groups) cap <<= 1;
   return cap;
+}
+
+uint64_t group_by_i64_groups(Ctx& c, const fdb_dev_column& key, uint64_t n, uint64_t expected_groups) {
+  if (expected_groups) return expected_groups;
+  if (n == 0) return 1;
+  if (!key.values) fail(FDB_E_ARG, "column without values");
+  // 15 % headroom over the sketch (about nine standard errors).
+  return std::min<uint64_t>(n, estimate_distinct_i64(c, key.values, n) * 115 / 100 + 64);
 }
 
 size_t group_by_i64_scratch(uint64_t expected_groups, double load_factor) {

@@ -1009,9 +1009,11 @@ static void run_aggregates(Plan& plan, const Rel& rel, const Query& q, fdb_resul
       fdb_group_i64* d = plan.dev<fdb_group_i64>(cap);
       uint64_t* dn = plan.dev<uint64_t>(1);
       plan.c.scratch_reset();
-      plan.c.ensure_scratch(group_by_i64_scratch(rel.nrows, 0.5) + (16u << 20));
+      const uint64_t eg = group_by_i64_groups(plan.c, col.dev, rel.nrows, 0);
+      plan.c.scratch_reset();
+      plan.c.ensure_scratch(group_by_i64_scratch(eg, 0.5) + (16u << 20));
       op_group_by_i64(plan.c, col.dev, col.dev, rel.nrows, prog.data(), (int)prog.size(), pcols.data(),
-                      (int)pcols.size(), rel.nrows, 0.5, d, cap, dn);
+                      (int)pcols.size(), eg, 0.5, d, cap, dn);
       plan.check();
       const uint64_t ng = plan.one(dn);
       std::vector<fdb_group_i64> g = plan.to_host(d, ng);
@@ -1155,9 +1157,10 @@ static void run_group_by(Plan& plan, const Rel& rel, const Query& q, fdb_result*
     uint64_t* dn = plan.dev<uint64_t>(1);
     std::vector<fdb_group_i64> groups;
     if (rel.nrows > 0) {
-      plan.c.ensure_scratch(group_by_i64_scratch(rel.nrows, 0.5) + (16u << 20));
+      const uint64_t eg = group_by_i64_groups(plan.c, key.dev, rel.nrows, 0);
+      plan.c.ensure_scratch(group_by_i64_scratch(eg, 0.5) + (16u << 20));
       op_group_by_i64(plan.c, key.dev, rel.cols[vc].dev, rel.nrows, prog.data(), (int)prog.size(), pcols.data(),
-                      (int)pcols.size(), rel.nrows, 0.5, d, cap, dn);
+                      (int)pcols.size(), eg, 0.5, d, cap, dn);
       plan.check();
       groups = plan.to_host(d, plan.one(dn));
     }
