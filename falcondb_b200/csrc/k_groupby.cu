@@ -219,12 +219,43 @@ __device__ void gb_codes_merge(const GbCodesParams& p, uint64_t* tab, unsigned i
     consumer_bar(nct);
     if (*s_last == 0) return;
     __threadfence();
-    // Last CTA: fold CTA partials in CTA order, one thread per table entry.
+    // Last CTA: fold the CTA partials of each table entry in CTA order.  The
+    // CTAs are cut into nseg contiguous ranges, each folded by its own thread
+    // with 8 loads in flight, and the range results are folded in range order:
+    // a fixed tree for a given grid, so FP64 sums repeat run to run.
+    const uint32_t G = gridDim.x;
+    uint32_t nseg = (uint32_t)nct / entries;
+    nseg = nseg < 1 ? 1 : (nseg > 16 ? 16 : nseg);
+    uint64_t* part = tab + entries;  // [entries][nseg], after the final entries
+    for (uint32_t w = ctid; w < entries * nseg; w += nct) {
+      const uint32_t e = w / nseg, sg = w % nseg;
+      const uint32_t b0 = (uint32_t)((uint64_t)G * sg / nseg), b1 = (uint32_t)((uint64_t)G * (sg + 1) / nseg);
+      const int kind = p.kind[e % ns];
+      uint64_t acc = 0;
+      bool first = true;
+      for (uint32_t b = b0; b < b1; b += 8) {
+        uint64_t v[8];
+#pragma unroll
+        for (int j = 0; j < 8; ++j) v[j] = b + j < b1 ? __ldcg(&p.partials[(size_t)(b + j) * entries + e]) : 0;
+#pragma unroll
+        for (int j = 0; j < 8; ++j)
+          if (b + j < b1) {
+            acc = first ? v[j] : slot_combine(kind, acc, v[j]);
+            first = false;
+          }
+      }
+      part[(size_t)e * nseg + sg] = acc;
+    }
+    consumer_bar(nct);
     for (uint32_t e = ctid; e < entries; e += nct) {
       const int kind = p.kind[e % ns];
-      uint64_t acc = __ldcg(&p.partials[e]);
-      for (uint32_t b = 1; b < gridDim.x; ++b)
-        acc = slot_combine(kind, acc, __ldcg(&p.partials[(size_t)b * entries + e]));
+      uint64_t acc = 0;
+      bool first = true;
+      for (uint32_t sg = 0; sg < nseg; ++sg) {
+        if ((uint64_t)G * sg / nseg == (uint64_t)G * (sg + 1) / nseg) continue;  // an empty range
+        acc = first ? part[(size_t)e * nseg + sg] : slot_combine(kind, acc, part[(size_t)e * nseg + sg]);
+        first = false;
+      }
       tab[e] = acc;
     }
     consumer_bar(nct);
@@ -513,6 +544,8 @@ __global__ void gb_hash_compact_kernel(const GSlot* __restrict__ table, uint64_t
 // ===========================================================================
 // Launchers
 // ===========================================================================
+constexpr uint64_t kGbTilesPerCta = 8;
+
 template <class Op, int NC, int TR, int STAGES, int NCW>
 static void launch_stream_gb(Ctx& c, const fdb_dev_column* cols, uint64_t n,
                              const typename Op::Params& p, size_t op_smem) {
@@ -538,7 +571,9 @@ static void launch_stream_gb(Ctx& c, const fdb_dev_column* cols, uint64_t n,
   if (per_sm < 1) per_sm = 1;
   if (per_sm > 4) per_sm = 4;
   const uint64_t ntiles = (src.m_end + TR - 1) / TR;
-  uint64_t want = ntiles ? ntiles : (n + NCW * 32 * 8 - 1) / (NCW * 32 * 8);
+  // At least kGbTilesPerCta tiles per CTA: on small inputs fewer CTAs means
+  // fewer partials for the last CTA to fold.
+  uint64_t want = ntiles ? (ntiles + kGbTilesPerCta - 1) / kGbTilesPerCta : (n + NCW * 32 * 8 - 1) / (NCW * 32 * 8);
   if (want < 1) want = 1;
   const int grid = (int)umin64(want, (uint64_t)c.sm_count * per_sm);
   kern<<<grid, (NCW + 1) * 32, smem, c.stream>>>(src, p, c.d_err, op_off);
