@@ -299,6 +299,16 @@ __device__ void gb_codes_merge(const GbCodesParams& p, uint64_t* tab, unsigned i
 // order; the CTA then folds the 256 columns in thread order: FP64 sums are
 // repeatable for a given grid.
 constexpr int kLaneEntries = 48;
+// Tile rows and ring stages of the three-column lane GROUP BY (config 0's shape).
+#ifndef FDB_LANE_TR3
+#define FDB_LANE_TR3 512
+#endif
+#ifndef FDB_LANE_ST3
+#define FDB_LANE_ST3 2
+#endif
+#ifndef FDB_LANE_NCW3
+#define FDB_LANE_NCW3 8
+#endif
 
 struct GbLaneOp {
   using Params = GbCodesParams;
@@ -657,13 +667,14 @@ void op_group_by_codes(Ctx& c, const fdb_dev_column* cols, int ncols, uint64_t n
   p.out = d_out;
   p.group_rows = d_group_rows;
   if ((uint64_t)p.ngroups * ns <= kLaneEntries) {
-    // Lane-private tables: 4 consumer warps per CTA, 512-row tiles.
-    const size_t sm = (size_t)p.ngroups * ns * 128 * 8 + 16;
+    // Lane-private tables: one table column per consumer thread.
+    const size_t sm4 = (size_t)p.ngroups * ns * 128 * 8 + 16;
+    const size_t smw = (size_t)p.ngroups * ns * (FDB_LANE_NCW3 * 32) * 8 + 16;
     switch (ncols) {
-      case 1: launch_stream_gb<GbLaneOp, 1, 2048, 3, 4>(c, cols, n, p, sm); break;
-      case 2: launch_stream_gb<GbLaneOp, 2, 1024, 3, 4>(c, cols, n, p, sm); break;
-      case 3: launch_stream_gb<GbLaneOp, 3, 1024, 3, 4>(c, cols, n, p, sm); break;
-      default: launch_stream_gb<GbLaneOp, 4, 1024, 2, 4>(c, cols, n, p, sm); break;
+      case 1: launch_stream_gb<GbLaneOp, 1, 2048, 3, 4>(c, cols, n, p, sm4); break;
+      case 2: launch_stream_gb<GbLaneOp, 2, 1024, 3, 4>(c, cols, n, p, sm4); break;
+      case 3: launch_stream_gb<GbLaneOp, 3, FDB_LANE_TR3, FDB_LANE_ST3, FDB_LANE_NCW3>(c, cols, n, p, smw); break;
+      default: launch_stream_gb<GbLaneOp, 4, 1024, 2, 4>(c, cols, n, p, sm4); break;
     }
     return;
   }
