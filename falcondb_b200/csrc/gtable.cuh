@@ -68,6 +68,27 @@ __device__ __forceinline__ GSlot* gtable_find(GSlot* table, uint64_t mask, uint6
   return nullptr;
 }
 
+// gtable_find for a caller that has already loaded `cur`, the key word of the
+// key's home slot h = mix64(skey) & mask (so that several lookups can have
+// their first load in flight together).
+__device__ __forceinline__ GSlot* gtable_find_from(GSlot* table, uint64_t mask, uint64_t skey, uint64_t h,
+                                                   uint64_t cur, int* err) {
+  const uint64_t limit = umin64(mask + 1, kGlobalProbeLimit);
+  for (uint64_t probe = 0; probe < limit; ++probe) {
+    GSlot* s = table + h;
+    if (probe) cur = *reinterpret_cast<volatile uint64_t*>(&s->key);
+    if (cur == skey) return s;
+    if (cur == 0) {
+      const uint64_t prev = atomicCAS(reinterpret_cast<unsigned long long*>(&s->key), 0ull,
+                                      (unsigned long long)skey);
+      if (prev == 0 || prev == skey) return s;
+    }
+    h = (h + 1) & mask;
+  }
+  atomicExch(err, kErrCapacity);
+  return nullptr;
+}
+
 // The CTA's shared-memory slot of `skey`, claiming one if free within
 // kSmemProbe probes; nullptr when the key has no room there.
 __device__ __forceinline__ GSlot* smem_table_slot(GSlot* tab, uint64_t skey) {

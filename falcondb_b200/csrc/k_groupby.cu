@@ -48,6 +48,15 @@ struct GbCodesParams {
   int32_t vslot[4];        // value slot of each aggregate (-1: none)
   int32_t cslot[4];        // count slot of each aggregate (-1: uses the row slot)
   int32_t kind[kMaxSlots];
+  // Specialised lane path (GbLaneFastOp): WHERE is absent or one FP64
+  // column compare, the key column and every value column have no NULLs, and
+  // every aggregate is COUNT(*), SUM or AVG.  Slot 0 counts rows; slot s >= 1
+  // sums column f_vcol[s-1].
+  int32_t f_cmp_col;       // WHERE column (-1: no WHERE)
+  uint32_t f_cmp_mask;     // accepted outcomes: bit 0 unordered, 1 less, 2 equal, 3 greater
+  double f_lit;
+  int32_t f_vcol[4];
+  uint32_t f_f64;          // bit s-1: slot s sums an FP64 column (else int64, wrapping)
   uint64_t* partials;      // [grid][ngroups][nslots]
   unsigned int* ticket;
   fdb_agg_value* out;      // [ngroups][naggs]
@@ -444,6 +453,101 @@ struct GbLaneOp {
   }
 };
 
+// The lane-private table for the common shape (GbCodesParams::f_*): NV summed
+// value slots, NCT = consumer threads.  Same table layout, init and fold as
+// GbLaneOp; the row loop differs:
+//   * every slot offset is a compile-time constant (slot s of a group is
+//     s * NCT words after slot 0), so a row's 1 + NV table words load
+//     together, independent of one another;
+//   * a thread first loads its kR rows' WHERE value, code and NV values
+//     (shared-memory loads only), then applies them to the table one row at a
+//     time: each row's read-modify-write chain is one load latency long;
+//   * the WHERE compare is branch-free: the outcome (unordered / less / equal
+//     / greater) indexes the accepted-outcome mask the host derived from the
+//     operator, with C++ semantics for NaN (only != accepts it).
+// Launch shapes (consumer warps, rows per thread per tile, ring stages),
+// measured on 100M and 1M rows of the three-column shape: large inputs run
+// 3 CTAs of 4 consumer warps per SM with 512-row tiles (0.39 ms at 100M rows);
+// small ones, where the launch and the final fold dominate, 8 consumer warps.
+#ifndef FDB_LF_BIG
+#define FDB_LF_BIG 4, 4, 2
+#endif
+#ifndef FDB_LF_SMALL
+#define FDB_LF_SMALL 8, 2, 3
+#endif
+constexpr uint64_t kLaneFastBigRows = 1ull << 24;
+template <int NV, int NCW, int R>
+struct GbLaneFastOp {
+  using Params = GbCodesParams;
+  struct Local {};
+  static constexpr int NCT = NCW * 32;
+  static constexpr int kR = R;
+  static constexpr int kTileRows = kR * NCT;
+
+  static __device__ void init(Local& l, const Params& p, unsigned char* sm, int ctid, int nct) {
+    GbLaneOp::Local g;
+    GbLaneOp::init(g, p, sm, ctid, nct);
+  }
+
+  template <class Acc>
+  static __device__ void step(Local&, const Params& p, unsigned char* sm, const Acc& acc, uint32_t rows,
+                              int ctid, int) {
+    uint64_t* tab = reinterpret_cast<uint64_t*>(sm) + ctid;
+    const int pc = p.f_cmp_col, kc = p.key_col;
+    const uint32_t pmask = p.f_cmp_mask;
+    const double plit = p.f_lit;
+    const uint32_t glast = p.ngroups - 1;
+    const uint32_t f64 = p.f_f64;
+    int vc[NV > 0 ? NV : 1];
+#pragma unroll
+    for (int s = 0; s < NV; ++s) vc[s] = p.f_vcol[s];
+    for (uint32_t b = 0; b < rows; b += kTileRows) {
+      uint32_t off[kR];
+      uint64_t val[kR][NV > 0 ? NV : 1];
+#pragma unroll
+      for (int j = 0; j < kR; ++j) {
+        const uint32_t i = b + j * NCT + ctid;
+        off[j] = 0xFFFFFFFFu;
+#pragma unroll
+        for (int s = 0; s < NV; ++s) val[j][s] = 0;
+        if (i < rows) {
+          bool pass = true;
+          if (pc >= 0) {
+            const double x = acc.template get<double>(pc, i);
+            const uint32_t o = (x < plit ? 1u : 0u) + (x == plit ? 2u : 0u) + (x > plit ? 3u : 0u);
+            pass = (pmask >> o) & 1u;
+          }
+          const uint32_t code = acc.template get<uint32_t>(kc, i);
+          const uint32_t gid = code >= glast ? glast : code;  // the NULL code is above every group
+          if (pass) off[j] = gid * (uint32_t)((1 + NV) * NCT);
+#pragma unroll
+          for (int s = 0; s < NV; ++s) val[j][s] = acc.template get<uint64_t>(vc[s], i);
+        }
+      }
+#pragma unroll
+      for (int j = 0; j < kR; ++j) {
+        if (off[j] == 0xFFFFFFFFu) continue;
+        uint64_t* t = tab + off[j];
+        uint64_t w[1 + NV];
+#pragma unroll
+        for (int s = 0; s <= NV; ++s) w[s] = t[s * NCT];
+        t[0] = w[0] + 1;
+#pragma unroll
+        for (int s = 0; s < NV; ++s) {
+          const uint64_t sum_f = (uint64_t)__double_as_longlong(__longlong_as_double((long long)w[s + 1]) +
+                                                                __longlong_as_double((long long)val[j][s]));
+          t[(s + 1) * NCT] = ((f64 >> s) & 1u) ? sum_f : w[s + 1] + val[j][s];
+        }
+      }
+    }
+  }
+
+  static __device__ void finish(Local&, const Params& p, unsigned char* sm, int ctid, int nct) {
+    GbLaneOp::Local g;
+    GbLaneOp::finish(g, p, sm, ctid, nct);
+  }
+};
+
 // ===========================================================================
 // 2. int64-key hash GROUP BY
 // ===========================================================================
@@ -461,47 +565,128 @@ __device__ __forceinline__ GSlot* gtable_slot(const GbHashParams& p, uint64_t sk
   return gtable_find(p.table, p.mask, skey, p.err);
 }
 
+// Rows whose key finds no room in the CTA table do not probe the global table
+// where they stand (a third of a warp's lanes, each waiting on a DRAM round
+// trip while the others idle).  The warp queues them in a ring in shared
+// memory and drains them 64 at a time: every lane takes two queued rows and
+// has both home-slot loads in flight before it resolves either.
+#ifndef FDB_GB_DRAIN
+#define FDB_GB_DRAIN 64
+#endif
 struct GbHashOp {
   using Params = GbHashParams;
-  struct Local {};
-  static constexpr size_t kSmem = (size_t)kSmemSlots * sizeof(GSlot) + sizeof(GSlot) + 16;
+  struct Local {
+    uint32_t head, tail;  // the warp's ring: entries [head, tail), warp-uniform
+  };
+  static constexpr int kNW = 8;             // consumer warps of every GbHashOp launch
+  static constexpr uint32_t kRing = 128;    // ring entries per warp (holds 63 + 32)
+  static constexpr uint32_t kDrain = FDB_GB_DRAIN;  // 32 or 64
+  static_assert(kDrain == 32 || kDrain == 64, "a drain takes one or two rows per lane");
+  static constexpr size_t kTabBytes = (size_t)(kSmemSlots + 1) * sizeof(GSlot);
+  static constexpr size_t kRingOff = kTabBytes + 16;
+  static constexpr size_t kSmem = kRingOff + (size_t)kNW * kRing * (8 + 8 + 1);
+  static_assert(kRingOff % 8 == 0, "ring alignment");
 
-  static __device__ void init(Local&, const Params&, unsigned char* sm, int ctid, int nct) {
-    uint64_t* w = reinterpret_cast<uint64_t*>(sm);
-    const size_t words = ((size_t)kSmemSlots + 1) * sizeof(GSlot) / 8;
-    for (size_t i = ctid; i < words; i += nct) w[i] = 0;
+  struct Ring {
+    uint64_t* key;
+    double* val;
+    unsigned char* has;
+  };
+  static __device__ __forceinline__ Ring ring(unsigned char* sm, int warp) {
+    Ring r;
+    r.key = reinterpret_cast<uint64_t*>(sm + kRingOff) + (size_t)warp * kRing;
+    r.val = reinterpret_cast<double*>(sm + kRingOff + (size_t)kNW * kRing * 8) + (size_t)warp * kRing;
+    r.has = sm + kRingOff + (size_t)kNW * kRing * 16 + (size_t)warp * kRing;
+    return r;
   }
 
-  template <class Acc>
-  static __device__ void step(Local&, const Params& p, unsigned char* sm, const Acc& acc,
-                              uint32_t rows, int ctid, int nct) {
-    GSlot* tab = reinterpret_cast<GSlot*>(sm);
-    GSlot* snull = tab + kSmemSlots;
-    for (uint32_t i = ctid; i < rows; i += nct) {
-      const uint64_t row = acc.row(i);
-      if (p.prog.n) {
-        GbGetter<Acc> get{p.cols, acc, i, row};
-        if (!eval_prog(p.prog, get)) continue;
-      }
-      const int64_t key = acc.template get<int64_t>(0, i);
-      const bool kvalid = p.cols[0].validity ? col_valid(p.cols[0], row) : true;
-      bool has_v = p.cols[1].validity ? col_valid(p.cols[1], row) : true;
-      double v = 0.0;
-      if (has_v)
-        v = p.cols[1].dtype == FDB_FLOAT64 ? acc.template get<double>(1, i)
-                                           : (double)acc.template get<int64_t>(1, i);
-      if (!kvalid || key == INT64_MIN) {  // NULL group (i64::MIN reads as NULL)
-        gslot_accum(snull, v, has_v);
-        continue;
-      }
-      const uint64_t skey = (uint64_t)key ^ (1ull << 63);
-      GSlot* dst = smem_table_slot(tab, skey);
-      if (dst == nullptr) dst = gtable_slot(p, skey);
-      if (dst) gslot_accum(dst, v, has_v);
+  static __device__ void init(Local& l, const Params&, unsigned char* sm, int ctid, int nct) {
+    uint64_t* w = reinterpret_cast<uint64_t*>(sm);
+    const size_t words = kTabBytes / 8;
+    for (size_t i = ctid; i < words; i += nct) w[i] = 0;
+    l.head = l.tail = 0;
+  }
+
+  // Apply the first `count` (<= kDrain) queued rows to the global table.
+  static __device__ void drain(Local& l, const Params& p, const Ring& r, int lane, uint32_t count) {
+    __syncwarp();
+    const uint32_t e0 = (l.head + lane) & (kRing - 1), e1 = (l.head + 32 + lane) & (kRing - 1);
+    const bool live0 = (uint32_t)lane < count, live1 = (uint32_t)lane + 32 < count;
+    const uint64_t k0 = r.key[e0], k1 = r.key[e1];
+    const double v0 = r.val[e0], v1 = r.val[e1];
+    const bool h0 = r.has[e0], h1 = r.has[e1];
+    __syncwarp();
+    l.head += count;
+    if (*reinterpret_cast<volatile int*>(p.err) != 0) return;
+    const uint64_t a0 = mix64(k0) & p.mask, a1 = mix64(k1) & p.mask;
+    const uint64_t c0 = live0 ? *reinterpret_cast<volatile uint64_t*>(&p.table[a0].key) : 0;
+    const uint64_t c1 = live1 ? *reinterpret_cast<volatile uint64_t*>(&p.table[a1].key) : 0;
+    if (live0) {
+      GSlot* d = gtable_find_from(p.table, p.mask, k0, a0, c0, p.err);
+      if (d) gslot_accum(d, v0, h0);
+    }
+    if (live1) {
+      GSlot* d = gtable_find_from(p.table, p.mask, k1, a1, c1, p.err);
+      if (d) gslot_accum(d, v1, h1);
     }
   }
 
-  static __device__ void finish(Local&, const Params& p, unsigned char* sm, int ctid, int nct) {
+  template <class Acc>
+  static __device__ void step(Local& l, const Params& p, unsigned char* sm, const Acc& acc,
+                              uint32_t rows, int ctid, int nct) {
+    GSlot* tab = reinterpret_cast<GSlot*>(sm);
+    GSlot* snull = tab + kSmemSlots;
+    const int lane = ctid & 31;
+    const Ring r = ring(sm, ctid >> 5);
+    for (uint32_t b = 0; b < rows; b += nct) {  // uniform trip count: the ballot below sees whole warps
+      const uint32_t i = b + ctid;
+      bool spill = false;
+      uint64_t skey = 0;
+      double v = 0.0;
+      bool has_v = false;
+      if (i < rows) {
+        const uint64_t row = acc.row(i);
+        bool pass = true;
+        if (p.prog.n) {
+          GbGetter<Acc> get{p.cols, acc, i, row};
+          pass = eval_prog(p.prog, get);
+        }
+        if (pass) {
+          const int64_t key = acc.template get<int64_t>(0, i);
+          const bool kvalid = p.cols[0].validity ? col_valid(p.cols[0], row) : true;
+          has_v = p.cols[1].validity ? col_valid(p.cols[1], row) : true;
+          if (has_v)
+            v = p.cols[1].dtype == FDB_FLOAT64 ? acc.template get<double>(1, i)
+                                               : (double)acc.template get<int64_t>(1, i);
+          if (!kvalid || key == INT64_MIN) {  // NULL group (i64::MIN reads as NULL)
+            gslot_accum(snull, v, has_v);
+          } else {
+            skey = (uint64_t)key ^ (1ull << 63);
+            GSlot* dst = smem_table_slot(tab, skey);
+            if (dst)
+              gslot_accum(dst, v, has_v);
+            else
+              spill = true;
+          }
+        }
+      }
+      const unsigned m = __ballot_sync(0xffffffffu, spill);
+      if (m) {
+        if (spill) {
+          const uint32_t pos = (l.tail + __popc(m & ((1u << lane) - 1u))) & (kRing - 1);
+          r.key[pos] = skey;
+          r.val[pos] = v;
+          r.has[pos] = has_v ? 1 : 0;
+        }
+        l.tail += __popc(m);
+        if (l.tail - l.head >= kDrain) drain(l, p, r, lane, kDrain);
+      }
+    }
+  }
+
+  static __device__ void finish(Local& l, const Params& p, unsigned char* sm, int ctid, int nct) {
+    const Ring r = ring(sm, ctid >> 5);
+    if (l.tail != l.head) drain(l, p, r, ctid & 31, l.tail - l.head);
     GSlot* tab = reinterpret_cast<GSlot*>(sm);
     consumer_bar(nct);
     for (uint32_t i = ctid; i < kSmemSlots; i += nct) {
@@ -614,6 +799,68 @@ static void gb_fill_prog(PredProg& pp, const fdb_pred_term* prog, int nterms, in
   if (nterms > 0 && depth != 1) fail(FDB_E_ARG, "malformed predicate program");
 }
 
+template <int NC, int NV, int NCW, int R, int ST>
+static void launch_lane_fast_shape(Ctx& c, const fdb_dev_column* cols, uint64_t n, const GbCodesParams& p) {
+  using Op = GbLaneFastOp<NV, NCW, R>;
+  const size_t smem = (size_t)p.ngroups * (1 + NV) * Op::NCT * 8 + 16;
+  launch_stream_gb<Op, NC, Op::kTileRows, ST, NCW>(c, cols, n, p, smem);
+}
+
+template <int NC, int NV>
+static void launch_lane_fast(Ctx& c, const fdb_dev_column* cols, uint64_t n, const GbCodesParams& p) {
+  if (n >= kLaneFastBigRows)
+    launch_lane_fast_shape<NC, NV, FDB_LF_BIG>(c, cols, n, p);
+  else
+    launch_lane_fast_shape<NC, NV, FDB_LF_SMALL>(c, cols, n, p);
+}
+
+// Launch GbLaneFastOp when the query has its shape; false otherwise.
+static bool gb_lane_fast(Ctx& c, const fdb_dev_column* cols, int ncols, uint64_t n, const fdb_pred_term* prog,
+                         int nterms, int key_col, const fdb_agg_spec* aggs, int naggs, GbCodesParams& p) {
+  if (cols[key_col].validity) return false;
+  p.f_cmp_col = -1;
+  if (nterms == 1) {
+    const fdb_pred_term& t = prog[0];
+    if (t.kind != FDB_TERM_CMP || cols[t.col].dtype != FDB_FLOAT64 || cols[t.col].validity) return false;
+    static const uint32_t kAccept[6] = {
+        1u << 2,                       // ==
+        (1u << 0) | (1u << 1) | (1u << 3),  // != (true for NaN)
+        1u << 1,                       // <
+        (1u << 1) | (1u << 2),         // <=
+        1u << 3,                       // >
+        (1u << 3) | (1u << 2)};        // >=
+    if (t.op < FDB_EQ || t.op > FDB_GE) return false;
+    p.f_cmp_col = t.col;
+    p.f_cmp_mask = kAccept[t.op];
+    p.f_lit = t.lit_type == FDB_FLOAT64 ? t.lit_f : (double)t.lit_i;
+  } else if (nterms != 0) {
+    return false;
+  }
+  p.f_f64 = 0;
+  for (int a = 0; a < naggs; ++a) {
+    const int f = aggs[a].func;
+    if (f == FDB_AGG_COUNT_STAR) continue;
+    if (f != FDB_AGG_SUM && f != FDB_AGG_AVG) return false;
+    const fdb_dev_column& col = cols[aggs[a].col];
+    if (col.validity || (col.dtype != FDB_FLOAT64 && col.dtype != FDB_INT64)) return false;
+    const int s = p.vslot[a];
+    if (s < 1 || s > 4 || p.cslot[a] >= 0) return false;
+    p.f_vcol[s - 1] = aggs[a].col;
+    if (col.dtype == FDB_FLOAT64) p.f_f64 |= 1u << (s - 1);
+  }
+  const int nv = p.nslots - 1;
+  switch (ncols * 8 + nv) {
+#define FDB_LF_CASE(NC, NV) \
+  case NC * 8 + NV: launch_lane_fast<NC, NV>(c, cols, n, p); return true;
+    FDB_LF_CASE(1, 0)
+    FDB_LF_CASE(2, 0) FDB_LF_CASE(2, 1) FDB_LF_CASE(2, 2) FDB_LF_CASE(2, 3)
+    FDB_LF_CASE(3, 0) FDB_LF_CASE(3, 1) FDB_LF_CASE(3, 2) FDB_LF_CASE(3, 3)
+    FDB_LF_CASE(4, 0) FDB_LF_CASE(4, 1) FDB_LF_CASE(4, 2) FDB_LF_CASE(4, 3)
+#undef FDB_LF_CASE
+    default: return false;
+  }
+}
+
 void op_group_by_codes(Ctx& c, const fdb_dev_column* cols, int ncols, uint64_t n,
                        const fdb_pred_term* prog, int nterms, int key_col, uint32_t dict_len,
                        const fdb_agg_spec* aggs, int naggs, fdb_agg_value* d_out,
@@ -666,6 +913,9 @@ void op_group_by_codes(Ctx& c, const fdb_dev_column* cols, int ncols, uint64_t n
   p.ticket = c.d_ticket;
   p.out = d_out;
   p.group_rows = d_group_rows;
+  if ((uint64_t)p.ngroups * ns <= kLaneEntries && gb_lane_fast(c, cols, ncols, n, prog, nterms, key_col, aggs,
+                                                               naggs, p))
+    return;
   if ((uint64_t)p.ngroups * ns <= kLaneEntries) {
     // Lane-private tables: one table column per consumer thread.
     const size_t sm4 = (size_t)p.ngroups * ns * 128 * 8 + 16;
@@ -742,6 +992,7 @@ void op_group_by_i64(Ctx& c, const fdb_dev_column& key, const fdb_dev_column& va
   p.err = c.d_err;
   if (n > 0) {
     switch (nc) {
+      // NCW = GbHashOp::kNW: the operator keeps one spill ring per consumer warp.
       case 2: launch_stream_gb<GbHashOp, 2, 1024, 3, 8>(c, all, n, p, GbHashOp::kSmem); break;
       case 3: launch_stream_gb<GbHashOp, 3, 1024, 2, 8>(c, all, n, p, GbHashOp::kSmem); break;
       default: launch_stream_gb<GbHashOp, 4, 512, 3, 8>(c, all, n, p, GbHashOp::kSmem); break;

@@ -44,6 +44,83 @@ def test_filter_group_by_dept(db, n):
         assert rec[d, 3]["f"] == g["fmin"][d]
 
 
+def _same_f(a, b):
+    return (np.isnan(a) and np.isnan(b)) or close(a, b)
+
+
+OPS = [F.EQ, F.NE, F.LT, F.LE, F.GT, F.GE]
+
+
+@pytest.mark.parametrize("op", OPS)
+@pytest.mark.parametrize("n,off,lit", [(1, 0, 50), (4099, 0, 50.0), (1_000_003, 0, 50), (100_001, 1, 49.5),
+                                       (16_777_219, 0, 50.0)])
+def test_lane_fast_path_every_operator(db, op, n, off, lit):
+    """WHERE score <op> literal GROUP BY code with COUNT(*), SUM(score),
+    AVG(salary) — the specialised lane kernel's shape — over NaN scores (only
+    != accepts them), scores equal to the literal, NULL and out-of-dictionary
+    codes, int and float literals, (off=1) views that are not 16-byte aligned,
+    which take the plain-load path, and both launch shapes (2^24 rows and
+    more run the large-input shape)."""
+    r = np.random.default_rng(n * 7 + op)
+    tot = n + off
+    codes = r.integers(0, 14, tot).astype(np.uint32)  # 12 and 13 are outside the 12-entry dictionary
+    codes[::17] = 0xFFFFFFFF
+    score = np.floor(r.random(tot) * 100.0)
+    score[::23] = np.nan
+    salary = r.integers(-(1 << 30), 1 << 30, tot)
+    cols = [dev(codes.view(np.int32))[off:], dev(score)[off:], dev(salary)[off:]]
+    codes, score, salary = codes[off:], score[off:], salary[off:]
+    out, rows = ops.group_by_codes(db, cols, n, [ops.cmp(1, op, lit)], 0, 12,
+                                   [(F.AGG_COUNT_STAR, 0), (F.AGG_SUM, 1), (F.AGG_AVG, 2)])
+    rec = ops.to_records(out, F.AGG_VALUE_DTYPE).reshape(13, 3)
+    g = O.group_codes(codes, 12, mask=O.cmp_mask(score, op, lit), fvals=score, ivals=salary)
+    assert list(rows.cpu().numpy()) == list(g["rows"])
+    for d in range(13):
+        assert rec[d, 0]["i"] == g["rows"][d]
+        if g["rows"][d] == 0:
+            continue
+        assert _same_f(rec[d, 1]["f"], g["fsum"][d])
+        assert rec[d, 2]["f"] == g["isum"][d] / g["icnt"][d]
+
+
+@pytest.mark.parametrize("n", [5, 777_777])
+def test_lane_fast_path_shapes(db, n):
+    """The specialised lane kernel with 0, 2 and 3 summed slots over 1, 2 and
+    4 staged columns (a column summed twice, int64 and FP64 slots mixed)."""
+    t = W.table_t(n, seed=n)
+    codes, score, salary, ids = t["dept"].codes, t["score"], t["salary"], t["id"]
+    dc, ds, dsal, did = dev(codes.view(np.int32)), dev(score), dev(salary), dev(ids)
+    # 1 column, COUNT(*) only.
+    out, rows = ops.group_by_codes(db, [dc], n, [], 0, 12, [(F.AGG_COUNT_STAR, 0)])
+    g = O.group_codes(codes, 12)
+    assert list(rows.cpu().numpy()) == list(g["rows"])
+    assert list(ops.to_records(out, F.AGG_VALUE_DTYPE)["i"]) == list(g["rows"])
+    # 2 columns: the WHERE column summed twice.
+    out, rows = ops.group_by_codes(db, [dc, ds], n, [ops.cmp(1, F.LT, 30.0)], 0, 12,
+                                   [(F.AGG_COUNT_STAR, 0), (F.AGG_SUM, 1), (F.AGG_AVG, 1)])
+    rec = ops.to_records(out, F.AGG_VALUE_DTYPE).reshape(13, 3)
+    g = O.group_codes(codes, 12, mask=O.cmp_mask(score, F.LT, 30.0), fvals=score)
+    assert list(rows.cpu().numpy()) == list(g["rows"])
+    for d in range(12):
+        if g["rows"][d]:
+            assert close(rec[d, 1]["f"], g["fsum"][d])
+            assert close(rec[d, 2]["f"], g["fsum"][d] / g["fcnt"][d])
+    # 4 columns, 3 summed slots.
+    out, rows = ops.group_by_codes(db, [dc, ds, dsal, did], n, [ops.cmp(1, F.GE, 10.5)], 0, 12,
+                                   [(F.AGG_SUM, 2), (F.AGG_SUM, 1), (F.AGG_AVG, 3), (F.AGG_COUNT_STAR, 0)])
+    rec = ops.to_records(out, F.AGG_VALUE_DTYPE).reshape(13, 4)
+    mask = O.cmp_mask(score, F.GE, 10.5)
+    g1 = O.group_codes(codes, 12, mask=mask, fvals=score, ivals=salary)
+    g2 = O.group_codes(codes, 12, mask=mask, ivals=ids)
+    assert list(rows.cpu().numpy()) == list(g1["rows"])
+    for d in range(12):
+        if g1["rows"][d]:
+            assert rec[d, 0]["f"] == g1["isum"][d]
+            assert close(rec[d, 1]["f"], g1["fsum"][d])
+            assert rec[d, 2]["f"] == g2["isum"][d] / g2["icnt"][d]
+            assert rec[d, 3]["i"] == g1["rows"][d]
+
+
 def test_group_by_codes_nulls_and_empty_groups(db):
     n = 50_000
     r = np.random.default_rng(3)
