@@ -38,6 +38,33 @@ __device__ __forceinline__ void gslot_accum(GSlot* s, double v, bool has_v) {
   }
 }
 
+// Shared-memory (CTA table) slots count rows with a 32-bit atomic on the low
+// word of `count`: shared memory has a native 32-bit atomic add, while its
+// 64-bit integer and FP64 adds are compare-and-swap loops that serialise on a
+// hot slot.  A CTA sees fewer than 2^32 rows of one query, and readers take
+// the whole 64-bit word (high word zero).
+__device__ __forceinline__ void sslot_accum(GSlot* s, double v, bool has_v) {
+  atomicAdd(reinterpret_cast<unsigned int*>(&s->count), 1u);
+  if (has_v) {
+    atomicAdd(&s->sum, v);
+    if (!isnan(v)) {
+      const uint64_t k = f64_ord_key(v);
+      atomicMax(&s->nmin, (unsigned long long)~k);
+      atomicMax(&s->max, (unsigned long long)k);
+    }
+  }
+}
+
+// A group of `n` rows folded beforehand: `has_sum` when at least one had a
+// value; nmin / max are 0 when none had a non-NaN value.
+__device__ __forceinline__ void sslot_accum_n(GSlot* s, uint32_t n, bool has_sum, double sum, uint64_t nmin,
+                                              uint64_t max) {
+  atomicAdd(reinterpret_cast<unsigned int*>(&s->count), n);
+  if (has_sum) atomicAdd(&s->sum, sum);
+  if (nmin) atomicMax(&s->nmin, (unsigned long long)nmin);
+  if (max) atomicMax(&s->max, (unsigned long long)max);
+}
+
 __device__ __forceinline__ void gslot_merge(GSlot* s, const GSlot& v) {
   atomicAdd(&s->count, v.count);
   atomicAdd(&s->sum, v.sum);

@@ -85,17 +85,20 @@ __global__ void __launch_bounds__(kBatchThreads) gb_batch_kernel(BatchArgs a) {
     reinterpret_cast<uint64_t*>(tab)[i] = 0;
   __syncthreads();
   int cur = -1;
+  uint64_t since_flush = 0;  // rows in the CTA table: its 32-bit row counts must not wrap
   for (;;) {
     if (threadIdx.x == 0) s_t = atomicAdd(a.claim, 1u);
     __syncthreads();
     const uint64_t t = s_t;
     if (t >= a.total_tiles) break;
     const int qi = batch_find(start, a.nq, t);
-    if (qi != cur) {
+    if (qi != cur || since_flush + a.tile_rows >= (1ull << 32)) {
       if (cur >= 0) batch_flush(tab, a.q[cur], a.err);
       __syncthreads();
       cur = qi;
+      since_flush = 0;
     }
+    since_flush += a.tile_rows;
     const BatchQuery& q = a.q[qi];
     const uint64_t r0 = (t - q.tile0) * a.tile_rows;
     const uint64_t r1 = umin64(r0 + a.tile_rows, q.n);
@@ -108,12 +111,16 @@ __global__ void __launch_bounds__(kBatchThreads) gb_batch_kernel(BatchArgs a) {
         v = q.val.dtype == FDB_FLOAT64 ? __ldcs(static_cast<const double*>(q.val.values) + r)
                                        : (double)__ldcs(static_cast<const int64_t*>(q.val.values) + r);
       if (!col_valid(q.key, r) || key == INT64_MIN) {  // NULL group
-        gslot_accum(tab + kSmemSlots, v, has_v);
+        sslot_accum(tab + kSmemSlots, v, has_v);
         continue;
       }
       const uint64_t skey = (uint64_t)key ^ (1ull << 63);
       GSlot* dst = smem_table_slot(tab, skey);
-      if (dst == nullptr) dst = gtable_find(q.table, q.mask, skey, a.err);
+      if (dst) {
+        sslot_accum(dst, v, has_v);
+        continue;
+      }
+      dst = gtable_find(q.table, q.mask, skey, a.err);
       if (dst) gslot_accum(dst, v, has_v);
     }
     __syncthreads();  // the tile is done before s_t is rewritten or the table flushed

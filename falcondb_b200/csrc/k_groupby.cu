@@ -635,11 +635,11 @@ struct GbHashOp {
   static __device__ void step(Local& l, const Params& p, unsigned char* sm, const Acc& acc,
                               uint32_t rows, int ctid, int nct) {
     GSlot* tab = reinterpret_cast<GSlot*>(sm);
-    GSlot* snull = tab + kSmemSlots;
     const int lane = ctid & 31;
     const Ring r = ring(sm, ctid >> 5);
     for (uint32_t b = 0; b < rows; b += nct) {  // uniform trip count: the ballot below sees whole warps
       const uint32_t i = b + ctid;
+      int j = -1;  // CTA slot of the row (kSmemSlots: the NULL group); -1: none
       bool spill = false;
       uint64_t skey = 0;
       double v = 0.0;
@@ -659,17 +659,18 @@ struct GbHashOp {
             v = p.cols[1].dtype == FDB_FLOAT64 ? acc.template get<double>(1, i)
                                                : (double)acc.template get<int64_t>(1, i);
           if (!kvalid || key == INT64_MIN) {  // NULL group (i64::MIN reads as NULL)
-            gslot_accum(snull, v, has_v);
+            j = (int)kSmemSlots;
           } else {
             skey = (uint64_t)key ^ (1ull << 63);
             GSlot* dst = smem_table_slot(tab, skey);
             if (dst)
-              gslot_accum(dst, v, has_v);
+              j = (int)(dst - tab);
             else
               spill = true;
           }
         }
       }
+      if (j >= 0) sslot_accum(tab + j, v, has_v);
       const unsigned m = __ballot_sync(0xffffffffu, spill);
       if (m) {
         if (spill) {
@@ -964,6 +965,8 @@ void op_group_by_i64(Ctx& c, const fdb_dev_column& key, const fdb_dev_column& va
   if (value.dtype != FDB_FLOAT64 && value.dtype != FDB_INT64)
     fail(FDB_E_TYPE, "hash GROUP BY value must be FLOAT64 or INT64");
   if (npred < 0 || npred > 2) fail(FDB_E_ARG, "at most 2 predicate columns");
+  // The CTA tables count rows in 32 bits; a CTA sees about n / grid rows.
+  if (n / (uint64_t)c.sm_count >= (1ull << 31)) fail(FDB_E_ARG, "more than 2^31 rows per SM in one GROUP BY");
   if (load_factor <= 0.0 || load_factor >= 1.0) load_factor = 0.5;
   if (expected_groups == 0) expected_groups = n ? n : 1;
   const uint64_t cap = gb_table_capacity(expected_groups, load_factor);

@@ -13,13 +13,15 @@
 //
 // serve_kernel is persistent and scans shared: the batch's COUNT, GROUP and
 // JOIN queries are grouped by the table they read, and each group's rows are
-// cut into kShareTile-row units.  A CTA that claims a unit stages the rows'
-// columns in shared memory once (for a join group it also probes every row
-// once: whether a build row matches does not depend on the query) and then
-// evaluates every query of the group that covers the unit from shared memory,
-// each with its own predicate.  HBM therefore sees each table once per batch,
-// not once per query.  Partial results go out with one atomic per warp (COUNT,
-// JOIN) or per group and field (GROUP BY) per query and unit.
+// cut into units that fill one pipeline stage (28 KB: 3584 rows of one 8-byte
+// column, 1280 rows of a GROUP or JOIN group's columns).  A CTA's producer warp
+// claims units from one counter and stages their columns into a ring of
+// shared-memory buffers with bulk copies; its consumer warps then probe a join
+// group's rows once (whether a build row matches does not depend on the query)
+// and evaluate every query of the group that covers the unit from shared
+// memory, each with its own predicate.  HBM therefore sees each table once per
+// batch, not once per query.  Partial results go out with one atomic per warp
+// (COUNT, JOIN) or per group and field (GROUP BY) per query and unit.
 // Top-k queries scan their own rows in kServeTile-row units claimed after the
 // shared ones: a CTA keeps a list per warp while its consecutive units belong
 // to one query and publishes its k best (below the query's running bound) as
@@ -44,14 +46,28 @@
 
 namespace fdb {
 
-constexpr int kServeThreads = 256;
+constexpr int kServeThreads = 256;                 // consumer threads (8 warps)
 constexpr int kServeWarps = kServeThreads / 32;
+constexpr int kServeBlock = kServeThreads + 32;    // + the producer warp
 constexpr uint32_t kServeTile = 8192;
 constexpr int kServeMaxBatch = 256;
-constexpr int kServeCtasPerSm = 3;
-constexpr uint32_t kShareTile = 2048;
-// Shared-scan staging: c0 (8 B/row), c1 (<= 8 B/row), c2 (8 B/row), matches (4 B/row).
-constexpr size_t kShareSmem = (size_t)kShareTile * (8 + 8 + 8 + 4);
+#ifndef FDB_SERVE_CTAS
+#define FDB_SERVE_CTAS 2
+#endif
+constexpr int kServeCtasPerSm = FDB_SERVE_CTAS;
+#ifndef FDB_SERVE_STAGES
+#define FDB_SERVE_STAGES 2
+#endif
+constexpr int kServeStages = FDB_SERVE_STAGES;
+// A stage holds one unit of a shared group: its columns c0 (8 B/row), c1 (0,
+// 4 or 8 B/row), c2 (0 or 8 B/row) and, for a join, the match counts (4 B/row),
+// one after another; a unit is as many rows (a multiple of 256) as fit.
+constexpr size_t kShareStage = 28 * 1024;
+// Barrier block: full[stages], empty[stages], the unit of each stage, and the
+// columns each stage's consumers must load themselves (bit c: column c).
+constexpr size_t kServeBar = 128;
+constexpr size_t kShareSmem = kServeBar + kServeStages * kShareStage;
+static_assert(kServeStages * (8 + 8 + 8 + 4) <= kServeBar, "barrier block");
 
 struct ServeQ {            // device descriptor of one query
   int32_t kind, k;
@@ -84,6 +100,8 @@ struct ServeG {             // a group of queries that read the same table
   const void* c2;
   uint32_t q0, nq;          // its queries, by rows descending
   uint64_t max_n, unit0;
+  uint32_t unit_rows;       // rows per unit
+  uint32_t off1, off2, offm;  // stage byte offsets of c1, c2 and the join match counts
   int32_t c1_bytes;         // 0 (not read), 4 (dictionary codes) or 8
   int32_t load_c2;
   int32_t join;             // c0 holds probe keys for the table below
@@ -111,19 +129,58 @@ struct ServeArgs {
   int* err;
 };
 
+// Descriptors the serving kernel keeps in shared memory (the first ones of a
+// batch; later ones are read from global memory).
+constexpr int kServeCacheG = 32;
+constexpr int kServeCacheQ = 64;
+static_assert(sizeof(ServeG) % 8 == 0 && sizeof(ServeQ) % 8 == 0, "descriptors copy as 8-byte words");
+
 struct ServeSmem {
   uint64_t start[kServeMaxBatch + 1];   // unit0 of each top-k query
   uint64_t gstart[kServeMaxBatch + 1];  // unit0 of each shared group
-  // GROUP BY partials: per warp, two copies (even and odd lanes) to halve
-  // the atomic contention of lanes that hit the same group.
-  unsigned long long gcount[kServeWarps][2][FDB_SERVE_MAX_GROUPS];
-  double gsum0[kServeWarps][2][FDB_SERVE_MAX_GROUPS];
-  long long gsum2[kServeWarps][2][FDB_SERVE_MAX_GROUPS];
+  ServeG g[kServeCacheG];
+  ServeQ q[kServeCacheQ];
+  // The CTA's partial results of the first kServeCacheQ queries, added to the
+  // global results once, when the CTA ends (per-unit global atomics would all
+  // meet on the few words of a query's result).
+  unsigned long long acount[kServeCacheQ];
+  unsigned long long asum[kServeCacheQ];
+  unsigned long long agcount[kServeCacheQ][FDB_SERVE_MAX_GROUPS];
+  double agsum0[kServeCacheQ][FDB_SERVE_MAX_GROUPS];
+  long long agsum2[kServeCacheQ][FDB_SERVE_MAX_GROUPS];
+  // GROUP BY partials of one unit, per warp (written by one lane at a time).
+  unsigned long long gcount[kServeWarps][FDB_SERVE_MAX_GROUPS];
+  double gsum0[kServeWarps][FDB_SERVE_MAX_GROUPS];
+  long long gsum2[kServeWarps][FDB_SERVE_MAX_GROUPS];
   uint64_t tkeys[kServeWarps][32];
   uint32_t trows[kServeWarps][32];
   unsigned long long red[kServeWarps][2];
   unsigned int t;
 };
+
+__device__ __forceinline__ const ServeG& serve_g(const ServeArgs& a, const ServeSmem& sm, int gi) {
+  return gi < kServeCacheG ? sm.g[gi] : a.g[gi];
+}
+__device__ __forceinline__ const ServeQ& serve_q(const ServeArgs& a, const ServeSmem& sm, int qi) {
+  return qi < kServeCacheQ ? sm.q[qi] : a.q[qi];
+}
+
+// Barriers among the consumer warps only (named barrier 1): the producer warp
+// never joins them.
+__device__ __forceinline__ void serve_bar() {
+  asm volatile("bar.sync 1, %0;" ::"r"(kServeThreads) : "memory");
+}
+// True on every consumer thread when `x` holds on any of them.
+__device__ __forceinline__ bool serve_bar_any(bool x) {
+  uint32_t r;
+  asm volatile(
+      "{\n\t.reg .pred p, q;\n\tsetp.ne.u32 p, %1, 0;\n\tbar.red.or.pred q, 1, %2, p;\n\t"
+      "selp.u32 %0, 1, 0, q;\n\t}"
+      : "=r"(r)
+      : "r"((uint32_t)x), "r"(kServeThreads)
+      : "memory");
+  return r != 0;
+}
 
 __device__ __forceinline__ int serve_find(const uint64_t* start, int nq, uint64_t t) {
   int lo = 0, hi = nq;  // start[lo] <= t < start[hi]
@@ -137,16 +194,16 @@ __device__ __forceinline__ int serve_find(const uint64_t* start, int nq, uint64_
 // Merge every warp's list into warp 0 (sorted-list merges, log2(warps) levels).
 __device__ void serve_tree_merge(ServeSmem& sm, RTLocal& s, uint32_t k, int warp, int lane) {
   for (int half = kServeWarps / 2; half >= 1; half >>= 1) {
-    __syncthreads();
+    serve_bar();
     if (warp >= half && warp < 2 * half) {
       const bool in = (uint32_t)lane < k;
       sm.tkeys[warp][lane] = in ? s.lk : ~0ull;
       sm.trows[warp][lane] = in ? s.lr : 0xFFFFFFFFu;
     }
-    __syncthreads();
+    serve_bar();
     if (warp < half) rt_merge_sorted(s, k, sm.tkeys[warp + half][lane], sm.trows[warp + half][lane], lane);
   }
-  __syncthreads();
+  serve_bar();
 }
 
 __device__ __forceinline__ void rt_reset(RTLocal& s) {
@@ -157,8 +214,8 @@ __device__ __forceinline__ void rt_reset(RTLocal& s) {
   s.steps = 0;
 }
 
-// Publish this CTA's top-k state for query qi (all threads call; ends with a barrier).
-__device__ void serve_publish(const ServeArgs& a, const ServeQ& q, int qi, ServeSmem& sm, RTLocal& tl) {
+// Publish this CTA's top-k state for query qi (all consumer threads call; ends with a barrier).
+__device__ void serve_publish(const ServeArgs& a, const ServeQ q, int qi, ServeSmem& sm, RTLocal& tl) {
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   ServeRes& r = a.res[qi];
   const uint32_t k = (uint32_t)q.k;
@@ -186,11 +243,11 @@ __device__ void serve_publish(const ServeArgs& a, const ServeQ& q, int qi, Serve
     }
   }
   rt_reset(tl);
-  __syncthreads();
+  serve_bar();
 }
 
 // Rows [r0, r1) of a top-k query: WHERE c0 < thr ORDER BY c0 DESC into the warp lists.
-__device__ __forceinline__ void serve_topk_tile(const ServeQ& q, uint64_t r0, uint64_t r1, RTLocal& tl) {
+__device__ __forceinline__ void serve_topk_tile(const ServeQ q, uint64_t r0, uint64_t r1, RTLocal& tl) {
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const uint64_t* c0 = static_cast<const uint64_t*>(q.c0);
   const uint32_t k = (uint32_t)q.k;
@@ -228,22 +285,23 @@ __device__ __forceinline__ void serve_topk_tile(const ServeQ& q, uint64_t r0, ui
   }
 }
 
-// Copy rows [r0, r0 + rows) of a column (esize 4 or 8) into shared memory.
+// Copy rows [r0, r0 + rows) of a column (esize 4 or 8) into shared memory
+// with plain loads (consumer threads; columns the bulk copies cannot take).
 __device__ __forceinline__ void share_load(unsigned char* dst, const void* src, uint64_t r0, uint32_t rows, int esize) {
   const unsigned char* s = static_cast<const unsigned char*>(src) + r0 * esize;
   const uint32_t bytes = rows * (uint32_t)esize;
   uint32_t done = 0;
   if (((uintptr_t)s & 15u) == 0) {
     const uint32_t nv = bytes / 16;
-    for (uint32_t i = threadIdx.x; i < nv; i += blockDim.x)
+    for (uint32_t i = threadIdx.x; i < nv; i += kServeThreads)
       reinterpret_cast<uint4*>(dst)[i] = __ldcs(reinterpret_cast<const uint4*>(s) + i);
     done = nv * 16;
   }
   if (esize == 8) {
-    for (uint32_t i = done / 8 + threadIdx.x; i < rows; i += blockDim.x)
+    for (uint32_t i = done / 8 + threadIdx.x; i < rows; i += kServeThreads)
       reinterpret_cast<uint64_t*>(dst)[i] = __ldcs(reinterpret_cast<const unsigned long long*>(s) + i);
   } else {
-    for (uint32_t i = done / 4 + threadIdx.x; i < rows; i += blockDim.x)
+    for (uint32_t i = done / 4 + threadIdx.x; i < rows; i += kServeThreads)
       reinterpret_cast<uint32_t*>(dst)[i] = __ldcs(reinterpret_cast<const unsigned int*>(s) + i);
   }
 }
@@ -254,17 +312,17 @@ __device__ __forceinline__ void share_load(unsigned char* dst, const void* src, 
 // round, so their L2 round trips overlap.
 constexpr int kProbeIlp = 4;
 
-__device__ void serve_probe_rows(const ServeG& g, uint64_t* s0, uint32_t* m, uint32_t rows) {
+__device__ void serve_probe_rows(const ServeG g, uint64_t* s0, uint32_t* m, uint32_t rows) {
   const int shift = join_shift(g.cap);
   const uint64_t mask = g.cap - 1;
   const uint64_t pol = l2_evict_last_policy();
-  for (uint32_t base = 0; base < rows; base += kProbeIlp * blockDim.x) {
+  for (uint32_t base = 0; base < rows; base += kProbeIlp * kServeThreads) {
     uint64_t sk[kProbeIlp], h[kProbeIlp], ps[kProbeIlp];
     uint32_t at[kProbeIlp];
     uint32_t todo = 0;
 #pragma unroll
     for (int j = 0; j < kProbeIlp; ++j) {
-      const uint32_t i = base + j * blockDim.x + threadIdx.x;
+      const uint32_t i = base + j * kServeThreads + threadIdx.x;
       at[j] = kNoSlot;
       ps[j] = 0;
       sk[j] = 0;
@@ -310,46 +368,78 @@ __device__ void serve_probe_rows(const ServeG& g, uint64_t* s0, uint32_t* m, uin
     }
 #pragma unroll
     for (int j = 0; j < kProbeIlp; ++j) {
-      const uint32_t i = base + j * blockDim.x + threadIdx.x;
+      const uint32_t i = base + j * kServeThreads + threadIdx.x;
       if (i >= rows) continue;
       m[i] = at[j] == kNoSlot ? 0u : (g.unique ? 1u : g.cnt[at[j]]);
       s0[i] = ps[j];
     }
   }
-  __syncthreads();
+  serve_bar();
 }
 
-// One shared unit: stage the group's rows, probe them once for a join group,
-// then evaluate every query of the group that reaches this unit.
-__device__ void serve_shared_unit(const ServeArgs& a, const ServeG& g, uint64_t tile, unsigned char* tsm,
-                                  ServeSmem& sm) {
+// The staged columns of a shared group's unit: column c at stage byte off[c].
+struct ShareCols {
+  const void* src[3];
+  int esize[3];  // 0: not read
+  uint32_t off[3];
+};
+
+__device__ __forceinline__ ShareCols share_cols(const ServeG& g) {
+  ShareCols c;
+  c.src[0] = g.c0;
+  c.esize[0] = 8;
+  c.off[0] = 0;
+  c.src[1] = g.c1;
+  c.esize[1] = g.c1_bytes;
+  c.off[1] = g.off1;
+  c.src[2] = g.c2;
+  c.esize[2] = g.load_c2 ? 8 : 0;
+  c.off[2] = g.off2;
+  return c;
+}
+
+// One shared unit whose rows are staged at `st` (the columns in `plain` are
+// loaded here by the consumers): probe them once for a join group, then
+// evaluate every query of the group that reaches this unit.
+// `g` is taken by value: the loops below store to shared memory, where a
+// cached descriptor may live, so fields read through a reference would be
+// reloaded after every store.
+__device__ void serve_shared_unit(const ServeArgs& a, const ServeG g, uint64_t tile, unsigned char* st,
+                                  uint32_t plain, ServeSmem& sm) {
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  const uint64_t r0 = tile * kShareTile;
-  const uint32_t rows = (uint32_t)umin64(kShareTile, g.max_n - r0);
-  uint64_t* s0 = reinterpret_cast<uint64_t*>(tsm);
-  unsigned char* s1 = tsm + (size_t)kShareTile * 8;
-  const int64_t* s2 = reinterpret_cast<const int64_t*>(tsm + (size_t)kShareTile * 16);
-  uint32_t* smm = reinterpret_cast<uint32_t*>(tsm + (size_t)kShareTile * 24);
-  share_load(tsm, g.c0, r0, rows, 8);
-  if (g.c1_bytes) share_load(s1, g.c1, r0, rows, g.c1_bytes);
-  if (g.load_c2) share_load(tsm + (size_t)kShareTile * 16, g.c2, r0, rows, 8);
-  __syncthreads();
+  const uint64_t r0 = tile * g.unit_rows;
+  const uint32_t rows = (uint32_t)umin64(g.unit_rows, g.max_n - r0);
+  uint64_t* s0 = reinterpret_cast<uint64_t*>(st);
+  unsigned char* s1 = st + g.off1;
+  const int64_t* s2 = reinterpret_cast<const int64_t*>(st + g.off2);
+  uint32_t* smm = reinterpret_cast<uint32_t*>(st + g.offm);
+  if (plain) {
+    const ShareCols cols = share_cols(g);
+#pragma unroll
+    for (int c = 0; c < 3; ++c)
+      if ((plain >> c) & 1u) share_load(st + cols.off[c], cols.src[c], r0, rows, cols.esize[c]);
+    serve_bar();
+  }
   if (g.join) serve_probe_rows(g, s0, smm, rows);
   for (uint32_t qi = g.q0; qi < g.q0 + g.nq; ++qi) {
-    const ServeQ& q = a.q[qi];
-    if (q.n <= r0) break;  // queries are by rows descending
-    const uint32_t re = (uint32_t)umin64(rows, q.n - r0);
+    const ServeQ& qref = serve_q(a, sm, (int)qi);
+    const uint64_t qn = qref.n;
+    if (qn <= r0) break;  // queries are by rows descending
+    const int qkind = qref.kind;
+    const double qthr = qref.thr;
+    const uint32_t qdict = qref.dict_len;
+    const uint32_t re = (uint32_t)umin64(rows, qn - r0);
     ServeRes& r = a.res[qi];
-    if (q.kind == FDB_SERVE_COUNT) {
+    if (qkind == FDB_SERVE_COUNT) {
       unsigned long long c = 0;
-      for (uint32_t i = threadIdx.x; i < re; i += blockDim.x) c += __longlong_as_double((long long)s0[i]) > q.thr;
+      for (uint32_t i = threadIdx.x; i < re; i += kServeThreads) c += __longlong_as_double((long long)s0[i]) > qthr;
       c = warp_sum_u64(c);
-      if (lane == 0 && c) atomicAdd(&r.count, c);
-    } else if (q.kind == FDB_SERVE_JOIN) {
-      const double lim = q.thr / 100.0;
+      if (lane == 0 && c) atomicAdd(qi < (uint32_t)kServeCacheQ ? &sm.acount[qi] : &r.count, c);
+    } else if (qkind == FDB_SERVE_JOIN) {
+      const double lim = qthr / 100.0;
       const double* v = reinterpret_cast<const double*>(s1);
       unsigned long long c = 0, ps = 0;
-      for (uint32_t i = threadIdx.x; i < re; i += blockDim.x)
+      for (uint32_t i = threadIdx.x; i < re; i += kServeThreads)
         if (v[i] < lim) {
           c += smm[i];
           ps += s0[i];
@@ -357,90 +447,221 @@ __device__ void serve_shared_unit(const ServeArgs& a, const ServeG& g, uint64_t 
       c = warp_sum_u64(c);
       ps = warp_sum_u64(ps);
       if (lane == 0 && c) {
-        atomicAdd(&r.count, c);
-        atomicAdd(reinterpret_cast<unsigned long long*>(&r.sum), ps);
+        const bool local = qi < (uint32_t)kServeCacheQ;
+        atomicAdd(local ? &sm.acount[qi] : &r.count, c);
+        atomicAdd(local ? &sm.asum[qi] : reinterpret_cast<unsigned long long*>(&r.sum), ps);
       }
     } else {  // GROUP
-      {
-        const int cp = lane >> 4, gi = lane & 15;  // 32 lanes clear 2 copies x 16 groups
-        sm.gcount[warp][cp][gi] = 0;
-        sm.gsum0[warp][cp][gi] = 0.0;
-        sm.gsum2[warp][cp][gi] = 0;
+      if (lane < FDB_SERVE_MAX_GROUPS) {
+        sm.gcount[warp][lane] = 0;
+        sm.gsum0[warp][lane] = 0.0;
+        sm.gsum2[warp][lane] = 0;
       }
       __syncwarp();
-      const int cp = lane & 1;
+      // 32 rows at a time: the lanes whose rows pass and share a group find
+      // one another (__match_any_sync on the code); the lowest of them folds
+      // the group's rows, in row order, straight from the staged columns and
+      // updates the warp's table with plain stores.  No two lanes of a warp
+      // ever write one group's words at once, and no other warp writes them.
       const uint32_t* codes = reinterpret_cast<const uint32_t*>(s1);
-      for (uint32_t i = threadIdx.x; i < re; i += blockDim.x) {
-        const double v = __longlong_as_double((long long)s0[i]);
-        const uint32_t gc = codes[i];
-        if (v > q.thr && gc < q.dict_len) {
-          atomicAdd(&sm.gcount[warp][cp][gc], 1ull);
-          atomicAdd(&sm.gsum0[warp][cp][gc], v);
-          atomicAdd(reinterpret_cast<unsigned long long*>(&sm.gsum2[warp][cp][gc]), (unsigned long long)s2[i]);
+      for (uint32_t b = (uint32_t)warp * 32; b < re; b += kServeThreads) {
+        const uint32_t i = b + lane;
+        uint32_t gc = 0xFFFFFFFFu;
+        if (i < re) {
+          const uint32_t c = codes[i];
+          if (__longlong_as_double((long long)s0[i]) > qthr && c < qdict) gc = c;
         }
+        const unsigned peers = __match_any_sync(0xffffffffu, gc);
+        if (gc != 0xFFFFFFFFu && lane == __ffs(peers) - 1) {
+          double v0 = 0.0;
+          long long v2 = 0;
+          for (unsigned m = peers; m; m &= m - 1) {
+            const uint32_t r = b + (uint32_t)(__ffs(m) - 1);
+            v0 += __longlong_as_double((long long)s0[r]);
+            v2 += s2[r];
+          }
+          sm.gcount[warp][gc] += (unsigned long long)__popc(peers);
+          sm.gsum0[warp][gc] += v0;
+          sm.gsum2[warp][gc] += v2;
+        }
+        __syncwarp();  // the next leader of this group reads these words
       }
-      __syncthreads();
-      if (threadIdx.x < q.dict_len) {
+      serve_bar();
+      if (threadIdx.x < qdict) {
         const uint32_t gc = threadIdx.x;
         unsigned long long c = 0;
         double v0 = 0.0;
         long long v2 = 0;
-        for (int w = 0; w < kServeWarps; ++w)
-          for (int c2 = 0; c2 < 2; ++c2) {
-            c += sm.gcount[w][c2][gc];
-            v0 += sm.gsum0[w][c2][gc];
-            v2 += sm.gsum2[w][c2][gc];
-          }
+        for (int w = 0; w < kServeWarps; ++w) {
+          c += sm.gcount[w][gc];
+          v0 += sm.gsum0[w][gc];
+          v2 += sm.gsum2[w][gc];
+        }
         if (c) {
-          atomicAdd(&r.gcount[gc], c);
-          atomicAdd(&r.gsum0[gc], v0);
-          atomicAdd(reinterpret_cast<unsigned long long*>(&r.gsum2[gc]), (unsigned long long)v2);
+          if (qi < (uint32_t)kServeCacheQ) {  // thread gc is the only writer of group gc
+            sm.agcount[qi][gc] += c;
+            sm.agsum0[qi][gc] += v0;
+            sm.agsum2[qi][gc] += v2;
+          } else {
+            atomicAdd(&r.gcount[gc], c);
+            atomicAdd(&r.gsum0[gc], v0);
+            atomicAdd(reinterpret_cast<unsigned long long*>(&r.gsum2[gc]), (unsigned long long)v2);
+          }
         }
       }
-      __syncthreads();
+      serve_bar();
     }
   }
-  __syncthreads();  // before the next unit overwrites the staged rows
 }
 
-__global__ void __launch_bounds__(kServeThreads, kServeCtasPerSm) serve_kernel(ServeArgs a) {
-  extern __shared__ __align__(16) unsigned char tsm[];
+// Persistent: the producer warp claims units one at a time (one global
+// counter) and stages each shared unit's columns into a ring of kServeStages
+// buffers with bulk copies; the consumer warps evaluate the units in claim
+// order.  A column the bulk copy cannot take (its rows do not start on a
+// 16-byte boundary, or its byte count is not a multiple of 16) is flagged for
+// the consumers to load with plain loads.  Top-k units carry only their id.
+__global__ void __launch_bounds__(kServeBlock, kServeCtasPerSm) serve_kernel(ServeArgs a) {
+  extern __shared__ __align__(128) unsigned char tsm[];
   __shared__ ServeSmem sm;
+  uint64_t* full = reinterpret_cast<uint64_t*>(tsm);
+  uint64_t* empty = full + kServeStages;
+  uint64_t* unit = empty + kServeStages;
+  uint32_t* plain = reinterpret_cast<uint32_t*>(unit + kServeStages);
+  unsigned char* stages = tsm + kServeBar;
   const int nq = a.hdr->nq, ng = a.hdr->ngroups, topk0 = a.hdr->topk0;
   const int ntopk = nq - topk0;
   const uint64_t shared = a.hdr->shared_units, total = a.hdr->total_units;
-  for (int i = threadIdx.x; i < ng; i += blockDim.x) sm.gstart[i] = a.g[i].unit0;
-  for (int i = threadIdx.x; i < ntopk; i += blockDim.x) sm.start[i] = a.q[topk0 + i].tile0;
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  for (int i = threadIdx.x; i < ng; i += kServeBlock) sm.gstart[i] = a.g[i].unit0;
+  for (int i = threadIdx.x; i < ntopk; i += kServeBlock) sm.start[i] = a.q[topk0 + i].tile0;
+  {
+    const int ngc = ng < kServeCacheG ? ng : kServeCacheG, nqc = nq < kServeCacheQ ? nq : kServeCacheQ;
+    const int gw = (int)(sizeof(ServeG) / 8), qw = (int)(sizeof(ServeQ) / 8);
+    for (int i = threadIdx.x; i < ngc * gw; i += kServeBlock)
+      reinterpret_cast<uint64_t*>(sm.g)[i] = reinterpret_cast<const uint64_t*>(a.g)[i];
+    for (int i = threadIdx.x; i < nqc * qw; i += kServeBlock)
+      reinterpret_cast<uint64_t*>(sm.q)[i] = reinterpret_cast<const uint64_t*>(a.q)[i];
+    for (int i = threadIdx.x; i < kServeCacheQ; i += kServeBlock) sm.acount[i] = sm.asum[i] = 0;
+    for (int i = threadIdx.x; i < kServeCacheQ * FDB_SERVE_MAX_GROUPS; i += kServeBlock) {
+      (&sm.agcount[0][0])[i] = 0;
+      (&sm.agsum0[0][0])[i] = 0.0;
+      (&sm.agsum2[0][0])[i] = 0;
+    }
+  }
   if (threadIdx.x == 0) {
     sm.gstart[ng] = shared;
     sm.start[ntopk] = total;
+    for (int s = 0; s < kServeStages; ++s) {
+      mbar_init(&full[s], 1);
+      mbar_init(&empty[s], kServeWarps);
+    }
+    fence_mbar_init();
   }
   __syncthreads();
+
+  if (warp == kServeWarps) {
+    // ---------------- producer warp ----------------
+    if (lane == 0) {
+      const uint64_t policy = l2_evict_first_policy();
+      // The next unit is claimed while the stage for the current one drains,
+      // so the counter's round trip overlaps the wait.
+      uint64_t next = atomicAdd(a.claim, 1u);
+      for (uint32_t it = 0;; ++it) {
+        const int s = it % kServeStages;
+        const uint32_t ph = (it / kServeStages) & 1u;
+        if (it >= kServeStages && !mbar_wait_backoff(&empty[s], ph ^ 1u, a.err, 64)) break;
+        const uint64_t t = next;
+        if (t < total) next = atomicAdd(a.claim, 1u);
+        unit[s] = t;
+        plain[s] = 0;
+        if (t >= shared) {  // a top-k unit or the end mark: no rows to stage
+          mbar_arrive(&full[s]);
+          if (t >= total) break;
+          continue;
+        }
+        const int gi = serve_find(sm.gstart, ng, t);
+        const ServeG g = serve_g(a, sm, gi);
+        const ShareCols cols = share_cols(g);
+        const uint64_t r0 = (t - sm.gstart[gi]) * g.unit_rows;
+        const uint32_t rows = (uint32_t)umin64(g.unit_rows, g.max_n - r0);
+        uint32_t bytes = 0, pm = 0;
+#pragma unroll
+        for (int c = 0; c < 3; ++c) {
+          if (!cols.esize[c]) continue;
+          const unsigned char* src = static_cast<const unsigned char*>(cols.src[c]) + r0 * cols.esize[c];
+          const uint32_t nb = rows * (uint32_t)cols.esize[c];
+          if ((((uintptr_t)src) & 15u) == 0 && (nb & 15u) == 0)
+            bytes += nb;
+          else
+            pm |= 1u << c;
+        }
+        plain[s] = pm;
+        if (bytes == 0) {
+          mbar_arrive(&full[s]);
+          continue;
+        }
+        mbar_arrive_expect_tx(&full[s], bytes);
+#pragma unroll
+        for (int c = 0; c < 3; ++c) {
+          if (!cols.esize[c] || ((pm >> c) & 1u)) continue;
+          const unsigned char* src = static_cast<const unsigned char*>(cols.src[c]) + r0 * cols.esize[c];
+          bulk_g2s(stages + (size_t)s * kShareStage + cols.off[c], src, rows * (uint32_t)cols.esize[c], &full[s],
+                   policy);
+        }
+      }
+    }
+    return;
+  }
+
+  // ---------------- consumer warps ----------------
   RTLocal tl;
   rt_reset(tl);
   int cur = -1;
-  for (;;) {
-    if (threadIdx.x == 0) sm.t = atomicAdd(a.claim, 1u);
-    __syncthreads();
-    const uint64_t t = sm.t;
+  for (uint32_t it = 0;; ++it) {
+    const int s = it % kServeStages;
+    const uint32_t ph = (it / kServeStages) & 1u;
+    // A wait that runs out has recorded the error; every consumer leaves
+    // together so that the named barriers stay uniform.
+    if (serve_bar_any(!mbar_wait(&full[s], ph, a.err))) break;
+    const uint64_t t = unit[s];
+    const uint32_t pm = plain[s];
     if (t >= total) break;
     if (t < shared) {  // claims only grow, so a CTA is done with shared units before any top-k unit
       const int gi = serve_find(sm.gstart, ng, t);
-      serve_shared_unit(a, a.g[gi], t - sm.gstart[gi], tsm, sm);
-      continue;
+      serve_shared_unit(a, serve_g(a, sm, gi), t - sm.gstart[gi], stages + (size_t)s * kShareStage, pm, sm);
+    } else {
+      const int qi = topk0 + serve_find(sm.start, ntopk, t);
+      if (qi != cur) {
+        if (cur >= 0) serve_publish(a, serve_q(a, sm, cur), cur, sm, tl);
+        cur = qi;
+      }
+      const ServeQ q = serve_q(a, sm, qi);
+      rt_bound(tl, ~*reinterpret_cast<volatile unsigned long long*>(&a.res[qi].nbound));
+      const uint64_t r0 = (t - q.tile0) * kServeTile;
+      serve_topk_tile(q, r0, umin64(r0 + kServeTile, q.n), tl);
     }
-    const int qi = topk0 + serve_find(sm.start, ntopk, t);
-    if (qi != cur) {
-      if (cur >= 0) serve_publish(a, a.q[cur], cur, sm, tl);
-      cur = qi;
-    }
-    const ServeQ& q = a.q[qi];
-    rt_bound(tl, ~*reinterpret_cast<volatile unsigned long long*>(&a.res[qi].nbound));
-    const uint64_t r0 = (t - q.tile0) * kServeTile;
-    serve_topk_tile(q, r0, umin64(r0 + kServeTile, q.n), tl);
-    __syncthreads();  // the unit is done before sm.t is rewritten
+    // The consumers wrote the stage (probe results, plain loads): order those
+    // writes before the producer's next bulk copy into it.
+    fence_proxy_async_smem();
+    serve_bar();  // every consumer is done with the stage (and with sm's per-unit state)
+    if (lane == 0) mbar_arrive(&empty[s]);
   }
-  if (cur >= 0) serve_publish(a, a.q[cur], cur, sm, tl);
+  if (cur >= 0) serve_publish(a, serve_q(a, sm, cur), cur, sm, tl);
+  // Flush the CTA's partials of the cached shared queries.
+  serve_bar();
+  const int nqc = topk0 < kServeCacheQ ? topk0 : kServeCacheQ;  // shared queries come first
+  for (int i = threadIdx.x; i < nqc; i += kServeThreads) {
+    if (sm.acount[i]) atomicAdd(&a.res[i].count, sm.acount[i]);
+    if (sm.asum[i]) atomicAdd(reinterpret_cast<unsigned long long*>(&a.res[i].sum), sm.asum[i]);
+  }
+  for (int i = threadIdx.x; i < nqc * FDB_SERVE_MAX_GROUPS; i += kServeThreads) {
+    const int qi = i / FDB_SERVE_MAX_GROUPS, gc = i % FDB_SERVE_MAX_GROUPS;
+    if (sm.agcount[qi][gc]) {
+      atomicAdd(&a.res[qi].gcount[gc], sm.agcount[qi][gc]);
+      atomicAdd(&a.res[qi].gsum0[gc], sm.agsum0[qi][gc]);
+      atomicAdd(reinterpret_cast<unsigned long long*>(&a.res[qi].gsum2[gc]), (unsigned long long)sm.agsum2[qi][gc]);
+    }
+  }
 }
 
 // Top-k queries: the k best of the CTAs' candidates, one CTA per query.
@@ -570,7 +791,7 @@ static void slot_capture(Server& s, ServeSlot& sl) {
   FDB_CUDA(cudaStreamBeginCapture(sl.stream, cudaStreamCaptureModeThreadLocal));
   cudaMemcpyAsync(sl.d_in.ptr, sl.h_in, kServeInBytes, cudaMemcpyHostToDevice, sl.stream);
   cudaMemsetAsync(sl.d_res.ptr, 0, kServeResBytes + 256, sl.stream);
-  serve_kernel<<<s.grid, kServeThreads, kShareSmem, sl.stream>>>(a);
+  serve_kernel<<<s.grid, kServeBlock, kShareSmem, sl.stream>>>(a);
   serve_finish_kernel<<<kServeMaxBatch, kServeThreads, 0, sl.stream>>>(a);
   cudaMemcpyAsync(sl.h_out, sl.d_res.ptr, kServeResBytes, cudaMemcpyDeviceToHost, sl.stream);
   cudaMemcpyAsync(sl.h_err, sl.d_err.ptr, sizeof(int), cudaMemcpyDeviceToHost, sl.stream);
@@ -730,10 +951,19 @@ static bool slot_launch(Server& s, ServeSlot& sl) {
     d.q0 = (uint32_t)sl.tickets.size();
     d.nq = (uint32_t)g.tickets.size();
     d.max_n = s.jobs[g.tickets.front()].q.nrows;
-    d.unit0 = units;
-    units += (d.max_n + kShareTile - 1) / kShareTile;
     d.c1_bytes = g.join ? 8 : (g.has_group ? 4 : 0);
     d.load_c2 = g.has_group ? 1 : 0;
+    {
+      const uint32_t row_bytes = 8u + (uint32_t)d.c1_bytes + (d.load_c2 ? 8u : 0u) + (g.join ? 4u : 0u);
+      // A join unit is a whole number of probe passes (kProbeIlp rows per thread).
+      const uint32_t quantum = g.join ? (uint32_t)(kProbeIlp * kServeThreads) : 256u;
+      d.unit_rows = (uint32_t)(kShareStage / row_bytes) / quantum * quantum;
+      d.off1 = 8u * d.unit_rows;
+      d.off2 = d.off1 + (uint32_t)d.c1_bytes * d.unit_rows;
+      d.offm = d.off2 + (d.load_c2 ? 8u : 0u) * d.unit_rows;
+    }
+    d.unit0 = units;
+    units += (d.max_n + d.unit_rows - 1) / d.unit_rows;
     d.join = g.join ? 1 : 0;
     if (g.join) {
       const JoinView v = join_view(hash_of(g.table));
@@ -805,7 +1035,7 @@ Server* server_start(fdb_db* db, Ctx& c, const fdb_serve_config* cfg) {
   s->resident = c.in_use.load();
   FDB_CUDA(cudaFuncSetAttribute(serve_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kShareSmem));
   int per_sm = 0;
-  FDB_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, serve_kernel, kServeThreads, kShareSmem));
+  FDB_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, serve_kernel, kServeBlock, kShareSmem));
   s->grid = c.sm_count * std::max(1, std::min(per_sm, kServeCtasPerSm));
   s->cand_cap = (uint32_t)s->grid * FDB_SERVE_MAX_K;
   s->slots.resize(s->cfg.slots);
