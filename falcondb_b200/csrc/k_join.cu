@@ -288,9 +288,6 @@ struct ProbeParams {
 #ifndef FDB_PROBE_TR
 #define FDB_PROBE_TR 2048
 #endif
-#ifndef FDB_PROBE_PR
-#define FDB_PROBE_PR 1
-#endif
 #ifndef FDB_PROBE_MINB
 #define FDB_PROBE_MINB 5
 #endif
@@ -318,99 +315,63 @@ struct ProbeOp {
                  : "l"(pair), "l"(pol));
   }
 
-  // kPR rows per thread per pass.  Each probe round reads the aligned pair of
+  // One row per thread per pass.  Each probe round reads the aligned pair of
   // slots around the current position and resolves both in probe order
   // without branches: the first slot counts only when the position is even;
-  // the walk ends at the key or at the first empty slot.  The first round of
-  // every row of the pass is issued together (kPR pair loads in flight per
-  // thread); the rare rows that need more rounds then walk on one at a time.
-  static constexpr int kPR = FDB_PROBE_PR;
-
-  // One probe round of row r: true while the walk goes on.
-  static __device__ __forceinline__ bool resolve(const JSlot& a, const JSlot& b, uint64_t sk, uint64_t& h,
-                                                 uint64_t mask, uint32_t& at, uint64_t& ps) {
-    const uint64_t base = h & ~1ull;
-    const bool even = (h & 1ull) == 0;
-    const bool hit0 = even && a.key == sk;
-    const bool stop0 = even && (a.key == sk || a.key == 0ull);
-    const bool hit1 = !stop0 && b.key == sk;
-    if (hit0 || hit1) {
-      at = (uint32_t)(base + (hit1 ? 1 : 0));
-      ps = hit1 ? b.psum : a.psum;
-      return false;
-    }
-    if (stop0 || b.key == 0ull) return false;
-    h = (base + 2) & mask;
-    return true;
-  }
-
+  // the walk ends at the key or at the first empty slot.
   template <class Acc>
   static __device__ void step(Local& st, const Params& p, unsigned char*, const Acc& acc, uint32_t rows,
                               int ctid, int nct) {
     const uint64_t mask = p.cap - 1;
     const int shift = join_shift(p.cap);
     const uint64_t pol = l2_evict_last_policy();  // keep the table resident against the streamed keys
-    for (uint32_t i0 = ctid; i0 < rows; i0 += kPR * nct) {
-      uint32_t at[kPR];
-      uint64_t ps[kPR], sk[kPR], h[kPR];
-      bool todo[kPR];
-#pragma unroll
-      for (int r = 0; r < kPR; ++r) {
-        const uint32_t i = i0 + r * nct;
-        at[r] = kNoSlot;
-        ps[r] = 0;
-        sk[r] = 0;
-        h[r] = 0;
-        todo[r] = false;
-        if (i < rows && (!p.key.validity || col_valid(p.key, acc.row(i)))) {  // a NULL key matches nothing
-          const int64_t k = acc.template get<int64_t>(0, i);
-          if (k == INT64_MIN) {
-            if (p.cnt[p.cap] != 0u) {
-              at[r] = (uint32_t)p.cap;
-              ps[r] = p.slots[p.cap].psum;
+    for (uint32_t i = ctid; i < rows; i += nct) {
+      uint32_t at = kNoSlot;
+      uint64_t ps = 0;
+      if (!p.key.validity || col_valid(p.key, acc.row(i))) {  // a NULL key matches nothing
+        const int64_t k = acc.template get<int64_t>(0, i);
+        if (k == INT64_MIN) {
+          if (p.cnt[p.cap] != 0u) {
+            at = (uint32_t)p.cap;
+            ps = p.slots[p.cap].psum;
+          }
+        } else {
+          const uint64_t sk = (uint64_t)k ^ (1ull << 63);
+          uint64_t h = join_hash(sk, shift);
+          for (uint64_t round = 0; round <= mask; ++round) {
+            const uint64_t base = h & ~1ull;
+            JSlot a, b;
+            load_pair(p.slots + base, pol, a, b);
+            const bool even = (h & 1ull) == 0;
+            const bool hit0 = even && a.key == sk;
+            const bool stop0 = even && (a.key == sk || a.key == 0ull);
+            const bool hit1 = !stop0 && b.key == sk;
+            if (hit0 || hit1) {
+              at = (uint32_t)(base + (hit1 ? 1 : 0));
+              ps = hit1 ? b.psum : a.psum;
+              break;
             }
-          } else {
-            sk[r] = (uint64_t)k ^ (1ull << 63);
-            h[r] = join_hash(sk[r], shift);
-            todo[r] = true;
+            if (stop0 || b.key == 0ull) break;
+            h = (base + 2) & mask;
           }
         }
       }
-      JSlot a[kPR], b[kPR];
-#pragma unroll
-      for (int r = 0; r < kPR; ++r)
-        if (todo[r]) load_pair(p.slots + (h[r] & ~1ull), pol, a[r], b[r]);
-#pragma unroll
-      for (int r = 0; r < kPR; ++r) {
-        if (!todo[r]) continue;
-        bool more = resolve(a[r], b[r], sk[r], h[r], mask, at[r], ps[r]);
-        for (uint64_t round = 1; more && round <= mask; ++round) {
-          JSlot x, y;
-          load_pair(p.slots + (h[r] & ~1ull), pol, x, y);
-          more = resolve(x, y, sk[r], h[r], mask, at[r], ps[r]);
-        }
+      unsigned long long matches = 0, prows = 0;
+      if (at != kNoSlot) {
+        matches = p.unique ? 1ull : (unsigned long long)p.cnt[at];
+        prows = p.payload_nulls ? (unsigned long long)p.pcnt[at] : matches;
       }
-#pragma unroll
-      for (int r = 0; r < kPR; ++r) {
-        const uint32_t i = i0 + r * nct;
-        if (i >= rows) continue;
-        unsigned long long matches = 0, prows = 0;
-        if (at[r] != kNoSlot) {
-          matches = p.unique ? 1ull : (unsigned long long)p.cnt[at[r]];
-          prows = p.payload_nulls ? (unsigned long long)p.pcnt[at[r]] : matches;
-        }
-        if constexpr (JT == FDB_JOIN_INNER || JT == FDB_JOIN_LEFT) {
-          st.a.count += (JT == FDB_JOIN_LEFT && matches == 0) ? 1ull : matches;
-          st.a.psum += (long long)ps[r];
-          st.a.prows += prows;
-        } else {
-          const bool keep = (JT == FDB_JOIN_SEMI) ? (matches != 0) : (matches == 0);
-          if (keep) {
-            st.a.count += 1;
-            if (p.has_value && (!p.value.validity || col_valid(p.value, acc.row(i)))) {
-              st.a.vsum += acc.template get<double>(1, i);
-              st.a.prows += 1;
-            }
+      if constexpr (JT == FDB_JOIN_INNER || JT == FDB_JOIN_LEFT) {
+        st.a.count += (JT == FDB_JOIN_LEFT && matches == 0) ? 1ull : matches;
+        st.a.psum += (long long)ps;
+        st.a.prows += prows;
+      } else {
+        const bool keep = (JT == FDB_JOIN_SEMI) ? (matches != 0) : (matches == 0);
+        if (keep) {
+          st.a.count += 1;
+          if (p.has_value && (!p.value.validity || col_valid(p.value, acc.row(i)))) {
+            st.a.vsum += acc.template get<double>(1, i);
+            st.a.prows += 1;
           }
         }
       }

@@ -3,8 +3,8 @@
 // A scheduler thread owns `slots` launch slots.  Each slot has a stream, a
 // pinned input buffer (a batch header and one descriptor per query), a pinned
 // output buffer (one result per query) and a CUDA graph captured once:
-//   H2D descriptors -> zero results -> serve_kernel -> serve_finish_kernel ->
-//   D2H results (+ the slot's error word).
+//   H2D descriptors -> zero results -> serve_kernel -> serve_topk_kernel ->
+//   serve_finish_kernel -> D2H results (+ the slot's error word).
 // Whenever a slot is free and queries are waiting, the scheduler admits them
 // in arrival order while the device-memory budget allows (resident tables plus
 // what admitted queries hold) up to max_batch, writes their descriptors and
@@ -14,19 +14,20 @@
 // serve_kernel is persistent and scans shared: the batch's COUNT, GROUP and
 // JOIN queries are grouped by the table they read, and each group's rows are
 // cut into units that fill one pipeline stage (28 KB: 3584 rows of one 8-byte
-// column, 1280 rows of a GROUP or JOIN group's columns).  A CTA's producer warp
-// claims units from one counter and stages their columns into a ring of
-// shared-memory buffers with bulk copies; its consumer warps then probe a join
-// group's rows once (whether a build row matches does not depend on the query)
-// and evaluate every query of the group that covers the unit from shared
-// memory, each with its own predicate.  HBM therefore sees each table once per
-// batch, not once per query.  Partial results go out with one atomic per warp
-// (COUNT, JOIN) or per group and field (GROUP BY) per query and unit.
-// Top-k queries scan their own rows in kServeTile-row units claimed after the
-// shared ones: a CTA keeps a list per warp while its consecutive units belong
-// to one query and publishes its k best (below the query's running bound) as
-// candidates when it moves on; serve_finish_kernel reduces them, one CTA per
-// query.
+// column, 1280 rows of a GROUP group's columns, 1024 of a JOIN group's).  A
+// CTA's producer warp claims units from one counter and stages their columns
+// into a ring of shared-memory buffers with bulk copies; its consumer warps
+// then probe a join group's rows once (whether a build row matches does not
+// depend on the query) and evaluate every query of the group that covers the
+// unit from shared memory, each with its own predicate.  HBM therefore sees
+// each table once per batch, not once per query.  A CTA folds its partial
+// results in shared memory and adds them to the global results when it ends.
+// serve_topk_kernel then runs the top-k queries over their own rows in
+// kServeTile-row units from a second counter: a CTA keeps a list per warp while
+// its consecutive units belong to one query and publishes its k best (below
+// the query's running bound) as candidates when it moves on;
+// serve_finish_kernel reduces them, one CTA per query.  Top-k lives in its own
+// kernel so that each kernel gets the registers and CTAs per SM it needs.
 #include <algorithm>
 #include <atomic>
 #include <chrono>
@@ -55,6 +56,7 @@ constexpr int kServeMaxBatch = 256;
 #define FDB_SERVE_CTAS 2
 #endif
 constexpr int kServeCtasPerSm = FDB_SERVE_CTAS;
+constexpr int kServeTopkCtasPerSm = 2;
 #ifndef FDB_SERVE_STAGES
 #define FDB_SERVE_STAGES 2
 #endif
@@ -129,17 +131,12 @@ struct ServeArgs {
   int* err;
 };
 
-// Descriptors the serving kernel keeps in shared memory (the first ones of a
-// batch; later ones are read from global memory).
-constexpr int kServeCacheG = 32;
-constexpr int kServeCacheQ = 64;
-static_assert(sizeof(ServeG) % 8 == 0 && sizeof(ServeQ) % 8 == 0, "descriptors copy as 8-byte words");
+// Shared queries whose partial results a CTA keeps in shared memory (the
+// first ones of a batch; later ones add theirs per unit).
+constexpr int kServeCacheQ = 32;
 
-struct ServeSmem {
-  uint64_t start[kServeMaxBatch + 1];   // unit0 of each top-k query
+struct ServeSmem {                      // the shared-scan kernel
   uint64_t gstart[kServeMaxBatch + 1];  // unit0 of each shared group
-  ServeG g[kServeCacheG];
-  ServeQ q[kServeCacheQ];
   // The CTA's partial results of the first kServeCacheQ queries, added to the
   // global results once, when the CTA ends (per-unit global atomics would all
   // meet on the few words of a query's result).
@@ -152,18 +149,14 @@ struct ServeSmem {
   unsigned long long gcount[kServeWarps][FDB_SERVE_MAX_GROUPS];
   double gsum0[kServeWarps][FDB_SERVE_MAX_GROUPS];
   long long gsum2[kServeWarps][FDB_SERVE_MAX_GROUPS];
-  uint64_t tkeys[kServeWarps][32];
-  uint32_t trows[kServeWarps][32];
-  unsigned long long red[kServeWarps][2];
-  unsigned int t;
 };
 
-__device__ __forceinline__ const ServeG& serve_g(const ServeArgs& a, const ServeSmem& sm, int gi) {
-  return gi < kServeCacheG ? sm.g[gi] : a.g[gi];
-}
-__device__ __forceinline__ const ServeQ& serve_q(const ServeArgs& a, const ServeSmem& sm, int qi) {
-  return qi < kServeCacheQ ? sm.q[qi] : a.q[qi];
-}
+struct TopkSmem {                       // the top-k and finish kernels
+  uint64_t start[kServeMaxBatch + 1];   // unit0 of each top-k query
+  uint64_t tkeys[kServeWarps][32];
+  uint32_t trows[kServeWarps][32];
+  unsigned int t;
+};
 
 // Barriers among the consumer warps only (named barrier 1): the producer warp
 // never joins them.
@@ -192,7 +185,7 @@ __device__ __forceinline__ int serve_find(const uint64_t* start, int nq, uint64_
 }
 
 // Merge every warp's list into warp 0 (sorted-list merges, log2(warps) levels).
-__device__ void serve_tree_merge(ServeSmem& sm, RTLocal& s, uint32_t k, int warp, int lane) {
+__device__ void serve_tree_merge(TopkSmem& sm, RTLocal& s, uint32_t k, int warp, int lane) {
   for (int half = kServeWarps / 2; half >= 1; half >>= 1) {
     serve_bar();
     if (warp >= half && warp < 2 * half) {
@@ -215,7 +208,7 @@ __device__ __forceinline__ void rt_reset(RTLocal& s) {
 }
 
 // Publish this CTA's top-k state for query qi (all consumer threads call; ends with a barrier).
-__device__ void serve_publish(const ServeArgs& a, const ServeQ q, int qi, ServeSmem& sm, RTLocal& tl) {
+__device__ void serve_publish(const ServeArgs& a, const ServeQ q, int qi, TopkSmem& sm, RTLocal& tl) {
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   ServeRes& r = a.res[qi];
   const uint32_t k = (uint32_t)q.k;
@@ -422,7 +415,7 @@ __device__ void serve_shared_unit(const ServeArgs& a, const ServeG g, uint64_t t
   }
   if (g.join) serve_probe_rows(g, s0, smm, rows);
   for (uint32_t qi = g.q0; qi < g.q0 + g.nq; ++qi) {
-    const ServeQ& qref = serve_q(a, sm, (int)qi);
+    const ServeQ& qref = a.q[qi];
     const uint64_t qn = qref.n;
     if (qn <= r0) break;  // queries are by rows descending
     const int qkind = qref.kind;
@@ -519,7 +512,7 @@ __device__ void serve_shared_unit(const ServeArgs& a, const ServeG g, uint64_t t
 // buffers with bulk copies; the consumer warps evaluate the units in claim
 // order.  A column the bulk copy cannot take (its rows do not start on a
 // 16-byte boundary, or its byte count is not a multiple of 16) is flagged for
-// the consumers to load with plain loads.  Top-k units carry only their id.
+// the consumers to load with plain loads.
 __global__ void __launch_bounds__(kServeBlock, kServeCtasPerSm) serve_kernel(ServeArgs a) {
   extern __shared__ __align__(128) unsigned char tsm[];
   __shared__ ServeSmem sm;
@@ -528,19 +521,12 @@ __global__ void __launch_bounds__(kServeBlock, kServeCtasPerSm) serve_kernel(Ser
   uint64_t* unit = empty + kServeStages;
   uint32_t* plain = reinterpret_cast<uint32_t*>(unit + kServeStages);
   unsigned char* stages = tsm + kServeBar;
-  const int nq = a.hdr->nq, ng = a.hdr->ngroups, topk0 = a.hdr->topk0;
-  const int ntopk = nq - topk0;
-  const uint64_t shared = a.hdr->shared_units, total = a.hdr->total_units;
+  const int ng = a.hdr->ngroups, topk0 = a.hdr->topk0;
+  const uint64_t shared = a.hdr->shared_units;
+  if (shared == 0) return;  // a batch of top-k queries only
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   for (int i = threadIdx.x; i < ng; i += kServeBlock) sm.gstart[i] = a.g[i].unit0;
-  for (int i = threadIdx.x; i < ntopk; i += kServeBlock) sm.start[i] = a.q[topk0 + i].tile0;
   {
-    const int ngc = ng < kServeCacheG ? ng : kServeCacheG, nqc = nq < kServeCacheQ ? nq : kServeCacheQ;
-    const int gw = (int)(sizeof(ServeG) / 8), qw = (int)(sizeof(ServeQ) / 8);
-    for (int i = threadIdx.x; i < ngc * gw; i += kServeBlock)
-      reinterpret_cast<uint64_t*>(sm.g)[i] = reinterpret_cast<const uint64_t*>(a.g)[i];
-    for (int i = threadIdx.x; i < nqc * qw; i += kServeBlock)
-      reinterpret_cast<uint64_t*>(sm.q)[i] = reinterpret_cast<const uint64_t*>(a.q)[i];
     for (int i = threadIdx.x; i < kServeCacheQ; i += kServeBlock) sm.acount[i] = sm.asum[i] = 0;
     for (int i = threadIdx.x; i < kServeCacheQ * FDB_SERVE_MAX_GROUPS; i += kServeBlock) {
       (&sm.agcount[0][0])[i] = 0;
@@ -550,7 +536,6 @@ __global__ void __launch_bounds__(kServeBlock, kServeCtasPerSm) serve_kernel(Ser
   }
   if (threadIdx.x == 0) {
     sm.gstart[ng] = shared;
-    sm.start[ntopk] = total;
     for (int s = 0; s < kServeStages; ++s) {
       mbar_init(&full[s], 1);
       mbar_init(&empty[s], kServeWarps);
@@ -571,16 +556,15 @@ __global__ void __launch_bounds__(kServeBlock, kServeCtasPerSm) serve_kernel(Ser
         const uint32_t ph = (it / kServeStages) & 1u;
         if (it >= kServeStages && !mbar_wait_backoff(&empty[s], ph ^ 1u, a.err, 64)) break;
         const uint64_t t = next;
-        if (t < total) next = atomicAdd(a.claim, 1u);
+        if (t < shared) next = atomicAdd(a.claim, 1u);
         unit[s] = t;
         plain[s] = 0;
-        if (t >= shared) {  // a top-k unit or the end mark: no rows to stage
+        if (t >= shared) {  // the end mark: no rows to stage
           mbar_arrive(&full[s]);
-          if (t >= total) break;
-          continue;
+          break;
         }
         const int gi = serve_find(sm.gstart, ng, t);
-        const ServeG g = serve_g(a, sm, gi);
+        const ServeG g = a.g[gi];
         const ShareCols cols = share_cols(g);
         const uint64_t r0 = (t - sm.gstart[gi]) * g.unit_rows;
         const uint32_t rows = (uint32_t)umin64(g.unit_rows, g.max_n - r0);
@@ -614,9 +598,6 @@ __global__ void __launch_bounds__(kServeBlock, kServeCtasPerSm) serve_kernel(Ser
   }
 
   // ---------------- consumer warps ----------------
-  RTLocal tl;
-  rt_reset(tl);
-  int cur = -1;
   for (uint32_t it = 0;; ++it) {
     const int s = it % kServeStages;
     const uint32_t ph = (it / kServeStages) & 1u;
@@ -625,30 +606,16 @@ __global__ void __launch_bounds__(kServeBlock, kServeCtasPerSm) serve_kernel(Ser
     if (serve_bar_any(!mbar_wait(&full[s], ph, a.err))) break;
     const uint64_t t = unit[s];
     const uint32_t pm = plain[s];
-    if (t >= total) break;
-    if (t < shared) {  // claims only grow, so a CTA is done with shared units before any top-k unit
-      const int gi = serve_find(sm.gstart, ng, t);
-      serve_shared_unit(a, serve_g(a, sm, gi), t - sm.gstart[gi], stages + (size_t)s * kShareStage, pm, sm);
-    } else {
-      const int qi = topk0 + serve_find(sm.start, ntopk, t);
-      if (qi != cur) {
-        if (cur >= 0) serve_publish(a, serve_q(a, sm, cur), cur, sm, tl);
-        cur = qi;
-      }
-      const ServeQ q = serve_q(a, sm, qi);
-      rt_bound(tl, ~*reinterpret_cast<volatile unsigned long long*>(&a.res[qi].nbound));
-      const uint64_t r0 = (t - q.tile0) * kServeTile;
-      serve_topk_tile(q, r0, umin64(r0 + kServeTile, q.n), tl);
-    }
+    if (t >= shared) break;
+    const int gi = serve_find(sm.gstart, ng, t);
+    serve_shared_unit(a, a.g[gi], t - sm.gstart[gi], stages + (size_t)s * kShareStage, pm, sm);
     // The consumers wrote the stage (probe results, plain loads): order those
     // writes before the producer's next bulk copy into it.
     fence_proxy_async_smem();
     serve_bar();  // every consumer is done with the stage (and with sm's per-unit state)
     if (lane == 0) mbar_arrive(&empty[s]);
   }
-  if (cur >= 0) serve_publish(a, serve_q(a, sm, cur), cur, sm, tl);
   // Flush the CTA's partials of the cached shared queries.
-  serve_bar();
   const int nqc = topk0 < kServeCacheQ ? topk0 : kServeCacheQ;  // shared queries come first
   for (int i = threadIdx.x; i < nqc; i += kServeThreads) {
     if (sm.acount[i]) atomicAdd(&a.res[i].count, sm.acount[i]);
@@ -664,9 +631,44 @@ __global__ void __launch_bounds__(kServeBlock, kServeCtasPerSm) serve_kernel(Ser
   }
 }
 
+// Top-k queries scan their own rows in kServeTile-row units, claimed from
+// their own counter after the shared scan: a CTA keeps a list per warp while
+// its consecutive units belong to one query and publishes its k best (below
+// the query's running bound) as candidates when it moves on.
+__global__ void __launch_bounds__(kServeThreads, kServeTopkCtasPerSm) serve_topk_kernel(ServeArgs a) {
+  __shared__ TopkSmem sm;
+  const int nq = a.hdr->nq, topk0 = a.hdr->topk0;
+  const int ntopk = nq - topk0;
+  if (ntopk == 0) return;
+  const uint64_t shared = a.hdr->shared_units, total = a.hdr->total_units;
+  for (int i = threadIdx.x; i < ntopk; i += kServeThreads) sm.start[i] = a.q[topk0 + i].tile0;
+  if (threadIdx.x == 0) sm.start[ntopk] = total;
+  __syncthreads();
+  RTLocal tl;
+  rt_reset(tl);
+  int cur = -1;
+  for (;;) {
+    if (threadIdx.x == 0) sm.t = atomicAdd(a.claim + 1, 1u);
+    __syncthreads();
+    const uint64_t t = shared + sm.t;
+    if (t >= total) break;
+    const int qi = topk0 + serve_find(sm.start, ntopk, t);
+    if (qi != cur) {
+      if (cur >= 0) serve_publish(a, a.q[cur], cur, sm, tl);
+      cur = qi;
+    }
+    const ServeQ q = a.q[qi];
+    rt_bound(tl, ~*reinterpret_cast<volatile unsigned long long*>(&a.res[qi].nbound));
+    const uint64_t r0 = (t - q.tile0) * kServeTile;
+    serve_topk_tile(q, r0, umin64(r0 + kServeTile, q.n), tl);
+    __syncthreads();  // the unit is done before sm.t is rewritten
+  }
+  if (cur >= 0) serve_publish(a, a.q[cur], cur, sm, tl);
+}
+
 // Top-k queries: the k best of the CTAs' candidates, one CTA per query.
 __global__ void __launch_bounds__(kServeThreads) serve_finish_kernel(ServeArgs a) {
-  __shared__ ServeSmem sm;
+  __shared__ TopkSmem sm;
   const int qi = blockIdx.x;
   if (qi >= a.hdr->nq) return;
   const ServeQ& q = a.q[qi];
@@ -749,7 +751,7 @@ struct Server {
   double first_arrival = 1e300, last_done = 0.0;
   Clock::time_point t0;
   uint32_t cand_cap = 0;
-  int grid = 0;
+  int grid = 0, grid_topk = 0;
   uint64_t split_rows = 1ull << 22;  // size classes of batches: fewer / at least this many rows
   std::string error;
 
@@ -792,6 +794,7 @@ static void slot_capture(Server& s, ServeSlot& sl) {
   cudaMemcpyAsync(sl.d_in.ptr, sl.h_in, kServeInBytes, cudaMemcpyHostToDevice, sl.stream);
   cudaMemsetAsync(sl.d_res.ptr, 0, kServeResBytes + 256, sl.stream);
   serve_kernel<<<s.grid, kServeBlock, kShareSmem, sl.stream>>>(a);
+  serve_topk_kernel<<<s.grid_topk, kServeThreads, 0, sl.stream>>>(a);
   serve_finish_kernel<<<kServeMaxBatch, kServeThreads, 0, sl.stream>>>(a);
   cudaMemcpyAsync(sl.h_out, sl.d_res.ptr, kServeResBytes, cudaMemcpyDeviceToHost, sl.stream);
   cudaMemcpyAsync(sl.h_err, sl.d_err.ptr, sizeof(int), cudaMemcpyDeviceToHost, sl.stream);
@@ -1037,7 +1040,10 @@ Server* server_start(fdb_db* db, Ctx& c, const fdb_serve_config* cfg) {
   int per_sm = 0;
   FDB_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, serve_kernel, kServeBlock, kShareSmem));
   s->grid = c.sm_count * std::max(1, std::min(per_sm, kServeCtasPerSm));
-  s->cand_cap = (uint32_t)s->grid * FDB_SERVE_MAX_K;
+  FDB_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, serve_topk_kernel, kServeThreads, 0));
+  s->grid_topk = c.sm_count * std::max(1, std::min(per_sm, kServeTopkCtasPerSm));
+  // A top-k CTA publishes at most once per query (its claims only grow).
+  s->cand_cap = (uint32_t)s->grid_topk * FDB_SERVE_MAX_K;
   s->slots.resize(s->cfg.slots);
   for (ServeSlot& sl : s->slots) {
     FDB_CUDA(cudaStreamCreateWithFlags(&sl.stream, cudaStreamNonBlocking));
