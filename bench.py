@@ -542,6 +542,8 @@ def run_secondary(args):
         db.drop_table("g")
     if args.workload in ("serve", "all"):
         run_serving(args, db, out, peak)
+    if args.workload == "serve_single":
+        run_serving_single(args, db, out)
     db.close()
     return out
 
@@ -627,6 +629,52 @@ def run_serving(args, db, out, peak):
                 "results_identical_batched_vs_serial": same})
 
 
+def run_serving_single(args, db, out):
+    """Each serving template on its own: 20 queries over all n rows of the
+    serving tables, 20 ms apart, so that every query runs alone on the GPU;
+    the line reports each template's median latency (submit to result on the
+    host) over the last 17.  Launch order: 20 COUNT, 20 GROUP, 20 JOIN, 20
+    TOPK batches."""
+    import torch
+
+    from falcondb_b200 import ops, serving as S, workloads as W
+
+    n = args.rows
+    dev = torch.device("cuda", 0)
+    t = W.table_t(n, seed=1)
+    score = torch.from_numpy(t["score"]).to(dev)
+    dept = torch.from_numpy(t["dept"].codes.view(np.int32)).to(dev)
+    sal = torch.from_numpy(t["salary"]).to(dev)
+    del t
+    bt, pt = W.join_tables(1_000_000, n, seed=7)
+    pkey = torch.from_numpy(pt["key"]).to(dev)
+    pval = torch.from_numpy(pt["value"]).to(dev)
+    del pt
+    ht = ops.HashTable(db, torch.from_numpy(bt["key"]).to(dev), torch.from_numpy(bt["payload"]).to(dev),
+                       len(bt["key"]))
+    torch.cuda.synchronize()
+    make = {
+        "count": lambda: S.count_query(score.data_ptr(), n, 50.0),
+        "group": lambda: S.group_query(score.data_ptr(), dept.data_ptr(), sal.data_ptr(), 12, n, 50.0),
+        "join": lambda: S.join_query(pkey.data_ptr(), pval.data_ptr(), ht._h.value, n, 50.0),
+        "topk": lambda: S.topk_query(score.data_ptr(), n, 50.0, k=10),
+    }
+    lat = {}
+    for name, f in make.items():
+        qs = []
+        for i in range(20):
+            q = f()
+            q.arrival_s = 0.02 * i
+            qs.append(q)
+        res, _ = S.serve_trace(db, qs, max_batch=128, slots=1, mem_budget=40 << 30)
+        ms = sorted((r.done_s - r.arrival_s) * 1e3 for r in res[3:])
+        lat[name] = round(ms[len(ms) // 2], 4)
+    ht.free()
+    out.append({"metric": METRIC, "workload": "serving_single", "unit": "ms", "higher_is_better": False,
+                "rows": n, "median_latency_ms": lat,
+                "queries": "20 per template over all rows, 20 ms apart (threshold 50; join value < 0.5; k = 10)"})
+
+
 def run_reference(args):
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
@@ -668,7 +716,7 @@ def main():
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--cpu-threads", type=int, default=0)
     ap.add_argument("--workload", default="scan",
-                    choices=["scan", "filter_groupby", "join", "groupby", "batch", "serve", "all"],
+                    choices=["scan", "filter_groupby", "join", "groupby", "batch", "serve", "serve_single", "all"],
                     help="scan = the headline line; the others print per-operator lines")
     ap.add_argument("--load-factor", type=float, default=0.5)
     ap.add_argument("--serve-queries", type=int, default=10_000)
