@@ -177,6 +177,7 @@ _SIGS = {
                                  C.c_double, C.POINTER(C.c_void_p)]),
     "fdb_join_free": (None, [C.c_void_p]),
     "fdb_join_capacity": (C.c_uint64, [C.c_void_p]),
+    "fdb_join_dense": (C.c_int, [C.c_void_p]),
     "fdb_join_probe_agg": (C.c_int, [C.c_void_p, C.c_void_p, C.POINTER(fdb_dev_column), C.POINTER(fdb_dev_column),
                                      C.c_uint64, C.c_int32, C.c_void_p]),
     "fdb_join_probe_pairs": (C.c_int, [C.c_void_p, C.c_void_p, C.POINTER(fdb_dev_column), C.c_uint64, C.c_int32,

@@ -575,6 +575,7 @@ void fdb_join_free(fdb_hash* h) {
 }
 
 uint64_t fdb_join_capacity(const fdb_hash* h) { return h ? join_capacity(h->h) : 0; }
+int fdb_join_dense(const fdb_hash* h) { return h ? join_view(h->h).dense : 0; }
 
 int fdb_join_probe_agg(fdb_db* db, const fdb_hash* h, const fdb_dev_column* probe_key, const fdb_dev_column* value,
                        uint64_t nrows, int32_t join_type, fdb_join_agg* d_out) {

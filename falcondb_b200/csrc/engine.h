@@ -156,7 +156,8 @@ struct JoinView {
   const unsigned int* cnt;   // build rows per slot
   uint64_t cap;
   int32_t unique;
-  int32_t _pad;
+  int32_t dense;             // key k lives in slot k - dmin (see join_table.cuh)
+  int64_t dmin;
 };
 JoinView join_view(const HashTable* h);
 

@@ -23,9 +23,26 @@ __host__ __device__ __forceinline__ uint64_t join_hash(uint64_t sk, int shift) {
 }
 __device__ __forceinline__ int join_shift(uint64_t cap) { return __clzll((long long)cap) + 1; }  // cap = 2^b
 
+// How keys map to home slots.  A table whose build keys span fewer values than
+// it has slots (max - min < cap: surrogate keys, dense id ranges) is dense:
+// key k lives in slot k - min, so a probe is one slot read and keys outside
+// [min, min + cap) read nothing.  Otherwise keys hash (join_hash) with linear
+// probing.  The NULL-group slot (key INT64_MIN) is slot cap either way.
+struct JoinMode {
+  int64_t dmin;   // dense: the smallest build key
+  int32_t dense;
+  int32_t shift;  // join_shift(cap)
+};
+
+// Home slot of key k (stored form sk), or a value >= cap when a dense table
+// cannot hold it.
+__device__ __forceinline__ uint64_t join_home(const JoinMode& m, int64_t k, uint64_t sk) {
+  return m.dense ? (uint64_t)k - (uint64_t)m.dmin : join_hash(sk, m.shift);
+}
+
 // Slot of probe key k, or kNoSlot.
 __device__ __forceinline__ uint32_t join_find(const JSlot* __restrict__ slots, const unsigned int* cnt,
-                                              uint64_t cap, int64_t k, JSlot* out) {
+                                              uint64_t cap, const JoinMode& mode, int64_t k, JSlot* out) {
   if (k == INT64_MIN) {
     if (cnt[cap] == 0u) return kNoSlot;
     *out = slots[cap];
@@ -33,7 +50,8 @@ __device__ __forceinline__ uint32_t join_find(const JSlot* __restrict__ slots, c
   }
   const unsigned long long sk = (unsigned long long)k ^ (1ull << 63);
   const uint64_t mask = cap - 1;
-  uint64_t h = join_hash(sk, join_shift(cap));
+  uint64_t h = join_home(mode, k, sk);
+  if (h >= cap) return kNoSlot;
   for (uint64_t probe = 0; probe <= mask; ++probe) {
     const JSlot s = slots[h];
     if (s.key == sk) {

@@ -34,7 +34,35 @@ struct HashTable {
   uint64_t nbuild = 0;
   bool unique = true;        // every key occurs once (cnt is 1 wherever set)
   bool payload_nulls = false;
+  bool dense = false;        // key k lives in slot k - dmin (join_table.cuh)
+  int64_t dmin = 0;
 };
+
+// Order keys of the smallest and largest valid build key (INT64_MIN, the
+// NULL group, excluded): out[0] = ~ord(min), out[1] = ord(max), both from a
+// zero identity (0 = no key).
+__global__ void join_key_range_kernel(const int64_t* __restrict__ keys, const uint64_t* kvalid, uint64_t kvoff,
+                                      uint64_t n, unsigned long long* out) {
+  unsigned long long mn = 0, mx = 0;
+  for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n;
+       i += (uint64_t)gridDim.x * blockDim.x) {
+    if (kvalid) {
+      const uint64_t b = kvoff + i;
+      if (!((kvalid[b >> 6] >> (b & 63)) & 1ull)) continue;
+    }
+    const int64_t k = keys[i];
+    if (k == INT64_MIN) continue;
+    const unsigned long long o = i64_ord_key(k);
+    mn = ~o > mn ? ~o : mn;
+    mx = o > mx ? o : mx;
+  }
+  mn = warp_max_u64(mn);
+  mx = warp_max_u64(mx);
+  if ((threadIdx.x & 31) == 0 && mx) {
+    atomicMax(&out[0], mn);
+    atomicMax(&out[1], mx);
+  }
+}
 
 // ---------------------------------------------------------------------------
 // Build
@@ -42,7 +70,7 @@ struct HashTable {
 __global__ void join_insert_kernel(const int64_t* __restrict__ keys, const uint64_t* kvalid, uint64_t kvoff,
                                    const int64_t* __restrict__ payload, const uint64_t* pvalid, uint64_t pvoff,
                                    uint64_t n, JSlot* slots, unsigned int* cnt, unsigned int* pcnt, uint64_t cap,
-                                   uint32_t* row_slot, unsigned int* dup, int* err) {
+                                   JoinMode mode, uint32_t* row_slot, unsigned int* dup, int* err) {
   const uint64_t mask = cap - 1;
   for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n;
        i += (uint64_t)gridDim.x * blockDim.x) {
@@ -59,7 +87,7 @@ __global__ void join_insert_kernel(const int64_t* __restrict__ keys, const uint6
       s = cap;
     } else {
       const unsigned long long sk = (unsigned long long)k ^ (1ull << 63);
-      uint64_t h = join_hash(sk, join_shift(cap));
+      uint64_t h = join_home(mode, k, sk);  // a dense table's range fits: h < cap
       for (uint64_t probe = 0; probe <= mask; ++probe) {  // cap > distinct keys: always ends
         const unsigned long long cur = *reinterpret_cast<volatile unsigned long long*>(&slots[h].key);
         if (cur == sk) { s = h; break; }
@@ -173,6 +201,16 @@ __global__ void join_scatter_kernel(const uint32_t* __restrict__ row_slot, uint6
   }
 }
 
+static JoinMode join_mode(const HashTable& h) {
+  JoinMode m;
+  m.dmin = h.dmin;
+  m.dense = h.dense ? 1 : 0;
+  int b = 0;
+  while ((1ull << b) < h.cap) ++b;
+  m.shift = 64 - b;  // join_shift(cap)
+  return m;
+}
+
 HashTable* op_join_build(Ctx& c, const fdb_dev_column& key, const fdb_dev_column& payload, uint64_t n,
                          double load_factor) {
   if (key.dtype != FDB_INT64) fail(FDB_E_TYPE, "join keys must be INT64");
@@ -203,13 +241,37 @@ HashTable* op_join_build(Ctx& c, const fdb_dev_column& key, const fdb_dev_column
   FDB_CUDA(cudaMemsetAsync(h->pcnt.ptr, 0, ns * 4, c.stream));
   FDB_CUDA(cudaMemsetAsync(fill, 0, ns * 4, c.stream));
   FDB_CUDA(cudaMemsetAsync(dup, 0, 4, c.stream));
+  // Dense or hashed: the build keys' range decides (one 16-byte read back).
+  bool dense = false;
+  int64_t dmin = 0;
+  if (n > 0) {
+    unsigned long long* range = static_cast<unsigned long long*>(c.scratch_take(16));
+    FDB_CUDA(cudaMemsetAsync(range, 0, 16, c.stream));
+    const unsigned blocks = (unsigned)umin64((n + 255) / 256, (uint64_t)c.sm_count * 8);
+    join_key_range_kernel<<<blocks, 256, 0, c.stream>>>(static_cast<const int64_t*>(key.values), key.validity,
+                                                         key.validity_offset, n, range);
+    FDB_CUDA(cudaGetLastError());
+    unsigned long long hr[2] = {0, 0};
+    FDB_CUDA(cudaMemcpyAsync(hr, range, 16, cudaMemcpyDeviceToHost, c.stream));
+    FDB_CUDA(cudaStreamSynchronize(c.stream));
+    if (hr[1] != 0) {
+      const uint64_t kmin = ~hr[0] ^ (1ull << 63), kmax = hr[1] ^ (1ull << 63);  // two's complement bits
+      if (kmax - kmin < cap) {
+        dense = true;
+        dmin = (int64_t)kmin;
+      }
+    }
+  }
+  h->dense = dense;
+  h->dmin = dmin;
+  const JoinMode mode = join_mode(*h);
   if (n > 0) {
     const unsigned blocks = (unsigned)umin64((n + 255) / 256, (uint64_t)c.sm_count * 16);
     join_insert_kernel<<<blocks, 256, 0, c.stream>>>(
         static_cast<const int64_t*>(key.values), key.validity, key.validity_offset,
         static_cast<const int64_t*>(payload.values), payload.validity, payload.validity_offset, n,
         static_cast<JSlot*>(h->slots.ptr), static_cast<unsigned int*>(h->cnt.ptr),
-        static_cast<unsigned int*>(h->pcnt.ptr), cap, row_slot, dup, c.d_err);
+        static_cast<unsigned int*>(h->pcnt.ptr), cap, mode, row_slot, dup, c.d_err);
   }
   scan_blocks_kernel<<<(unsigned)nblocks, kScanThreads, 0, c.stream>>>(static_cast<const unsigned int*>(h->cnt.ptr),
                                                                         ns, bsums);
@@ -251,6 +313,8 @@ JoinView join_view(const HashTable* h) {
   v.cnt = static_cast<const unsigned int*>(h->cnt.ptr);
   v.cap = h->cap;
   v.unique = h->unique ? 1 : 0;
+  v.dense = h->dense ? 1 : 0;
+  v.dmin = h->dmin;
   return v;
 }
 
@@ -271,6 +335,7 @@ struct ProbeParams {
   const unsigned int* cnt;
   const unsigned int* pcnt;
   uint64_t cap;
+  JoinMode mode;
   int32_t unique;
   int32_t payload_nulls;
   int32_t has_value;
@@ -323,7 +388,6 @@ struct ProbeOp {
   static __device__ void step(Local& st, const Params& p, unsigned char*, const Acc& acc, uint32_t rows,
                               int ctid, int nct) {
     const uint64_t mask = p.cap - 1;
-    const int shift = join_shift(p.cap);
     const uint64_t pol = l2_evict_last_policy();  // keep the table resident against the streamed keys
     for (uint32_t i = ctid; i < rows; i += nct) {
       uint32_t at = kNoSlot;
@@ -337,8 +401,10 @@ struct ProbeOp {
           }
         } else {
           const uint64_t sk = (uint64_t)k ^ (1ull << 63);
-          uint64_t h = join_hash(sk, shift);
-          for (uint64_t round = 0; round <= mask; ++round) {
+          uint64_t h = join_home(p.mode, k, sk);
+          // A dense table holds key k only in slot k - min, so its walk ends in
+          // the first round; a key outside its range reads nothing.
+          for (uint64_t round = 0; h <= mask && round <= mask; ++round) {
             const uint64_t base = h & ~1ull;
             JSlot a, b;
             load_pair(p.slots + base, pol, a, b);
@@ -493,6 +559,7 @@ void op_join_probe_agg(Ctx& c, const HashTable& h, const fdb_dev_column& key, co
   p.cnt = static_cast<const unsigned int*>(h.cnt.ptr);
   p.pcnt = static_cast<const unsigned int*>(h.pcnt.ptr);
   p.cap = h.cap;
+  p.mode = join_mode(h);
   p.unique = h.unique ? 1 : 0;
   p.payload_nulls = h.payload_nulls ? 1 : 0;
   p.has_value = (has_value && (join_type == FDB_JOIN_SEMI || join_type == FDB_JOIN_ANTI)) ? 1 : 0;
@@ -522,7 +589,8 @@ void op_join_probe_agg(Ctx& c, const HashTable& h, const fdb_dev_column& key, co
 // ---------------------------------------------------------------------------
 __global__ void join_pairs_kernel(const int64_t* __restrict__ keys, const uint64_t* kvalid, uint64_t kvoff,
                                   uint64_t n, const JSlot* __restrict__ slots, const unsigned int* cnt,
-                                  const uint32_t* off, const uint32_t* brows, uint64_t cap, int join_type,
+                                  const uint32_t* off, const uint32_t* brows, uint64_t cap, JoinMode mode,
+                                  int join_type,
                                   uint32_t* out_l, uint32_t* out_r, uint64_t capacity,
                                   unsigned long long* counter, int* err) {
   for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n;
@@ -535,7 +603,7 @@ __global__ void join_pairs_kernel(const int64_t* __restrict__ keys, const uint64
     uint32_t at = kNoSlot;
     if (valid) {
       JSlot s;
-      at = join_find(slots, cnt, cap, keys[i], &s);
+      at = join_find(slots, cnt, cap, mode, keys[i], &s);
     }
     const uint32_t m = at == kNoSlot ? 0u : cnt[at];
     if (join_type == FDB_JOIN_INNER || join_type == FDB_JOIN_LEFT) {
@@ -576,7 +644,8 @@ void op_join_probe_pairs(Ctx& c, const HashTable& h, const fdb_dev_column& key, 
     join_pairs_kernel<<<blocks, 256, 0, c.stream>>>(
         static_cast<const int64_t*>(key.values), key.validity, key.validity_offset, n,
         static_cast<const JSlot*>(h.slots.ptr), static_cast<const unsigned int*>(h.cnt.ptr),
-        static_cast<const uint32_t*>(h.off.ptr), static_cast<const uint32_t*>(h.rows.ptr), h.cap, join_type, d_left,
+        static_cast<const uint32_t*>(h.off.ptr), static_cast<const uint32_t*>(h.rows.ptr), h.cap, join_mode(h),
+        join_type, d_left,
         d_right, capacity, counter, c.d_err);
     FDB_CUDA(cudaGetLastError());
   }

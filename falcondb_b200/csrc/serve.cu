@@ -111,6 +111,8 @@ struct ServeG {             // a group of queries that read the same table
   const JSlot* slots;
   const unsigned int* cnt;
   uint64_t cap;
+  int64_t dmin;             // dense table: key k lives in slot k - dmin
+  int32_t dense, _pad3;
 };
 
 struct ServeHeader {
@@ -306,7 +308,10 @@ __device__ __forceinline__ void share_load(unsigned char* dst, const void* src, 
 constexpr int kProbeIlp = 4;
 
 __device__ void serve_probe_rows(const ServeG g, uint64_t* s0, uint32_t* m, uint32_t rows) {
-  const int shift = join_shift(g.cap);
+  JoinMode mode;
+  mode.dmin = g.dmin;
+  mode.dense = g.dense;
+  mode.shift = join_shift(g.cap);
   const uint64_t mask = g.cap - 1;
   const uint64_t pol = l2_evict_last_policy();
   for (uint32_t base = 0; base < rows; base += kProbeIlp * kServeThreads) {
@@ -330,8 +335,8 @@ __device__ void serve_probe_rows(const ServeG g, uint64_t* s0, uint32_t* m, uint
         continue;
       }
       sk[j] = (uint64_t)key ^ (1ull << 63);
-      h[j] = join_hash(sk[j], shift);
-      todo |= 1u << j;
+      h[j] = join_home(mode, key, sk[j]);
+      if (h[j] <= mask) todo |= 1u << j;  // a dense table cannot hold a key outside its range
     }
     for (uint64_t round = 0; todo && round <= mask; ++round) {
       JSlot lo[kProbeIlp], hi[kProbeIlp];
@@ -974,6 +979,8 @@ static bool slot_launch(Server& s, ServeSlot& sl) {
       d.cnt = v.cnt;
       d.cap = v.cap;
       d.unique = v.unique;
+      d.dmin = v.dmin;
+      d.dense = v.dense;
     }
     for (uint64_t tk : g.tickets) put(tk);
   }

@@ -292,6 +292,12 @@ class HashTable:
     def capacity(self) -> int:
         return int(lib().fdb_join_capacity(self._h))
 
+    @property
+    def dense(self) -> bool:
+        """True when the table is direct-addressed (build keys span fewer
+        values than it has slots); False when keys are hashed."""
+        return bool(lib().fdb_join_dense(self._h))
+
     def free(self) -> None:
         if self._h is not None and self._h.value:
             lib().fdb_join_free(self._h)

@@ -328,6 +328,11 @@ int fdb_join_build(fdb_db* db, const fdb_dev_column* key, const fdb_dev_column* 
                    uint64_t nrows, double load_factor, fdb_hash** out);
 void fdb_join_free(fdb_hash* h);
 uint64_t fdb_join_capacity(const fdb_hash* h);
+/* 1 when the table is direct-addressed: its build keys span fewer values than
+ * it has slots, so key k lives in slot k - min(key) and a probe reads one slot;
+ * 0 when keys are hashed with linear probing.  No counterpart in the reference
+ * (its IntHashTable always hashes, join.rs:1368-1429); results are the same. */
+int fdb_join_dense(const fdb_hash* h);
 
 /* Probe with aggregation fused in (probe_in_place / probe_one + execute_agg_only,
  * join.rs:297-375, 657-723; execute_hash_semi_anti_join, join.rs:49-132):

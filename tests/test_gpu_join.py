@@ -17,14 +17,42 @@ def dev(a):
     return torch.from_numpy(np.ascontiguousarray(a)).cuda()
 
 
-def agg(db, b, p, jt, bvalid=None, pvalid=None, lf=0.0):
+def agg(db, b, p, jt, bvalid=None, pvalid=None, lf=0.0, dense=None):
+    """Build, probe with aggregation, free; `dense` (when given) is the table
+    mode the build must have chosen."""
     bk = (dev(b["key"]), dev(bvalid.view(np.int64))) if bvalid is not None else dev(b["key"])
     pk = (dev(p["key"]), dev(pvalid.view(np.int64))) if pvalid is not None else dev(p["key"])
     h = ops.HashTable(db, bk, dev(b["payload"]), len(b["key"]), lf)
+    if dense is not None:
+        assert h.dense == dense
     out = h.probe_agg(pk, len(p["key"]), jt, value=dev(p["value"]))
     rec = ops.to_records(out, F.JOIN_AGG_DTYPE, 1)[0]
     h.free()
     return rec
+
+
+def check_agg(got, want, jt):
+    assert got["count"] == want["count"]
+    if jt <= 1:
+        assert got["sum_payload"] == want["sum_payload"]
+        assert got["payload_rows"] == want["payload_rows"]
+    else:
+        assert abs(got["sum_value"] - want["sum_value"]) <= 1e-12 * max(abs(want["sum_value"]), 1e-300)
+
+
+I64 = np.iinfo(np.int64)
+
+
+def _edge_probes(r, keys, n):
+    """n probe keys: build keys, keys just outside the build range on both
+    sides, int64 extremes and INT64_MIN."""
+    lo, hi = int(keys.min()), int(keys.max())
+    pk = r.choice(keys, n)
+    m = n // 8
+    pk[:m] = r.integers(max(I64.min + 1, lo - 5000), lo, m) if lo > I64.min + 1 else pk[:m]
+    pk[m:2 * m] = r.integers(hi + 1, min(I64.max, hi + 5000), m) if hi < I64.max - 1 else pk[m:2 * m]
+    pk[2 * m:2 * m + 4] = [I64.max, I64.min + 1, I64.min, lo]
+    return pk
 
 
 @pytest.mark.parametrize("nb,np_", [(1, 1), (10, 1000), (1000, 100_003), (100_000, 3_000_017)])
@@ -93,3 +121,55 @@ def test_join_load_factors(db):
     want = O.join_agg(b["key"], b["payload"], p["key"], p["value"], F.JOIN_INNER)
     for lf in (0.25, 0.5, 0.75):
         assert agg(db, b, p, F.JOIN_INNER, lf=lf)["sum_payload"] == want["sum_payload"]
+
+
+@pytest.mark.parametrize("kind", ["dense_offset", "dense_negative", "hashed"])
+@pytest.mark.parametrize("jt", TYPES)
+def test_join_dense_and_hashed_tables(db, kind, jt):
+    """The build picks a direct-addressed table when its keys span fewer values
+    than it has slots, else it hashes; both give the oracle's answers, with
+    duplicate build keys, NULL keys on both sides, probe keys outside the
+    build range and at the int64 extremes."""
+    r = np.random.default_rng(11 + jt)
+    nb, npr = 20_000, 400_000
+    if kind == "dense_offset":
+        keys = 10**15 + r.permutation(nb)
+    elif kind == "dense_negative":
+        keys = -7 * 10**12 + r.integers(0, nb // 2, nb)  # many duplicates
+    else:
+        keys = r.integers(-(1 << 62), 1 << 62, nb)
+    b = {"key": keys.astype(np.int64), "payload": r.integers(-1000, 1000, nb)}
+    p = {"key": _edge_probes(r, b["key"], npr).astype(np.int64), "value": r.random(npr)}
+    bvalid = F.validity_words(r.random(nb) > 0.05)
+    pvalid = F.validity_words(r.random(npr) > 0.05)
+    got = agg(db, b, p, jt, bvalid, pvalid, dense=kind != "hashed")
+    want = O.join_agg(b["key"], b["payload"], p["key"], p["value"], jt, bvalid=bvalid, pvalid=pvalid)
+    check_agg(got, want, jt)
+
+
+@pytest.mark.parametrize("span_extra,dense", [(0, True), (1, False)])
+def test_join_dense_threshold(db, span_extra, dense):
+    """Build keys spanning exactly the table's slot count minus one are dense;
+    one more value and the table hashes.  Row pairs and aggregates match the
+    oracle either way."""
+    r = np.random.default_rng(5)
+    nb = 1000
+    h0 = ops.HashTable(db, dev(np.arange(nb, dtype=np.int64)), None, nb)
+    cap = h0.capacity
+    h0.free()
+    keys = np.arange(nb, dtype=np.int64) - 40
+    keys[-1] = keys[0] + cap - 1 + span_extra
+    pk = np.concatenate([keys, r.integers(-100, cap + 100, 50_000)]).astype(np.int64)
+    b = {"key": keys, "payload": r.integers(0, 50, nb)}
+    p = {"key": pk, "value": r.random(len(pk))}
+    for jt in TYPES:
+        check_agg(agg(db, b, p, jt, dense=dense), O.join_agg(b["key"], b["payload"], p["key"], p["value"], jt), jt)
+    h = ops.HashTable(db, dev(keys), None, nb)
+    assert h.capacity == cap and h.dense == dense
+    want_l, want_r = O.join_pairs(keys, pk, F.JOIN_INNER)
+    left, right, cnt = h.probe_pairs(dev(pk), len(pk), F.JOIN_INNER, capacity=len(want_l) + 16)
+    c = int(cnt.item())
+    assert c == len(want_l)
+    got = sorted(zip(left[:c].cpu().numpy().view(np.uint32).tolist(), right[:c].cpu().numpy().view(np.uint32).tolist()))
+    assert got == sorted(zip(want_l.tolist(), want_r.tolist()))
+    h.free()

@@ -131,3 +131,26 @@ def test_online_server_submit_wait(db, env):
         srv.wait(tickets[0], timeout_s=0.0)  # a ticket is handed out once
     st = srv.stop()
     assert st.batches >= 1 and st.qps > 0
+
+
+def test_serve_join_on_a_hashed_table(db, env):
+    """JOIN queries served over a table whose keys hash (they span far more
+    values than it has slots); the fixture's table is direct-addressed."""
+    cols, ht, host = env
+    bkey = host["bkey"] * 7919 + 3
+    pkey = host["pkey"] * 7919 + 3
+    hh = ops.HashTable(db, torch.from_numpy(bkey).cuda(), torch.from_numpy(host["bpay"]).cuda(), len(bkey))
+    assert ht.dense and not hh.dense
+    dpk = torch.from_numpy(pkey).cuda()
+    r = np.random.default_rng(77)
+    qs = []
+    for i in range(24):
+        n = int(min(N, max(1, np.floor(10 ** (1 + 5.3 * r.random())))))
+        qs.append(S.join_query(dpk.data_ptr(), cols["pval"].data_ptr(), hh._h.value, n, float(r.random() * 100)))
+    res, _ = S.serve_trace(db, qs, max_batch=16, slots=1)
+    for q, rr in zip(qs, res):
+        assert rr.status == 0
+        sel = pkey[:q.nrows][host["pval"][:q.nrows] < q.threshold / 100]
+        o = O.join_agg(bkey, host["bpay"], sel, np.zeros(len(sel)), F.JOIN_INNER)
+        assert (rr.count, rr.sum_payload) == (o["count"], o["sum_payload"])
+    hh.free()
