@@ -461,30 +461,39 @@ def run_secondary(args):
 
     if args.workload in ("join", "all"):
         nb, npb = 1_000_000, n
-        b, p = W.join_tables(nb, npb, seed=7)
-        db.create_table("b", b)
-        db.create_table("p", p)
-        bk, bp = db.column("b", "key"), db.column("b", "payload")
-        pk, pv = db.column("p", "key"), db.column("p", "value")
-        res = ops._bytes(F.JOIN_AGG_DTYPE.itemsize, db)
-        ms_build = _time_steps(lambda: ops.HashTable(db, bk, bp, nb).free(), max(3, K // 5), 2, stream, torch)
-        h = ops.HashTable(db, bk, bp, nb)
-        for jt, name in [(F.JOIN_INNER, "inner"), (F.JOIN_LEFT, "left"), (F.JOIN_SEMI, "semi"), (F.JOIN_ANTI, "anti")]:
-            val = pv if jt >= F.JOIN_SEMI else None
-            ms = _time_steps(lambda: h.probe_agg(pk, npb, jt, value=val, out=res), K, Wm, stream, torch)
-            got = ops.to_records(res, F.JOIN_AGG_DTYPE, 1)[0]
-            nbytes = 8 * npb + (8 * npb if jt >= F.JOIN_SEMI else 0)
-            line(f"join_probe_{name}", ms, nbytes, {"build_rows": nb, "probe_rows": npb, "count": int(got["count"]),
-                                                   "build_ms": round(ms_build, 4),
-                                                   "query_ms_build_plus_probe": round(ms + ms_build, 4),
-                                                   "query_GBps": round((nbytes + 16 * nb) / ((ms + ms_build) / 1e3)
-                                                                       / 1e9, 1)})
-        want = O.join_agg(b["key"], b["payload"], p["key"], p["value"], F.JOIN_INNER)
-        got = ops.to_records(h.probe_agg(pk, npb, F.JOIN_INNER, out=res), F.JOIN_AGG_DTYPE, 1)[0]
-        assert int(got["count"]) == want["count"] and int(got["sum_payload"]) == want["sum_payload"]
-        h.free()
-        db.drop_table("b")
-        db.drop_table("p")
+        b0, p0 = W.join_tables(nb, npb, seed=7)
+        # The build keys are a permutation of 0..nb-1, so the table is direct-
+        # addressed; "_hashed" scatters every key (x 7919 + 3) so that the same
+        # join runs on a hashed table.
+        for tag, scale in (("", None), ("_hashed", 7919)):
+            b, p = dict(b0), dict(p0)
+            if scale:
+                b["key"] = b0["key"] * scale + 3
+                p["key"] = p0["key"] * scale + 3
+            db.create_table("b", b)
+            db.create_table("p", p)
+            bk, bp = db.column("b", "key"), db.column("b", "payload")
+            pk, pv = db.column("p", "key"), db.column("p", "value")
+            res = ops._bytes(F.JOIN_AGG_DTYPE.itemsize, db)
+            ms_build = _time_steps(lambda: ops.HashTable(db, bk, bp, nb).free(), max(3, K // 5), 2, stream, torch)
+            h = ops.HashTable(db, bk, bp, nb)
+            for jt, name in [(F.JOIN_INNER, "inner"), (F.JOIN_LEFT, "left"), (F.JOIN_SEMI, "semi"),
+                             (F.JOIN_ANTI, "anti")]:
+                val = pv if jt >= F.JOIN_SEMI else None
+                ms = _time_steps(lambda: h.probe_agg(pk, npb, jt, value=val, out=res), K, Wm, stream, torch)
+                got = ops.to_records(res, F.JOIN_AGG_DTYPE, 1)[0]
+                nbytes = 8 * npb + (8 * npb if jt >= F.JOIN_SEMI else 0)
+                line(f"join_probe_{name}{tag}", ms, nbytes, {
+                    "build_rows": nb, "probe_rows": npb, "count": int(got["count"]),
+                    "table": "direct-addressed" if h.dense else "hashed", "build_ms": round(ms_build, 4),
+                    "query_ms_build_plus_probe": round(ms + ms_build, 4),
+                    "query_GBps": round((nbytes + 16 * nb) / ((ms + ms_build) / 1e3) / 1e9, 1)})
+            want = O.join_agg(b["key"], b["payload"], p["key"], p["value"], F.JOIN_INNER)
+            got = ops.to_records(h.probe_agg(pk, npb, F.JOIN_INNER, out=res), F.JOIN_AGG_DTYPE, 1)[0]
+            assert int(got["count"]) == want["count"] and int(got["sum_payload"]) == want["sum_payload"]
+            h.free()
+            db.drop_table("b")
+            db.drop_table("p")
 
     if args.workload in ("groupby", "all"):
         g = W.groupby_table(n, distinct=10_000_000, seed=11)
