@@ -457,32 +457,38 @@ __device__ void serve_shared_unit(const ServeArgs& a, const ServeG g, uint64_t t
       }
       __syncwarp();
       // 32 rows at a time: the lanes whose rows pass and share a group find
-      // one another (__match_any_sync on the code); the lowest of them folds
-      // the group's rows, in row order, straight from the staged columns and
-      // updates the warp's table with plain stores.  No two lanes of a warp
-      // ever write one group's words at once, and no other warp writes them.
+      // one another (__match_any_sync on the code) and take their rank among
+      // them.  Round r then lets every lane of rank r add its row to its
+      // group's words of the warp's table with plain stores: lanes of one
+      // rank never share a group, and no other warp writes these words.  Each
+      // lane keeps its own row's values in registers.
       const uint32_t* codes = reinterpret_cast<const uint32_t*>(s1);
+      const unsigned below = (1u << lane) - 1u;
       for (uint32_t b = (uint32_t)warp * 32; b < re; b += kServeThreads) {
         const uint32_t i = b + lane;
         uint32_t gc = 0xFFFFFFFFu;
+        double v = 0.0;
+        long long v2 = 0;
         if (i < re) {
           const uint32_t c = codes[i];
-          if (__longlong_as_double((long long)s0[i]) > qthr && c < qdict) gc = c;
+          v = __longlong_as_double((long long)s0[i]);
+          if (v > qthr && c < qdict) {
+            gc = c;
+            v2 = s2[i];
+          }
         }
         const unsigned peers = __match_any_sync(0xffffffffu, gc);
-        if (gc != 0xFFFFFFFFu && lane == __ffs(peers) - 1) {
-          double v0 = 0.0;
-          long long v2 = 0;
-          for (unsigned m = peers; m; m &= m - 1) {
-            const uint32_t r = b + (uint32_t)(__ffs(m) - 1);
-            v0 += __longlong_as_double((long long)s0[r]);
-            v2 += s2[r];
+        const bool in = gc != 0xFFFFFFFFu;
+        const unsigned rank = __popc(peers & below);
+        const unsigned rounds = __reduce_max_sync(0xffffffffu, in ? (unsigned)__popc(peers) : 0u);
+        if (in && rank == 0) sm.gcount[warp][gc] += (unsigned long long)__popc(peers);
+        for (unsigned r = 0; r < rounds; ++r) {
+          if (in && rank == r) {
+            sm.gsum0[warp][gc] += v;
+            sm.gsum2[warp][gc] += v2;
           }
-          sm.gcount[warp][gc] += (unsigned long long)__popc(peers);
-          sm.gsum0[warp][gc] += v0;
-          sm.gsum2[warp][gc] += v2;
+          __syncwarp();  // the next rank's lane reads these words
         }
-        __syncwarp();  // the next leader of this group reads these words
       }
       serve_bar();
       if (threadIdx.x < qdict) {
