@@ -112,7 +112,8 @@ struct ServeG {             // a group of queries that read the same table
   const unsigned int* cnt;
   uint64_t cap;
   int64_t dmin;             // dense table: key k lives in slot k - dmin
-  int32_t dense, _pad3;
+  int32_t dense;
+  int32_t ngroupq;          // GROUP queries in the group
 };
 
 struct ServeHeader {
@@ -136,6 +137,10 @@ struct ServeArgs {
 // Shared queries whose partial results a CTA keeps in shared memory (the
 // first ones of a batch; later ones add theirs per unit).
 constexpr int kServeCacheQ = 32;
+// GROUP queries one unit evaluates together, and the fewest worth it (with
+// fewer, the per-query fold is faster than the binned atomics).
+constexpr int kShareGroupQ = 32;
+constexpr int kShareGroupMin = 4;
 
 struct ServeSmem {                      // the shared-scan kernel
   uint64_t gstart[kServeMaxBatch + 1];  // unit0 of each shared group
@@ -151,6 +156,16 @@ struct ServeSmem {                      // the shared-scan kernel
   unsigned long long gcount[kServeWarps][FDB_SERVE_MAX_GROUPS];
   double gsum0[kServeWarps][FDB_SERVE_MAX_GROUPS];
   long long gsum2[kServeWarps][FDB_SERVE_MAX_GROUPS];
+  // GROUP queries evaluated together over one unit (serve_group_shared):
+  // their thresholds ascending, their indices, which queries those are, and
+  // the unit's rows binned by (code, number of thresholds below the score).
+  double sthr[kShareGroupQ];
+  uint32_t sqid[kShareGroupQ];
+  uint32_t taken[kServeMaxBatch / 32];
+  int32_t sna;
+  unsigned int dcount[FDB_SERVE_MAX_GROUPS * kShareGroupQ];
+  double dsum0[FDB_SERVE_MAX_GROUPS * kShareGroupQ];
+  unsigned long long dsum2[FDB_SERVE_MAX_GROUPS * kShareGroupQ];
 };
 
 struct TopkSmem {                       // the top-k and finish kernels
@@ -338,6 +353,27 @@ __device__ void serve_probe_rows(const ServeG g, uint64_t* s0, uint32_t* m, uint
       h[j] = join_home(mode, key, sk[j]);
       if (h[j] <= mask) todo |= 1u << j;  // a dense table cannot hold a key outside its range
     }
+    if (mode.dense && todo) {
+      // Direct-addressed: key k can only be in slot k - dmin, so one 16-byte
+      // read per row resolves it.
+      JSlot sl[kProbeIlp];
+#pragma unroll
+      for (int j = 0; j < kProbeIlp; ++j) {
+        sl[j].key = 0;
+        sl[j].psum = 0;
+        if ((todo >> j) & 1u)
+          asm volatile("ld.global.L2::cache_hint.v2.u64 {%0, %1}, [%2], %3;"
+                       : "=l"(sl[j].key), "=l"(sl[j].psum)
+                       : "l"(g.slots + h[j]), "l"(pol));
+      }
+#pragma unroll
+      for (int j = 0; j < kProbeIlp; ++j)
+        if (((todo >> j) & 1u) && sl[j].key == sk[j]) {
+          at[j] = (uint32_t)h[j];
+          ps[j] = sl[j].psum;
+        }
+      todo = 0;
+    }
     for (uint64_t round = 0; todo && round <= mask; ++round) {
       JSlot lo[kProbeIlp], hi[kProbeIlp];
 #pragma unroll
@@ -396,6 +432,111 @@ __device__ __forceinline__ ShareCols share_cols(const ServeG& g) {
   return c;
 }
 
+// The GROUP queries of a group that cover all `rows` rows of this unit, up
+// to kShareGroupQ of them, in one pass over the rows.  Query j (thresholds
+// t_0 <= t_1 <= ...) takes a row when t_j < score, so a row whose score is
+// above exactly k thresholds belongs to queries 0..k-1: it is added once, to
+// bin (code, k-1), and query j's group total is the sum of bins j..na-1.  The
+// per-row work does not grow with the number of queries.  Sets sm.taken for
+// the queries it answered (none when fewer than kShareGroupMin qualify).
+__device__ void serve_group_shared(const ServeArgs& a, const ServeG& g, uint64_t r0, uint32_t rows,
+                                   const uint64_t* s0, const uint32_t* codes, const int64_t* s2, ServeSmem& sm) {
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const unsigned below = (1u << lane) - 1u;
+  if (warp == 0) {
+    if (lane < kServeMaxBatch / 32) sm.taken[lane] = 0;
+    int na = 0;
+    for (uint32_t c0 = 0; c0 < g.nq && na < kShareGroupQ; c0 += 32) {
+      const uint32_t qi = g.q0 + c0 + lane;
+      bool el = false;
+      double thr = 0.0;
+      if (c0 + lane < g.nq) {
+        const ServeQ& q = a.q[qi];
+        el = q.kind == FDB_SERVE_GROUP && q.n >= r0 + rows;
+        thr = q.thr;
+      }
+      const unsigned m = __ballot_sync(0xffffffffu, el);
+      const int pos = na + __popc(m & below);
+      if (el && pos < kShareGroupQ) {
+        sm.sthr[pos] = thr;
+        sm.sqid[pos] = qi;
+      }
+      na += __popc(m);
+    }
+    if (na > kShareGroupQ) na = kShareGroupQ;
+    if (na < kShareGroupMin) na = 0;
+    __syncwarp();
+    // Rank the thresholds (ties by position) and store them ascending.
+    const double t = lane < na ? sm.sthr[lane] : 0.0;
+    const uint32_t q = lane < na ? sm.sqid[lane] : 0u;
+    int rank = 0;
+    for (int j = 0; j < na; ++j) {
+      const double tj = __shfl_sync(0xffffffffu, t, j);
+      rank += (tj < t || (tj == t && j < lane)) ? 1 : 0;
+    }
+    __syncwarp();
+    if (lane < na) {
+      sm.sthr[rank] = t;
+      sm.sqid[rank] = q;
+      atomicOr(&sm.taken[(q - g.q0) >> 5], 1u << ((q - g.q0) & 31));
+    }
+    if (lane == 0) sm.sna = na;
+  }
+  serve_bar();
+  const int na = sm.sna;
+  if (na == 0) return;
+  for (int i = threadIdx.x; i < FDB_SERVE_MAX_GROUPS * kShareGroupQ; i += kServeThreads) {
+    sm.dcount[i] = 0;
+    sm.dsum0[i] = 0.0;
+    sm.dsum2[i] = 0;
+  }
+  serve_bar();
+  for (uint32_t i = threadIdx.x; i < rows; i += kServeThreads) {
+    const uint32_t code = codes[i];
+    if (code >= FDB_SERVE_MAX_GROUPS) continue;  // beyond every query's dictionary
+    const double v = __longlong_as_double((long long)s0[i]);
+    int lo = 0, hi = na;  // k = number of thresholds below v (none for NaN)
+    while (lo < hi) {
+      const int mid = (lo + hi) >> 1;
+      if (sm.sthr[mid] < v)
+        lo = mid + 1;
+      else
+        hi = mid;
+    }
+    if (lo == 0) continue;
+    const int cell = (int)code * kShareGroupQ + lo - 1;
+    atomicAdd(&sm.dcount[cell], 1u);
+    atomicAdd(&sm.dsum0[cell], v);
+    atomicAdd(&sm.dsum2[cell], (unsigned long long)s2[i]);
+  }
+  serve_bar();
+  if (threadIdx.x < FDB_SERVE_MAX_GROUPS) {  // thread gc: the only writer of group gc's totals
+    const uint32_t gc = threadIdx.x;
+    unsigned long long c = 0;
+    double v0 = 0.0;
+    long long v2 = 0;
+    for (int k = na - 1; k >= 0; --k) {
+      const int cell = (int)gc * kShareGroupQ + k;
+      c += sm.dcount[cell];
+      v0 += sm.dsum0[cell];
+      v2 += (long long)sm.dsum2[cell];
+      const uint32_t qi = sm.sqid[k];
+      if (c == 0 || gc >= a.q[qi].dict_len) continue;
+      if (qi < (uint32_t)kServeCacheQ) {
+        sm.agcount[qi][gc] += c;
+        sm.agsum0[qi][gc] += v0;
+        sm.agsum2[qi][gc] += v2;
+      } else {
+        ServeRes& r = a.res[qi];
+        atomicAdd(&r.gcount[gc], c);
+        atomicAdd(&r.gsum0[gc], v0);
+        atomicAdd(reinterpret_cast<unsigned long long*>(&r.gsum2[gc]), (unsigned long long)v2);
+      }
+    }
+  }
+  serve_bar();
+}
+
 // One shared unit whose rows are staged at `st` (the columns in `plain` are
 // loaded here by the consumers): probe them once for a join group, then
 // evaluate every query of the group that reaches this unit.
@@ -419,11 +560,19 @@ __device__ void serve_shared_unit(const ServeArgs& a, const ServeG g, uint64_t t
     serve_bar();
   }
   if (g.join) serve_probe_rows(g, s0, smm, rows);
+  bool shared_group = false;
+  if (g.ngroupq >= kShareGroupMin) {
+    serve_group_shared(a, g, r0, rows, s0, reinterpret_cast<const uint32_t*>(s1), s2, sm);
+    shared_group = sm.sna != 0;
+  }
   for (uint32_t qi = g.q0; qi < g.q0 + g.nq; ++qi) {
     const ServeQ& qref = a.q[qi];
     const uint64_t qn = qref.n;
     if (qn <= r0) break;  // queries are by rows descending
     const int qkind = qref.kind;
+    if (shared_group && qkind == FDB_SERVE_GROUP &&
+        ((sm.taken[(qi - g.q0) >> 5] >> ((qi - g.q0) & 31)) & 1u))
+      continue;  // answered by serve_group_shared
     const double qthr = qref.thr;
     const uint32_t qdict = qref.dict_len;
     const uint32_t re = (uint32_t)umin64(rows, qn - r0);
@@ -978,6 +1127,8 @@ static bool slot_launch(Server& s, ServeSlot& sl) {
     }
     d.unit0 = units;
     units += (d.max_n + d.unit_rows - 1) / d.unit_rows;
+    d.ngroupq = 0;
+    for (uint64_t tk : g.tickets) d.ngroupq += s.jobs[tk].q.kind == FDB_SERVE_GROUP ? 1 : 0;
     d.join = g.join ? 1 : 0;
     if (g.join) {
       const JoinView v = join_view(hash_of(g.table));

@@ -154,3 +154,36 @@ def test_serve_join_on_a_hashed_table(db, env):
         o = O.join_agg(bkey, host["bpay"], sel, np.zeros(len(sel)), F.JOIN_INNER)
         assert (rr.count, rr.sum_payload) == (o["count"], o["sum_payload"])
     hh.free()
+
+
+def test_serve_many_group_queries_in_one_batch(db, env):
+    """40 GROUP queries in one batch: up to 32 that cover a whole unit are
+    answered together by threshold rank, the rest one by one.  Thresholds
+    repeat and reach both ends of the score range, prefixes differ (so queries
+    cover units partly) and two dictionary sizes are mixed; every answer must
+    match the query run alone."""
+    cols, ht, host = env
+    r = np.random.default_rng(40)
+    thr = [50.0, 50.0, 50.0, -1.0, 100.0, 0.0, 99.9] + [float(x) for x in r.random(33) * 100]
+    qs = []
+    for i, x in enumerate(thr):
+        n = N if i % 3 else int(r.integers(1, N))
+        dict_len = 12 if i % 5 else 7
+        qs.append(S.group_query(cols["score"].data_ptr(), cols["dept"].data_ptr(), cols["salary"].data_ptr(),
+                                dict_len, n, x))
+    res, st = S.serve_trace(db, qs, max_batch=64, slots=1)
+    assert st.batches >= 1
+    for q, rr in zip(qs, res):
+        assert rr.status == 0
+        n, x, d = q.nrows, q.threshold, q.dict_len
+        sel = host["score"][:n] > x
+        c = host["codes"][:n][sel]
+        keep = c < d
+        c = c[keep]
+        cnt = np.bincount(c, minlength=16)
+        s0 = np.bincount(c, weights=host["score"][:n][sel][keep], minlength=16)
+        s2 = np.bincount(c, weights=host["salary"][:n][sel][keep].astype(np.float64), minlength=16)
+        assert list(rr.group_count[:16]) == list(cnt)
+        assert list(rr.group_sum2[:16]) == [int(v) for v in s2]
+        for gi in range(16):
+            assert abs(rr.group_sum0[gi] - s0[gi]) <= RTOL * max(abs(s0[gi]), 1e-300)
