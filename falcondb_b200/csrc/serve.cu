@@ -114,6 +114,8 @@ struct ServeG {             // a group of queries that read the same table
   int64_t dmin;             // dense table: key k lives in slot k - dmin
   int32_t dense;
   int32_t ngroupq;          // GROUP queries in the group
+  int32_t ncountq, njoinq;  // COUNT and JOIN queries in the group
+  int32_t _pad4;
 };
 
 struct ServeHeader {
@@ -163,6 +165,9 @@ struct ServeSmem {                      // the shared-scan kernel
   uint32_t sqid[kShareGroupQ];
   uint32_t taken[kServeMaxBatch / 32];
   int32_t sna;
+  unsigned int wcnt[kServeWarps][kShareGroupQ];        // COUNT bins, per warp
+  unsigned long long wjc[kServeWarps][kShareGroupQ];   // JOIN bins, per warp: matches
+  unsigned long long wjp[kServeWarps][kShareGroupQ];   //   and payload sums
   unsigned int dcount[FDB_SERVE_MAX_GROUPS * kShareGroupQ];
   double dsum0[FDB_SERVE_MAX_GROUPS * kShareGroupQ];
   unsigned long long dsum2[FDB_SERVE_MAX_GROUPS * kShareGroupQ];
@@ -432,33 +437,30 @@ __device__ __forceinline__ ShareCols share_cols(const ServeG& g) {
   return c;
 }
 
-// The GROUP queries of a group that cover all `rows` rows of this unit, up
-// to kShareGroupQ of them, in one pass over the rows.  Query j (thresholds
-// t_0 <= t_1 <= ...) takes a row when t_j < score, so a row whose score is
-// above exactly k thresholds belongs to queries 0..k-1: it is added once, to
-// bin (code, k-1), and query j's group total is the sum of bins j..na-1.  The
-// per-row work does not grow with the number of queries.  Sets sm.taken for
-// the queries it answered (none when fewer than kShareGroupMin qualify).
-__device__ void serve_group_shared(const ServeArgs& a, const ServeG& g, uint64_t r0, uint32_t rows,
-                                   const uint64_t* s0, const uint32_t* codes, const int64_t* s2, ServeSmem& sm) {
+// Queries of kind `kind` in group g that cover all `rows` rows of this unit
+// (up to kShareGroupQ, in list order) are evaluated together in one pass over
+// the rows: their keys (the threshold; a JOIN's value limit, threshold / 100)
+// go to sm.sthr ascending and their indices to sm.sqid, sm.sna is their number
+// (0 when fewer than kShareGroupMin qualify) and sm.taken marks them.  Ends
+// with a consumer barrier.
+__device__ void serve_pick(const ServeArgs& a, const ServeG& g, uint64_t r0, uint32_t rows, int kind, ServeSmem& sm) {
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const unsigned below = (1u << lane) - 1u;
   if (warp == 0) {
-    if (lane < kServeMaxBatch / 32) sm.taken[lane] = 0;
     int na = 0;
     for (uint32_t c0 = 0; c0 < g.nq && na < kShareGroupQ; c0 += 32) {
       const uint32_t qi = g.q0 + c0 + lane;
       bool el = false;
-      double thr = 0.0;
+      double key = 0.0;
       if (c0 + lane < g.nq) {
         const ServeQ& q = a.q[qi];
-        el = q.kind == FDB_SERVE_GROUP && q.n >= r0 + rows;
-        thr = q.thr;
+        el = q.kind == kind && q.n >= r0 + rows;
+        key = kind == FDB_SERVE_JOIN ? q.thr / 100.0 : q.thr;
       }
       const unsigned m = __ballot_sync(0xffffffffu, el);
       const int pos = na + __popc(m & below);
       if (el && pos < kShareGroupQ) {
-        sm.sthr[pos] = thr;
+        sm.sthr[pos] = key;
         sm.sqid[pos] = qi;
       }
       na += __popc(m);
@@ -466,7 +468,7 @@ __device__ void serve_group_shared(const ServeArgs& a, const ServeG& g, uint64_t
     if (na > kShareGroupQ) na = kShareGroupQ;
     if (na < kShareGroupMin) na = 0;
     __syncwarp();
-    // Rank the thresholds (ties by position) and store them ascending.
+    // Rank the keys (ties by position) and store them ascending.
     const double t = lane < na ? sm.sthr[lane] : 0.0;
     const uint32_t q = lane < na ? sm.sqid[lane] : 0u;
     int rank = 0;
@@ -483,6 +485,144 @@ __device__ void serve_group_shared(const ServeArgs& a, const ServeG& g, uint64_t
     if (lane == 0) sm.sna = na;
   }
   serve_bar();
+}
+
+// Number of the na ascending keys below v (strict: none for NaN).
+__device__ __forceinline__ int serve_rank_below(const double* keys, int na, double v) {
+  int lo = 0, hi = na;
+  while (lo < hi) {
+    const int mid = (lo + hi) >> 1;
+    if (keys[mid] < v)
+      lo = mid + 1;
+    else
+      hi = mid;
+  }
+  return lo;
+}
+
+// Adds a shared query's partial result: to the CTA's copy when the query's
+// partials are kept in shared memory, else to the global result.
+__device__ __forceinline__ void serve_add_count(const ServeArgs& a, ServeSmem& sm, uint32_t qi, unsigned long long c,
+                                                unsigned long long ps, bool with_sum) {
+  if (qi < (uint32_t)kServeCacheQ) {
+    sm.acount[qi] += c;
+    if (with_sum) sm.asum[qi] += ps;
+  } else {
+    if (c) atomicAdd(&a.res[qi].count, c);
+    if (with_sum && ps) atomicAdd(reinterpret_cast<unsigned long long*>(&a.res[qi].sum), ps);
+  }
+}
+
+// COUNT(*) WHERE score > t for the picked COUNT queries: a row above exactly k
+// thresholds counts for queries 0..k-1, so it goes to bin k-1 and query j's
+// count is the sum of bins j..na-1.  Bins are per warp; the lowest lane of the
+// lanes that share a bin adds their number.
+__device__ void serve_count_shared(const ServeArgs& a, uint32_t rows, const uint64_t* s0, ServeSmem& sm) {
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int na = sm.sna;
+  sm.wcnt[warp][lane] = 0;
+  __syncwarp();
+  for (uint32_t b = (uint32_t)warp * 32; b < rows; b += kServeThreads) {
+    const uint32_t i = b + lane;
+    int k = 0;
+    if (i < rows) k = serve_rank_below(sm.sthr, na, __longlong_as_double((long long)s0[i]));
+    const unsigned peers = __match_any_sync(0xffffffffu, k);
+    if (k > 0 && lane == __ffs(peers) - 1) sm.wcnt[warp][k - 1] += (unsigned)__popc(peers);
+    __syncwarp();
+  }
+  serve_bar();
+  if (warp == 0) {
+    unsigned long long c = 0;
+    if (lane < na)
+      for (int w = 0; w < kServeWarps; ++w) c += sm.wcnt[w][lane];
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {  // suffix sums: lane j gets bins j..31
+      const unsigned long long x = __shfl_down_sync(0xffffffffu, c, o);
+      if (lane + o < 32) c += x;
+    }
+    if (lane < na) serve_add_count(a, sm, sm.sqid[lane], c, 0, false);
+  }
+  serve_bar();
+}
+
+// The picked JOIN queries (WHERE value < limit, limits ascending): a row whose
+// value is at or above exactly k limits counts for queries k..na-1, so its
+// matches and payload sum go to bin k and query j's result is the sum of bins
+// 0..j.  Bins are per warp; lanes that share a bin add their row in rank
+// rounds with plain stores.  A NaN value is under no limit.
+__device__ void serve_join_shared(const ServeArgs& a, uint32_t rows, const uint64_t* s0, const double* v,
+                                  const uint32_t* smm, ServeSmem& sm) {
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const unsigned below = (1u << lane) - 1u;
+  const int na = sm.sna;
+  sm.wjc[warp][lane] = 0;
+  sm.wjp[warp][lane] = 0;
+  __syncwarp();
+  for (uint32_t b = (uint32_t)warp * 32; b < rows; b += kServeThreads) {
+    const uint32_t i = b + lane;
+    int k = na;  // na: in no query
+    if (i < rows) {
+      const double x = v[i];
+      if (!isnan(x)) {
+        int lo = 0, hi = na;  // limits at or below x
+        while (lo < hi) {
+          const int mid = (lo + hi) >> 1;
+          if (sm.sthr[mid] <= x)
+            lo = mid + 1;
+          else
+            hi = mid;
+        }
+        k = lo;
+      }
+    }
+    const bool in = k < na;
+    const unsigned peers = __match_any_sync(0xffffffffu, in ? k : -1);
+    const unsigned rank = __popc(peers & below);
+    const unsigned rounds = __reduce_max_sync(0xffffffffu, in ? (unsigned)__popc(peers) : 0u);
+    unsigned long long mc = 0, ps = 0;
+    if (in) {
+      mc = smm[i];
+      ps = s0[i];
+    }
+    for (unsigned r = 0; r < rounds; ++r) {
+      if (in && rank == r) {
+        sm.wjc[warp][k] += mc;
+        sm.wjp[warp][k] += ps;
+      }
+      __syncwarp();
+    }
+  }
+  serve_bar();
+  if (warp == 0) {
+    unsigned long long c = 0, ps = 0;
+    if (lane < na)
+      for (int w = 0; w < kServeWarps; ++w) {
+        c += sm.wjc[w][lane];
+        ps += sm.wjp[w][lane];
+      }
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {  // prefix sums: lane j gets bins 0..j
+      const unsigned long long xc = __shfl_up_sync(0xffffffffu, c, o);
+      const unsigned long long xp = __shfl_up_sync(0xffffffffu, ps, o);
+      if (lane >= o) {
+        c += xc;
+        ps += xp;
+      }
+    }
+    if (lane < na) serve_add_count(a, sm, sm.sqid[lane], c, ps, true);
+  }
+  serve_bar();
+}
+
+// The GROUP queries of a group that cover all `rows` rows of this unit, up
+// to kShareGroupQ of them, in one pass over the rows.  Query j (thresholds
+// t_0 <= t_1 <= ...) takes a row when t_j < score, so a row whose score is
+// above exactly k thresholds belongs to queries 0..k-1: it is added once, to
+// bin (code, k-1), and query j's group total is the sum of bins j..na-1.  The
+// per-row work does not grow with the number of queries.
+__device__ void serve_group_shared(const ServeArgs& a, const ServeG& g, uint64_t r0, uint32_t rows,
+                                   const uint64_t* s0, const uint32_t* codes, const int64_t* s2, ServeSmem& sm) {
+  serve_pick(a, g, r0, rows, FDB_SERVE_GROUP, sm);
   const int na = sm.sna;
   if (na == 0) return;
   for (int i = threadIdx.x; i < FDB_SERVE_MAX_GROUPS * kShareGroupQ; i += kServeThreads) {
@@ -560,19 +700,28 @@ __device__ void serve_shared_unit(const ServeArgs& a, const ServeG g, uint64_t t
     serve_bar();
   }
   if (g.join) serve_probe_rows(g, s0, smm, rows);
-  bool shared_group = false;
-  if (g.ngroupq >= kShareGroupMin) {
-    serve_group_shared(a, g, r0, rows, s0, reinterpret_cast<const uint32_t*>(s1), s2, sm);
-    shared_group = sm.sna != 0;
+  // Kinds with enough queries in the group are evaluated together, once per
+  // row (serve_pick); the loop below skips the queries they answered.
+  const bool share = g.ngroupq >= kShareGroupMin || g.ncountq >= kShareGroupMin || g.njoinq >= kShareGroupMin;
+  if (share) {
+    if (threadIdx.x < kServeMaxBatch / 32) sm.taken[threadIdx.x] = 0;  // ordered by serve_pick's barrier
+    if (g.ngroupq >= kShareGroupMin)
+      serve_group_shared(a, g, r0, rows, s0, reinterpret_cast<const uint32_t*>(s1), s2, sm);
+    if (g.ncountq >= kShareGroupMin) {
+      serve_pick(a, g, r0, rows, FDB_SERVE_COUNT, sm);
+      if (sm.sna) serve_count_shared(a, rows, s0, sm);
+    }
+    if (g.njoinq >= kShareGroupMin) {
+      serve_pick(a, g, r0, rows, FDB_SERVE_JOIN, sm);
+      if (sm.sna) serve_join_shared(a, rows, s0, reinterpret_cast<const double*>(s1), smm, sm);
+    }
   }
   for (uint32_t qi = g.q0; qi < g.q0 + g.nq; ++qi) {
     const ServeQ& qref = a.q[qi];
     const uint64_t qn = qref.n;
     if (qn <= r0) break;  // queries are by rows descending
     const int qkind = qref.kind;
-    if (shared_group && qkind == FDB_SERVE_GROUP &&
-        ((sm.taken[(qi - g.q0) >> 5] >> ((qi - g.q0) & 31)) & 1u))
-      continue;  // answered by serve_group_shared
+    if (share && ((sm.taken[(qi - g.q0) >> 5] >> ((qi - g.q0) & 31)) & 1u)) continue;  // answered together
     const double qthr = qref.thr;
     const uint32_t qdict = qref.dict_len;
     const uint32_t re = (uint32_t)umin64(rows, qn - r0);
@@ -1127,8 +1276,13 @@ static bool slot_launch(Server& s, ServeSlot& sl) {
     }
     d.unit0 = units;
     units += (d.max_n + d.unit_rows - 1) / d.unit_rows;
-    d.ngroupq = 0;
-    for (uint64_t tk : g.tickets) d.ngroupq += s.jobs[tk].q.kind == FDB_SERVE_GROUP ? 1 : 0;
+    d.ngroupq = d.ncountq = d.njoinq = 0;
+    for (uint64_t tk : g.tickets) {
+      const int kind = s.jobs[tk].q.kind;
+      d.ngroupq += kind == FDB_SERVE_GROUP ? 1 : 0;
+      d.ncountq += kind == FDB_SERVE_COUNT ? 1 : 0;
+      d.njoinq += kind == FDB_SERVE_JOIN ? 1 : 0;
+    }
     d.join = g.join ? 1 : 0;
     if (g.join) {
       const JoinView v = join_view(hash_of(g.table));

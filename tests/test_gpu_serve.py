@@ -187,3 +187,21 @@ def test_serve_many_group_queries_in_one_batch(db, env):
         assert list(rr.group_sum2[:16]) == [int(v) for v in s2]
         for gi in range(16):
             assert abs(rr.group_sum0[gi] - s0[gi]) <= RTOL * max(abs(s0[gi]), 1e-300)
+
+
+def test_serve_many_count_and_join_queries_in_one_batch(db, env):
+    """40 COUNT and 40 JOIN queries in one batch: those covering a whole unit
+    are answered together by threshold rank (a suffix sum of binned rows for
+    COUNT, a prefix sum for JOIN's value < limit), the rest one by one.
+    Thresholds repeat and reach both ends; prefixes differ."""
+    cols, ht, host = env
+    r = np.random.default_rng(41)
+    thr = [50.0, 50.0, 50.0, -1.0, 100.0, 0.0, 99.9, 100.5] + [float(x) for x in r.random(32) * 100]
+    qs = []
+    for i, x in enumerate(thr):
+        n = N if i % 3 else int(r.integers(1, N))
+        qs.append(S.count_query(cols["score"].data_ptr(), n, x))
+        qs.append(S.join_query(cols["pkey"].data_ptr(), cols["pval"].data_ptr(), ht._h.value, n, x))
+    res, _ = S.serve_trace(db, qs, max_batch=128, slots=1)
+    for q, rr in zip(qs, res):
+        check(q, rr, host)
