@@ -207,7 +207,12 @@ int  fdb_table_column(const fdb_db* db, const char* table, const char* column,
                       fdb_dev_column* out, uint64_t* nrows);
 
 /* Execute SQL (falcondb_sql, c_ffi.rs:86-99 -> Database::sql, db.rs:242-316).
- * *out is NULL on error. Supported shapes: see DESIGN.md of the package. */
+ * *out is NULL on error.  Supported shapes (others fail with FDB_E_SQL):
+ *   SELECT items FROM t [[INNER] | LEFT [OUTER] JOIN u ON t.k = u.k] [WHERE pred]
+ *          [GROUP BY col] [ORDER BY col|alias [ASC|DESC] [NULLS FIRST|LAST], ...] [LIMIT n]
+ *   items: *, col, COUNT(*), COUNT(col), COUNT(DISTINCT col), SUM/AVG/MIN/MAX(col) [AS a]
+ *   pred : col op literal, IS [NOT] NULL, [NOT] IN (...), [NOT] LIKE (Utf8), AND, OR,
+ *          parentheses, and [NOT] EXISTS (SELECT ... FROM u WHERE u.k = t.k). */
 int  fdb_sql(fdb_db* db, const char* sql, fdb_result** out);
 
 /* Result accessors (c_ffi.rs:103-127). */
