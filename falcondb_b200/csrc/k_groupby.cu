@@ -469,11 +469,23 @@ struct GbLaneOp {
 // measured on 100M and 1M rows of the three-column shape: large inputs run
 // 3 CTAs of 4 consumer warps per SM with 512-row tiles (0.39 ms at 100M rows);
 // small ones, where the launch and the final fold dominate, 8 consumer warps.
-#ifndef FDB_LF_BIG
-#define FDB_LF_BIG 4, 4, 2
+#ifndef FDB_LF_BIG_NCW
+#define FDB_LF_BIG_NCW 4
 #endif
-#ifndef FDB_LF_SMALL
-#define FDB_LF_SMALL 8, 2, 3
+#ifndef FDB_LF_BIG_R
+#define FDB_LF_BIG_R 4
+#endif
+#ifndef FDB_LF_BIG_ST
+#define FDB_LF_BIG_ST 2
+#endif
+#ifndef FDB_LF_SMALL_NCW
+#define FDB_LF_SMALL_NCW 8
+#endif
+#ifndef FDB_LF_SMALL_R
+#define FDB_LF_SMALL_R 2
+#endif
+#ifndef FDB_LF_SMALL_ST
+#define FDB_LF_SMALL_ST 3
 #endif
 constexpr uint64_t kLaneFastBigRows = 1ull << 24;
 template <int NV, int NCW, int R>
@@ -810,9 +822,9 @@ static void launch_lane_fast_shape(Ctx& c, const fdb_dev_column* cols, uint64_t 
 template <int NC, int NV>
 static void launch_lane_fast(Ctx& c, const fdb_dev_column* cols, uint64_t n, const GbCodesParams& p) {
   if (n >= kLaneFastBigRows)
-    launch_lane_fast_shape<NC, NV, FDB_LF_BIG>(c, cols, n, p);
+    launch_lane_fast_shape<NC, NV, FDB_LF_BIG_NCW, FDB_LF_BIG_R, FDB_LF_BIG_ST>(c, cols, n, p);
   else
-    launch_lane_fast_shape<NC, NV, FDB_LF_SMALL>(c, cols, n, p);
+    launch_lane_fast_shape<NC, NV, FDB_LF_SMALL_NCW, FDB_LF_SMALL_R, FDB_LF_SMALL_ST>(c, cols, n, p);
 }
 
 // Launch GbLaneFastOp when the query has its shape; false otherwise.
