@@ -1165,6 +1165,8 @@ static void slot_complete(Server& s, ServeSlot& sl) {
 // Admit queued queries into a free slot and launch it (s.mu held).  The
 // admitted queries are laid out group by group (queries reading the same
 // table, by rows descending), then the top-k queries.
+constexpr int kBigBatchBacklog = 3;  // long scans waiting before they are batched together
+
 static bool slot_launch(Server& s, ServeSlot& sl) {
   const uint64_t room = s.budget > s.resident ? s.budget - s.resident : 0;
   const double t = s.now();
@@ -1173,7 +1175,18 @@ static bool slot_launch(Server& s, ServeSlot& sl) {
   // happened to be admitted with it.  Within the class, arrival order.
   std::vector<uint64_t> admitted;
   const bool big = s.jobs[s.queue.front()].q.nrows >= s.split_rows;
-  for (auto it = s.queue.begin(); it != s.queue.end() && (int)admitted.size() < s.cfg.max_batch;) {
+  // Long scans are batched only under a backlog.  Two long scans in one batch
+  // both finish when the batch does, while one at a time the first finishes
+  // early; so at light load each runs alone, and once kBigBatchBacklog of them
+  // are waiting, batching them shares their reads and raises throughput.
+  int cap = s.cfg.max_batch;
+  if (big) {
+    int waiting = 0;
+    for (auto it = s.queue.begin(); it != s.queue.end() && waiting < kBigBatchBacklog; ++it)
+      waiting += s.jobs[*it].q.nrows >= s.split_rows ? 1 : 0;
+    if (waiting < kBigBatchBacklog) cap = 1;
+  }
+  for (auto it = s.queue.begin(); it != s.queue.end() && (int)admitted.size() < cap;) {
     ServeJob& j = s.jobs[*it];
     if ((j.q.nrows >= s.split_rows) != big) {
       ++it;
