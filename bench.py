@@ -729,7 +729,7 @@ def main():
                     help="scan = the headline line; the others print per-operator lines")
     ap.add_argument("--load-factor", type=float, default=0.5)
     ap.add_argument("--serve-queries", type=int, default=10_000)
-    ap.add_argument("--serve-slots", type=int, default=1)
+    ap.add_argument("--serve-slots", type=int, default=2)
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3

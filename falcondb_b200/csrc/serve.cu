@@ -1167,14 +1167,27 @@ static void slot_complete(Server& s, ServeSlot& sl) {
 // table, by rows descending), then the top-k queries.
 constexpr int kBigBatchBacklog = 3;  // long scans waiting before they are batched together
 
-static bool slot_launch(Server& s, ServeSlot& sl) {
+// small_only: this slot runs only batches of the small size class.  Slot 0
+// runs any batch and the others only small ones, so at most one long scan is
+// on the GPU at a time and short queries never wait behind one.
+static bool slot_launch(Server& s, ServeSlot& sl, bool small_only) {
   const uint64_t room = s.budget > s.resident ? s.budget - s.resident : 0;
   const double t = s.now();
   // A batch holds queries of one size class, the class of the oldest waiting
   // query: a query that reads few rows never waits for a long scan that
   // happened to be admitted with it.  Within the class, arrival order.
   std::vector<uint64_t> admitted;
-  const bool big = s.jobs[s.queue.front()].q.nrows >= s.split_rows;
+  bool big = s.jobs[s.queue.front()].q.nrows >= s.split_rows;
+  if (small_only && big) {
+    bool any = false;
+    for (uint64_t tk : s.queue)
+      if (s.jobs[tk].q.nrows < s.split_rows) {
+        any = true;
+        break;
+      }
+    if (!any) return false;
+    big = false;
+  }
   // Long scans are batched only under a backlog.  Two long scans in one batch
   // both finish when the batch does, while one at a time the first finishes
   // early; so at light load each runs alone, and once kBigBatchBacklog of them
@@ -1345,8 +1358,8 @@ static void server_loop(Server* s) {
         }
       }
       try {
-        for (ServeSlot& sl : s->slots)
-          if (!sl.busy && !s->queue.empty()) progress |= slot_launch(*s, sl);
+        for (size_t i = 0; i < s->slots.size(); ++i)
+          if (!s->slots[i].busy && !s->queue.empty()) progress |= slot_launch(*s, s->slots[i], i > 0);
       } catch (const Error& e) {
         s->error = e.what();
       }

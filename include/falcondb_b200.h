@@ -462,7 +462,8 @@ typedef struct fdb_serve_result {
 
 typedef struct fdb_serve_config {
     int32_t  max_batch;        /* queries per launch (1 = one query at a time)    */
-    int32_t  slots;            /* launches in flight                              */
+    int32_t  slots;            /* launches in flight; slot 0 runs any batch, the
+                                  others only batches of short scans            */
     uint64_t mem_budget;       /* bytes resident tables + admitted queries may hold; 0 = the context's budget */
 } fdb_serve_config;
 
