@@ -56,6 +56,10 @@ constexpr int kServeMaxBatch = 256;
 #define FDB_SERVE_CTAS 2
 #endif
 constexpr int kServeCtasPerSm = FDB_SERVE_CTAS;
+#ifndef FDB_SERVE_JOIN_CTAS
+#define FDB_SERVE_JOIN_CTAS 2
+#endif
+constexpr int kServeJoinCtasPerSm = FDB_SERVE_JOIN_CTAS;
 constexpr int kServeTopkCtasPerSm = 2;
 #ifndef FDB_SERVE_STAGES
 #define FDB_SERVE_STAGES 2
@@ -122,6 +126,8 @@ struct ServeHeader {
   int32_t nq, ngroups;
   int32_t topk0, _pad;      // top-k queries are descriptors [topk0, nq)
   uint64_t shared_units, total_units;
+  uint64_t join_units;      // join groups come first: units [0, join_units) are theirs
+  int32_t join_groups, _pad2;
 };
 
 struct ServeArgs {
@@ -683,6 +689,7 @@ __device__ void serve_group_shared(const ServeArgs& a, const ServeG& g, uint64_t
 // `g` is taken by value: the loops below store to shared memory, where a
 // cached descriptor may live, so fields read through a reference would be
 // reloaded after every store.
+template <bool JOIN>
 __device__ void serve_shared_unit(const ServeArgs& a, const ServeG g, uint64_t tile, unsigned char* st,
                                   uint32_t plain, ServeSmem& sm) {
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
@@ -699,21 +706,22 @@ __device__ void serve_shared_unit(const ServeArgs& a, const ServeG g, uint64_t t
       if ((plain >> c) & 1u) share_load(st + cols.off[c], cols.src[c], r0, rows, cols.esize[c]);
     serve_bar();
   }
-  if (g.join) serve_probe_rows(g, s0, smm, rows);
+  if constexpr (JOIN) serve_probe_rows(g, s0, smm, rows);
   // Kinds with enough queries in the group are evaluated together, once per
   // row (serve_pick); the loop below skips the queries they answered.
-  const bool share = g.ngroupq >= kShareGroupMin || g.ncountq >= kShareGroupMin || g.njoinq >= kShareGroupMin;
+  const bool share = JOIN ? g.njoinq >= kShareGroupMin : (g.ngroupq >= kShareGroupMin || g.ncountq >= kShareGroupMin);
   if (share) {
     if (threadIdx.x < kServeMaxBatch / 32) sm.taken[threadIdx.x] = 0;  // ordered by serve_pick's barrier
-    if (g.ngroupq >= kShareGroupMin)
-      serve_group_shared(a, g, r0, rows, s0, reinterpret_cast<const uint32_t*>(s1), s2, sm);
-    if (g.ncountq >= kShareGroupMin) {
-      serve_pick(a, g, r0, rows, FDB_SERVE_COUNT, sm);
-      if (sm.sna) serve_count_shared(a, rows, s0, sm);
-    }
-    if (g.njoinq >= kShareGroupMin) {
+    if constexpr (JOIN) {
       serve_pick(a, g, r0, rows, FDB_SERVE_JOIN, sm);
       if (sm.sna) serve_join_shared(a, rows, s0, reinterpret_cast<const double*>(s1), smm, sm);
+    } else {
+      if (g.ngroupq >= kShareGroupMin)
+        serve_group_shared(a, g, r0, rows, s0, reinterpret_cast<const uint32_t*>(s1), s2, sm);
+      if (g.ncountq >= kShareGroupMin) {
+        serve_pick(a, g, r0, rows, FDB_SERVE_COUNT, sm);
+        if (sm.sna) serve_count_shared(a, rows, s0, sm);
+      }
     }
   }
   for (uint32_t qi = g.q0; qi < g.q0 + g.nq; ++qi) {
@@ -726,12 +734,12 @@ __device__ void serve_shared_unit(const ServeArgs& a, const ServeG g, uint64_t t
     const uint32_t qdict = qref.dict_len;
     const uint32_t re = (uint32_t)umin64(rows, qn - r0);
     ServeRes& r = a.res[qi];
-    if (qkind == FDB_SERVE_COUNT) {
+    if (!JOIN && qkind == FDB_SERVE_COUNT) {
       unsigned long long c = 0;
       for (uint32_t i = threadIdx.x; i < re; i += kServeThreads) c += __longlong_as_double((long long)s0[i]) > qthr;
       c = warp_sum_u64(c);
       if (lane == 0 && c) atomicAdd(qi < (uint32_t)kServeCacheQ ? &sm.acount[qi] : &r.count, c);
-    } else if (qkind == FDB_SERVE_JOIN) {
+    } else if (JOIN) {
       const double lim = qthr / 100.0;
       const double* v = reinterpret_cast<const double*>(s1);
       unsigned long long c = 0, ps = 0;
@@ -822,7 +830,8 @@ __device__ void serve_shared_unit(const ServeArgs& a, const ServeG g, uint64_t t
 // order.  A column the bulk copy cannot take (its rows do not start on a
 // 16-byte boundary, or its byte count is not a multiple of 16) is flagged for
 // the consumers to load with plain loads.
-__global__ void __launch_bounds__(kServeBlock, kServeCtasPerSm) serve_kernel(ServeArgs a) {
+template <bool JOIN>
+__global__ void __launch_bounds__(kServeBlock, JOIN ? kServeJoinCtasPerSm : kServeCtasPerSm) serve_kernel(ServeArgs a) {
   extern __shared__ __align__(128) unsigned char tsm[];
   __shared__ ServeSmem sm;
   uint64_t* full = reinterpret_cast<uint64_t*>(tsm);
@@ -830,11 +839,17 @@ __global__ void __launch_bounds__(kServeBlock, kServeCtasPerSm) serve_kernel(Ser
   uint64_t* unit = empty + kServeStages;
   uint32_t* plain = reinterpret_cast<uint32_t*>(unit + kServeStages);
   unsigned char* stages = tsm + kServeBar;
-  const int ng = a.hdr->ngroups, topk0 = a.hdr->topk0;
-  const uint64_t shared = a.hdr->shared_units;
-  if (shared == 0) return;  // a batch of top-k queries only
+  // This instance's groups and units: the join groups come first.
+  const int topk0 = a.hdr->topk0;
+  const int njg = a.hdr->join_groups;
+  const int g0 = JOIN ? 0 : njg;
+  const int ng = JOIN ? njg : a.hdr->ngroups - njg;
+  const uint64_t lo = JOIN ? 0 : a.hdr->join_units;
+  const uint64_t shared = JOIN ? a.hdr->join_units : a.hdr->shared_units;  // end of this instance's units
+  if (lo == shared) return;  // no group of this kind in the batch
+  unsigned int* claim = a.claim + (JOIN ? 0 : 2);
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  for (int i = threadIdx.x; i < ng; i += kServeBlock) sm.gstart[i] = a.g[i].unit0;
+  for (int i = threadIdx.x; i < ng; i += kServeBlock) sm.gstart[i] = a.g[g0 + i].unit0;
   {
     for (int i = threadIdx.x; i < kServeCacheQ; i += kServeBlock) sm.acount[i] = sm.asum[i] = 0;
     for (int i = threadIdx.x; i < kServeCacheQ * FDB_SERVE_MAX_GROUPS; i += kServeBlock) {
@@ -859,13 +874,13 @@ __global__ void __launch_bounds__(kServeBlock, kServeCtasPerSm) serve_kernel(Ser
       const uint64_t policy = l2_evict_first_policy();
       // The next unit is claimed while the stage for the current one drains,
       // so the counter's round trip overlaps the wait.
-      uint64_t next = atomicAdd(a.claim, 1u);
+      uint64_t next = lo + atomicAdd(claim, 1u);
       for (uint32_t it = 0;; ++it) {
         const int s = it % kServeStages;
         const uint32_t ph = (it / kServeStages) & 1u;
         if (it >= kServeStages && !mbar_wait_backoff(&empty[s], ph ^ 1u, a.err, 64)) break;
         const uint64_t t = next;
-        if (t < shared) next = atomicAdd(a.claim, 1u);
+        if (t < shared) next = lo + atomicAdd(claim, 1u);
         unit[s] = t;
         plain[s] = 0;
         if (t >= shared) {  // the end mark: no rows to stage
@@ -873,7 +888,7 @@ __global__ void __launch_bounds__(kServeBlock, kServeCtasPerSm) serve_kernel(Ser
           break;
         }
         const int gi = serve_find(sm.gstart, ng, t);
-        const ServeG g = a.g[gi];
+        const ServeG g = a.g[g0 + gi];
         const ShareCols cols = share_cols(g);
         const uint64_t r0 = (t - sm.gstart[gi]) * g.unit_rows;
         const uint32_t rows = (uint32_t)umin64(g.unit_rows, g.max_n - r0);
@@ -917,7 +932,7 @@ __global__ void __launch_bounds__(kServeBlock, kServeCtasPerSm) serve_kernel(Ser
     const uint32_t pm = plain[s];
     if (t >= shared) break;
     const int gi = serve_find(sm.gstart, ng, t);
-    serve_shared_unit(a, a.g[gi], t - sm.gstart[gi], stages + (size_t)s * kShareStage, pm, sm);
+    serve_shared_unit<JOIN>(a, a.g[g0 + gi], t - sm.gstart[gi], stages + (size_t)s * kShareStage, pm, sm);
     // The consumers wrote the stage (probe results, plain loads): order those
     // writes before the producer's next bulk copy into it.
     fence_proxy_async_smem();
@@ -1060,7 +1075,7 @@ struct Server {
   double first_arrival = 1e300, last_done = 0.0;
   Clock::time_point t0;
   uint32_t cand_cap = 0;
-  int grid = 0, grid_topk = 0;
+  int grid = 0, grid_join = 0, grid_topk = 0;
   uint64_t split_rows = 1ull << 22;  // size classes of batches: fewer / at least this many rows
   std::string error;
 
@@ -1102,7 +1117,8 @@ static void slot_capture(Server& s, ServeSlot& sl) {
   FDB_CUDA(cudaStreamBeginCapture(sl.stream, cudaStreamCaptureModeThreadLocal));
   cudaMemcpyAsync(sl.d_in.ptr, sl.h_in, kServeInBytes, cudaMemcpyHostToDevice, sl.stream);
   cudaMemsetAsync(sl.d_res.ptr, 0, kServeResBytes + 256, sl.stream);
-  serve_kernel<<<s.grid, kServeBlock, kShareSmem, sl.stream>>>(a);
+  serve_kernel<true><<<s.grid_join, kServeBlock, kShareSmem, sl.stream>>>(a);
+  serve_kernel<false><<<s.grid, kServeBlock, kShareSmem, sl.stream>>>(a);
   serve_topk_kernel<<<s.grid_topk, kServeThreads, 0, sl.stream>>>(a);
   serve_finish_kernel<<<kServeMaxBatch, kServeThreads, 0, sl.stream>>>(a);
   cudaMemcpyAsync(sl.h_out, sl.d_res.ptr, kServeResBytes, cudaMemcpyDeviceToHost, sl.stream);
@@ -1256,6 +1272,8 @@ static bool slot_launch(Server& s, ServeSlot& sl, bool small_only) {
     }
     home->tickets.push_back(tk);
   }
+  // Join groups first: serve_kernel<true> takes units [0, join_units).
+  std::stable_partition(groups.begin(), groups.end(), [](const G& g) { return g.join; });
 
   ServeHeader* hdr = reinterpret_cast<ServeHeader*>(sl.h_in);
   ServeQ* dq = reinterpret_cast<ServeQ*>(sl.h_in + kServeQOff);
@@ -1323,6 +1341,12 @@ static bool slot_launch(Server& s, ServeSlot& sl, bool small_only) {
   }
   hdr->nq = (int32_t)admitted.size();
   hdr->ngroups = (int32_t)groups.size();
+  {
+    int32_t njg = 0;
+    while (njg < (int32_t)groups.size() && groups[njg].join) ++njg;
+    hdr->join_groups = njg;
+    hdr->join_units = njg ? dg[njg - 1].unit0 + (dg[njg - 1].max_n + dg[njg - 1].unit_rows - 1) / dg[njg - 1].unit_rows : 0;
+  }
   hdr->topk0 = (int32_t)sl.tickets.size();
   hdr->shared_units = units;
   for (uint64_t tk : topk) {
@@ -1380,10 +1404,13 @@ Server* server_start(fdb_db* db, Ctx& c, const fdb_serve_config* cfg) {
   s->budget = cfg && cfg->mem_budget ? cfg->mem_budget : c.budget;
   s->cfg.mem_budget = s->budget;
   s->resident = c.in_use.load();
-  FDB_CUDA(cudaFuncSetAttribute(serve_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kShareSmem));
+  FDB_CUDA(cudaFuncSetAttribute(serve_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kShareSmem));
+  FDB_CUDA(cudaFuncSetAttribute(serve_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kShareSmem));
   int per_sm = 0;
-  FDB_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, serve_kernel, kServeBlock, kShareSmem));
+  FDB_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, serve_kernel<false>, kServeBlock, kShareSmem));
   s->grid = c.sm_count * std::max(1, std::min(per_sm, kServeCtasPerSm));
+  FDB_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, serve_kernel<true>, kServeBlock, kShareSmem));
+  s->grid_join = c.sm_count * std::max(1, std::min(per_sm, kServeJoinCtasPerSm));
   FDB_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, serve_topk_kernel, kServeThreads, 0));
   s->grid_topk = c.sm_count * std::max(1, std::min(per_sm, kServeTopkCtasPerSm));
   // A top-k CTA publishes at most once per query (its claims only grow).
