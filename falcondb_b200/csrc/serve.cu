@@ -333,7 +333,11 @@ __device__ __forceinline__ void share_load(unsigned char* dst, const void* src, 
 // round, so their L2 round trips overlap.
 constexpr int kProbeIlp = 4;
 
-__device__ void serve_probe_rows(const ServeG g, uint64_t* s0, uint32_t* m, uint32_t rows) {
+// fused (a join group with one query, whose value limit is `lim`): only rows
+// with v[i] < lim are probed, and their matches and payload sums are added to
+// *c / *psum instead of being written back for the queries to read.
+__device__ void serve_probe_rows(const ServeG g, uint64_t* s0, uint32_t* m, uint32_t rows, bool fused,
+                                 const double* v, double lim, unsigned long long* c, unsigned long long* psum) {
   JoinMode mode;
   mode.dmin = g.dmin;
   mode.dense = g.dense;
@@ -352,6 +356,7 @@ __device__ void serve_probe_rows(const ServeG g, uint64_t* s0, uint32_t* m, uint
       sk[j] = 0;
       h[j] = 0;
       if (i >= rows) continue;
+      if (fused && !(v[i] < lim)) continue;
       const int64_t key = (int64_t)s0[i];
       if (key == INT64_MIN) {
         if (g.cnt[g.cap] != 0u) {
@@ -415,11 +420,17 @@ __device__ void serve_probe_rows(const ServeG g, uint64_t* s0, uint32_t* m, uint
     for (int j = 0; j < kProbeIlp; ++j) {
       const uint32_t i = base + j * kServeThreads + threadIdx.x;
       if (i >= rows) continue;
-      m[i] = at[j] == kNoSlot ? 0u : (g.unique ? 1u : g.cnt[at[j]]);
-      s0[i] = ps[j];
+      const uint32_t mc = at[j] == kNoSlot ? 0u : (g.unique ? 1u : g.cnt[at[j]]);
+      if (fused) {
+        *c += mc;
+        *psum += mc ? ps[j] : 0ull;
+      } else {
+        m[i] = mc;
+        s0[i] = ps[j];
+      }
     }
   }
-  serve_bar();
+  if (!fused) serve_bar();
 }
 
 // The staged columns of a shared group's unit: column c at stage byte off[c].
@@ -706,7 +717,29 @@ __device__ void serve_shared_unit(const ServeArgs& a, const ServeG g, uint64_t t
       if ((plain >> c) & 1u) share_load(st + cols.off[c], cols.src[c], r0, rows, cols.esize[c]);
     serve_bar();
   }
-  if constexpr (JOIN) serve_probe_rows(g, s0, smm, rows);
+  bool fused = false;
+  if constexpr (JOIN) {
+    // A join group with one query: filter, probe and count in one pass.
+    fused = g.nq == 1;
+    unsigned long long c = 0, ps = 0;
+    double lim = 0.0;
+    uint32_t prows = rows;
+    if (fused) {
+      const ServeQ& q = a.q[g.q0];
+      lim = q.thr / 100.0;
+      prows = q.n > r0 ? (uint32_t)umin64(rows, q.n - r0) : 0u;
+    }
+    serve_probe_rows(g, s0, smm, prows, fused, reinterpret_cast<const double*>(s1), lim, &c, &ps);
+    if (fused) {
+      c = warp_sum_u64(c);
+      ps = warp_sum_u64(ps);
+      if (lane == 0 && c) {
+        const bool local = g.q0 < (uint32_t)kServeCacheQ;
+        atomicAdd(local ? &sm.acount[g.q0] : &a.res[g.q0].count, c);
+        atomicAdd(local ? &sm.asum[g.q0] : reinterpret_cast<unsigned long long*>(&a.res[g.q0].sum), ps);
+      }
+    }
+  }
   // Kinds with enough queries in the group are evaluated together, once per
   // row (serve_pick); the loop below skips the queries they answered.
   const bool share = JOIN ? g.njoinq >= kShareGroupMin : (g.ngroupq >= kShareGroupMin || g.ncountq >= kShareGroupMin);
@@ -724,7 +757,7 @@ __device__ void serve_shared_unit(const ServeArgs& a, const ServeG g, uint64_t t
       }
     }
   }
-  for (uint32_t qi = g.q0; qi < g.q0 + g.nq; ++qi) {
+  for (uint32_t qi = g.q0; !fused && qi < g.q0 + g.nq; ++qi) {
     const ServeQ& qref = a.q[qi];
     const uint64_t qn = qref.n;
     if (qn <= r0) break;  // queries are by rows descending
