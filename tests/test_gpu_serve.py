@@ -147,12 +147,16 @@ def test_serve_join_on_a_hashed_table(db, env):
     for i in range(24):
         n = int(min(N, max(1, np.floor(10 ** (1 + 5.3 * r.random())))))
         qs.append(S.join_query(dpk.data_ptr(), cols["pval"].data_ptr(), hh._h.value, n, float(r.random() * 100)))
-    res, _ = S.serve_trace(db, qs, max_batch=16, slots=1)
-    for q, rr in zip(qs, res):
-        assert rr.status == 0
-        sel = pkey[:q.nrows][host["pval"][:q.nrows] < q.threshold / 100]
-        o = O.join_agg(bkey, host["bpay"], sel, np.zeros(len(sel)), F.JOIN_INNER)
-        assert (rr.count, rr.sum_payload) == (o["count"], o["sum_payload"])
+    # Batches of up to 16 (groups of several queries probe once and share the
+    # result), then one query at a time (a one-query group filters, probes and
+    # counts in one pass).
+    for mb in (16, 1):
+        res, _ = S.serve_trace(db, qs, max_batch=mb, slots=1)
+        for q, rr in zip(qs, res):
+            assert rr.status == 0
+            sel = pkey[:q.nrows][host["pval"][:q.nrows] < q.threshold / 100]
+            o = O.join_agg(bkey, host["bpay"], sel, np.zeros(len(sel)), F.JOIN_INNER)
+            assert (rr.count, rr.sum_payload) == (o["count"], o["sum_payload"])
     hh.free()
 
 
