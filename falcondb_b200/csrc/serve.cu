@@ -332,6 +332,9 @@ __device__ __forceinline__ void share_load(unsigned char* dst, const void* src, 
 // kProbeIlp rows together, one 32-byte slot pair (one L2 sector) per row per
 // round, so their L2 round trips overlap.
 constexpr int kProbeIlp = 4;
+#ifndef FDB_SERVE_PAIR_ILP
+#define FDB_SERVE_PAIR_ILP 2
+#endif
 
 // fused (a join group with one query, whose value limit is `lim`): only rows
 // with v[i] < lim are probed, and their matches and payload sums are added to
@@ -390,26 +393,34 @@ __device__ void serve_probe_rows(const ServeG g, uint64_t* s0, uint32_t* m, uint
         }
       todo = 0;
     }
-    for (uint64_t round = 0; todo && round <= mask; ++round) {
-      JSlot lo[kProbeIlp], hi[kProbeIlp];
+    // Hashed table: rounds over slot pairs, kPairIlp rows' pairs in flight at a
+    // time (fewer than kProbeIlp, to keep the registers of the pairs down).
+    constexpr int kPairIlp = FDB_SERVE_PAIR_ILP;
 #pragma unroll
-      for (int j = 0; j < kProbeIlp; ++j)
+    for (int j0 = 0; j0 < kProbeIlp; j0 += kPairIlp)
+    for (uint64_t round = 0; ((todo >> j0) & ((1u << kPairIlp) - 1u)) && round <= mask; ++round) {
+      JSlot lo[kPairIlp], hi[kPairIlp];
+#pragma unroll
+      for (int jj = 0; jj < kPairIlp; ++jj) {
+        const int j = j0 + jj;
         if ((todo >> j) & 1u)
           asm volatile("ld.global.L2::cache_hint.v4.u64 {%0, %1, %2, %3}, [%4], %5;"
-                       : "=l"(lo[j].key), "=l"(lo[j].psum), "=l"(hi[j].key), "=l"(hi[j].psum)
+                       : "=l"(lo[jj].key), "=l"(lo[jj].psum), "=l"(hi[jj].key), "=l"(hi[jj].psum)
                        : "l"(g.slots + (h[j] & ~1ull)), "l"(pol));
+      }
 #pragma unroll
-      for (int j = 0; j < kProbeIlp; ++j) {
+      for (int jj = 0; jj < kPairIlp; ++jj) {
+        const int j = j0 + jj;
         if (!((todo >> j) & 1u)) continue;
         const bool even = (h[j] & 1ull) == 0;
-        const bool hit0 = even && lo[j].key == sk[j];
-        const bool stop0 = even && (lo[j].key == sk[j] || lo[j].key == 0ull);
-        const bool hit1 = !stop0 && hi[j].key == sk[j];
+        const bool hit0 = even && lo[jj].key == sk[j];
+        const bool stop0 = even && (lo[jj].key == sk[j] || lo[jj].key == 0ull);
+        const bool hit1 = !stop0 && hi[jj].key == sk[j];
         if (hit0 || hit1) {
           at[j] = (uint32_t)((h[j] & ~1ull) + (hit1 ? 1 : 0));
-          ps[j] = hit1 ? hi[j].psum : lo[j].psum;
+          ps[j] = hit1 ? hi[jj].psum : lo[jj].psum;
           todo &= ~(1u << j);
-        } else if (stop0 || hi[j].key == 0ull) {
+        } else if (stop0 || hi[jj].key == 0ull) {
           todo &= ~(1u << j);
         } else {
           h[j] = ((h[j] & ~1ull) + 2) & mask;
