@@ -13,8 +13,8 @@
 //
 // serve_kernel is persistent and scans shared: the batch's COUNT, GROUP and
 // JOIN queries are grouped by the table they read, and each group's rows are
-// cut into units that fill one pipeline stage (28 KB: 3584 rows of one 8-byte
-// column, 1280 rows of a GROUP group's columns, 1024 of a JOIN group's).  A
+// cut into units that fill one pipeline stage (22 KB: 2816 rows of one 8-byte
+// column, 1024 rows of a GROUP or JOIN group's columns).  A
 // CTA's producer warp claims units from one counter and stages their columns
 // into a ring of shared-memory buffers with bulk copies; its consumer warps
 // then probe a join group's rows once (whether a build row matches does not
@@ -53,7 +53,7 @@ constexpr int kServeBlock = kServeThreads + 32;    // + the producer warp
 constexpr uint32_t kServeTile = 8192;
 constexpr int kServeMaxBatch = 256;
 #ifndef FDB_SERVE_CTAS
-#define FDB_SERVE_CTAS 2
+#define FDB_SERVE_CTAS 3
 #endif
 constexpr int kServeCtasPerSm = FDB_SERVE_CTAS;
 #ifndef FDB_SERVE_JOIN_CTAS
@@ -68,7 +68,10 @@ constexpr int kServeStages = FDB_SERVE_STAGES;
 // A stage holds one unit of a shared group: its columns c0 (8 B/row), c1 (0,
 // 4 or 8 B/row), c2 (0 or 8 B/row) and, for a join, the match counts (4 B/row),
 // one after another; a unit is as many rows (a multiple of 256) as fit.
-constexpr size_t kShareStage = 28 * 1024;
+#ifndef FDB_SERVE_STAGE_KB
+#define FDB_SERVE_STAGE_KB 22
+#endif
+constexpr size_t kShareStage = FDB_SERVE_STAGE_KB * 1024;
 // Barrier block: full[stages], empty[stages], the unit of each stage, and the
 // columns each stage's consumers must load themselves (bit c: column c).
 constexpr size_t kServeBar = 128;
@@ -144,7 +147,10 @@ struct ServeArgs {
 
 // Shared queries whose partial results a CTA keeps in shared memory (the
 // first ones of a batch; later ones add theirs per unit).
-constexpr int kServeCacheQ = 32;
+#ifndef FDB_SERVE_CACHE_Q
+#define FDB_SERVE_CACHE_Q 24
+#endif
+constexpr int kServeCacheQ = FDB_SERVE_CACHE_Q;
 // GROUP queries one unit evaluates together, and the fewest worth it (with
 // fewer, the per-query fold is faster than the binned atomics).
 constexpr int kShareGroupQ = 32;
