@@ -549,6 +549,39 @@ def run_secondary(args):
             "serial": "the same 64 queries as fdb_group_by_i64 calls in sequence, tables sized to the exact "
                       "group counts"})
         db.drop_table("g")
+    if args.workload in ("sort", "all"):
+        # ORDER BY score DESC over 100M FLOAT64 rows, no LIMIT: an LSD radix
+        # sort of (order key, row) pairs.  Algorithmic bytes: the key build
+        # (read 8, write 12 per row), per digit pass the histogram read (8) and
+        # the scatter (read 12, write 12), and the row copy-out (read 4, write 4).
+        host_sc = W.table_t(n, seed=1)["score"]
+        sc = torch.from_numpy(host_sc).to(dev)
+        rows_out = torch.empty(n, dtype=torch.int32, device=dev)
+        ms = _time_steps(lambda: ops.sort(db, sc, n, True, rows=rows_out), K, Wm, stream, torch)
+        bits = host_sc.view(np.uint64)
+        ordk = np.where(bits >> np.uint64(63) == 0, bits ^ np.uint64(1 << 63), ~bits)  # f64_ord_key
+        vary = int(np.bitwise_or.reduce(ordk)) ^ int(np.bitwise_and.reduce(ordk))
+        passes = sum(1 for byte in range(8) if (vary >> (8 * byte)) & 255)
+        del bits, ordk
+        r = rows_out[:n].long()
+        s_sorted = sc[r]
+        assert bool((s_sorted[1:] <= s_sorted[:-1]).all())
+        seen = torch.zeros(n, dtype=torch.bool, device=dev)
+        seen[r] = True
+        assert bool(seen.all())
+        del r, s_sorted, seen
+        nbytes = n * (20 + 32 * passes + 8)
+        sample = 2_000_000
+        hs = sc[:sample].cpu().numpy()
+        t0 = time.perf_counter()
+        O.sort(hs, True)
+        cpu_s = time.perf_counter() - t0
+        line("sort", ms, nbytes, {"rows": n, "query": "SELECT score FROM t ORDER BY score DESC",
+                                  "digit_passes": passes, "mrows_per_s": round(n / (ms / 1e3) / 1e6, 1),
+                                  "cpu_sample": {"rows": sample, "mrows_per_s": round(sample / cpu_s / 1e6, 2),
+                                                 "cores": 1, "kind": "port",
+                                                 "what": "oracle std::sort of (order key, row) pairs"}})
+        torch.cuda.empty_cache()
     if args.workload in ("serve", "all"):
         run_serving(args, db, out, peak)
     if args.workload == "serve_single":
@@ -725,7 +758,7 @@ def main():
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--cpu-threads", type=int, default=0)
     ap.add_argument("--workload", default="scan",
-                    choices=["scan", "filter_groupby", "join", "groupby", "batch", "serve", "serve_single", "all"],
+                    choices=["scan", "filter_groupby", "join", "groupby", "batch", "sort", "serve", "serve_single", "all"],
                     help="scan = the headline line; the others print per-operator lines")
     ap.add_argument("--load-factor", type=float, default=0.5)
     ap.add_argument("--serve-queries", type=int, default=10_000)

@@ -608,6 +608,15 @@ int fdb_topk(fdb_db* db, const fdb_dev_column* col, uint64_t nrows, uint32_t k, 
   });
 }
 
+int fdb_sort(fdb_db* db, const fdb_dev_column* col, uint64_t nrows, int32_t desc, int32_t nulls_last,
+             uint32_t* d_rows) {
+  if (!db || !col || (!d_rows && nrows)) return set_error(FDB_E_ARG, "fdb_sort: bad arguments");
+  return guarded([&] {
+    CallScope s(db, default_scratch(db->ctx));
+    op_sort(s.c, *col, nrows, desc != 0, nulls_last != 0, d_rows);
+  });
+}
+
 int fdb_gb_batch_prepare(fdb_db* db, const fdb_gb_query* queries, int32_t nqueries, const fdb_batch_tuning* tuning,
                          fdb_batch** out) {
   if (out) *out = nullptr;

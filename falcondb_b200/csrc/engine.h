@@ -183,6 +183,10 @@ void op_gb_batch_free(BatchPlan* p);
 double op_gb_batch_autotune(Ctx& c, const fdb_gb_query* qs, int nq, int reps, fdb_batch_tuning* best);
 void op_topk(Ctx& c, const fdb_dev_column& col, uint64_t n, uint32_t k, bool desc,
              bool nulls_last, uint32_t* d_rows, uint64_t* d_count);
+// Every row of one FLOAT64 / INT64 column in ORDER BY order (k_sort.cu):
+// d_rows receives n row numbers.
+void op_sort(Ctx& c, const fdb_dev_column& col, uint64_t n, bool desc, bool nulls_last,
+             uint32_t* d_rows);
 
 struct HashTable;  // join build side (k_join.cu)
 HashTable* op_join_build(Ctx& c, const fdb_dev_column& key, const fdb_dev_column& payload,

@@ -1,0 +1,507 @@
+// Full ORDER BY on one FLOAT64 / INT64 column (execute_sort / sort_merged ->
+// try_typed_sort, FalconDB src/query/sort.rs:118-133, 209-350): the rows of a
+// column in the order of (order key, row), NULL rows first or last in row
+// order (assemble, sort.rs:773-791).  Order keys are the ones the top-k uses
+// (f64_ord_key, sort.rs:451-454; the sign flip for int64; bitwise NOT for
+// DESC), so -0.0 sorts before +0.0 and NaN above +inf, as in the reference.
+//
+// A stable LSD radix sort of (order key, row) pairs with 8-bit digits:
+//   * the key pass writes the pairs and ORs / ANDs every key, so a byte that
+//     is the same in every key costs no pass;
+//   * per pass, radix_hist_kernel counts the digits of each 4096-key tile
+//     (histogram laid out digit-major, [digit][tile]); an exclusive scan of the
+//     histogram gives every (digit, tile) its output offset;
+//     radix_scatter_kernel stages each tile in shared memory (TMA bulk
+//     copies, double-buffered), ranks its keys stably with warp votes, permutes
+//     the tile into digit order in place and writes it out in runs;
+//   * the last pass writes the row numbers straight into the output.
+// Every scatter position is checked against the key count (an error, never an
+// out-of-bounds write).
+#include <algorithm>
+#include <cstring>
+
+#include "common.cuh"
+#include "engine.h"
+#include "topk_warp.cuh"
+
+namespace fdb {
+
+constexpr int kSortThreads = 256;
+constexpr int kSortItems = 16;
+constexpr uint32_t kSortTile = kSortThreads * kSortItems;
+constexpr int kSortWarps = kSortThreads / 32;
+
+// Keys of the selected rows (sel[i], or row i when sel is null) and their
+// rows; vary[0] |= every key, vary[1] &= every key.
+template <int DT, bool DESC>
+__global__ void sort_key_kernel(DevCol col, const uint32_t* sel, uint32_t m, uint64_t* keys, uint32_t* vals,
+                                unsigned long long* vary) {
+  unsigned long long o = 0, a = ~0ull;
+  const uint64_t* v = static_cast<const uint64_t*>(col.values);
+  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < m; i += gridDim.x * blockDim.x) {
+    const uint32_t row = sel ? sel[i] : i;
+    const uint64_t k = wt_key<DT, DESC>(v[row]);
+    keys[i] = k;
+    vals[i] = row;
+    o |= k;
+    a &= k;
+  }
+#pragma unroll
+  for (int s = 16; s > 0; s >>= 1) {
+    o |= __shfl_xor_sync(0xffffffffu, o, s);
+    a &= __shfl_xor_sync(0xffffffffu, a, s);
+  }
+  if ((threadIdx.x & 31) == 0) {
+    atomicOr(&vary[0], o);
+    atomicAnd(&vary[1], a);
+  }
+}
+
+// Digit counts of one tile: hist[d * ntiles + tile].  Each thread counts a
+// run of equal digits before it adds it to its warp's counters, so a byte that
+// takes few values (the exponent bytes of a float column) costs few atomics.
+__global__ void __launch_bounds__(kSortThreads) radix_hist_kernel(const uint64_t* __restrict__ keys, uint32_t m,
+                                                                  int shift, uint32_t ntiles, uint32_t* hist) {
+  __shared__ uint32_t cnt[kSortWarps][256];
+  const int tid = threadIdx.x, warp = tid >> 5;
+#pragma unroll
+  for (int w = 0; w < kSortWarps; ++w) cnt[w][tid] = 0;
+  __syncthreads();
+  const uint64_t t0 = (uint64_t)blockIdx.x * kSortTile;
+  uint64_t k[kSortItems];
+#pragma unroll
+  for (int r = 0; r < kSortItems; ++r) {
+    const uint64_t i = t0 + (uint64_t)r * kSortThreads + tid;
+    k[r] = i < m ? keys[i] : 0ull;
+  }
+  uint32_t run_d = 0, run_c = 0;
+#pragma unroll
+  for (int r = 0; r < kSortItems; ++r) {
+    const uint64_t i = t0 + (uint64_t)r * kSortThreads + tid;
+    if (i < m) {
+      const uint32_t d = (uint32_t)(k[r] >> shift) & 255u;
+      if (d != run_d && run_c) {
+        atomicAdd(&cnt[warp][run_d], run_c);
+        run_c = 0;
+      }
+      run_d = d;
+      ++run_c;
+    }
+  }
+  if (run_c) atomicAdd(&cnt[warp][run_d], run_c);
+  __syncthreads();
+  uint32_t t = 0;
+#pragma unroll
+  for (int w = 0; w < kSortWarps; ++w) t += cnt[w][tid];
+  hist[(size_t)tid * ntiles + blockIdx.x] = t;
+}
+
+// Exclusive scan of n uint32 in place: per-block sums, a scan of the sums,
+// then each block's scan offset by its sum.
+constexpr int kScanT = 1024, kScanPer = 4, kScanB = kScanT * kScanPer;
+
+__device__ uint32_t sort_block_scan(uint32_t v, uint32_t* sm, uint32_t* total) {
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+  uint32_t x = v;
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    const uint32_t y = __shfl_up_sync(0xffffffffu, x, o);
+    if (lane >= o) x += y;
+  }
+  if (lane == 31) sm[warp] = x;
+  __syncthreads();
+  if (warp == 0) {
+    uint32_t s = lane < nw ? sm[lane] : 0u;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const uint32_t y = __shfl_up_sync(0xffffffffu, s, o);
+      if (lane >= o) s += y;
+    }
+    if (lane < nw) sm[lane] = s;
+  }
+  __syncthreads();
+  const uint32_t base = warp ? sm[warp - 1] : 0u;
+  if (total) *total = sm[nw - 1];
+  __syncthreads();
+  return base + x - v;
+}
+
+__global__ void sort_scan_sums_kernel(const uint32_t* in, uint64_t n, uint32_t* bsum) {
+  __shared__ uint32_t sm[32];
+  const uint64_t i0 = (uint64_t)blockIdx.x * kScanB + threadIdx.x * kScanPer;
+  uint32_t s = 0;
+#pragma unroll
+  for (int j = 0; j < kScanPer; ++j)
+    if (i0 + j < n) s += in[i0 + j];
+  uint32_t tot;
+  sort_block_scan(s, sm, &tot);
+  if (threadIdx.x == 0) bsum[blockIdx.x] = tot;
+}
+
+__global__ void sort_scan_top_kernel(uint32_t* bsum, uint64_t nb) {
+  __shared__ uint32_t sm[32];
+  const uint64_t per = (nb + blockDim.x - 1) / blockDim.x;
+  const uint64_t b0 = threadIdx.x * per;
+  uint32_t local = 0;
+  for (uint64_t i = b0; i < b0 + per && i < nb; ++i) local += bsum[i];
+  uint32_t base = sort_block_scan(local, sm, nullptr);
+  for (uint64_t i = b0; i < b0 + per && i < nb; ++i) {
+    const uint32_t v = bsum[i];
+    bsum[i] = base;
+    base += v;
+  }
+}
+
+__global__ void sort_scan_apply_kernel(uint32_t* data, uint64_t n, const uint32_t* bsum) {
+  __shared__ uint32_t sm[32];
+  const uint64_t i0 = (uint64_t)blockIdx.x * kScanB + threadIdx.x * kScanPer;
+  uint32_t v[kScanPer];
+  uint32_t s = 0;
+#pragma unroll
+  for (int j = 0; j < kScanPer; ++j) {
+    v[j] = i0 + j < n ? data[i0 + j] : 0u;
+    s += v[j];
+  }
+  uint32_t run = bsum[blockIdx.x] + sort_block_scan(s, sm, nullptr);
+#pragma unroll
+  for (int j = 0; j < kScanPer; ++j) {
+    if (i0 + j < n) data[i0 + j] = run;
+    run += v[j];
+  }
+}
+
+// Stable scatter of the tiles by digit.  Persistent CTAs take tiles
+// round-robin; thread 0 stages each tile's keys and rows into one of two
+// shared-memory buffers with TMA bulk copies, so the next tile arrives while
+// this one is ranked (a ragged last tile, whose byte count is not a multiple
+// of 16, is read with plain loads).  Warp w ranks the 512 keys
+// [w*512, (w+1)*512) of the tile in index order (nine warp votes group a
+// round's equal digits; a per-warp counter per digit carries the rank across
+// rounds); one block-wide scan turns (digit, warp, rank) into the key's place
+// in the tile sorted by digit; the tile is permuted into that order in place
+// and written out in it, so neighbouring threads store neighbouring addresses
+// of one digit's output range.  The last pass stores no keys.
+constexpr int kScatterThreads = 256;
+constexpr int kScatterWarps = kScatterThreads / 32;
+constexpr int kSubTile = kSortTile / kScatterWarps;  // 512 keys per warp
+constexpr int kSubRounds = kSubTile / 32;
+constexpr int kScatterItems = kSortTile / kScatterThreads;
+constexpr int kScatterCtasPerSm = 2;
+struct ScatterSmem {
+  uint64_t keys[2][kSortTile];
+  uint32_t vals[2][kSortTile];
+  uint16_t wc[kScatterWarps][256];  // per-warp digit counts, then tile offsets (< 4096)
+  uint32_t gbase[256];
+  uint32_t wsum[8];
+  uint64_t full[2];
+};
+
+// The lanes of the warp whose d equals this lane's, d < 2^NB: one vote per bit.
+template <int NB>
+__device__ __forceinline__ unsigned warp_match_digit(uint32_t d) {
+  unsigned peers = 0xffffffffu;
+#pragma unroll
+  for (int b = 0; b < NB; ++b) {
+    const bool bit = (d >> b) & 1u;
+    const unsigned vote = __ballot_sync(0xffffffffu, bit);
+    peers &= bit ? vote : ~vote;
+  }
+  return peers;
+}
+
+__device__ __forceinline__ bool sort_tile_ragged(uint64_t t, uint64_t ntiles, uint32_t m) {
+  return t + 1 == ntiles && (m % kSortTile) % 4u != 0;
+}
+
+__device__ __forceinline__ void sort_stage_tile(ScatterSmem& S, int s, uint64_t t, uint32_t m,
+                                                const uint64_t* kin, const uint32_t* vin, uint64_t policy) {
+  const uint64_t t0 = t * kSortTile;
+  const uint32_t n = (uint32_t)umin64(kSortTile, m - t0);
+  mbar_arrive_expect_tx(&S.full[s], n * 12u);
+  bulk_g2s(S.keys[s], kin + t0, n * 8u, &S.full[s], policy);
+  bulk_g2s(S.vals[s], vin + t0, n * 4u, &S.full[s], policy);
+}
+
+__global__ void __launch_bounds__(kScatterThreads, kScatterCtasPerSm)
+    radix_scatter_kernel(const uint64_t* __restrict__ kin, const uint32_t* __restrict__ vin, uint32_t m, int shift,
+                         const uint32_t* __restrict__ off, uint32_t ntiles, uint64_t* __restrict__ kout,
+                         uint32_t* __restrict__ vout, bool write_keys, int* err) {
+  extern __shared__ __align__(128) unsigned char smem_raw[];
+  ScatterSmem& S = *reinterpret_cast<ScatterSmem*>(smem_raw);
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  const unsigned below = (1u << lane) - 1u;
+  uint64_t policy = 0;
+  if (tid == 0) {
+    mbar_init(&S.full[0], 1);
+    mbar_init(&S.full[1], 1);
+    fence_mbar_init();
+    policy = l2_evict_first_policy();
+  }
+  __syncthreads();
+  // Thread 0: per stage, a copy issued and not yet seen complete, and the
+  // iteration it is for (its phase parity is (iteration / 2) & 1).
+  uint32_t pending = 0;                // bit j: stage j
+  uint32_t pend_it0 = 0, pend_it1 = 1;
+  if (tid == 0) {
+    for (int j = 0; j < 2; ++j) {
+      const uint64_t t = blockIdx.x + (uint64_t)j * gridDim.x;
+      if (t < ntiles && !sort_tile_ragged(t, ntiles, m)) {
+        sort_stage_tile(S, j, t, m, kin, vin, policy);
+        pending |= 1u << j;
+      }
+    }
+  }
+  bool dead = false;
+  uint32_t it = 0;
+  for (uint64_t t = blockIdx.x; t < ntiles; t += gridDim.x, ++it) {
+    const int s = it & 1;
+    const uint64_t t0 = t * kSortTile;
+    const uint32_t tile_n = (uint32_t)umin64(kSortTile, m - t0);
+    if (sort_tile_ragged(t, ntiles, m)) {
+      for (uint32_t i = tid; i < tile_n; i += kScatterThreads) {
+        S.keys[s][i] = kin[t0 + i];
+        S.vals[s][i] = vin[t0 + i];
+      }
+      __syncthreads();
+    } else {
+      const bool ok = !dead && mbar_wait(&S.full[s], (it >> 1) & 1u, err);
+      if (!ok) dead = true;  // the tile is processed from whatever the stage holds
+      if (tid == 0 && ok) pending &= ~(1u << s);
+    }
+
+#pragma unroll
+    for (int j = 0; j < 256; j += 32) S.wc[warp][j + lane] = 0;
+    __syncwarp();
+    const uint32_t w0 = (uint32_t)warp * kSubTile;
+    const bool full_tile = tile_n == kSortTile;
+    uint64_t k[kSubRounds];
+    uint32_t rk[kSubRounds / 2];  // ranks (< 512) two to a register
+#pragma unroll
+    for (int r = 0; r < kSubRounds; ++r) {
+      const uint32_t i = w0 + r * 32 + lane;
+      k[r] = i < tile_n ? S.keys[s][i] : 0ull;
+    }
+#pragma unroll
+    for (int r = 0; r < kSubRounds; ++r) {
+      const uint32_t i = w0 + r * 32 + lane;
+      const uint32_t d = i < tile_n ? (uint32_t)(k[r] >> shift) & 255u : 256u;
+      const unsigned peers = full_tile ? warp_match_digit<8>(d) : warp_match_digit<9>(d);
+      const int leader = __ffs(peers) - 1;
+      uint32_t pre = 0;
+      if (d < 256u && lane == leader) {
+        pre = S.wc[warp][d];
+        S.wc[warp][d] = (uint16_t)(pre + (uint32_t)__popc(peers));
+      }
+      pre = __shfl_sync(0xffffffffu, pre, leader);
+      const uint32_t rank = pre + (uint32_t)__popc(peers & below);
+      if (r & 1)
+        rk[r >> 1] |= rank << 16;
+      else
+        rk[r >> 1] = rank;
+      __syncwarp();
+    }
+    __syncthreads();
+
+    // Threads 0..255 own digit tid: its count in this tile, where it starts
+    // in the tile's digit order, and where each warp's keys of it start.
+    uint32_t tot = 0, x = 0;
+    if (tid < 256) {
+#pragma unroll
+      for (int w = 0; w < kScatterWarps; ++w) {
+        const uint32_t c = S.wc[w][tid];
+        S.wc[w][tid] = (uint16_t)tot;
+        tot += c;
+      }
+      x = tot;
+#pragma unroll
+      for (int o = 1; o < 32; o <<= 1) {
+        const uint32_t y = __shfl_up_sync(0xffffffffu, x, o);
+        if (lane >= o) x += y;
+      }
+      if (lane == 31) S.wsum[warp] = x;
+    }
+    __syncthreads();
+    if (tid < 256) {
+      uint32_t dstart = x - tot;
+#pragma unroll
+      for (int w = 0; w < 8; ++w)
+        if (w < warp) dstart += S.wsum[w];
+#pragma unroll
+      for (int w = 0; w < kScatterWarps; ++w) S.wc[w][tid] = (uint16_t)(S.wc[w][tid] + dstart);
+      S.gbase[tid] = off[(size_t)tid * ntiles + t] - dstart;
+    }
+    uint32_t v[kSubRounds];
+#pragma unroll
+    for (int r = 0; r < kSubRounds; ++r) {
+      const uint32_t i = w0 + r * 32 + lane;
+      v[r] = i < tile_n ? S.vals[s][i] : 0u;
+    }
+    __syncthreads();
+
+    // Permute the tile in place into digit order.
+#pragma unroll
+    for (int r = 0; r < kSubRounds; ++r) {
+      const uint32_t i = w0 + r * 32 + lane;
+      if (i < tile_n) {
+        const uint32_t d = (uint32_t)(k[r] >> shift) & 255u;
+        const uint32_t lp = S.wc[warp][d] + ((rk[r >> 1] >> ((r & 1) * 16)) & 0xFFFFu);
+        S.keys[s][lp] = k[r];
+        S.vals[s][lp] = v[r];
+      }
+    }
+    __syncthreads();
+
+#pragma unroll 4
+    for (int j = 0; j < kScatterItems; ++j) {
+      const uint32_t i = (uint32_t)j * kScatterThreads + tid;
+      if (i < tile_n) {
+        const uint64_t kk = S.keys[s][i];
+        const uint32_t pos = S.gbase[(uint32_t)(kk >> shift) & 255u] + i;
+        if (pos < m) {
+          if (write_keys) kout[pos] = kk;
+          vout[pos] = S.vals[s][i];
+        } else {
+          atomicExch(err, kErrCapacity);
+        }
+      }
+    }
+    fence_proxy_async_smem();  // this thread's stores to stage s come before the next bulk copy into it
+    __syncthreads();           // stage s and the counters are free again
+    if (tid == 0 && !dead) {  // after a time-out no further copies are started
+      const uint64_t tn = t + 2ull * gridDim.x;
+      if (tn < ntiles && !sort_tile_ragged(tn, ntiles, m)) {
+        sort_stage_tile(S, s, tn, m, kin, vin, policy);
+        pending |= 1u << s;
+        if (s)
+          pend_it1 = it + 2;
+        else
+          pend_it0 = it + 2;
+      }
+    }
+  }
+  // After a timed-out wait, let this CTA's own copies land before it exits.
+  if (tid == 0) {
+    if (pending & 1u) mbar_wait(&S.full[0], (pend_it0 >> 1) & 1u, nullptr);
+    if (pending & 2u) mbar_wait(&S.full[1], (pend_it1 >> 1) & 1u, nullptr);
+  }
+}
+
+// Validity bits of rows [0, n) re-aligned to row 0 (the column's bits start at
+// bit voff), or their complement when `nulls` is set; bits past n are zero.
+__global__ void sort_valid_mask_kernel(DevCol col, uint64_t n, bool nulls, uint64_t* mask) {
+  const uint64_t words = (n + 63) / 64;
+  for (uint64_t w = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; w < words; w += (uint64_t)gridDim.x * blockDim.x) {
+    const uint64_t rows = n - w * 64 < 64 ? n - w * 64 : 64;
+    const uint64_t b = col.voff + w * 64;
+    const int sh = (int)(b & 63);
+    uint64_t x = col.validity[b >> 6] >> sh;
+    if (sh != 0 && (uint64_t)(64 - sh) < rows) x |= col.validity[(b >> 6) + 1] << (64 - sh);
+    if (nulls) x = ~x;
+    if (rows < 64) x &= (1ull << rows) - 1;
+    mask[w] = x;
+  }
+}
+
+template <int DT, bool DESC>
+static void launch_sort_keys(Ctx& c, const DevCol& col, const uint32_t* sel, uint32_t m, uint64_t* keys,
+                             uint32_t* vals, unsigned long long* vary) {
+  const unsigned grid = (unsigned)std::max<uint64_t>(1, std::min<uint64_t>((m + 255) / 256, (uint64_t)c.sm_count * 8));
+  sort_key_kernel<DT, DESC><<<grid, 256, 0, c.stream>>>(col, sel, m, keys, vals, vary);
+}
+
+void op_sort(Ctx& c, const fdb_dev_column& col, uint64_t n, bool desc, bool nulls_last, uint32_t* d_rows) {
+  if (col.dtype != FDB_FLOAT64 && col.dtype != FDB_INT64) fail(FDB_E_TYPE, "ORDER BY needs a FLOAT64 or INT64 column");
+  if (n >= 0xFFFFFFFFull) fail(FDB_E_ARG, "a sort addresses rows as uint32");
+  if (n == 0) return;
+  if (!col.values) fail(FDB_E_ARG, "column without values");
+  const DevCol dc{col.dtype, col.values, col.validity, col.validity_offset};
+
+  FDB_CUDA(cudaFuncSetAttribute(radix_scatter_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                (int)sizeof(ScatterSmem)));
+  int scatter_grid = 0;
+  // Working memory comes from the context's scratch arena, which grows once
+  // and stays resident: two (key, row) buffers, the histogram and its scan
+  // sums, and with a validity bitmap the mask and the two row lists.
+  const uint64_t words = (n + 63) / 64;
+  const uint64_t ntiles_max = (n + kSortTile - 1) / kSortTile;
+  const uint64_t hn_max = 256ull * ntiles_max;
+  const uint64_t nb_max = (hn_max + kScanB - 1) / kScanB;
+  size_t need = 2 * n * 8 + 2 * n * 4 + hn_max * 4 + nb_max * 4 + 16;
+  if (col.validity) need += words * 8 + 2 * n * 4 + 16;
+  c.ensure_scratch(c.scratch_top + need + (2u << 20));  // + 256-byte rounding and the compaction's chunk counts
+
+  // NULL rows leave the sort: the valid rows are sorted, the NULL rows keep
+  // their row order before or after them.
+  const uint32_t* sel = nullptr;
+  uint32_t* nulls = nullptr;
+  uint64_t m = n, nnull = 0;
+  if (col.validity) {
+    uint64_t* mask = static_cast<uint64_t*>(c.scratch_take(words * 8));
+    uint32_t* vrows = static_cast<uint32_t*>(c.scratch_take(n * 4));
+    nulls = static_cast<uint32_t*>(c.scratch_take(n * 4));
+    uint64_t* cnt = static_cast<uint64_t*>(c.scratch_take(16));
+    const unsigned g = (unsigned)std::max<uint64_t>(1, std::min<uint64_t>((words + 255) / 256, (uint64_t)c.sm_count * 4));
+    sort_valid_mask_kernel<<<g, 256, 0, c.stream>>>(dc, n, false, mask);
+    op_compact_mask(c, mask, n, vrows, n, cnt);
+    sort_valid_mask_kernel<<<g, 256, 0, c.stream>>>(dc, n, true, mask);
+    op_compact_mask(c, mask, n, nulls, n, cnt + 1);
+    uint64_t hc[2] = {0, 0};
+    FDB_CUDA(cudaMemcpyAsync(hc, cnt, 16, cudaMemcpyDeviceToHost, c.stream));
+    FDB_CUDA(cudaStreamSynchronize(c.stream));
+    if (hc[0] + hc[1] != n) fail(FDB_E_GENERIC, "sort: valid and NULL rows do not add up to the row count");
+    m = hc[0];
+    nnull = hc[1];
+    sel = vrows;
+  }
+  uint32_t* sorted_out = d_rows + (nulls_last ? 0 : nnull);
+  if (m > 0) {
+    const uint32_t mm = (uint32_t)m;
+    uint64_t* ka = static_cast<uint64_t*>(c.scratch_take(m * 8));
+    uint64_t* kb = static_cast<uint64_t*>(c.scratch_take(m * 8));
+    uint32_t* va = static_cast<uint32_t*>(c.scratch_take(m * 4));
+    uint32_t* vb = static_cast<uint32_t*>(c.scratch_take(m * 4));
+    const uint32_t ntiles = (uint32_t)((m + kSortTile - 1) / kSortTile);
+    const uint64_t hn = 256ull * ntiles;
+    const uint64_t nb = (hn + kScanB - 1) / kScanB;
+    uint32_t* hist = static_cast<uint32_t*>(c.scratch_take(hn * 4));
+    uint32_t* bsum = static_cast<uint32_t*>(c.scratch_take(nb * 4));
+    unsigned long long* vary = static_cast<unsigned long long*>(c.scratch_take(16));
+    FDB_CUDA(cudaMemsetAsync(vary, 0, 8, c.stream));
+    FDB_CUDA(cudaMemsetAsync(vary + 1, 0xFF, 8, c.stream));
+    if (col.dtype == FDB_FLOAT64)
+      desc ? launch_sort_keys<FDB_FLOAT64, true>(c, dc, sel, mm, ka, va, vary)
+           : launch_sort_keys<FDB_FLOAT64, false>(c, dc, sel, mm, ka, va, vary);
+    else
+      desc ? launch_sort_keys<FDB_INT64, true>(c, dc, sel, mm, ka, va, vary)
+           : launch_sort_keys<FDB_INT64, false>(c, dc, sel, mm, ka, va, vary);
+    FDB_CUDA(cudaGetLastError());
+    unsigned long long hv[2] = {0, 0};
+    FDB_CUDA(cudaMemcpyAsync(hv, vary, 16, cudaMemcpyDeviceToHost, c.stream));
+    FDB_CUDA(cudaStreamSynchronize(c.stream));
+    const uint64_t varying = hv[0] ^ hv[1];  // bits that are not the same in every key
+    int last_byte = -1;
+    for (int byte = 0; byte < 8; ++byte)
+      if ((varying >> (8 * byte)) & 0xFFull) last_byte = byte;
+    scatter_grid = (int)std::min<uint64_t>(ntiles, (uint64_t)kScatterCtasPerSm * c.sm_count);
+    for (int byte = 0; byte < 8; ++byte) {
+      const int shift = 8 * byte;
+      if (((varying >> shift) & 0xFFull) == 0) continue;  // one digit for every key: order unchanged
+      radix_hist_kernel<<<ntiles, kSortThreads, 0, c.stream>>>(ka, mm, shift, ntiles, hist);
+      sort_scan_sums_kernel<<<(unsigned)nb, kScanT, 0, c.stream>>>(hist, hn, bsum);
+      sort_scan_top_kernel<<<1, kScanT, 0, c.stream>>>(bsum, nb);
+      sort_scan_apply_kernel<<<(unsigned)nb, kScanT, 0, c.stream>>>(hist, hn, bsum);
+      const bool last = byte == last_byte;  // rows go straight to the output; keys are not needed
+      radix_scatter_kernel<<<scatter_grid, kScatterThreads, sizeof(ScatterSmem), c.stream>>>(
+          ka, va, mm, shift, hist, ntiles, kb, last ? sorted_out : vb, !last, c.d_err);
+      std::swap(ka, kb);
+      std::swap(va, vb);
+    }
+    FDB_CUDA(cudaGetLastError());
+    if (last_byte < 0)  // every key equal: row order is the answer
+      FDB_CUDA(cudaMemcpyAsync(sorted_out, va, m * 4, cudaMemcpyDeviceToDevice, c.stream));
+  }
+  if (nnull)
+    FDB_CUDA(cudaMemcpyAsync(d_rows + (nulls_last ? m : 0), nulls, nnull * 4, cudaMemcpyDeviceToDevice, c.stream));
+}
+
+}  // namespace fdb

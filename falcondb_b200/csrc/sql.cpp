@@ -1288,7 +1288,49 @@ static void run_projection(Plan& plan, const Rel& rel, const Query& q, fdb_resul
     }
   }
 
-  // 3. Everything else: bring the selected rows to the host; sort / limit there.
+  // 3. ORDER BY one FLOAT64 / INT64 column with no LIMIT or a larger one: GPU
+  //    radix sort of the selected rows (the single-key typed sort,
+  //    try_typed_sort, sort.rs:209-350), then the LIMIT.
+  if (q.order.size() == 1 && nsel > 0) {
+    const OrderItem& o = q.order[0];
+    int oc = -1;
+    if (!o.ref.col.empty() && o.ref.col[0] == '#') {
+      const int pos = std::atoi(o.ref.col.c_str() + 1) - 1;
+      if (pos >= 0 && pos < (int)outcols.size()) oc = outcols[pos];
+    } else {
+      for (size_t i = 0; i < items.size(); ++i)
+        if (items[i].alias == o.ref.col) oc = outcols[i];
+      if (oc < 0) oc = resolve(rel, o.ref);
+    }
+    if (oc >= 0 && rel.cols[oc].dtype != FDB_UTF8) {
+      uint32_t* order = plan.dev<uint32_t>(nsel);
+      if (all_rows) {
+        op_sort(plan.c, rel.cols[oc].dev, n, o.desc, o.nulls_last, order);
+      } else {
+        const RelCol& ocol = rel.cols[oc];
+        uint64_t* vals = plan.dev<uint64_t>(nsel);
+        uint64_t* valid = ocol.dev.validity ? plan.dev<uint64_t>((nsel + 63) / 64) : nullptr;
+        op_gather(plan.c, ocol.dev, d_rows, nsel, vals, valid);
+        fdb_dev_column g{};
+        g.dtype = ocol.dtype;
+        g.values = vals;
+        g.validity = valid;
+        uint32_t* local = plan.dev<uint32_t>(nsel);
+        op_sort(plan.c, g, nsel, o.desc, o.nulls_last, local);
+        fdb_dev_column rows_col{};
+        rows_col.dtype = FDB_UTF8;  // 4-byte gather of row numbers
+        rows_col.values = d_rows;
+        op_gather(plan.c, rows_col, local, nsel, order, nullptr);
+      }
+      plan.check();
+      const uint64_t take = q.limit >= 0 ? std::min<uint64_t>((uint64_t)q.limit, nsel) : nsel;
+      for (size_t i = 0; i < outcols.size(); ++i) fetch_rows(plan, rel, outcols[i], order, take, res->cols[i]);
+      res->rows = take;
+      return;
+    }
+  }
+
+  // 4. Everything else: bring the selected rows to the host; sort / limit there.
   uint64_t take = nsel;
   if (q.order.empty() && q.limit >= 0) take = std::min<uint64_t>(take, (uint64_t)q.limit);
   if (all_rows) {

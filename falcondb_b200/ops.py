@@ -350,6 +350,19 @@ def topk(db: Database, col: ColArg, nrows: int, k: int, desc: bool, nulls_last: 
     return rows, count
 
 
+def sort(db: Database, col: ColArg, nrows: int, desc: bool, nulls_last: Optional[bool] = None,
+         rows: Optional[torch.Tensor] = None) -> torch.Tensor:
+    """ORDER BY col [DESC] without LIMIT: all nrows row numbers in order
+    (int32 holding uint32).  NULLs default to last for DESC, first for ASC."""
+    if nulls_last is None:
+        nulls_last = desc
+    raw = dev_column(col)
+    rows = rows if rows is not None else torch.empty(max(1, nrows), dtype=torch.int32, device=_dev(db))
+    with _Fenced(db):
+        check(lib().fdb_sort(db.handle, C.byref(raw), nrows, int(desc), int(nulls_last), rows.data_ptr()))
+    return rows
+
+
 class GroupByBatch:
     """Many int64-key GROUP BY queries (COUNT(*), SUM, MIN, MAX of a value
     column) captured as one CUDA graph: fdb_gb_batch_prepare / _run / _free.

@@ -366,6 +366,16 @@ int fdb_join_probe_pairs(fdb_db* db, const fdb_hash* h, const fdb_dev_column* pr
 int fdb_topk(fdb_db* db, const fdb_dev_column* col, uint64_t nrows, uint32_t k,
              int32_t desc, int32_t nulls_last, uint32_t* d_rows, uint64_t* d_count);
 
+/* ORDER BY col [DESC] over one FLOAT64 / INT64 column, no LIMIT
+ * (execute_sort -> sort_merged -> try_typed_sort -> assemble, sort.rs:118-133,
+ * 209-350, 773-791): all nrows row numbers in order.  Keys are the reference's
+ * order keys (f64_ord_key, sort.rs:451-454; sign flip for INT64; every bit
+ * flipped for DESC), so -0.0 sorts before +0.0 and NaN after +inf; ties keep
+ * row order; NULL rows come first or last, in row order, as `nulls_last` says.
+ * d_rows holds nrows entries (device); nrows < 2^32 - 1. */
+int fdb_sort(fdb_db* db, const fdb_dev_column* col, uint64_t nrows, int32_t desc,
+             int32_t nulls_last, uint32_t* d_rows);
+
 /* ---- Batched GROUP BY -------------------------------------------------------
  * Many independent `GROUP BY key` queries (COUNT(*), SUM, MIN, MAX of one
  * value column, each over its own rows, e.g. slices of one table) run as one

@@ -472,4 +472,37 @@ uint64_t orc_topk(int dtype, const void* values, const uint64_t* validity, uint6
   return o;
 }
 
+// ---------------------------------------------------------------------------
+// ORDER BY col [DESC] without LIMIT (sort_merged -> try_typed_sort, sort.rs:
+// 118-133, 209-350): (order key, row) pairs of the non-NULL rows sorted as
+// tuples (sort_pairs_ord, 692-698; the INT64 arm's sort_pairs, 749-760,
+// compares keys only and leaves ties unordered -- row order is one of its
+// outcomes), NULL rows before or after in row order (assemble, 773-791).
+// Writes n row numbers.
+// ---------------------------------------------------------------------------
+void orc_sort(int dtype, const void* values, const uint64_t* validity, uint64_t n, int desc, int nulls_last,
+              uint32_t* out) {
+  typedef std::pair<uint64_t, uint32_t> P;
+  std::vector<P> pairs;
+  pairs.reserve(n);
+  std::vector<uint32_t> nulls;
+  for (uint64_t i = 0; i < n; ++i) {
+    if (!valid_at(validity, i)) {
+      nulls.push_back((uint32_t)i);
+      continue;
+    }
+    uint64_t key = dtype == 2 ? ord_f64(static_cast<const double*>(values)[i])
+                              : ((uint64_t)static_cast<const int64_t*>(values)[i] ^ (1ull << 63));
+    if (desc) key = ~key;
+    pairs.push_back(P{key, (uint32_t)i});
+  }
+  std::sort(pairs.begin(), pairs.end());
+  uint64_t o = 0;
+  if (!nulls_last)
+    for (uint32_t r : nulls) out[o++] = r;
+  for (const P& p : pairs) out[o++] = p.second;
+  if (nulls_last)
+    for (uint32_t r : nulls) out[o++] = r;
+}
+
 }  // extern "C"

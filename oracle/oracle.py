@@ -36,6 +36,7 @@ _SIGS = {
     "orc_join_agg": (None, [P, P, P, P, U64, P, P, P, P, U64, C.c_int, P, P, P, P]),
     "orc_join_pairs": (U64, [P, P, U64, P, P, U64, C.c_int, P, P, U64]),
     "orc_topk": (U64, [C.c_int, P, P, U64, C.c_uint32, C.c_int, C.c_int, P]),
+    "orc_sort": (None, [C.c_int, P, P, U64, C.c_int, C.c_int, P]),
     "ref_hardware_threads": (C.c_int, []),
     "ref_sum_f64": (C.c_double, [P, U64, C.c_int]),
     "ref_count_cmp_f64": (U64, [P, U64, C.c_int, C.c_double]),
@@ -207,6 +208,18 @@ def topk(values, k, desc, nulls_last=None, validity=None) -> np.ndarray:
     out = np.zeros(max(1, k), dtype=np.uint32)
     m = lib().orc_topk(dtype, _p(v), _p(_c(validity, np.uint64)), len(v), k, int(desc), int(nulls_last), _p(out))
     return out[:m]
+
+
+def sort(values, desc, nulls_last=None, validity=None) -> np.ndarray:
+    """Every row number in ORDER BY order (orc_sort)."""
+    v = np.ascontiguousarray(values)
+    dtype = 2 if v.dtype.kind == "f" else 1
+    v = v.astype(np.float64 if dtype == 2 else np.int64, copy=False)
+    if nulls_last is None:
+        nulls_last = desc
+    out = np.zeros(max(1, len(v)), dtype=np.uint32)
+    lib().orc_sort(dtype, _p(v), _p(_c(validity, np.uint64)), len(v), int(desc), int(nulls_last), _p(out))
+    return out[:len(v)]
 
 
 # ---------------------------------------------------------------------------- reference-shaped engine

@@ -1,0 +1,136 @@
+"""GPU parity of ORDER BY without LIMIT against the oracle's restatement of
+sort_merged -> try_typed_sort -> assemble (sort.rs:118-133, 209-350, 773-791):
+bit-exact row lists, (order key, row) order, NULL rows first or last in row
+order.  Full-size cases check size-independent properties instead: the output
+is a permutation and the keys it reads are non-decreasing."""
+import ctypes as C
+
+import numpy as np
+import pytest
+import torch
+
+import falcondb_b200 as F
+from falcondb_b200 import ops
+from oracle import oracle as O
+
+pytestmark = pytest.mark.gpu
+
+
+def dev(a):
+    return torch.from_numpy(np.ascontiguousarray(a)).cuda()
+
+
+def run(db, col, n, desc, nulls_last=None):
+    rows = ops.sort(db, col, n, desc, nulls_last)
+    return rows[:n].cpu().numpy().view(np.uint32)
+
+
+@pytest.mark.parametrize("n", [1, 2, 31, 4095, 4096, 4097, 65_537, 1_000_003])
+@pytest.mark.parametrize("desc", [False, True])
+def test_sort_f64_random(db, n, desc):
+    v = np.random.default_rng(n).standard_normal(n) * 1e3
+    assert np.array_equal(run(db, dev(v), n, desc), O.sort(v, desc))
+
+
+@pytest.mark.parametrize("n", [7, 5000, 300_001])
+@pytest.mark.parametrize("desc", [False, True])
+def test_sort_i64_full_range(db, n, desc):
+    """Keys varying in every byte, the int64 extremes included."""
+    rng = np.random.default_rng(n + 1)
+    v = rng.integers(np.iinfo(np.int64).min, np.iinfo(np.int64).max, n, dtype=np.int64, endpoint=True)
+    v[0] = np.iinfo(np.int64).min
+    v[-1] = np.iinfo(np.int64).max
+    assert np.array_equal(run(db, dev(v), n, desc), O.sort(v, desc))
+
+
+def test_sort_float_specials(db):
+    """NaN (both signs), +-inf, +-0.0, subnormals, repeated values."""
+    base = np.array([3.0, -0.0, 0.0, np.nan, -1.0, np.inf, 3.0, -np.inf, 5e-324, -5e-324,
+                     np.float64(np.nan) * -1, 1e308, -1e308, 0.0, -0.0])
+    v = np.tile(base, 701)
+    n = len(v)
+    for desc in (False, True):
+        assert np.array_equal(run(db, dev(v), n, desc), O.sort(v, desc)), desc
+
+
+@pytest.mark.parametrize("n", [9, 10_000, 2_000_003])
+def test_sort_ties_keep_row_order(db, n):
+    for v in (np.full(n, 42.5), np.zeros(n, dtype=np.int64), (np.arange(n) % 3).astype(np.int64),
+              (np.arange(n) // 1000).astype(np.float64)):
+        for desc in (False, True):
+            assert np.array_equal(run(db, dev(v), n, desc), O.sort(v, desc)), (v.dtype, desc)
+
+
+@pytest.mark.parametrize("n", [1, 63, 64, 65, 4097, 100_003])
+@pytest.mark.parametrize("nulls_last", [False, True])
+def test_sort_nulls(db, n, nulls_last):
+    rng = np.random.default_rng(n)
+    v = rng.random(n) * 10
+    valid = rng.random(n) > 0.3
+    words = F.validity_words(valid)
+    for desc in (False, True):
+        got = run(db, (dev(v), dev(words.view(np.int64))), n, desc, nulls_last)
+        assert np.array_equal(got, O.sort(v, desc, nulls_last=nulls_last, validity=words)), desc
+
+
+def test_sort_all_null_and_no_null_bitmap(db):
+    n = 5000
+    v = np.arange(n, dtype=np.float64)
+    none = F.validity_words(np.zeros(n, dtype=bool))
+    allv = F.validity_words(np.ones(n, dtype=bool))
+    for nl in (False, True):
+        assert list(run(db, (dev(v), dev(none.view(np.int64))), n, True, nl)) == list(range(n))
+        assert np.array_equal(run(db, (dev(v), dev(allv.view(np.int64))), n, True, nl), O.sort(v, True))
+
+
+@pytest.mark.parametrize("voff", [1, 37, 64, 100])
+def test_sort_validity_offset(db, voff):
+    """A column whose validity bits start at bit `voff` of its bitmap."""
+    n = 10_007
+    rng = np.random.default_rng(voff)
+    v = rng.integers(-50, 50, n).astype(np.int64)
+    valid = rng.random(n) > 0.25
+    shifted = np.concatenate([np.zeros(voff, dtype=bool), valid])
+    words = F.validity_words(shifted)
+    dv, dw = dev(v), dev(words.view(np.int64))
+    raw = F.fdb_dev_column()
+    raw.dtype = F.INT64
+    raw.values = dv.data_ptr()
+    raw.validity = dw.data_ptr()
+    raw.validity_offset = voff
+    out = torch.empty(n, dtype=torch.int32, device="cuda")
+    F.check(F.lib().fdb_sort(db.handle, C.byref(raw), n, 0, 1, out.data_ptr()))
+    torch.cuda.synchronize()
+    exp = O.sort(v, False, nulls_last=True, validity=F.validity_words(valid))
+    assert np.array_equal(out.cpu().numpy().view(np.uint32), exp)
+
+
+def test_sort_empty_and_errors(db):
+    v = dev(np.zeros(4, dtype=np.float64))
+    assert ops.sort(db, v, 0, False).numel() >= 1
+    with pytest.raises(F.FalconError):
+        ops.sort(db, dev(np.zeros(4, dtype=np.int32)), 4, False)
+
+
+@pytest.mark.parametrize("dtype", [np.float64, np.int64])
+def test_sort_full_size_properties(db, dtype):
+    """100M rows: a permutation whose order keys never decrease (ties in row
+    order), checked on the device."""
+    n = 100_000_000
+    g = torch.Generator(device="cuda").manual_seed(7)
+    if dtype == np.float64:
+        t = torch.rand(n, device="cuda", dtype=torch.float64, generator=g) * 100
+    else:
+        t = torch.randint(-(1 << 40), 1 << 40, (n,), device="cuda", dtype=torch.int64, generator=g)
+    for desc in (False, True):
+        rows = ops.sort(db, t, n, desc)[:n].long()
+        seen = torch.zeros(n, dtype=torch.bool, device="cuda")
+        seen[rows] = True
+        assert bool(seen.all())
+        s = t[rows]
+        d = s[1:] - s[:-1]
+        assert bool((d <= 0).all() if desc else (d >= 0).all())
+        ties = d == 0
+        assert bool((rows[1:][ties] > rows[:-1][ties]).all())
+        del rows, seen, s, d, ties
+        torch.cuda.empty_cache()

@@ -112,3 +112,38 @@ def test_errors_are_reported(db):
     assert e.value.code == -5
     with pytest.raises(F.FalconError):
         db.sql("SELECT x FROM nope")
+
+
+def test_order_by_without_small_limit_sorts_on_the_gpu(db):
+    """ORDER BY one numeric column with no LIMIT, or one above the top-k bound,
+    with and without WHERE, by name, alias and position: the oracle's full sort
+    (try_typed_sort, sort.rs:209-350) of the selected rows."""
+    t = W.table_t(300_000, seed=5)
+    db.create_table("t", t)
+    r = db.sql("SELECT id, score FROM t ORDER BY score")
+    assert list(r.column(0)) == list(O.sort(t["score"], False))
+    r = db.sql("SELECT score AS s, id FROM t ORDER BY s DESC LIMIT 10000")
+    assert list(r.column(1)) == list(O.sort(t["score"], True)[:10000])
+    r = db.sql("SELECT id FROM t ORDER BY 1 DESC")
+    assert list(r.column(0)) == list(range(299_999, -1, -1))
+    sel = np.flatnonzero(t["score"] > 60)
+    r = db.sql("SELECT id, salary FROM t WHERE score > 60 ORDER BY salary DESC")
+    assert list(r.column(0)) == list(sel[O.sort(t["salary"][sel], True)])
+    r = db.sql("SELECT id FROM t WHERE score > 60 ORDER BY score LIMIT 5000")
+    assert list(r.column(0)) == list(sel[O.sort(t["score"][sel], False)][:5000])
+
+
+@pytest.mark.parametrize("nulls", ["", " NULLS FIRST", " NULLS LAST"])
+def test_order_by_nullable_column(db, nulls):
+    n = 50_000
+    rng = np.random.default_rng(3)
+    x = np.ma.masked_array(rng.standard_normal(n), mask=rng.random(n) < 0.2)
+    x[5] = -0.0
+    x[6] = 0.0
+    db.create_table("u", {"id": np.arange(n, dtype=np.int64), "x": x})
+    valid = F.validity_words(~np.ma.getmaskarray(x))
+    for desc in (False, True):
+        nl = desc if not nulls else nulls == " NULLS LAST"
+        r = db.sql(f"SELECT id FROM u ORDER BY x{' DESC' if desc else ''}{nulls}")
+        want = O.sort(np.ma.getdata(x), desc, nulls_last=nl, validity=valid)
+        assert list(r.column(0)) == list(want), (desc, nulls)

@@ -231,6 +231,77 @@ def test_topk_ascending_column_desc():
     assert list(O.topk(v, 10, True)) == list(range(99_999, 99_989, -1))
 
 
+def _xorshift_keys(n):
+    """sort.rs:1677-1690: xorshift64 keys from 0x2545F4914F6CDD1D."""
+    state, out = 0x2545F4914F6CDD1D, []
+    m = (1 << 64) - 1
+    for _ in range(n):
+        state ^= (state << 13) & m
+        state ^= state >> 7
+        state ^= (state << 17) & m
+        out.append(state)
+    return out
+
+
+def test_full_sort_known_answers():
+    """sort.rs:1642-1672 (make_batch, sort_asc, sort_desc) and 1729-1740
+    (sort_nulls_last)."""
+    score = np.array([7.0, 9.5, 8.0, 6.0])
+    asc = O.sort(score, False)
+    assert score[asc[0]] == 6.0 and score[asc[3]] == 9.5
+    assert score[O.sort(score, True)[0]] == 9.5
+    x = np.array([1.0, 0.0, 3.0])
+    valid = F.validity_words(np.array([True, False, True]))
+    assert list(O.sort(x, False, nulls_last=True, validity=valid)) == [0, 2, 1]
+    assert list(O.sort(x, False, nulls_last=False, validity=valid)) == [1, 0, 2]
+
+
+def test_full_sort_matches_the_tuple_sort_of_order_keys():
+    """sort.rs:1675-1690 (radix_sort_matches_comparison_sort): 2 * 8192 + 37
+    xorshift keys sort as (key, row) tuples.  An INT64 column whose values are
+    key XOR 2^63 has exactly these order keys."""
+    keys = _xorshift_keys(2 * 8192 + 37)
+    vals = np.array([k ^ (1 << 63) for k in keys], dtype=np.uint64).view(np.int64)
+    expect = [r for _, r in sorted((k, r) for r, k in enumerate(keys))]
+    assert list(O.sort(vals, False)) == expect
+
+
+def test_full_sort_constant_and_duplicate_keys():
+    """sort.rs:1693-1705: constant keys keep row order; i % 3 keys sort as
+    (key, row) tuples."""
+    n = 8192 + 5
+    assert list(O.sort(np.full(n, 42, dtype=np.int64), False)) == list(range(n))
+    dup = np.arange(n, dtype=np.int64) % 3
+    assert list(O.sort(dup, False)) == [r for _, r in sorted((int(dup[r]), r) for r in range(n))]
+
+
+def test_full_sort_large_float_column_is_ordered():
+    """sort.rs:1707-1723: 16,384 scattered floats come out non-decreasing."""
+    n = 2 * 8192
+    i = np.arange(n)
+    v = ((i * 7919) % n).astype(np.float64) - n // 2
+    got = v[O.sort(v, False)]
+    assert np.all(np.diff(got) >= 0)
+    assert sorted(O.sort(v, False)) == list(range(n))
+
+
+def test_full_sort_float_order_keys():
+    """f64_ord_key (sort.rs:451-454): -0.0 before +0.0, NaN after +inf, DESC
+    flips the keys, ties stay in row order in both directions."""
+    v = np.array([3.0, -0.0, 0.0, np.nan, -1.0, np.inf, 3.0, -np.inf])
+    assert list(O.sort(v, False)) == [7, 4, 1, 2, 0, 6, 5, 3]
+    assert list(O.sort(v, True)) == [3, 5, 0, 6, 2, 1, 4, 7]
+
+
+def test_full_sort_head_is_the_topk():
+    scores, valid, null = _topk_fixture()
+    for desc in (False, True):
+        for nulls_last in (False, True):
+            full = O.sort(scores, desc, nulls_last=nulls_last, validity=valid)
+            assert list(full) == _full_sort_head(scores, null, ROWS, desc, nulls_last)
+            assert list(full[:15]) == list(O.topk(scores, 15, desc, nulls_last=nulls_last, validity=valid))
+
+
 def test_reference_engine_agrees_with_the_serial_oracle():
     """The timed CPU baseline computes the same answers as the serial oracle."""
     from falcondb_b200 import workloads as W
