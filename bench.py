@@ -581,6 +581,20 @@ def run_secondary(args):
                                   "cpu_sample": {"rows": sample, "mrows_per_s": round(sample / cpu_s / 1e6, 2),
                                                  "cores": 1, "kind": "port",
                                                  "what": "oracle std::sort of (order key, row) pairs"}})
+        # SELECT DISTINCT score (first occurrence per value, row order): the same
+        # radix sort on value keys, a run-head pass and a compaction.
+        dcount = torch.empty(1, dtype=torch.int64, device=dev)
+        ms_d = _time_steps(lambda: ops.distinct(db, sc, n, rows=rows_out, count=dcount), K, Wm, stream, torch)
+        kept = int(dcount.item())
+        assert kept == int(torch.unique(sc).numel())
+        t0 = time.perf_counter()
+        O.distinct(hs)
+        cpu_d = time.perf_counter() - t0
+        line("distinct", ms_d, n * (20 + 32 * passes + 16) + kept * 4,
+             {"rows": n, "query": "SELECT DISTINCT score FROM t", "distinct_values": kept,
+              "mrows_per_s": round(n / (ms_d / 1e3) / 1e6, 1),
+              "cpu_sample": {"rows": sample, "mrows_per_s": round(sample / cpu_d / 1e6, 2), "cores": 1,
+                             "kind": "port", "what": "oracle hash-set first-occurrence scan"}})
         torch.cuda.empty_cache()
     if args.workload in ("serve", "all"):
         run_serving(args, db, out, peak)

@@ -185,6 +185,7 @@ _SIGS = {
     "fdb_topk": (C.c_int, [C.c_void_p, C.POINTER(fdb_dev_column), C.c_uint64, C.c_uint32, C.c_int32, C.c_int32,
                            C.c_void_p, C.c_void_p]),
     "fdb_sort": (C.c_int, [C.c_void_p, C.POINTER(fdb_dev_column), C.c_uint64, C.c_int32, C.c_int32, C.c_void_p]),
+    "fdb_distinct": (C.c_int, [C.c_void_p, C.POINTER(fdb_dev_column), C.c_uint64, C.c_void_p, C.c_void_p]),
     "fdb_gb_batch_prepare": (C.c_int, [C.c_void_p, C.POINTER(fdb_gb_query), C.c_int32, C.POINTER(fdb_batch_tuning),
                                        C.POINTER(C.c_void_p)]),
     "fdb_gb_batch_run": (C.c_int, [C.c_void_p]),

@@ -617,6 +617,14 @@ int fdb_sort(fdb_db* db, const fdb_dev_column* col, uint64_t nrows, int32_t desc
   });
 }
 
+int fdb_distinct(fdb_db* db, const fdb_dev_column* col, uint64_t nrows, uint32_t* d_rows, uint64_t* d_count) {
+  if (!db || !col || !d_count || (!d_rows && nrows)) return set_error(FDB_E_ARG, "fdb_distinct: bad arguments");
+  return guarded([&] {
+    CallScope s(db, default_scratch(db->ctx));
+    op_distinct(s.c, *col, nrows, d_rows, d_count);
+  });
+}
+
 int fdb_gb_batch_prepare(fdb_db* db, const fdb_gb_query* queries, int32_t nqueries, const fdb_batch_tuning* tuning,
                          fdb_batch** out) {
   if (out) *out = nullptr;

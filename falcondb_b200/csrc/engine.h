@@ -187,6 +187,9 @@ void op_topk(Ctx& c, const fdb_dev_column& col, uint64_t n, uint32_t k, bool des
 // d_rows receives n row numbers.
 void op_sort(Ctx& c, const fdb_dev_column& col, uint64_t n, bool desc, bool nulls_last,
              uint32_t* d_rows);
+// SELECT DISTINCT over one FLOAT64 / INT64 / UTF8 column (k_sort.cu): the
+// positions of each value's first occurrence, ascending; *d_count = how many.
+void op_distinct(Ctx& c, const fdb_dev_column& col, uint64_t n, uint32_t* d_rows, uint64_t* d_count);
 
 struct HashTable;  // join build side (k_join.cu)
 HashTable* op_join_build(Ctx& c, const fdb_dev_column& key, const fdb_dev_column& payload,

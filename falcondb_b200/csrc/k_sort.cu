@@ -32,15 +32,36 @@ constexpr uint32_t kSortTile = kSortThreads * kSortItems;
 constexpr int kSortWarps = kSortThreads / 32;
 
 // Keys of the selected rows (sel[i], or row i when sel is null) and their
-// rows; vary[0] |= every key, vary[1] &= every key.
-template <int DT, bool DESC>
+// rows; vary[0] |= every key, vary[1] &= every key.  ORDER BY keys are order
+// keys (wt_key); DISTINCT keys (DISTINCT_KEY) only have to be equal exactly
+// when the values are: FLOAT64 bits with every NaN made one NaN and -0.0 made
+// +0.0 (norm_f64, select.rs:201-204), INT64 bits, UTF8 codes.
+constexpr int DISTINCT_KEY = -1;
+template <int DT, int MODE>
+__device__ __forceinline__ uint64_t sort_key_of(const DevCol& col, uint32_t row) {
+  if constexpr (MODE == DISTINCT_KEY) {
+    if constexpr (DT == FDB_UTF8) {
+      return static_cast<const uint32_t*>(col.values)[row];
+    } else {
+      uint64_t b = static_cast<const uint64_t*>(col.values)[row];
+      if constexpr (DT == FDB_FLOAT64) {
+        if ((b & 0x7FFFFFFFFFFFFFFFull) > 0x7FF0000000000000ull) b = 0x7FF8000000000000ull;  // NaN
+        if (b == 0x8000000000000000ull) b = 0;                                                 // -0.0
+      }
+      return b;
+    }
+  } else {
+    return wt_key<DT, MODE != 0>(static_cast<const uint64_t*>(col.values)[row]);
+  }
+}
+
+template <int DT, int MODE>
 __global__ void sort_key_kernel(DevCol col, const uint32_t* sel, uint32_t m, uint64_t* keys, uint32_t* vals,
                                 unsigned long long* vary) {
   unsigned long long o = 0, a = ~0ull;
-  const uint64_t* v = static_cast<const uint64_t*>(col.values);
   for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < m; i += gridDim.x * blockDim.x) {
     const uint32_t row = sel ? sel[i] : i;
-    const uint64_t k = wt_key<DT, DESC>(v[row]);
+    const uint64_t k = sort_key_of<DT, MODE>(col, row);
     keys[i] = k;
     vals[i] = row;
     o |= k;
@@ -54,6 +75,23 @@ __global__ void sort_key_kernel(DevCol col, const uint32_t* sel, uint32_t m, uin
   if ((threadIdx.x & 31) == 0) {
     atomicOr(&vary[0], o);
     atomicAnd(&vary[1], a);
+  }
+}
+
+// DISTINCT: the first row of every run of equal keys in the sorted pairs, and
+// the first NULL row (nulls[0] when *nnull > 0), set in a row mask.
+__global__ void distinct_heads_kernel(const uint64_t* __restrict__ keys, const uint32_t* __restrict__ rows,
+                                      uint32_t m, const uint32_t* nulls, const uint64_t* nnull,
+                                      unsigned long long* mask) {
+  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < m; i += gridDim.x * blockDim.x) {
+    if (i == 0 || keys[i] != keys[i - 1]) {
+      const uint32_t r = rows[i];
+      atomicOr(&mask[r >> 6], 1ull << (r & 63));
+    }
+  }
+  if (blockIdx.x == 0 && threadIdx.x == 0 && nnull && *nnull > 0) {
+    const uint32_t r = nulls[0];
+    atomicOr(&mask[r >> 6], 1ull << (r & 63));
   }
 }
 
@@ -402,11 +440,112 @@ __global__ void sort_valid_mask_kernel(DevCol col, uint64_t n, bool nulls, uint6
   }
 }
 
-template <int DT, bool DESC>
+template <int DT, int MODE>
 static void launch_sort_keys(Ctx& c, const DevCol& col, const uint32_t* sel, uint32_t m, uint64_t* keys,
                              uint32_t* vals, unsigned long long* vary) {
   const unsigned grid = (unsigned)std::max<uint64_t>(1, std::min<uint64_t>((m + 255) / 256, (uint64_t)c.sm_count * 8));
-  sort_key_kernel<DT, DESC><<<grid, 256, 0, c.stream>>>(col, sel, m, keys, vals, vary);
+  sort_key_kernel<DT, MODE><<<grid, 256, 0, c.stream>>>(col, sel, m, keys, vals, vary);
+}
+
+// Scratch a sort of up to n pairs needs (see SortWork), with or without the
+// NULL split.
+static size_t sort_scratch_bytes(uint64_t n, bool nullable) {
+  const uint64_t words = (n + 63) / 64;
+  const uint64_t ntiles = (n + kSortTile - 1) / kSortTile;
+  const uint64_t hn = 256ull * ntiles;
+  const uint64_t nb = (hn + kScanB - 1) / kScanB;
+  size_t need = 2 * n * 8 + 2 * n * 4 + hn * 4 + nb * 4 + 16;
+  if (nullable) need += words * 8 + 2 * n * 4 + 16;
+  return need + (2u << 20);  // + 256-byte rounding and the compaction's chunk counts
+}
+
+// The rows of a column split into non-NULL rows (`sel`, row order) and NULL
+// rows (`nulls`, row order); both counts are also left on the device
+// (d_counts[0], d_counts[1]).
+struct NullSplit {
+  const uint32_t* sel = nullptr;
+  uint32_t* nulls = nullptr;
+  uint64_t* d_counts = nullptr;
+  uint64_t m = 0, nnull = 0;
+};
+
+static NullSplit split_nulls(Ctx& c, const DevCol& dc, uint64_t n) {
+  NullSplit r;
+  r.m = n;
+  if (!dc.validity) return r;
+  const uint64_t words = (n + 63) / 64;
+  uint64_t* mask = static_cast<uint64_t*>(c.scratch_take(words * 8));
+  uint32_t* vrows = static_cast<uint32_t*>(c.scratch_take(n * 4));
+  r.nulls = static_cast<uint32_t*>(c.scratch_take(n * 4));
+  r.d_counts = static_cast<uint64_t*>(c.scratch_take(16));
+  const unsigned g = (unsigned)std::max<uint64_t>(1, std::min<uint64_t>((words + 255) / 256, (uint64_t)c.sm_count * 4));
+  sort_valid_mask_kernel<<<g, 256, 0, c.stream>>>(dc, n, false, mask);
+  op_compact_mask(c, mask, n, vrows, n, r.d_counts);
+  sort_valid_mask_kernel<<<g, 256, 0, c.stream>>>(dc, n, true, mask);
+  op_compact_mask(c, mask, n, r.nulls, n, r.d_counts + 1);
+  uint64_t hc[2] = {0, 0};
+  FDB_CUDA(cudaMemcpyAsync(hc, r.d_counts, 16, cudaMemcpyDeviceToHost, c.stream));
+  FDB_CUDA(cudaStreamSynchronize(c.stream));
+  if (hc[0] + hc[1] != n) fail(FDB_E_GENERIC, "sort: valid and NULL rows do not add up to the row count");
+  r.m = hc[0];
+  r.nnull = hc[1];
+  r.sel = vrows;
+  return r;
+}
+
+// Stable radix sort of the (key, row) pairs of `sel` (m rows): builds the
+// pairs with key kernel `keys_fn`, then runs one pass per byte that varies.
+// With `rows_out`, the last pass writes the rows there and no keys (and the
+// result is in rows_out); otherwise the sorted keys and rows are returned in
+// *keys_sorted / *rows_sorted (scratch).
+template <class KeysFn>
+static void radix_sort_pairs(Ctx& c, uint32_t m, KeysFn keys_fn, uint32_t* rows_out, const uint64_t** keys_sorted,
+                             const uint32_t** rows_sorted) {
+  uint64_t* ka = static_cast<uint64_t*>(c.scratch_take(m * 8));
+  uint64_t* kb = static_cast<uint64_t*>(c.scratch_take(m * 8));
+  uint32_t* va = static_cast<uint32_t*>(c.scratch_take(m * 4));
+  uint32_t* vb = static_cast<uint32_t*>(c.scratch_take(m * 4));
+  const uint32_t ntiles = (uint32_t)((m + kSortTile - 1) / kSortTile);
+  const uint64_t hn = 256ull * ntiles;
+  const uint64_t nb = (hn + kScanB - 1) / kScanB;
+  uint32_t* hist = static_cast<uint32_t*>(c.scratch_take(hn * 4));
+  uint32_t* bsum = static_cast<uint32_t*>(c.scratch_take(nb * 4));
+  unsigned long long* vary = static_cast<unsigned long long*>(c.scratch_take(16));
+  FDB_CUDA(cudaMemsetAsync(vary, 0, 8, c.stream));
+  FDB_CUDA(cudaMemsetAsync(vary + 1, 0xFF, 8, c.stream));
+  keys_fn(ka, va, vary);
+  FDB_CUDA(cudaGetLastError());
+  unsigned long long hv[2] = {0, 0};
+  FDB_CUDA(cudaMemcpyAsync(hv, vary, 16, cudaMemcpyDeviceToHost, c.stream));
+  FDB_CUDA(cudaStreamSynchronize(c.stream));
+  const uint64_t varying = hv[0] ^ hv[1];  // bits that are not the same in every key
+  int last_byte = -1;
+  for (int byte = 0; byte < 8; ++byte)
+    if ((varying >> (8 * byte)) & 0xFFull) last_byte = byte;
+  const int grid = (int)std::min<uint64_t>(ntiles, (uint64_t)kScatterCtasPerSm * c.sm_count);
+  for (int byte = 0; byte <= last_byte; ++byte) {
+    const int shift = 8 * byte;
+    if (((varying >> shift) & 0xFFull) == 0) continue;  // one digit for every key: order unchanged
+    radix_hist_kernel<<<ntiles, kSortThreads, 0, c.stream>>>(ka, m, shift, ntiles, hist);
+    sort_scan_sums_kernel<<<(unsigned)nb, kScanT, 0, c.stream>>>(hist, hn, bsum);
+    sort_scan_top_kernel<<<1, kScanT, 0, c.stream>>>(bsum, nb);
+    sort_scan_apply_kernel<<<(unsigned)nb, kScanT, 0, c.stream>>>(hist, hn, bsum);
+    const bool direct = rows_out && byte == last_byte;  // rows go straight to the output; keys are not needed
+    radix_scatter_kernel<<<grid, kScatterThreads, sizeof(ScatterSmem), c.stream>>>(
+        ka, va, m, shift, hist, ntiles, kb, direct ? rows_out : vb, !direct, c.d_err);
+    std::swap(ka, kb);
+    std::swap(va, vb);
+  }
+  FDB_CUDA(cudaGetLastError());
+  if (rows_out && last_byte < 0)  // every key equal: row order is the answer
+    FDB_CUDA(cudaMemcpyAsync(rows_out, va, (size_t)m * 4, cudaMemcpyDeviceToDevice, c.stream));
+  if (keys_sorted) *keys_sorted = ka;
+  if (rows_sorted) *rows_sorted = va;
+}
+
+static void set_scatter_smem() {
+  FDB_CUDA(cudaFuncSetAttribute(radix_scatter_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                (int)sizeof(ScatterSmem)));
 }
 
 void op_sort(Ctx& c, const fdb_dev_column& col, uint64_t n, bool desc, bool nulls_last, uint32_t* d_rows) {
@@ -415,93 +554,67 @@ void op_sort(Ctx& c, const fdb_dev_column& col, uint64_t n, bool desc, bool null
   if (n == 0) return;
   if (!col.values) fail(FDB_E_ARG, "column without values");
   const DevCol dc{col.dtype, col.values, col.validity, col.validity_offset};
-
-  FDB_CUDA(cudaFuncSetAttribute(radix_scatter_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                (int)sizeof(ScatterSmem)));
-  int scatter_grid = 0;
+  set_scatter_smem();
   // Working memory comes from the context's scratch arena, which grows once
-  // and stays resident: two (key, row) buffers, the histogram and its scan
-  // sums, and with a validity bitmap the mask and the two row lists.
-  const uint64_t words = (n + 63) / 64;
-  const uint64_t ntiles_max = (n + kSortTile - 1) / kSortTile;
-  const uint64_t hn_max = 256ull * ntiles_max;
-  const uint64_t nb_max = (hn_max + kScanB - 1) / kScanB;
-  size_t need = 2 * n * 8 + 2 * n * 4 + hn_max * 4 + nb_max * 4 + 16;
-  if (col.validity) need += words * 8 + 2 * n * 4 + 16;
-  c.ensure_scratch(c.scratch_top + need + (2u << 20));  // + 256-byte rounding and the compaction's chunk counts
+  // and stays resident.
+  c.ensure_scratch(c.scratch_top + sort_scratch_bytes(n, col.validity != nullptr));
 
   // NULL rows leave the sort: the valid rows are sorted, the NULL rows keep
   // their row order before or after them.
-  const uint32_t* sel = nullptr;
-  uint32_t* nulls = nullptr;
-  uint64_t m = n, nnull = 0;
-  if (col.validity) {
-    uint64_t* mask = static_cast<uint64_t*>(c.scratch_take(words * 8));
-    uint32_t* vrows = static_cast<uint32_t*>(c.scratch_take(n * 4));
-    nulls = static_cast<uint32_t*>(c.scratch_take(n * 4));
-    uint64_t* cnt = static_cast<uint64_t*>(c.scratch_take(16));
-    const unsigned g = (unsigned)std::max<uint64_t>(1, std::min<uint64_t>((words + 255) / 256, (uint64_t)c.sm_count * 4));
-    sort_valid_mask_kernel<<<g, 256, 0, c.stream>>>(dc, n, false, mask);
-    op_compact_mask(c, mask, n, vrows, n, cnt);
-    sort_valid_mask_kernel<<<g, 256, 0, c.stream>>>(dc, n, true, mask);
-    op_compact_mask(c, mask, n, nulls, n, cnt + 1);
-    uint64_t hc[2] = {0, 0};
-    FDB_CUDA(cudaMemcpyAsync(hc, cnt, 16, cudaMemcpyDeviceToHost, c.stream));
-    FDB_CUDA(cudaStreamSynchronize(c.stream));
-    if (hc[0] + hc[1] != n) fail(FDB_E_GENERIC, "sort: valid and NULL rows do not add up to the row count");
-    m = hc[0];
-    nnull = hc[1];
-    sel = vrows;
+  const NullSplit ns = split_nulls(c, dc, n);
+  if (ns.m > 0) {
+    const uint32_t m = (uint32_t)ns.m;
+    auto keys = [&](uint64_t* k, uint32_t* v, unsigned long long* vary) {
+      if (col.dtype == FDB_FLOAT64)
+        desc ? launch_sort_keys<FDB_FLOAT64, 1>(c, dc, ns.sel, m, k, v, vary)
+             : launch_sort_keys<FDB_FLOAT64, 0>(c, dc, ns.sel, m, k, v, vary);
+      else
+        desc ? launch_sort_keys<FDB_INT64, 1>(c, dc, ns.sel, m, k, v, vary)
+             : launch_sort_keys<FDB_INT64, 0>(c, dc, ns.sel, m, k, v, vary);
+    };
+    radix_sort_pairs(c, m, keys, d_rows + (nulls_last ? 0 : ns.nnull), nullptr, nullptr);
   }
-  uint32_t* sorted_out = d_rows + (nulls_last ? 0 : nnull);
-  if (m > 0) {
-    const uint32_t mm = (uint32_t)m;
-    uint64_t* ka = static_cast<uint64_t*>(c.scratch_take(m * 8));
-    uint64_t* kb = static_cast<uint64_t*>(c.scratch_take(m * 8));
-    uint32_t* va = static_cast<uint32_t*>(c.scratch_take(m * 4));
-    uint32_t* vb = static_cast<uint32_t*>(c.scratch_take(m * 4));
-    const uint32_t ntiles = (uint32_t)((m + kSortTile - 1) / kSortTile);
-    const uint64_t hn = 256ull * ntiles;
-    const uint64_t nb = (hn + kScanB - 1) / kScanB;
-    uint32_t* hist = static_cast<uint32_t*>(c.scratch_take(hn * 4));
-    uint32_t* bsum = static_cast<uint32_t*>(c.scratch_take(nb * 4));
-    unsigned long long* vary = static_cast<unsigned long long*>(c.scratch_take(16));
-    FDB_CUDA(cudaMemsetAsync(vary, 0, 8, c.stream));
-    FDB_CUDA(cudaMemsetAsync(vary + 1, 0xFF, 8, c.stream));
-    if (col.dtype == FDB_FLOAT64)
-      desc ? launch_sort_keys<FDB_FLOAT64, true>(c, dc, sel, mm, ka, va, vary)
-           : launch_sort_keys<FDB_FLOAT64, false>(c, dc, sel, mm, ka, va, vary);
-    else
-      desc ? launch_sort_keys<FDB_INT64, true>(c, dc, sel, mm, ka, va, vary)
-           : launch_sort_keys<FDB_INT64, false>(c, dc, sel, mm, ka, va, vary);
-    FDB_CUDA(cudaGetLastError());
-    unsigned long long hv[2] = {0, 0};
-    FDB_CUDA(cudaMemcpyAsync(hv, vary, 16, cudaMemcpyDeviceToHost, c.stream));
-    FDB_CUDA(cudaStreamSynchronize(c.stream));
-    const uint64_t varying = hv[0] ^ hv[1];  // bits that are not the same in every key
-    int last_byte = -1;
-    for (int byte = 0; byte < 8; ++byte)
-      if ((varying >> (8 * byte)) & 0xFFull) last_byte = byte;
-    scatter_grid = (int)std::min<uint64_t>(ntiles, (uint64_t)kScatterCtasPerSm * c.sm_count);
-    for (int byte = 0; byte < 8; ++byte) {
-      const int shift = 8 * byte;
-      if (((varying >> shift) & 0xFFull) == 0) continue;  // one digit for every key: order unchanged
-      radix_hist_kernel<<<ntiles, kSortThreads, 0, c.stream>>>(ka, mm, shift, ntiles, hist);
-      sort_scan_sums_kernel<<<(unsigned)nb, kScanT, 0, c.stream>>>(hist, hn, bsum);
-      sort_scan_top_kernel<<<1, kScanT, 0, c.stream>>>(bsum, nb);
-      sort_scan_apply_kernel<<<(unsigned)nb, kScanT, 0, c.stream>>>(hist, hn, bsum);
-      const bool last = byte == last_byte;  // rows go straight to the output; keys are not needed
-      radix_scatter_kernel<<<scatter_grid, kScatterThreads, sizeof(ScatterSmem), c.stream>>>(
-          ka, va, mm, shift, hist, ntiles, kb, last ? sorted_out : vb, !last, c.d_err);
-      std::swap(ka, kb);
-      std::swap(va, vb);
-    }
-    FDB_CUDA(cudaGetLastError());
-    if (last_byte < 0)  // every key equal: row order is the answer
-      FDB_CUDA(cudaMemcpyAsync(sorted_out, va, m * 4, cudaMemcpyDeviceToDevice, c.stream));
+  if (ns.nnull)
+    FDB_CUDA(cudaMemcpyAsync(d_rows + (nulls_last ? ns.m : 0), ns.nulls, ns.nnull * 4, cudaMemcpyDeviceToDevice,
+                             c.stream));
+}
+
+void op_distinct(Ctx& c, const fdb_dev_column& col, uint64_t n, uint32_t* d_rows, uint64_t* d_count) {
+  if (col.dtype != FDB_FLOAT64 && col.dtype != FDB_INT64 && col.dtype != FDB_UTF8)
+    fail(FDB_E_TYPE, "DISTINCT needs a FLOAT64, INT64 or UTF8 column");
+  if (n >= 0xFFFFFFFFull) fail(FDB_E_ARG, "DISTINCT addresses rows as uint32");
+  if (n == 0) {
+    FDB_CUDA(cudaMemsetAsync(d_count, 0, 8, c.stream));
+    return;
   }
-  if (nnull)
-    FDB_CUDA(cudaMemcpyAsync(d_rows + (nulls_last ? m : 0), nulls, nnull * 4, cudaMemcpyDeviceToDevice, c.stream));
+  if (!col.values) fail(FDB_E_ARG, "column without values");
+  const DevCol dc{col.dtype, col.values, col.validity, col.validity_offset};
+  set_scatter_smem();
+  const uint64_t words = (n + 63) / 64;
+  c.ensure_scratch(c.scratch_top + sort_scratch_bytes(n, col.validity != nullptr) + words * 8 + 256);
+  unsigned long long* heads = static_cast<unsigned long long*>(c.scratch_take(words * 8));
+  FDB_CUDA(cudaMemsetAsync(heads, 0, words * 8, c.stream));
+
+  const NullSplit ns = split_nulls(c, dc, n);
+  const uint64_t* skeys = nullptr;
+  const uint32_t* srows = nullptr;
+  if (ns.m > 0) {
+    const uint32_t m = (uint32_t)ns.m;
+    auto keys = [&](uint64_t* k, uint32_t* v, unsigned long long* vary) {
+      if (col.dtype == FDB_FLOAT64)
+        launch_sort_keys<FDB_FLOAT64, DISTINCT_KEY>(c, dc, ns.sel, m, k, v, vary);
+      else if (col.dtype == FDB_INT64)
+        launch_sort_keys<FDB_INT64, DISTINCT_KEY>(c, dc, ns.sel, m, k, v, vary);
+      else
+        launch_sort_keys<FDB_UTF8, DISTINCT_KEY>(c, dc, ns.sel, m, k, v, vary);
+    };
+    radix_sort_pairs(c, m, keys, nullptr, &skeys, &srows);
+  }
+  const unsigned g = (unsigned)std::max<uint64_t>(1, std::min<uint64_t>((ns.m + 255) / 256, (uint64_t)c.sm_count * 8));
+  distinct_heads_kernel<<<g, 256, 0, c.stream>>>(skeys, srows, (uint32_t)ns.m, ns.nulls,
+                                                 ns.nnull ? ns.d_counts + 1 : nullptr, heads);
+  FDB_CUDA(cudaGetLastError());
+  op_compact_mask(c, reinterpret_cast<const uint64_t*>(heads), n, d_rows, n, d_count);
 }
 
 }  // namespace fdb

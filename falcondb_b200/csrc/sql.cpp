@@ -1,10 +1,10 @@
 // Database::sql for the relational hot path: a small SQL front end and a
 // planner that maps each query shape onto the GPU operators, in the fixed
 // operator order of FalconDB's execute_plan (src/db.rs:1410-1416: scan+WHERE ->
-// joins -> GROUP BY -> ORDER BY(+LIMIT) -> LIMIT -> projection).
+// joins -> GROUP BY -> ORDER BY(+LIMIT) -> LIMIT -> projection -> DISTINCT).
 //
 // Supported shapes (everything else fails with FDB_E_SQL):
-//   SELECT <items> FROM t [[INNER] | LEFT [OUTER]] JOIN u ON t.k = u.k]
+//   SELECT [DISTINCT] <items> FROM t [[INNER] | LEFT [OUTER]] JOIN u ON t.k = u.k]
 //          [WHERE <pred>] [GROUP BY col] [ORDER BY col|alias [ASC|DESC]
 //          [NULLS FIRST|LAST], ...] [LIMIT n]
 //   items: *, col, COUNT(*), COUNT(col), COUNT(DISTINCT col), SUM/AVG/MIN/MAX(col) [AS a]
@@ -14,7 +14,9 @@
 //          (rewritten to a SEMI / ANTI join as db.rs:1582-1604 does).
 // Fast paths kept from execute_plan: COUNT(*) + WHERE counts the mask
 // (db.rs:1439-1476); aggregate-only queries scan once (db.rs:1483-1518);
-// ORDER BY col LIMIT k takes the bounded top-k (sort.rs:59-115).
+// ORDER BY col LIMIT k takes the bounded top-k (sort.rs:59-115); ORDER BY one
+// numeric column otherwise runs the GPU radix sort.  SELECT DISTINCT takes one
+// column and keeps each value's first row in output order.
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -158,6 +160,7 @@ struct Query {
   ColRef group;
   std::vector<OrderItem> order;
   int64_t limit = -1;
+  bool distinct = false;  // SELECT DISTINCT (applied after ORDER BY and LIMIT, db.rs:1699-1729)
 };
 
 // ===========================================================================
@@ -439,6 +442,7 @@ struct Parser {
   Query query() {
     Query q;
     expect_kw("SELECT");
+    if (accept_kw("DISTINCT")) q.distinct = true;
     do {
       q.items.push_back(sel_item());
     } while (accept_sym(","));
@@ -1209,6 +1213,63 @@ static void run_group_by(Plan& plan, const Rel& rel, const Query& q, fdb_result*
 // ---------------------------------------------------------------------------
 // Projection (SELECT cols [WHERE] [ORDER BY] [LIMIT])
 // ---------------------------------------------------------------------------
+// The result rows `d_list` (n entries, in output order; null = rows 0..n-1)
+// fetched into the result columns; with SELECT DISTINCT (one column) only each
+// value's first occurrence in that order is kept (dedup_batches,
+// select.rs:238-457).
+static void emit_rows(Plan& plan, const Rel& rel, const std::vector<int>& outcols, const Query& q,
+                      const uint32_t* d_list, uint64_t n, fdb_result* res) {
+  if (q.distinct && n > 0) {
+    const RelCol& col = rel.cols[outcols[0]];
+    fdb_dev_column g = col.dev;
+    if (d_list) {
+      void* vals = plan.dev<uint8_t>(n * dtype_size(col.dtype));
+      uint64_t* valid = col.dev.validity ? plan.dev<uint64_t>((n + 63) / 64) : nullptr;
+      op_gather(plan.c, col.dev, d_list, n, vals, valid);
+      g = fdb_dev_column{};
+      g.dtype = col.dtype;
+      g.values = vals;
+      g.validity = valid;
+    }
+    uint32_t* pos = plan.dev<uint32_t>(n);
+    uint64_t* dcount = plan.dev<uint64_t>(1);
+    op_distinct(plan.c, g, n, pos, dcount);
+    plan.check();
+    const uint64_t k = plan.one(dcount);
+    uint32_t* kept = pos;
+    if (d_list) {
+      kept = plan.dev<uint32_t>(std::max<uint64_t>(k, 1));
+      fdb_dev_column list{};
+      list.dtype = FDB_UTF8;  // 4-byte gather of row numbers
+      list.values = d_list;
+      op_gather(plan.c, list, pos, k, kept, nullptr);
+    }
+    fetch_rows(plan, rel, outcols[0], kept, k, res->cols[0]);
+    res->rows = k;
+    if (col.dtype == FDB_UTF8) {
+      // Codes name strings; a dictionary that holds one string under two codes
+      // still yields the string once (value semantics, row_eq on get_str).
+      fdb_result::Col& rc = res->cols[0];
+      std::set<std::string> seen;
+      bool null_seen = false;
+      fdb_result::Col out;
+      out.name = rc.name;
+      out.dtype = rc.dtype;
+      for (uint64_t i = 0; i < k; ++i) {
+        const bool is_null = !rc.nulls.empty() && rc.nulls[i];
+        if (is_null ? std::exchange(null_seen, true) : !seen.insert(rc.str[i]).second) continue;
+        out.str.push_back(rc.str[i]);
+        out.nulls.push_back(is_null ? 1 : 0);
+      }
+      res->rows = out.str.size();
+      rc = std::move(out);
+    }
+    return;
+  }
+  for (size_t i = 0; i < outcols.size(); ++i) fetch_rows(plan, rel, outcols[i], d_list, n, res->cols[i]);
+  res->rows = n;
+}
+
 static void run_projection(Plan& plan, const Rel& rel, const Query& q, fdb_result* res) {
   // Output column list.
   std::vector<int> outcols;
@@ -1229,6 +1290,7 @@ static void run_projection(Plan& plan, const Rel& rel, const Query& q, fdb_resul
     }
   }
   for (size_t i = 0; i < outcols.size(); ++i) push_col(res, out_name(items[i]), rel.cols[outcols[i]].dtype);
+  if (q.distinct && outcols.size() != 1) fail(FDB_E_SQL, "SELECT DISTINCT over more than one column is not supported");
 
   // 1. Selected rows (all rows, or the WHERE survivors in row order).
   const uint64_t n = rel.nrows;
@@ -1282,8 +1344,7 @@ static void run_projection(Plan& plan, const Rel& rel, const Query& q, fdb_resul
       }
       plan.check();
       const uint64_t got = plan.one(dcount);
-      for (size_t i = 0; i < outcols.size(); ++i) fetch_rows(plan, rel, outcols[i], top, got, res->cols[i]);
-      res->rows = got;
+      emit_rows(plan, rel, outcols, q, top, got, res);
       return;
     }
   }
@@ -1324,8 +1385,7 @@ static void run_projection(Plan& plan, const Rel& rel, const Query& q, fdb_resul
       }
       plan.check();
       const uint64_t take = q.limit >= 0 ? std::min<uint64_t>((uint64_t)q.limit, nsel) : nsel;
-      for (size_t i = 0; i < outcols.size(); ++i) fetch_rows(plan, rel, outcols[i], order, take, res->cols[i]);
-      res->rows = take;
+      emit_rows(plan, rel, outcols, q, order, take, res);
       return;
     }
   }
@@ -1333,6 +1393,12 @@ static void run_projection(Plan& plan, const Rel& rel, const Query& q, fdb_resul
   // 4. Everything else: bring the selected rows to the host; sort / limit there.
   uint64_t take = nsel;
   if (q.order.empty() && q.limit >= 0) take = std::min<uint64_t>(take, (uint64_t)q.limit);
+  if (q.distinct) {
+    if (!q.order.empty())
+      fail(FDB_E_SQL, "SELECT DISTINCT with ORDER BY over several keys or a text column is not supported");
+    emit_rows(plan, rel, outcols, q, all_rows ? nullptr : d_rows, take, res);
+    return;
+  }
   if (all_rows) {
     d_rows = plan.dev<uint32_t>(take);
     std::vector<uint32_t> iota(take);
@@ -1528,11 +1594,14 @@ static void run_join(Plan& plan, Query& q, const JoinSpec& js, fdb_result* res) 
   rest.group = q.group;
   rest.order = q.order;
   rest.limit = q.limit;
+  rest.distinct = q.distinct;
   // A WHERE beside the JOIN filters the joined rows (the EXISTS form was the
   // join itself).
   if (q.where && !(q.where->kind == P_EXISTS || q.where->kind == P_NOTEXISTS)) rest.where = std::move(q.where);
   bool all_agg = !rest.items.empty();
   for (const SelItem& it : rest.items) all_agg = all_agg && it.agg >= 0;
+  if (rest.distinct && (rest.has_group || all_agg))
+    fail(FDB_E_SQL, "SELECT DISTINCT with aggregates or GROUP BY is not supported");
   if (rest.has_group) run_group_by(plan, joined, rest, res);
   else if (all_agg) run_aggregates(plan, joined, rest, res);
   else run_projection(plan, joined, rest, res);
@@ -1645,6 +1714,8 @@ fdb_result* run_sql(Ctx& c, const std::string& sql) {
     add_table_cols(c, rel, *find_table(c, q.table), q.alias);
     bool all_agg = !q.items.empty();
     for (const SelItem& it : q.items) all_agg = all_agg && it.agg >= 0;
+    if (q.distinct && (q.has_group || all_agg))
+      fail(FDB_E_SQL, "SELECT DISTINCT with aggregates or GROUP BY is not supported");
     if (q.has_group) run_group_by(plan, rel, q, res.get());
     else if (all_agg) run_aggregates(plan, rel, q, res.get());
     else run_projection(plan, rel, q, res.get());

@@ -363,6 +363,19 @@ def sort(db: Database, col: ColArg, nrows: int, desc: bool, nulls_last: Optional
     return rows
 
 
+def distinct(db: Database, col: ColArg, nrows: int, rows: Optional[torch.Tensor] = None,
+             count: Optional[torch.Tensor] = None) -> Tuple[torch.Tensor, torch.Tensor]:
+    """SELECT DISTINCT col: row numbers of each value's first occurrence, in row
+    order (int32 holding uint32), and their count."""
+    raw = dev_column(col)
+    dev = _dev(db)
+    rows = rows if rows is not None else torch.empty(max(1, nrows), dtype=torch.int32, device=dev)
+    count = count if count is not None else torch.empty(1, dtype=torch.int64, device=dev)
+    with _Fenced(db):
+        check(lib().fdb_distinct(db.handle, C.byref(raw), nrows, rows.data_ptr(), count.data_ptr()))
+    return rows, count
+
+
 class GroupByBatch:
     """Many int64-key GROUP BY queries (COUNT(*), SUM, MIN, MAX of a value
     column) captured as one CUDA graph: fdb_gb_batch_prepare / _run / _free.

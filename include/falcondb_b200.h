@@ -1,6 +1,7 @@
 /*
  * falcondb_b200.h — C ABI of the B200 execution engine for FalconDB's relational
- * hot path: scan, filter, aggregate, GROUP BY, hash join and ORDER BY ... LIMIT.
+ * hot path: scan, filter, aggregate, GROUP BY, hash join, ORDER BY (top-k and
+ * full sort) and SELECT DISTINCT.
  *
  * Two layers, both plain C (opaque handles, pointers and sizes; no C++ or torch
  * types cross this boundary):
@@ -208,11 +209,15 @@ int  fdb_table_column(const fdb_db* db, const char* table, const char* column,
 
 /* Execute SQL (falcondb_sql, c_ffi.rs:86-99 -> Database::sql, db.rs:242-316).
  * *out is NULL on error.  Supported shapes (others fail with FDB_E_SQL):
- *   SELECT items FROM t [[INNER] | LEFT [OUTER] JOIN u ON t.k = u.k] [WHERE pred]
- *          [GROUP BY col] [ORDER BY col|alias [ASC|DESC] [NULLS FIRST|LAST], ...] [LIMIT n]
+ *   SELECT [DISTINCT] items FROM t [[INNER] | LEFT [OUTER] JOIN u ON t.k = u.k] [WHERE pred]
+ *          [GROUP BY col] [ORDER BY col|alias|n [ASC|DESC] [NULLS FIRST|LAST], ...] [LIMIT n]
  *   items: *, col, COUNT(*), COUNT(col), COUNT(DISTINCT col), SUM/AVG/MIN/MAX(col) [AS a]
  *   pred : col op literal, IS [NOT] NULL, [NOT] IN (...), [NOT] LIKE (Utf8), AND, OR,
- *          parentheses, and [NOT] EXISTS (SELECT ... FROM u WHERE u.k = t.k). */
+ *          parentheses, and [NOT] EXISTS (SELECT ... FROM u WHERE u.k = t.k).
+ * ORDER BY one FLOAT64 / INT64 column runs on the GPU (fdb_topk for LIMIT <= 4096,
+ * else fdb_sort); several keys or a UTF8 key are ordered on the host after the
+ * fetch.  DISTINCT takes one column and runs after ORDER BY and LIMIT, as the
+ * reference does (db.rs:1699-1729). */
 int  fdb_sql(fdb_db* db, const char* sql, fdb_result** out);
 
 /* Result accessors (c_ffi.rs:103-127). */
@@ -375,6 +380,16 @@ int fdb_topk(fdb_db* db, const fdb_dev_column* col, uint64_t nrows, uint32_t k,
  * d_rows holds nrows entries (device); nrows < 2^32 - 1. */
 int fdb_sort(fdb_db* db, const fdb_dev_column* col, uint64_t nrows, int32_t desc,
              int32_t nulls_last, uint32_t* d_rows);
+
+/* SELECT DISTINCT col over one FLOAT64 / INT64 / UTF8 column (dedup_batches ->
+ * dedup_single_primitive and the row_hash / row_eq path, select.rs:171-457):
+ * the row numbers of each value's first occurrence, in row order.  FLOAT64
+ * values are compared with every NaN equal and -0.0 equal to +0.0 (norm_f64,
+ * select.rs:201-204); UTF8 compares codes (a code names one string); all NULL
+ * rows are one value, kept at its first row.  d_rows holds nrows entries
+ * (device); d_count receives how many were written. */
+int fdb_distinct(fdb_db* db, const fdb_dev_column* col, uint64_t nrows, uint32_t* d_rows,
+                 uint64_t* d_count);
 
 /* ---- Batched GROUP BY -------------------------------------------------------
  * Many independent `GROUP BY key` queries (COUNT(*), SUM, MIN, MAX of one

@@ -505,4 +505,39 @@ void orc_sort(int dtype, const void* values, const uint64_t* validity, uint64_t 
     for (uint32_t r : nulls) out[o++] = r;
 }
 
+// ---------------------------------------------------------------------------
+// SELECT DISTINCT col (dedup_batches, select.rs:238-269, and its one-column
+// fast path dedup_single_primitive, 311-457): first occurrence wins, output in
+// row order.  Values compare as row_eq does (select.rs:210-236): FLOAT64 with
+// every NaN one value and -0.0 == +0.0 (norm_f64, 201-204), INT64 exactly,
+// UTF8 by code (dtype 3, uint32 codes); all NULL rows are one value.
+// Writes the kept row numbers; returns their count.
+// ---------------------------------------------------------------------------
+uint64_t orc_distinct(int dtype, const void* values, const uint64_t* validity, uint64_t n, uint32_t* out) {
+  std::unordered_map<uint64_t, char> seen;
+  bool null_seen = false;
+  uint64_t o = 0;
+  for (uint64_t i = 0; i < n; ++i) {
+    if (!valid_at(validity, i)) {
+      if (!null_seen) out[o++] = (uint32_t)i;
+      null_seen = true;
+      continue;
+    }
+    uint64_t k;
+    if (dtype == 3) {
+      k = static_cast<const uint32_t*>(values)[i];
+    } else {
+      std::memcpy(&k, static_cast<const char*>(values) + i * 8, 8);
+      if (dtype == 2) {
+        double d;
+        std::memcpy(&d, &k, 8);
+        if (std::isnan(d)) k = 0x7FF8000000000000ull;
+        else if (d == 0.0) k = 0;
+      }
+    }
+    if (seen.emplace(k, 1).second) out[o++] = (uint32_t)i;
+  }
+  return o;
+}
+
 }  // extern "C"

@@ -37,6 +37,7 @@ _SIGS = {
     "orc_join_pairs": (U64, [P, P, U64, P, P, U64, C.c_int, P, P, U64]),
     "orc_topk": (U64, [C.c_int, P, P, U64, C.c_uint32, C.c_int, C.c_int, P]),
     "orc_sort": (None, [C.c_int, P, P, U64, C.c_int, C.c_int, P]),
+    "orc_distinct": (U64, [C.c_int, P, P, U64, P]),
     "ref_hardware_threads": (C.c_int, []),
     "ref_sum_f64": (C.c_double, [P, U64, C.c_int]),
     "ref_count_cmp_f64": (U64, [P, U64, C.c_int, C.c_double]),
@@ -220,6 +221,21 @@ def sort(values, desc, nulls_last=None, validity=None) -> np.ndarray:
     out = np.zeros(max(1, len(v)), dtype=np.uint32)
     lib().orc_sort(dtype, _p(v), _p(_c(validity, np.uint64)), len(v), int(desc), int(nulls_last), _p(out))
     return out[:len(v)]
+
+
+def distinct(values, validity=None) -> np.ndarray:
+    """Row numbers of each value's first occurrence (orc_distinct).  A uint32
+    array is taken as UTF8 codes."""
+    v = np.ascontiguousarray(values)
+    if v.dtype == np.uint32:
+        dtype = 3
+    elif v.dtype.kind == "f":
+        dtype, v = 2, v.astype(np.float64, copy=False)
+    else:
+        dtype, v = 1, v.astype(np.int64, copy=False)
+    out = np.zeros(max(1, len(v)), dtype=np.uint32)
+    k = lib().orc_distinct(dtype, _p(v), _p(_c(validity, np.uint64)), len(v), _p(out))
+    return out[:k]
 
 
 # ---------------------------------------------------------------------------- reference-shaped engine

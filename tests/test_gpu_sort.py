@@ -134,3 +134,70 @@ def test_sort_full_size_properties(db, dtype):
         assert bool((rows[1:][ties] > rows[:-1][ties]).all())
         del rows, seen, s, d, ties
         torch.cuda.empty_cache()
+
+
+# ----------------------------------------------------------------------------- DISTINCT
+def run_distinct(db, col, n):
+    rows, cnt = ops.distinct(db, col, n)
+    return rows[:int(cnt.item())].cpu().numpy().view(np.uint32)
+
+
+@pytest.mark.parametrize("n", [1, 2, 100, 4097, 65_537, 1_000_003])
+def test_distinct_int_and_float(db, n):
+    rng = np.random.default_rng(n)
+    for card in (1, 7, 1000, n):
+        v = rng.integers(-card, card + 1, n).astype(np.int64)
+        assert np.array_equal(run_distinct(db, dev(v), n), O.distinct(v)), ("i64", card)
+        f = v.astype(np.float64) * 0.25
+        assert np.array_equal(run_distinct(db, dev(f), n), O.distinct(f)), ("f64", card)
+
+
+def test_distinct_float_specials(db):
+    base = np.array([np.nan, -0.0, 0.0, -np.nan, 2.0, np.inf, -np.inf, 5e-324, -5e-324, 1e308])
+    v = np.tile(base, 997)[np.random.default_rng(3).permutation(9970)]
+    assert np.array_equal(run_distinct(db, dev(v), len(v)), O.distinct(v))
+
+
+@pytest.mark.parametrize("n", [5, 4096, 300_007])
+def test_distinct_utf8_codes(db, n):
+    codes = np.random.default_rng(n).integers(0, 12, n).astype(np.uint32)
+    codes[::5] = 0xFFFFFFFF  # the NULL code is one value
+    got = run_distinct(db, dev(codes.view(np.int32)), n)
+    assert np.array_equal(got, O.distinct(codes))
+
+
+@pytest.mark.parametrize("n", [1, 64, 65, 10_007])
+def test_distinct_nulls(db, n):
+    rng = np.random.default_rng(n)
+    v = rng.integers(0, 20, n).astype(np.int64)
+    valid = rng.random(n) > 0.4
+    words = F.validity_words(valid)
+    got = run_distinct(db, (dev(v), dev(words.view(np.int64))), n)
+    assert np.array_equal(got, O.distinct(v, validity=words))
+    none = F.validity_words(np.zeros(n, dtype=bool))
+    assert list(run_distinct(db, (dev(v), dev(none.view(np.int64))), n)) == [0]
+
+
+def test_distinct_empty_and_errors(db):
+    rows, cnt = ops.distinct(db, dev(np.zeros(4, dtype=np.int64)), 0)
+    assert int(cnt.item()) == 0
+    with pytest.raises(F.FalconError):
+        ops.distinct(db, dev(np.zeros(4, dtype=np.int16)), 4)
+
+
+def test_distinct_full_size_properties(db):
+    """100M rows, 10M-value domain: the kept rows ascend, hold every value once,
+    and each is its value's first row (checked against a scatter-min on the
+    device)."""
+    n = 100_000_000
+    g = torch.Generator(device="cuda").manual_seed(11)
+    t = torch.randint(0, 10_000_000, (n,), device="cuda", dtype=torch.int64, generator=g)
+    rows, cnt = ops.distinct(db, t, n)
+    k = int(cnt.item())
+    r = rows[:k].long()
+    assert bool((r[1:] > r[:-1]).all())
+    vals = t[r]
+    assert k == int(torch.unique(t).numel()) == int(torch.unique(vals).numel())
+    first = torch.full((10_000_000,), n, dtype=torch.int64, device="cuda")
+    first.scatter_reduce_(0, t, torch.arange(n, device="cuda"), reduce="amin")
+    assert bool((first[vals] == r).all())

@@ -147,3 +147,57 @@ def test_order_by_nullable_column(db, nulls):
         r = db.sql(f"SELECT id FROM u ORDER BY x{' DESC' if desc else ''}{nulls}")
         want = O.sort(np.ma.getdata(x), desc, nulls_last=nl, validity=valid)
         assert list(r.column(0)) == list(want), (desc, nulls)
+
+
+def test_select_distinct(db):
+    """SELECT DISTINCT: each value's first row in output order (dedup_batches,
+    select.rs:238-457), after ORDER BY and LIMIT (db.rs:1699-1729); the
+    reference's own cases (sort_and_dedup_paths.rs:143-206,
+    sql_integration.rs:1326-1338) restated."""
+    db.create_table("t", {"v": np.array([1, 2, 1, 3, 2], dtype=np.int64)})
+    assert list(db.sql("SELECT DISTINCT v FROM t").column(0)) == [1, 2, 3]
+    db.create_table("t", {"v": np.array([7, 7, 7], dtype=np.int64)})
+    assert list(db.sql("SELECT DISTINCT v FROM t").column(0)) == [7]
+    db.create_table("t", {"v": np.ma.masked_array(np.array([0, 0, 1], dtype=np.int64), mask=[True, True, False])})
+    assert db.sql("SELECT DISTINCT v FROM t").rows == 2
+    db.create_table("t", {"s": F.Utf8(np.array([0, 1, 0], dtype=np.uint32), ["alpha", "beta"])})
+    assert list(db.sql("SELECT DISTINCT s FROM t").column(0)) == ["alpha", "beta"]
+    db.create_table("t", {"v": np.array([1.5, 2.5, 1.5])})
+    assert db.sql("SELECT DISTINCT v FROM t").rows == 2
+    db.create_table("t", {"v": np.arange(3000, dtype=np.int64) % 137})
+    assert db.sql("SELECT DISTINCT v FROM t").rows == 137
+    db.create_table("t", {"n": np.array([3, 1, 2, 1, 3], dtype=np.int64)})
+    assert list(db.sql("SELECT DISTINCT n FROM t ORDER BY n ASC").column(0)) == [1, 2, 3]
+    assert list(db.sql("SELECT DISTINCT n FROM t ORDER BY n DESC LIMIT 3").column(0)) == [3, 2]
+    assert list(db.sql("SELECT DISTINCT n FROM t LIMIT 3").column(0)) == [3, 1, 2]
+    with pytest.raises(F.FalconError) as e:
+        db.sql("SELECT DISTINCT n, n FROM t")
+    assert e.value.code == -5
+
+
+@pytest.mark.parametrize("n", [1000, 1_000_003])
+def test_select_distinct_against_the_oracle(db, n):
+    rng = np.random.default_rng(n)
+    t = W.table_t(n, seed=4)
+    sal = t["salary"] % 5000
+    f = np.round(rng.standard_normal(n), 2)
+    f[::997] = np.nan
+    f[1::991] = -0.0
+    f[2::983] = 0.0
+    xv = rng.integers(0, 300, n).astype(np.int64)
+    null = rng.random(n) < 0.05
+    db.create_table("u", {"id": t["id"], "dept": t["dept"], "salary": sal, "f": f,
+                          "x": np.ma.masked_array(xv, mask=null)})
+    r = db.sql("SELECT DISTINCT salary FROM u")
+    assert list(r.column(0)) == list(sal[O.distinct(sal)])
+    got = np.array(db.sql("SELECT DISTINCT f FROM u").column(0), dtype=np.float64)
+    exp = f[O.distinct(f)]
+    assert np.array_equal(got, exp, equal_nan=True)
+    assert np.array_equal(np.signbit(got), np.signbit(exp))  # the first zero's sign is kept
+    sel = np.flatnonzero(sal > 1000)
+    keep = sel[O.distinct(xv[sel], validity=F.validity_words(~null[sel]))]
+    r = db.sql("SELECT DISTINCT x FROM u WHERE salary > 1000")
+    assert r.rows == len(keep)
+    assert [None if null[k] else int(xv[k]) for k in keep] == [r.value(i, 0) for i in range(r.rows)]
+    r = db.sql("SELECT DISTINCT dept FROM u")
+    assert list(r.column(0)) == [W.DEPTS[c] for c in t["dept"].codes[O.distinct(t["dept"].codes)]]

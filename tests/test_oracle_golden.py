@@ -302,6 +302,29 @@ def test_full_sort_head_is_the_topk():
             assert list(full[:15]) == list(O.topk(scores, 15, desc, nulls_last=nulls_last, validity=valid))
 
 
+def test_distinct_known_answers():
+    """tests/sort_and_dedup_paths.rs:143-206 and sql_integration.rs:1326-1338,
+    restated on the oracle: first occurrence kept, in row order."""
+    assert list(O.distinct(np.array([1, 2, 1, 3, 2], dtype=np.int64))) == [0, 1, 3]
+    assert list(O.distinct(np.array([7, 7, 7], dtype=np.int64))) == [0]
+    v = np.array([0, 0, 1], dtype=np.int64)  # two NULLs then 1: NULLs are one value
+    assert list(O.distinct(v, validity=F.validity_words(np.array([False, False, True])))) == [0, 2]
+    assert list(O.distinct(np.array([0, 1, 0], dtype=np.uint32))) == [0, 1]  # alpha, beta, alpha
+    assert len(O.distinct(np.array([1.5, 2.5, 1.5]))) == 2
+    assert len(O.distinct(np.concatenate([[1], np.arange(40) % 5]).astype(np.int64))) == 5
+    assert len(O.distinct(np.arange(3000, dtype=np.int64) % 137)) == 137
+    assert len(O.distinct(np.array([0, 1, 0, 1, 0], dtype=np.uint32))) == 2  # eng, hr
+    n = np.array([3, 1, 2, 1, 3], dtype=np.int64)  # DISTINCT n ORDER BY n: ORDER BY first, then dedup
+    order = O.sort(n, False)
+    assert list(n[order][O.distinct(n[order])]) == [1, 2, 3]
+
+
+def test_distinct_float_equality():
+    """row_eq / norm_f64 (select.rs:201-236): NaNs are one value, -0.0 == +0.0."""
+    v = np.array([np.nan, -0.0, 0.0, -np.nan, 2.0, np.inf, -np.inf, 2.0, np.inf])
+    assert list(O.distinct(v)) == [0, 1, 4, 5, 6]
+
+
 def test_reference_engine_agrees_with_the_serial_oracle():
     """The timed CPU baseline computes the same answers as the serial oracle."""
     from falcondb_b200 import workloads as W
