@@ -595,7 +595,27 @@ def run_secondary(args):
               "mrows_per_s": round(n / (ms_d / 1e3) / 1e6, 1),
               "cpu_sample": {"rows": sample, "mrows_per_s": round(sample / cpu_d / 1e6, 2), "cores": 1,
                              "kind": "port", "what": "oracle hash-set first-occurrence scan"}})
+        del rows_out
         torch.cuda.empty_cache()
+        # The same operators end to end through Database::sql at the sizes the
+        # reference publishes them (100K and 1M rows): host wall time per query,
+        # result rows fetched to host memory included.
+        for rows in (100_000, 1_000_000):
+            db.create_table("s", W.table_t(rows, seed=2))
+            for name, sql in (("order_by_full", "SELECT id FROM s ORDER BY score DESC"),
+                              ("distinct", "SELECT DISTINCT score FROM s"),
+                              ("row_number", "SELECT ROW_NUMBER() OVER (ORDER BY score DESC) AS rn FROM s")):
+                for _ in range(Wm):
+                    db.sql(sql)
+                times = []
+                for _ in range(K):
+                    t0 = time.perf_counter()
+                    r = db.sql(sql)
+                    times.append((time.perf_counter() - t0) * 1e3)
+                out.append({"metric": "SQL wall time", "workload": f"sql_{name}", "rows": rows, "query": sql,
+                            "value": round(statistics.median(times), 4), "unit": "ms", "result_rows": r.rows,
+                            "steps": K, "warmup": Wm, "higher_is_better": False})
+            db.drop_table("s")
     if args.workload in ("serve", "all"):
         run_serving(args, db, out, peak)
     if args.workload == "serve_single":

@@ -305,7 +305,28 @@ class Result:
             self.dtypes.append(dt)
             self.data[key] = vals
             self.nulls[key] = nulls
-        self.display = L.fdb_result_display(handle).decode()
+        # The display table is formatted on first use (QueryResult::display,
+        # db.rs:63-64), from the copied columns.
+        self._display: Optional[str] = None
+
+    @property
+    def display(self) -> str:
+        if self._display is None:
+            self._display = self._format()
+        return self._display
+
+    def _format(self) -> str:
+        """The result as the engine's text table (fdb_result_display's layout)."""
+        cells = [[("NULL" if self.nulls[k][r] else _fmt(self.value(r, k), dt)) for k, dt in
+                  zip(self.columns, self.dtypes)] for r in range(self.rows)]
+        w = [max([len(k)] + [len(row[j]) for row in cells]) for j, k in enumerate(self.columns)]
+        line = "".join("+" + "-" * (x + 2) for x in w) + "+\n"
+        out = [line, "".join(f"| {k}{' ' * (w[j] - len(k) + 1)}" for j, k in enumerate(self.columns)) + "|\n", line]
+        for row in cells:
+            out.append("".join(f"| {c}{' ' * (w[j] - len(c) + 1)}" for j, c in enumerate(row)) + "|\n")
+        out.append(line)
+        out.append(f"{self.rows} row{'' if self.rows == 1 else 's'}\n")
+        return "".join(out)
 
     def row_count(self) -> int:
         return self.rows
@@ -337,8 +358,14 @@ class Result:
 
 
 def _fmt(v, dt) -> str:
+    """A cell as display text: NaN, inf and -inf as Rust prints them, whole
+    floats without a fraction, others in the shortest form that reads back."""
     if dt == FLOAT64:
         f = float(v)
+        if f != f:
+            return "NaN"
+        if f in (float("inf"), float("-inf")):
+            return "inf" if f > 0 else "-inf"
         if f == int(f) and abs(f) < 1e15:
             return str(int(f))
         return repr(f)

@@ -420,7 +420,7 @@ const uint8_t* fdb_result_column_nulls(const fdb_result* r, int32_t col) {
   const auto& c = r->cols[col];
   return c.has_nulls() ? c.nulls.data() : nullptr;
 }
-const char* fdb_result_display(fdb_result* r) { return r ? r->display.c_str() : nullptr; }
+const char* fdb_result_display(fdb_result* r) { return r ? r->display_text().c_str() : nullptr; }
 void fdb_result_free(fdb_result* r) { delete r; }
 
 double fdb_last_kernel_ms(const fdb_db* db) { return db ? db->ctx.last_kernel_ms : 0.0; }

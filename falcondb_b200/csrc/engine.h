@@ -190,6 +190,11 @@ void op_sort(Ctx& c, const fdb_dev_column& col, uint64_t n, bool desc, bool null
 // SELECT DISTINCT over one FLOAT64 / INT64 / UTF8 column (k_sort.cu): the
 // positions of each value's first occurrence, ascending; *d_count = how many.
 void op_distinct(Ctx& c, const fdb_dev_column& col, uint64_t n, uint32_t* d_rows, uint64_t* d_count);
+// op_sort with, when int_as_f64, an INT64 column ordered by its f64 value.
+void op_sort_keyed(Ctx& c, const fdb_dev_column& col, uint64_t n, bool desc, bool nulls_last, bool int_as_f64,
+                   uint32_t* d_rows);
+// d_rn[list[order[j]]] = j + 1 for j < n (order / list null = identity).
+void op_row_numbers(Ctx& c, const uint32_t* d_order, const uint32_t* d_list, uint64_t n, int64_t* d_rn);
 
 struct HashTable;  // join build side (k_join.cu)
 HashTable* op_join_build(Ctx& c, const fdb_dev_column& key, const fdb_dev_column& payload,

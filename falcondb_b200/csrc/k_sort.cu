@@ -33,7 +33,8 @@ constexpr int kSortWarps = kSortThreads / 32;
 
 // Keys of the selected rows (sel[i], or row i when sel is null) and their
 // rows; vary[0] |= every key, vary[1] &= every key.  ORDER BY keys are order
-// keys (wt_key); DISTINCT keys (DISTINCT_KEY) only have to be equal exactly
+// keys (wt_key; MODE 0 ascending, 1 descending, 2 / 3 the same for an INT64
+// column taken as f64); DISTINCT keys (DISTINCT_KEY) only have to be equal exactly
 // when the values are: FLOAT64 bits with every NaN made one NaN and -0.0 made
 // +0.0 (norm_f64, select.rs:201-204), INT64 bits, UTF8 codes.
 constexpr int DISTINCT_KEY = -1;
@@ -50,6 +51,10 @@ __device__ __forceinline__ uint64_t sort_key_of(const DevCol& col, uint32_t row)
       }
       return b;
     }
+  } else if constexpr (MODE >= 2) {
+    // An INT64 key read as f64 first (ROW_NUMBER's eval_dense_f64, expr.rs:232).
+    const double d = (double)static_cast<const int64_t*>(col.values)[row];
+    return wt_key<FDB_FLOAT64, MODE == 3>((uint64_t)__double_as_longlong(d));
   } else {
     return wt_key<DT, MODE != 0>(static_cast<const uint64_t*>(col.values)[row]);
   }
@@ -548,7 +553,29 @@ static void set_scatter_smem() {
                                 (int)sizeof(ScatterSmem)));
 }
 
+// rows[i] = position of row i in the order: ROW_NUMBER() OVER (ORDER BY ..)
+// numbers the rows 1..n in sorted order (rank_dense, window.rs:259-300).
+__global__ void row_number_kernel(const uint32_t* order, const uint32_t* list, uint32_t n, int64_t* rn) {
+  for (uint32_t j = blockIdx.x * blockDim.x + threadIdx.x; j < n; j += gridDim.x * blockDim.x) {
+    const uint32_t o = order ? order[j] : j;
+    rn[list ? list[o] : o] = (int64_t)j + 1;
+  }
+}
+
+void op_row_numbers(Ctx& c, const uint32_t* d_order, const uint32_t* d_list, uint64_t n, int64_t* d_rn) {
+  if (n == 0) return;
+  if (n >= 0xFFFFFFFFull) fail(FDB_E_ARG, "ROW_NUMBER addresses rows as uint32");
+  const unsigned g = (unsigned)std::max<uint64_t>(1, std::min<uint64_t>((n + 255) / 256, (uint64_t)c.sm_count * 8));
+  row_number_kernel<<<g, 256, 0, c.stream>>>(d_order, d_list, (uint32_t)n, d_rn);
+  FDB_CUDA(cudaGetLastError());
+}
+
 void op_sort(Ctx& c, const fdb_dev_column& col, uint64_t n, bool desc, bool nulls_last, uint32_t* d_rows) {
+  op_sort_keyed(c, col, n, desc, nulls_last, false, d_rows);
+}
+
+void op_sort_keyed(Ctx& c, const fdb_dev_column& col, uint64_t n, bool desc, bool nulls_last, bool int_as_f64,
+                   uint32_t* d_rows) {
   if (col.dtype != FDB_FLOAT64 && col.dtype != FDB_INT64) fail(FDB_E_TYPE, "ORDER BY needs a FLOAT64 or INT64 column");
   if (n >= 0xFFFFFFFFull) fail(FDB_E_ARG, "a sort addresses rows as uint32");
   if (n == 0) return;
@@ -568,6 +595,9 @@ void op_sort(Ctx& c, const fdb_dev_column& col, uint64_t n, bool desc, bool null
       if (col.dtype == FDB_FLOAT64)
         desc ? launch_sort_keys<FDB_FLOAT64, 1>(c, dc, ns.sel, m, k, v, vary)
              : launch_sort_keys<FDB_FLOAT64, 0>(c, dc, ns.sel, m, k, v, vary);
+      else if (int_as_f64)
+        desc ? launch_sort_keys<FDB_INT64, 3>(c, dc, ns.sel, m, k, v, vary)
+             : launch_sort_keys<FDB_INT64, 2>(c, dc, ns.sel, m, k, v, vary);
       else
         desc ? launch_sort_keys<FDB_INT64, 1>(c, dc, ns.sel, m, k, v, vary)
              : launch_sort_keys<FDB_INT64, 0>(c, dc, ns.sel, m, k, v, vary);

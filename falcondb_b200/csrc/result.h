@@ -23,8 +23,12 @@ struct fdb_result {
   };
   std::vector<Col> cols;
   uint64_t rows = 0;
-  std::string display;
-  void finalize();  // fills str_ptrs and the display text
+  void finalize();                    // fills str_ptrs
+  const std::string& display_text();  // the table as text, built on first use (QueryResult::display, db.rs:63-64)
+
+ private:
+  std::string display_;
+  bool display_built_ = false;
 };
 
 namespace fdb {

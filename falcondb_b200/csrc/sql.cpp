@@ -7,7 +7,8 @@
 //   SELECT [DISTINCT] <items> FROM t [[INNER] | LEFT [OUTER]] JOIN u ON t.k = u.k]
 //          [WHERE <pred>] [GROUP BY col] [ORDER BY col|alias [ASC|DESC]
 //          [NULLS FIRST|LAST], ...] [LIMIT n]
-//   items: *, col, COUNT(*), COUNT(col), COUNT(DISTINCT col), SUM/AVG/MIN/MAX(col) [AS a]
+//   items: *, col, COUNT(*), COUNT(col), COUNT(DISTINCT col), SUM/AVG/MIN/MAX(col),
+//          ROW_NUMBER() OVER ([ORDER BY col [ASC|DESC]]) [AS a]
 //   pred : col op literal, literal op col, col IS [NOT] NULL, col [NOT] IN (...),
 //          col [NOT] LIKE 'pattern' (Utf8), AND, OR, parentheses, and
 //          [NOT] EXISTS (SELECT ... FROM u WHERE u.k = t.k) as the whole WHERE
@@ -135,18 +136,21 @@ struct Pred {
   std::string sub_table, sub_alias;
   ColRef sub_a, sub_b;
 };
-struct SelItem {
-  bool star = false;
-  int agg = -1;        // FDB_AGG_* or -1
-  bool distinct = false;
-  ColRef col;          // empty col for COUNT(*)
-  std::string alias;
-  std::string text;    // default output name
-};
 struct OrderItem {
   ColRef ref;
   bool desc = false;
   bool nulls_last = false;
+};
+struct SelItem {
+  bool star = false;
+  int agg = -1;        // FDB_AGG_* or -1
+  bool distinct = false;
+  bool row_number = false;  // ROW_NUMBER() OVER ([ORDER BY worder])
+  bool has_worder = false;
+  OrderItem worder;
+  ColRef col;          // empty col for COUNT(*)
+  std::string alias;
+  std::string text;    // default output name
 };
 struct Query {
   std::vector<SelItem> items;
@@ -394,6 +398,30 @@ struct Parser {
     if (accept_sym("*")) {
       it.star = true;
       it.text = "*";
+      return it;
+    }
+    if (peek().kind == T_IDENT && peek().up == "ROW_NUMBER" && peek(1).kind == T_SYM && peek(1).text == "(") {
+      // ROW_NUMBER() OVER ([ORDER BY col [ASC|DESC]]) (window.rs:97-260)
+      p += 2;
+      expect_sym(")");
+      if (!(peek().kind == T_IDENT && peek().up == "OVER")) fail(FDB_E_SQL, "ROW_NUMBER() needs OVER (...)");
+      ++p;
+      expect_sym("(");
+      if (peek().kind == T_IDENT && peek().up == "PARTITION")
+        fail(FDB_E_SQL, "ROW_NUMBER() OVER (PARTITION BY ..) is not supported");
+      it.row_number = true;
+      it.text = "ROW_NUMBER()";
+      if (accept_kw("ORDER")) {
+        expect_kw("BY");
+        it.has_worder = true;
+        it.worder.ref = colref();
+        if (accept_kw("DESC")) it.worder.desc = true;
+        else accept_kw("ASC");
+        if (sym(",")) fail(FDB_E_SQL, "ROW_NUMBER() OVER (ORDER BY ..) takes one key");
+      }
+      expect_sym(")");
+      if (accept_kw("AS")) it.alias = ident();
+      else if (peek().kind == T_IDENT && !reserved(peek().up)) it.alias = ident();
       return it;
     }
     static const std::pair<const char*, int> aggs[] = {{"COUNT", FDB_AGG_COUNT}, {"SUM", FDB_AGG_SUM},
@@ -782,25 +810,26 @@ static void fetch_rows(Plan& plan, const Rel& r, int rc, const uint32_t* d_rows,
   std::vector<uint64_t> vw;
   if (d_valid) vw = plan.to_host(d_valid, (n + 63) / 64);
   out.nulls.assign(n, 0);
-  for (uint64_t i = 0; i < n; ++i) {
-    const bool valid = vw.empty() || ((vw[i >> 6] >> (i & 63)) & 1ull);
+  if (col.dtype == FDB_INT64 || col.dtype == FDB_FLOAT64) {
     if (col.dtype == FDB_INT64) {
-      int64_t v;
-      std::memcpy(&v, raw.data() + i * 8, 8);
-      out.i64.push_back(v);
-    } else if (col.dtype == FDB_FLOAT64) {
-      double v;
-      std::memcpy(&v, raw.data() + i * 8, 8);
-      out.f64.push_back(v);
+      out.i64.resize(n);
+      if (n) std::memcpy(out.i64.data(), raw.data(), n * 8);
     } else {
-      uint32_t code;
-      std::memcpy(&code, raw.data() + i * 4, 4);
-      const bool ok = valid && code != 0xFFFFFFFFu && code < col.dict->size();
-      out.str.push_back(ok ? (*col.dict)[code] : std::string());
-      if (!ok) out.nulls[i] = 1;
-      continue;
+      out.f64.resize(n);
+      if (n) std::memcpy(out.f64.data(), raw.data(), n * 8);
     }
-    if (!valid) out.nulls[i] = 1;
+    if (!vw.empty())
+      for (uint64_t i = 0; i < n; ++i) out.nulls[i] = ((vw[i >> 6] >> (i & 63)) & 1ull) ? 0 : 1;
+    return;
+  }
+  out.str.reserve(n);
+  for (uint64_t i = 0; i < n; ++i) {  // UTF8: codes to strings
+    const bool valid = vw.empty() || ((vw[i >> 6] >> (i & 63)) & 1ull);
+    uint32_t code;
+    std::memcpy(&code, raw.data() + i * 4, 4);
+    const bool ok = valid && code != 0xFFFFFFFFu && code < col.dict->size();
+    out.str.push_back(ok ? (*col.dict)[code] : std::string());
+    if (!ok) out.nulls[i] = 1;
   }
 }
 
@@ -1270,12 +1299,30 @@ static void emit_rows(Plan& plan, const Rel& rel, const std::vector<int>& outcol
   res->rows = n;
 }
 
-static void run_projection(Plan& plan, const Rel& rel, const Query& q, fdb_result* res) {
+static void run_projection(Plan& plan, const Rel& rel_in, const Query& q, fdb_result* res) {
+  // The relation plus one INT64 column per ROW_NUMBER() item, filled once the
+  // WHERE survivors are known (windows run after WHERE, db.rs:1660-1697).
+  Rel rel;
+  rel.nrows = rel_in.nrows;
+  rel.cols = rel_in.cols;
+  std::vector<std::pair<int, const SelItem*>> windows;  // (rel column, item)
   // Output column list.
   std::vector<int> outcols;
   std::vector<SelItem> items;
   for (const SelItem& it : q.items) {
     if (it.agg >= 0) fail(FDB_E_SQL, "mixing aggregates and plain columns needs GROUP BY");
+    if (it.row_number) {
+      RelCol rc;
+      rc.name = it.alias.empty() ? std::string("row_number") : it.alias;
+      rc.dtype = FDB_INT64;
+      rc.dev.dtype = FDB_INT64;
+      rc.dev.values = plan.dev<int64_t>(std::max<uint64_t>(rel.nrows, 1));
+      rel.cols.push_back(rc);
+      windows.push_back({(int)rel.cols.size() - 1, &it});
+      outcols.push_back((int)rel.cols.size() - 1);
+      items.push_back(it);
+      continue;
+    }
     if (it.star) {
       for (size_t i = 0; i < rel.cols.size(); ++i) {
         outcols.push_back((int)i);
@@ -1310,6 +1357,34 @@ static void run_projection(Plan& plan, const Rel& rel, const Query& q, fdb_resul
     plan.check();
     nsel = plan.one(dc);
     all_rows = false;
+  }
+
+  // ROW_NUMBER() columns: the selected rows numbered 1..nsel in the window's
+  // order -- the single-key typed sort (try_dense_partition_sort,
+  // window.rs:308-331: f64_ord_key of the value, an INT64 read as f64, NOT for
+  // DESC, ties by position) -- or in row order without ORDER BY.
+  for (auto& w : windows) {
+    int64_t* rn = static_cast<int64_t*>(const_cast<void*>(rel.cols[w.first].dev.values));
+    const uint32_t* list = all_rows ? nullptr : d_rows;
+    if (!w.second->has_worder || nsel == 0) {
+      op_row_numbers(plan.c, nullptr, list, nsel, rn);
+      continue;
+    }
+    const int oc = resolve(rel_in, w.second->worder.ref);
+    const RelCol& ocol = rel.cols[oc];
+    if (ocol.dtype == FDB_UTF8) fail(FDB_E_SQL, "ROW_NUMBER() OVER (ORDER BY a text column) is not supported");
+    if (ocol.dev.validity) fail(FDB_E_SQL, "ROW_NUMBER() OVER (ORDER BY a nullable column) is not supported");
+    fdb_dev_column g = ocol.dev;
+    if (!all_rows) {
+      uint64_t* vals = plan.dev<uint64_t>(nsel);
+      op_gather(plan.c, ocol.dev, d_rows, nsel, vals, nullptr);
+      g = fdb_dev_column{};
+      g.dtype = ocol.dtype;
+      g.values = vals;
+    }
+    uint32_t* order = plan.dev<uint32_t>(nsel);
+    op_sort_keyed(plan.c, g, nsel, w.second->worder.desc, false, true, order);
+    op_row_numbers(plan.c, order, list, nsel, rn);
   }
 
   // 2. ORDER BY one column + small LIMIT: bounded top-k on the GPU.
@@ -1602,6 +1677,8 @@ static void run_join(Plan& plan, Query& q, const JoinSpec& js, fdb_result* res) 
   for (const SelItem& it : rest.items) all_agg = all_agg && it.agg >= 0;
   if (rest.distinct && (rest.has_group || all_agg))
     fail(FDB_E_SQL, "SELECT DISTINCT with aggregates or GROUP BY is not supported");
+  for (const SelItem& it : rest.items)
+    if (it.row_number && rest.has_group) fail(FDB_E_SQL, "ROW_NUMBER() with GROUP BY is not supported");
   if (rest.has_group) run_group_by(plan, joined, rest, res);
   else if (all_agg) run_aggregates(plan, joined, rest, res);
   else run_projection(plan, joined, rest, res);
@@ -1636,6 +1713,11 @@ void fdb_result::finalize() {
       for (size_t i = 0; i < c.str.size(); ++i) c.str_ptrs.push_back(c.nulls[i] ? nullptr : c.str[i].c_str());
     }
   }
+}
+
+const std::string& fdb_result::display_text() {
+  if (display_built_) return display_;
+  display_built_ = true;
   std::ostringstream o;
   std::vector<std::vector<std::string>> cells(rows, std::vector<std::string>(cols.size()));
   std::vector<size_t> w(cols.size());
@@ -1665,7 +1747,8 @@ void fdb_result::finalize() {
   }
   line();
   o << rows << " row" << (rows == 1 ? "" : "s") << "\n";
-  display = o.str();
+  display_ = o.str();
+  return display_;
 }
 
 namespace fdb {
@@ -1716,6 +1799,8 @@ fdb_result* run_sql(Ctx& c, const std::string& sql) {
     for (const SelItem& it : q.items) all_agg = all_agg && it.agg >= 0;
     if (q.distinct && (q.has_group || all_agg))
       fail(FDB_E_SQL, "SELECT DISTINCT with aggregates or GROUP BY is not supported");
+    for (const SelItem& it : q.items)
+      if (it.row_number && q.has_group) fail(FDB_E_SQL, "ROW_NUMBER() with GROUP BY is not supported");
     if (q.has_group) run_group_by(plan, rel, q, res.get());
     else if (all_agg) run_aggregates(plan, rel, q, res.get());
     else run_projection(plan, rel, q, res.get());

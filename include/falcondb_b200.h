@@ -211,7 +211,8 @@ int  fdb_table_column(const fdb_db* db, const char* table, const char* column,
  * *out is NULL on error.  Supported shapes (others fail with FDB_E_SQL):
  *   SELECT [DISTINCT] items FROM t [[INNER] | LEFT [OUTER] JOIN u ON t.k = u.k] [WHERE pred]
  *          [GROUP BY col] [ORDER BY col|alias|n [ASC|DESC] [NULLS FIRST|LAST], ...] [LIMIT n]
- *   items: *, col, COUNT(*), COUNT(col), COUNT(DISTINCT col), SUM/AVG/MIN/MAX(col) [AS a]
+ *   items: *, col, COUNT(*), COUNT(col), COUNT(DISTINCT col), SUM/AVG/MIN/MAX(col),
+ *          ROW_NUMBER() OVER ([ORDER BY col [ASC|DESC]]) [AS a]
  *   pred : col op literal, IS [NOT] NULL, [NOT] IN (...), [NOT] LIKE (Utf8), AND, OR,
  *          parentheses, and [NOT] EXISTS (SELECT ... FROM u WHERE u.k = t.k).
  * ORDER BY one FLOAT64 / INT64 column runs on the GPU (fdb_topk for LIMIT <= 4096,

@@ -201,3 +201,46 @@ def test_select_distinct_against_the_oracle(db, n):
     assert [None if null[k] else int(xv[k]) for k in keep] == [r.value(i, 0) for i in range(r.rows)]
     r = db.sql("SELECT DISTINCT dept FROM u")
     assert list(r.column(0)) == [W.DEPTS[c] for c in t["dept"].codes[O.distinct(t["dept"].codes)]]
+
+
+def _row_numbers(vals, desc):
+    """ROW_NUMBER() OVER (ORDER BY vals): try_dense_partition_sort
+    (window.rs:308-331) -- f64 order keys, ties by position -- via the oracle's
+    sort of the values as f64."""
+    rn = np.empty(len(vals), dtype=np.int64)
+    rn[O.sort(np.asarray(vals, dtype=np.float64), desc)] = np.arange(1, len(vals) + 1)
+    return rn
+
+
+@pytest.mark.parametrize("n", [20, 1_000_003])
+def test_row_number_over_order_by(db, n):
+    t = W.table_t(n, seed=6)
+    db.create_table("t", t)
+    r = db.sql("SELECT id, ROW_NUMBER() OVER (ORDER BY score DESC) AS rn FROM t")
+    assert r.rows == n
+    assert list(r.column(0)) == list(range(n))
+    assert np.array_equal(np.asarray(r.column(1)), _row_numbers(t["score"], True))
+    r = db.sql("SELECT ROW_NUMBER() OVER (ORDER BY salary) AS rn, id FROM t WHERE score > 30")
+    sel = np.flatnonzero(t["score"] > 30)
+    assert list(r.column(1)) == list(sel)
+    assert np.array_equal(np.asarray(r.column(0)), _row_numbers(t["salary"][sel], False))
+    r = db.sql("SELECT id, ROW_NUMBER() OVER (ORDER BY score DESC) AS rn FROM t ORDER BY rn LIMIT 5")
+    assert list(r.column(0)) == list(O.sort(t["score"], True)[:5])
+    r = db.sql("SELECT id, ROW_NUMBER() OVER () AS rn FROM t WHERE score < 10")
+    assert list(r.column(1)) == list(range(1, int((t["score"] < 10).sum()) + 1))
+
+
+def test_row_number_semantics(db):
+    # window.rs:978-995 restated without PARTITION BY: salaries 100, 120, 90,
+    # 80, 110 DESC -> 3, 1, 4, 5, 2.
+    db.create_table("t", {"salary": np.array([100, 120, 90, 80, 110], dtype=np.int64)})
+    r = db.sql("SELECT salary, ROW_NUMBER() OVER (ORDER BY salary DESC) AS rn FROM t")
+    assert list(r.column(1)) == [3, 1, 4, 5, 2]
+    # An INT64 key is read as f64 (expr.rs:232): 2^60 + 1, 2^60, 2^60 + 2 are one
+    # value there, so they number in row order.
+    big = np.array([2**60 + 1, 2**60, 2**60 + 2, 5], dtype=np.int64)
+    db.create_table("b", {"k": big})
+    assert list(db.sql("SELECT ROW_NUMBER() OVER (ORDER BY k) AS rn FROM b").column(0)) == [2, 3, 4, 1]
+    with pytest.raises(F.FalconError) as e:
+        db.sql("SELECT ROW_NUMBER() OVER (PARTITION BY k ORDER BY k) FROM b")
+    assert e.value.code == -5
