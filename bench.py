@@ -551,9 +551,10 @@ def run_secondary(args):
         db.drop_table("g")
     if args.workload in ("sort", "all"):
         # ORDER BY score DESC over 100M FLOAT64 rows, no LIMIT: an LSD radix
-        # sort of (order key, row) pairs.  Algorithmic bytes: the key build
-        # (read 8, write 12 per row), per digit pass the histogram read (8) and
-        # the scatter (read 12, write 12), and the row copy-out (read 4, write 4).
+        # sort of (order key, row) pairs.  Algorithmic bytes per row: the key
+        # build (read 8, write 12), per digit pass the histogram read (8) and
+        # the scatter (read 12, write 12), except that the last pass writes
+        # only the row (4) straight into the output.
         host_sc = W.table_t(n, seed=1)["score"]
         sc = torch.from_numpy(host_sc).to(dev)
         rows_out = torch.empty(n, dtype=torch.int32, device=dev)
@@ -570,7 +571,7 @@ def run_secondary(args):
         seen[r] = True
         assert bool(seen.all())
         del r, s_sorted, seen
-        nbytes = n * (20 + 32 * passes + 8)
+        nbytes = n * (20 + 32 * passes - 8)
         sample = 2_000_000
         hs = sc[:sample].cpu().numpy()
         t0 = time.perf_counter()
@@ -582,7 +583,9 @@ def run_secondary(args):
                                                  "cores": 1, "kind": "port",
                                                  "what": "oracle std::sort of (order key, row) pairs"}})
         # SELECT DISTINCT score (first occurrence per value, row order): the same
-        # radix sort on value keys, a run-head pass and a compaction.
+        # radix sort on value keys (every pass writes keys), a run-head pass
+        # (read 12 per row, a bit per row of mask) and the mask's compaction
+        # (4 bytes per kept row).
         dcount = torch.empty(1, dtype=torch.int64, device=dev)
         ms_d = _time_steps(lambda: ops.distinct(db, sc, n, rows=rows_out, count=dcount), K, Wm, stream, torch)
         kept = int(dcount.item())
@@ -590,7 +593,7 @@ def run_secondary(args):
         t0 = time.perf_counter()
         O.distinct(hs)
         cpu_d = time.perf_counter() - t0
-        line("distinct", ms_d, n * (20 + 32 * passes + 16) + kept * 4,
+        line("distinct", ms_d, n * (20 + 32 * passes + 12) + n // 4 + kept * 4,
              {"rows": n, "query": "SELECT DISTINCT score FROM t", "distinct_values": kept,
               "mrows_per_s": round(n / (ms_d / 1e3) / 1e6, 1),
               "cpu_sample": {"rows": sample, "mrows_per_s": round(sample / cpu_d / 1e6, 2), "cores": 1,

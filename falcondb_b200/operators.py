@@ -493,17 +493,16 @@ class LimitOp(Operator):
 
 
 class SortOp(Operator):
-    """ORDER BY one column [DESC] with a LIMIT, blocking (operators.rs:122-148):
-    the GPU top-k (execute_sort_limit's top_k path, sort.rs:59-115), ties broken
-    by row position in arrival order.  A sort without a LIMIT, or on several
-    keys, is not on the GPU path and raises."""
+    """ORDER BY one column [DESC] [LIMIT k], blocking (operators.rs:122-148):
+    with LIMIT k <= 4096 the GPU top-k (execute_sort_limit's top_k path,
+    sort.rs:59-115), otherwise the GPU radix sort of the FLOAT64 / INT64 key
+    (sort_merged -> try_typed_sort, sort.rs:118-133, 209-350) and then the
+    LIMIT.  Ties follow arrival order; several keys raise."""
 
     def __init__(self, db: Database, keys: Sequence[Tuple[str, bool]], limit: Optional[int],
                  nulls_last: Optional[bool] = None):
-        if len(keys) != 1 or limit is None:
-            raise FalconError(-5, "SortOp runs ORDER BY <one column> LIMIT k on the GPU")
-        if limit > 4096:
-            raise FalconError(-2, "LIMIT above 4096 is not supported by the GPU top-k")
+        if len(keys) != 1:
+            raise FalconError(-5, "SortOp orders by one column on the GPU")
         self.db = db
         self.key, self.desc = keys[0]
         self.limit = limit
@@ -522,8 +521,12 @@ class SortOp(Operator):
         n = b.row_count()
         if n == 0 or self.limit == 0:
             return []
-        rows, cnt = ops.topk(self.db, _arg(b.column(self.key)), n, self.limit, self.desc, self.nulls_last)
-        k = int(cnt.item())
+        if self.limit is not None and self.limit <= 4096:
+            rows, cnt = ops.topk(self.db, _arg(b.column(self.key)), n, self.limit, self.desc, self.nulls_last)
+            k = int(cnt.item())
+        else:
+            rows = ops.sort(self.db, _arg(b.column(self.key)), n, self.desc, self.nulls_last)
+            k = n if self.limit is None else min(n, self.limit)
         return [_gather(self.db, b, rows, k)] if k else []
 
     def name(self) -> str:
@@ -693,9 +696,10 @@ class AggregateOp(Operator):
 
 
 class DistinctOp(Operator):
-    """SELECT DISTINCT of one column, blocking (operators.rs:182-205): a Utf8
-    column through its dictionary-code presence bitmap, an Int64 one through
-    the hash GROUP BY.  Output in ascending order (dictionary order for Utf8)."""
+    """SELECT DISTINCT of one column, blocking (operators.rs:182-205 ->
+    dedup_batches, select.rs:238-457): each value's first row in arrival order,
+    on the GPU (fdb_distinct).  FLOAT64 NaNs are one value and -0.0 == +0.0;
+    all NULLs are one value."""
 
     def __init__(self, db: Database, column: str):
         self.db = db
@@ -711,31 +715,12 @@ class DistinctOp(Operator):
         if not held:
             return []
         b = _concat(self.db, held, [self.column])
-        c = b.column(self.column)
         n = b.row_count()
-        dev = torch.device("cuda", self.db.device)
-        if c.dtype == UTF8:
-            d = c.dictionary or []
-            bits = ops.distinct_codes(self.db, [_arg(c)], n, [], 0, len(d))
-            words = bits.cpu().numpy().view(np.uint64)
-            present = [i for i in range(len(d)) if (int(words[i >> 6]) >> (i & 63)) & 1]
-            has_null = bool(ops.filter_count(self.db, [_arg(c)], n, [ops.is_null(0)]).item())
-            codes = np.array(present + ([0xFFFFFFFF] if has_null else []), dtype=np.uint32).view(np.int32)
-            vw = None
-            if has_null:
-                w = np.zeros(max(1, (len(codes) + 63) // 64), dtype=np.uint64)
-                for i in range(len(present)):
-                    w[i >> 6] |= np.uint64(1) << np.uint64(i & 63)
-                vw = torch.from_numpy(w.view(np.int64)).to(dev)
-            col_ = tensor_column(torch.from_numpy(np.ascontiguousarray(codes)).to(dev), vw, d)
-            return [Batch({self.column: col_}, len(codes))]
-        if c.dtype != INT64:
-            raise FalconError(-7, "DISTINCT runs on Utf8 or Int64 columns")
-        out, ng = ops.group_by_i64(self.db, _arg(c), _arg(c), n)
-        recs = ops.to_records(out, GROUP_I64_DTYPE, int(ng.item()))
-        keys = np.sort(recs["key"])
-        return [Batch({self.column: tensor_column(torch.from_numpy(np.ascontiguousarray(keys)).to(dev))},
-                      len(keys))]
+        if n == 0:
+            return []
+        rows, cnt = ops.distinct(self.db, _arg(b.column(self.column)), n)
+        k = int(cnt.item())
+        return [_gather(self.db, b, rows, k)] if k else []
 
     def name(self) -> str:
         return "Distinct"

@@ -33,6 +33,14 @@ def values(batches, name="v"):
     return out
 
 
+def fbatch(vals):
+    return Batch({"f": tensor_column(dev(np.asarray(vals, dtype=np.float64)))}, len(vals))
+
+
+def fvalues(batches):
+    return np.concatenate([b.column("f").to_numpy() for b in batches]) if batches else np.zeros(0)
+
+
 def run(ops_, *batches):
     return Pipeline(ops_, chunk_rows=CH).run(list(batches))
 
@@ -65,6 +73,32 @@ def test_sort_ties_follow_arrival_order(db):
 def test_distinct_removes_duplicates_across_chunks(db):
     got = run([DistinctOp(db, "v")], vbatch([i % 100 for i in range(5000)]))
     assert values(got) == list(range(100))
+
+
+def test_sort_without_a_limit_and_above_the_top_k_bound(db):
+    """SortOp with no LIMIT, or one above 4096, runs the GPU radix sort
+    (try_typed_sort, sort.rs:209-350): the oracle's full sort, ties in
+    arrival order."""
+    v = np.random.default_rng(8).integers(0, 50, 20_000)
+    got = run([SortOp(db, [("v", True)], None)], vbatch(v))
+    assert values(got) == list(v[O.sort(v, True)])
+    got = run([SortOp(db, [("v", False)], 10_000), LimitOp(9_990, 100)], vbatch(v))
+    assert values(got) == list(v[O.sort(v, False)][9_990:10_000])
+    f = np.random.default_rng(9).standard_normal(9_000)
+    got = fvalues(run([SortOp(db, [("f", False)], None)], fbatch(f)))
+    assert np.array_equal(got, f[O.sort(f, False)])
+
+
+def test_distinct_keeps_first_occurrences_in_arrival_order(db):
+    """dedup_batches (select.rs:238-457): first occurrence wins, in the order
+    rows arrive across chunks; float NaNs are one value, -0.0 == +0.0."""
+    v = np.random.default_rng(4).integers(0, 3000, 20_000)
+    assert values(run([DistinctOp(db, "v")], vbatch(v))) == list(v[O.distinct(v)])
+    f = np.array([2.5, np.nan, -0.0, 2.5, 0.0, np.nan, 1.0] * 700)
+    got = fvalues(run([DistinctOp(db, "f")], fbatch(f)))
+    exp = f[O.distinct(f)]
+    assert len(got) == len(exp) == 4
+    assert np.array_equal(got, exp, equal_nan=True)
 
 
 def test_config0_filter_group_by_pipeline(db):
