@@ -406,6 +406,7 @@ class Database:
         self._h = h
         self.device = device
         self._keep: Dict[str, Any] = {}
+        self._schemas: Dict[str, List[Tuple[str, int, bool]]] = {}
 
     @property
     def handle(self) -> C.c_void_p:
@@ -473,6 +474,9 @@ class Database:
         check(rc)
         # Keep host buffers referenced until the upload is known complete.
         self._keep[name] = keep
+        self._schemas[name] = [(cname, UTF8 if isinstance(col, Utf8) else
+                                (FLOAT64 if np.asarray(np.ma.getdata(col)).dtype.kind == "f" else INT64),
+                                isinstance(col, np.ma.MaskedArray)) for cname, col in columns.items()]
         self._dicts = getattr(self, "_dicts", {})
         for cname, col in columns.items():
             if isinstance(col, Utf8):
@@ -503,6 +507,22 @@ class Database:
     def drop_table(self, name: str) -> None:
         check(lib().fdb_table_drop(self.handle, name.encode()))
         self._keep.pop(name, None)
+        self._schemas.pop(name, None)
+
+    def tables(self) -> List[str]:
+        """Names of the tables created through :meth:`create_table`, sorted."""
+        return sorted(self._schemas)
+
+    def table_info(self, name: str) -> Optional[Dict[str, Any]]:
+        """Name, row count and columns (name, type, nullable) of a table created
+        through :meth:`create_table` (Database::table_info, db.rs:2727-2741);
+        None if there is no such table."""
+        cols = self._schemas.get(name)
+        if cols is None:
+            return None
+        tname = {INT64: "Int64", FLOAT64: "Float64", UTF8: "Utf8"}
+        return {"name": name, "row_count": self.table_row_count(name), "col_count": len(cols),
+                "columns": [{"name": c, "data_type": tname[d], "nullable": nl} for c, d, nl in cols]}
 
     def column(self, table: str, column: str) -> DevColumn:
         raw = fdb_dev_column()
