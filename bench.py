@@ -619,12 +619,78 @@ def run_secondary(args):
                             "value": round(statistics.median(times), 4), "unit": "ms", "result_rows": r.rows,
                             "steps": K, "warmup": Wm, "higher_is_better": False})
             db.drop_table("s")
+    if args.workload in ("rest", "all"):
+        run_rest(args, db, out)
     if args.workload in ("serve", "all"):
         run_serving(args, db, out, peak)
     if args.workload == "serve_single":
         run_serving_single(args, db, out)
     db.close()
     return out
+
+
+def run_rest(args, db, out):
+    """POST /sql through the REST front end: 32 closed-loop HTTP clients send
+    2000 requests drawn from the four serving templates (random thresholds)
+    over a 10M-row table and a 1M x 10M join.  Once with the serving loop
+    batching template requests, once with every request through fdb_sql (the
+    reference server's one-request-at-a-time shape).  Client-side latency and
+    throughput; every answer is checked against a fdb_sql run of the same text."""
+    import json
+    import urllib.request
+    from concurrent.futures import ThreadPoolExecutor
+
+    from falcondb_b200 import rest as R, workloads as W
+
+    db.create_table("t", W.table_t(10_000_000, seed=21))
+    b, p = W.join_tables(1_000_000, 10_000_000, seed=22)
+    db.create_table("b", b)
+    db.create_table("p", p)
+    rng = np.random.default_rng(23)
+    shapes = ["SELECT COUNT(*) FROM t WHERE score > {x}",
+              "SELECT dept, COUNT(*), SUM(score), AVG(salary) FROM t WHERE score > {x} GROUP BY dept",
+              "SELECT id, score FROM t WHERE score < {x} ORDER BY score DESC LIMIT 10",
+              "SELECT COUNT(*), SUM(b.payload) FROM p JOIN b ON p.key = b.key WHERE p.value < {y}"]
+    texts = []
+    for _ in range(2000):
+        x = round(float(rng.uniform(0, 100)), 2)
+        texts.append(shapes[int(rng.integers(0, 4))].format(x=x, y=f"{x / 100:.4f}"))
+    check = {t: db.sql(t).rows for t in set(texts[:50])}
+
+    def post(port, sql):
+        req = urllib.request.Request(f"http://127.0.0.1:{port}/sql", data=json.dumps({"sql": sql}).encode(),
+                                     method="POST", headers={"Content-Type": "application/json"})
+        t0 = time.perf_counter()
+        with urllib.request.urlopen(req, timeout=120) as r:
+            body = json.loads(r.read())
+        return sql, body, (time.perf_counter() - t0) * 1e3
+
+    res = {}
+    for batching in (True, False):
+        srv = R.RestServer(db, port=0, batching=batching, max_batch=64, slots=2).start()
+        try:
+            with ThreadPoolExecutor(32) as ex:
+                list(ex.map(lambda s_: post(srv.port, s_), texts[:64]))  # warm-up
+                t0 = time.perf_counter()
+                got = list(ex.map(lambda s_: post(srv.port, s_), texts))
+                wall = time.perf_counter() - t0
+        finally:
+            srv.stop()
+        for sql, body, _ in got:
+            if sql in check:
+                assert body["row_count"] == check[sql], sql
+        lat = np.array([g[2] for g in got])
+        served = sum(1 for g in got if g[1]["path"] == "serving")
+        res[batching] = {"qps": round(len(texts) / wall, 1), "p50_ms": round(float(np.percentile(lat, 50)), 3),
+                         "p99_ms": round(float(np.percentile(lat, 99)), 3), "served": served,
+                         "mean_batch": round(float(np.mean([g[1].get("batch_size", 1) for g in got])), 2)}
+    out.append({"metric": "REST /sql throughput", "workload": "rest_sql", "value": res[True]["qps"],
+                "unit": "requests/s", "higher_is_better": True, "requests": len(texts), "clients": 32,
+                "batched": res[True], "sql_only": res[False],
+                "speedup_vs_sql_only": round(res[True]["qps"] / res[False]["qps"], 2),
+                "tables": "t: 10M rows; join: 1M build x 10M probe"})
+    for name in ("t", "b", "p"):
+        db.drop_table(name)
 
 
 def run_serving(args, db, out, peak):
@@ -795,7 +861,8 @@ def main():
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--cpu-threads", type=int, default=0)
     ap.add_argument("--workload", default="scan",
-                    choices=["scan", "filter_groupby", "join", "groupby", "batch", "sort", "serve", "serve_single", "all"],
+                    choices=["scan", "filter_groupby", "join", "groupby", "batch", "sort", "rest", "serve", "serve_single",
+                             "all"],
                     help="scan = the headline line; the others print per-operator lines")
     ap.add_argument("--load-factor", type=float, default=0.5)
     ap.add_argument("--serve-queries", type=int, default=10_000)

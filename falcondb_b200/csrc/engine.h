@@ -193,6 +193,9 @@ void op_distinct(Ctx& c, const fdb_dev_column& col, uint64_t n, uint32_t* d_rows
 // op_sort with, when int_as_f64, an INT64 column ordered by its f64 value.
 void op_sort_keyed(Ctx& c, const fdb_dev_column& col, uint64_t n, bool desc, bool nulls_last, bool int_as_f64,
                    uint32_t* d_rows);
+// Join row pairs (d_left[i], d_right[i]) put in (left, right) order in place;
+// d_right may be null (left rows only).
+void op_sort_row_pairs(Ctx& c, uint32_t* d_left, uint32_t* d_right, uint64_t n);
 // d_rn[list[order[j]]] = j + 1 for j < n (order / list null = identity).
 void op_row_numbers(Ctx& c, const uint32_t* d_order, const uint32_t* d_list, uint64_t n, int64_t* d_rn);
 

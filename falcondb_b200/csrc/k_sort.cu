@@ -553,6 +553,52 @@ static void set_scatter_smem() {
                                 (int)sizeof(ScatterSmem)));
 }
 
+// Join row pairs as sort keys: (left << 32) | right (right = 0 without one).
+__global__ void pair_key_kernel(const uint32_t* __restrict__ left, const uint32_t* __restrict__ right, uint32_t n,
+                                uint64_t* keys, uint32_t* vals, unsigned long long* vary) {
+  unsigned long long o = 0, a = ~0ull;
+  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    const uint64_t k = ((uint64_t)left[i] << 32) | (right ? right[i] : 0u);
+    keys[i] = k;
+    vals[i] = i;
+    o |= k;
+    a &= k;
+  }
+#pragma unroll
+  for (int s = 16; s > 0; s >>= 1) {
+    o |= __shfl_xor_sync(0xffffffffu, o, s);
+    a &= __shfl_xor_sync(0xffffffffu, a, s);
+  }
+  if ((threadIdx.x & 31) == 0) {
+    atomicOr(&vary[0], o);
+    atomicAnd(&vary[1], a);
+  }
+}
+
+__global__ void pair_unpack_kernel(const uint64_t* __restrict__ keys, uint32_t n, uint32_t* left, uint32_t* right) {
+  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    const uint64_t k = keys[i];
+    left[i] = (uint32_t)(k >> 32);
+    if (right) right[i] = (uint32_t)k;
+  }
+}
+
+void op_sort_row_pairs(Ctx& c, uint32_t* d_left, uint32_t* d_right, uint64_t n) {
+  if (n == 0) return;
+  if (n >= 0xFFFFFFFFull) fail(FDB_E_ARG, "a sort addresses rows as uint32");
+  set_scatter_smem();
+  c.ensure_scratch(c.scratch_top + sort_scratch_bytes(n, false));
+  const uint32_t m = (uint32_t)n;
+  const unsigned g = (unsigned)std::max<uint64_t>(1, std::min<uint64_t>((n + 255) / 256, (uint64_t)c.sm_count * 8));
+  auto keys = [&](uint64_t* k, uint32_t* v, unsigned long long* vary) {
+    pair_key_kernel<<<g, 256, 0, c.stream>>>(d_left, d_right, m, k, v, vary);
+  };
+  const uint64_t* sorted = nullptr;
+  radix_sort_pairs(c, m, keys, nullptr, &sorted, nullptr);
+  pair_unpack_kernel<<<g, 256, 0, c.stream>>>(sorted, m, d_left, d_right);
+  FDB_CUDA(cudaGetLastError());
+}
+
 // rows[i] = position of row i in the order: ROW_NUMBER() OVER (ORDER BY ..)
 // numbers the rows 1..n in sorted order (rank_dense, window.rs:259-300).
 __global__ void row_number_kernel(const uint32_t* order, const uint32_t* list, uint32_t n, int64_t* rn) {

@@ -1263,6 +1263,7 @@ static void emit_rows(Plan& plan, const Rel& rel, const std::vector<int>& outcol
     uint32_t* pos = plan.dev<uint32_t>(n);
     uint64_t* dcount = plan.dev<uint64_t>(1);
     op_distinct(plan.c, g, n, pos, dcount);
+    plan.c.scratch_reset();  // the sort's working memory is free for the next operator
     plan.check();
     const uint64_t k = plan.one(dcount);
     uint32_t* kept = pos;
@@ -1384,6 +1385,7 @@ static void run_projection(Plan& plan, const Rel& rel_in, const Query& q, fdb_re
     }
     uint32_t* order = plan.dev<uint32_t>(nsel);
     op_sort_keyed(plan.c, g, nsel, w.second->worder.desc, false, true, order);
+    plan.c.scratch_reset();
     op_row_numbers(plan.c, order, list, nsel, rn);
   }
 
@@ -1442,6 +1444,7 @@ static void run_projection(Plan& plan, const Rel& rel_in, const Query& q, fdb_re
       uint32_t* order = plan.dev<uint32_t>(nsel);
       if (all_rows) {
         op_sort(plan.c, rel.cols[oc].dev, n, o.desc, o.nulls_last, order);
+        plan.c.scratch_reset();
       } else {
         const RelCol& ocol = rel.cols[oc];
         uint64_t* vals = plan.dev<uint64_t>(nsel);
@@ -1453,6 +1456,7 @@ static void run_projection(Plan& plan, const Rel& rel_in, const Query& q, fdb_re
         g.validity = valid;
         uint32_t* local = plan.dev<uint32_t>(nsel);
         op_sort(plan.c, g, nsel, o.desc, o.nulls_last, local);
+        plan.c.scratch_reset();
         fdb_dev_column rows_col{};
         rows_col.dtype = FDB_UTF8;  // 4-byte gather of row numbers
         rows_col.values = d_rows;
@@ -1622,22 +1626,10 @@ static void run_join(Plan& plan, Query& q, const JoinSpec& js, fdb_result* res) 
   if (got != npairs) fail(FDB_E_GENERIC, "join pair count changed between passes");
   // Pair order from the device is unspecified: order by (left row, right row)
   // so the joined relation is deterministic (the reference probes left rows in
-  // order, join.rs:297-375).
-  std::vector<uint32_t> hl = plan.to_host(dl, npairs), hr;
-  if (dr) hr = plan.to_host(dr, npairs);
-  std::vector<uint64_t> ord(npairs);
-  std::iota(ord.begin(), ord.end(), 0);
-  std::sort(ord.begin(), ord.end(), [&](uint64_t a, uint64_t b) {
-    if (hl[a] != hl[b]) return hl[a] < hl[b];
-    return !hr.empty() && hr[a] < hr[b];
-  });
-  std::vector<uint32_t> sl(npairs), sr(hr.empty() ? 0 : npairs);
-  for (uint64_t i = 0; i < npairs; ++i) {
-    sl[i] = hl[ord[i]];
-    if (!hr.empty()) sr[i] = hr[ord[i]];
-  }
-  if (npairs) FDB_CUDA(cudaMemcpyAsync(dl, sl.data(), npairs * 4, cudaMemcpyHostToDevice, c.stream));
-  if (dr && npairs) FDB_CUDA(cudaMemcpyAsync(dr, sr.data(), npairs * 4, cudaMemcpyHostToDevice, c.stream));
+  // order, join.rs:297-375).  The GPU radix sort does it in place.
+  c.scratch_reset();
+  op_sort_row_pairs(c, dl, dr, npairs);
+  c.scratch_reset();
 
   Rel joined;
   joined.nrows = npairs;
