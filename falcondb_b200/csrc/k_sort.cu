@@ -452,8 +452,8 @@ static void launch_sort_keys(Ctx& c, const DevCol& col, const uint32_t* sel, uin
   sort_key_kernel<DT, MODE><<<grid, 256, 0, c.stream>>>(col, sel, m, keys, vals, vary);
 }
 
-// Scratch a sort of up to n pairs needs (see SortWork), with or without the
-// NULL split.
+// Scratch a sort of up to n pairs takes: two (key, row) buffers, the
+// histogram and its scan sums, and with the NULL split its mask and row lists.
 static size_t sort_scratch_bytes(uint64_t n, bool nullable) {
   const uint64_t words = (n + 63) / 64;
   const uint64_t ntiles = (n + kSortTile - 1) / kSortTile;
