@@ -168,7 +168,7 @@ struct CallScope {
   }
 };
 
-size_t default_scratch(Ctx& c) { return (size_t)64 << 20; }
+size_t default_scratch(Ctx&) { return (size_t)64 << 20; }
 
 void need(bool ok, const char* msg) {
   if (!ok) fail(FDB_E_ARG, msg);
