@@ -407,6 +407,7 @@ class Database:
         self.device = device
         self._keep: Dict[str, Any] = {}
         self._schemas: Dict[str, List[Tuple[str, int, bool]]] = {}
+        self.generation = 0  # bumped by every table create / drop (catalog caches check it)
 
     @property
     def handle(self) -> C.c_void_p:
@@ -474,6 +475,7 @@ class Database:
         check(rc)
         # Keep host buffers referenced until the upload is known complete.
         self._keep[name] = keep
+        self.generation += 1
         self._schemas[name] = [(cname, UTF8 if isinstance(col, Utf8) else
                                 (FLOAT64 if np.asarray(np.ma.getdata(col)).dtype.kind == "f" else INT64),
                                 isinstance(col, np.ma.MaskedArray)) for cname, col in columns.items()]
@@ -493,6 +495,7 @@ class Database:
     def create_table_from_pointers(self, name: str, specs: List[Tuple[str, int, int]], nrows: int) -> int:
         """Create a table from raw host pointers: ``specs`` = [(name, dtype, ptr)]
         (dtype INT64 / FLOAT64; UTF8 needs :meth:`create_table`)."""
+        self.generation += 1
         cols = (fdb_column * max(1, len(specs)))()
         for j, (cname, dtype, ptr) in enumerate(specs):
             cols[j].name = cname.encode()
@@ -506,6 +509,7 @@ class Database:
 
     def drop_table(self, name: str) -> None:
         check(lib().fdb_table_drop(self.handle, name.encode()))
+        self.generation += 1
         self._keep.pop(name, None)
         self._schemas.pop(name, None)
 

@@ -115,13 +115,32 @@ class Served:
 
 
 class _Catalog:
-    """What the matcher needs to know about a table: its columns' types, NULLs,
-    device views and dictionaries."""
+    """What the matcher needs to know about a table: its columns' types, NULLs
+    and device views.  Lookups are remembered until the database's
+    ``generation`` changes (a table created or dropped), so a request that
+    matches a template makes no library call that waits on a running query."""
 
     def __init__(self, db: Database):
         self.db = db
+        self._gen = None
+        self._cols: Dict[Tuple[str, str], Any] = {}
+        self._names: Dict[str, Optional[List[str]]] = {}
+
+    def _fresh(self) -> None:
+        gen = getattr(self.db, "generation", None)
+        if gen is None or gen != self._gen:
+            self._cols.clear()
+            self._names.clear()
+            self._gen = gen
 
     def col(self, table: str, name: str):
+        self._fresh()
+        key = (table, name)
+        if key not in self._cols:
+            self._cols[key] = self._lookup(table, name)
+        return self._cols[key]
+
+    def _lookup(self, table: str, name: str):
         info = self.db.table_info(table)
         if info is None:
             return None
@@ -135,15 +154,19 @@ class _Catalog:
         return None
 
     def names(self, table: str) -> Optional[List[str]]:
-        info = self.db.table_info(table)
-        return None if info is None else [c["name"] for c in info["columns"]]
+        self._fresh()
+        if table not in self._names:
+            info = self.db.table_info(table)
+            self._names[table] = None if info is None else [c["name"] for c in info["columns"]]
+        return self._names[table]
 
 
-def match_template(db: Database, sql: str, join_tables: Optional[Callable] = None) -> Optional[Served]:
+def match_template(db: Database, sql: str, join_tables: Optional[Callable] = None,
+                   catalog: Optional[_Catalog] = None) -> Optional[Served]:
     """The serving template `sql` is, bound to `db`'s resident columns; None when
     it is not one (or a column is nullable, of another type, or out of range)."""
     s = _norm(sql)
-    cat = _Catalog(db)
+    cat = catalog if catalog is not None else _Catalog(db)
     m = _PATTERNS["count"].match(s)
     if m:
         t, c, x = m.groups()
@@ -254,6 +277,8 @@ class RestServer:
         self.batching = batching
         self._server = serving.Server(db, max_batch=max_batch, slots=slots) if batching else None
         self._joins: Dict[Tuple[str, str, str], ops.HashTable] = {}
+        self._catalog = _Catalog(db)
+        self._join_gen = getattr(db, "generation", None)
         self._lock = threading.Lock()        # join-table cache and the table catalog
         self._inflight = 0                   # served queries not yet answered
         self._idle = threading.Condition(self._lock)
@@ -349,7 +374,16 @@ class RestServer:
         return 200, {"dropped": name}
 
     def _join_table(self, b: str, key: str, payload: str, bkey, bpay) -> int:
-        """The resident build table of b(key -> payload), built on first use."""
+        """The resident build table of b(key -> payload), built on first use and
+        rebuilt after any table is created or dropped (self._lock held)."""
+        gen = getattr(self.db, "generation", None)
+        if gen != self._join_gen:
+            while self._inflight:  # served joins may still read the old tables
+                self._idle.wait()
+            for h in self._joins.values():
+                h.free()
+            self._joins.clear()
+            self._join_gen = gen
         k = (b, key, payload)
         h = self._joins.get(k)
         if h is None:
@@ -364,7 +398,7 @@ class RestServer:
         if self._server is not None:
             with self._lock:
                 try:
-                    served = match_template(self.db, sql, self._join_table)
+                    served = match_template(self.db, sql, self._join_table, self._catalog)
                 except FalconError:
                     served = None
                 if served is not None:

@@ -116,6 +116,42 @@ def test_template_text_matching():
     assert R._lit("50") == 50.0 and R._lit("-2.5") == -2.5
 
 
+class _ColDb:
+    """Counts the catalog calls the template matcher makes."""
+
+    def __init__(self):
+        self.generation = 0
+        self.calls = 0
+
+    def table_info(self, name):
+        self.calls += 1
+        if name != "t":
+            return None
+        return {"name": "t", "row_count": 10, "col_count": 1,
+                "columns": [{"name": "score", "data_type": "Float64", "nullable": False}]}
+
+    def column(self, table, name):
+        self.calls += 1
+
+        class _Dc:
+            ptr, validity = 4096, 0
+        return _Dc()
+
+
+def test_catalog_lookups_are_cached_per_generation():
+    db = _ColDb()
+    cat = R._Catalog(db)
+    first = cat.col("t", "score")
+    assert first[0] == R.FLOAT64 and first[2] == 10
+    n = db.calls
+    assert cat.col("t", "score") is first and db.calls == n  # no library call on a hit
+    assert cat.col("t", "nope") is None
+    db.generation += 1  # a table was created or dropped
+    cat.col("t", "score")
+    assert db.calls > n + 1
+    assert cat.names("t") == ["score"] and cat.names("u") is None
+
+
 def test_join_threshold_is_exact():
     """x with x / 100 == v in f64, as the serving join compares value < x / 100."""
     for v in [0.0, 0.25, 0.29, 0.1, 0.3, 0.7, 0.99, 1e-9, 0.123456789]:
