@@ -212,6 +212,8 @@ def match_template(db: Database, sql: str, join_tables: Optional[Callable] = Non
         if not key or key[0] != FLOAT64:
             return None
         names = cat.names(t) if sel == "*" else [c.strip() for c in sel.split(",")]
+        if names is None or len(set(names)) != len(names):
+            return None  # a repeated column is renamed by fdb_sql's result: let it answer
         outs = [cat.col(t, n) for n in names]
         if any(o is None for o in outs):
             return None
