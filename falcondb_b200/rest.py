@@ -326,7 +326,21 @@ class RestServer:
         tables; returns the serving loop's statistics (None without batching)."""
         self._http.shutdown()
         self._http.server_close()
+        return self._close()
+
+    def serve_forever(self) -> None:
+        """Serve on the calling thread until interrupted, then shut down as stop() does."""
+        try:
+            self._http.serve_forever()
+        except KeyboardInterrupt:
+            pass
+        finally:
+            self._http.server_close()
+            self._close()
+
+    def _close(self):
         stats = self._server.stop() if self._server else None
+        self._server = None
         for h in self._joins.values():
             h.free()
         self._joins.clear()
@@ -423,3 +437,48 @@ class RestServer:
         res = self.db.sql(sql)
         return 200, {"columns": list(res.columns), "rows": res.to_rows(), "row_count": res.rows,
                      "elapsed_ms": int((time.perf_counter() - t0) * 1e3), "path": "sql"}
+
+
+def _parse_bind(bind: str) -> Tuple[str, int]:
+    """host:port as FALCONDB_BIND gives it (server.rs:178, default 127.0.0.1:8080)."""
+    host, _, port = bind.rpartition(":")
+    if not host or not port.isdigit():
+        raise ValueError(f"FALCONDB_BIND must be host:port, got {bind!r}")
+    return host, int(port)
+
+
+def _parse_loads(args: List[str]) -> List[Tuple[str, str]]:
+    """`table=path.parquet` arguments: the tables to load before serving."""
+    out = []
+    for a in args:
+        table, sep, path = a.partition("=")
+        if not sep or not table or not path:
+            raise ValueError(f"expected table=path.parquet, got {a!r}")
+        out.append((table, path))
+    return out
+
+
+def main(argv: Optional[List[str]] = None) -> None:
+    """Run the server as the reference's binary does: bind from FALCONDB_BIND,
+    one database on GPU 0; `table=path.parquet` arguments are loaded first."""
+    import os
+    import sys
+
+    from .parquet import load_parquet
+
+    host, port = _parse_bind(os.environ.get("FALCONDB_BIND", "127.0.0.1:8080"))
+    loads = _parse_loads(list(sys.argv[1:] if argv is None else argv))
+    db = Database(0)
+    for table, path in loads:
+        n = load_parquet(db, path, table)
+        print(f"loaded {n} rows into '{table}'")
+    srv = RestServer(db, host=host, port=port)
+    print(f"falcondb server listening on http://{host}:{srv.port}")
+    try:
+        srv.serve_forever()
+    finally:
+        db.close()
+
+
+if __name__ == "__main__":
+    main()

@@ -152,6 +152,16 @@ def test_catalog_lookups_are_cached_per_generation():
     assert cat.names("t") == ["score"] and cat.names("u") is None
 
 
+def test_command_line_parsing():
+    assert R._parse_bind("127.0.0.1:8080") == ("127.0.0.1", 8080)
+    assert R._parse_bind("0.0.0.0:9") == ("0.0.0.0", 9)
+    with pytest.raises(ValueError):
+        R._parse_bind("8080")
+    assert R._parse_loads(["t=/data/t.parquet", "b=b.parquet"]) == [("t", "/data/t.parquet"), ("b", "b.parquet")]
+    with pytest.raises(ValueError):
+        R._parse_loads(["t.parquet"])
+
+
 def test_join_threshold_is_exact():
     """x with x / 100 == v in f64, as the serving join compares value < x / 100."""
     for v in [0.0, 0.25, 0.29, 0.1, 0.3, 0.7, 0.99, 1e-9, 0.123456789]:
