@@ -572,16 +572,18 @@ def run_secondary(args):
         assert bool(seen.all())
         del r, s_sorted, seen
         nbytes = n * (20 + 32 * passes - 8)
-        sample = 2_000_000
+        sample = 10_000_000 if n >= 10_000_000 else n
         hs = sc[:sample].cpu().numpy()
+        threads = args.cpu_threads or O.hardware_threads()
         t0 = time.perf_counter()
-        O.sort(hs, True)
+        O.ref_sort(hs, True, threads)
         cpu_s = time.perf_counter() - t0
         line("sort", ms, nbytes, {"rows": n, "query": "SELECT score FROM t ORDER BY score DESC",
                                   "digit_passes": passes, "mrows_per_s": round(n / (ms / 1e3) / 1e6, 1),
                                   "cpu_sample": {"rows": sample, "mrows_per_s": round(sample / cpu_s / 1e6, 2),
-                                                 "cores": 1, "kind": "port",
-                                                 "what": "oracle std::sort of (order key, row) pairs"}})
+                                                 "cores": threads, "kind": "port",
+                                                 "what": "reference-shaped sort: (order key, row) pair loop, "
+                                                         "parallel tuple sort (oracle/refengine.cpp ref_sort)"}})
         # SELECT DISTINCT score (first occurrence per value, row order): the same
         # radix sort on value keys (every pass writes keys), a run-head pass
         # (read 12 per row, a bit per row of mask) and the mask's compaction
@@ -590,13 +592,14 @@ def run_secondary(args):
         ms_d = _time_steps(lambda: ops.distinct(db, sc, n, rows=rows_out, count=dcount), K, Wm, stream, torch)
         kept = int(dcount.item())
         assert kept == int(torch.unique(sc).numel())
+        hs_d = hs[:2_000_000]
         t0 = time.perf_counter()
-        O.distinct(hs)
+        O.distinct(hs_d)
         cpu_d = time.perf_counter() - t0
         line("distinct", ms_d, n * (20 + 32 * passes + 12) + n // 4 + kept * 4,
              {"rows": n, "query": "SELECT DISTINCT score FROM t", "distinct_values": kept,
               "mrows_per_s": round(n / (ms_d / 1e3) / 1e6, 1),
-              "cpu_sample": {"rows": sample, "mrows_per_s": round(sample / cpu_d / 1e6, 2), "cores": 1,
+              "cpu_sample": {"rows": len(hs_d), "mrows_per_s": round(len(hs_d) / cpu_d / 1e6, 2), "cores": 1,
                              "kind": "port", "what": "oracle hash-set first-occurrence scan"}})
         del rows_out
         torch.cuda.empty_cache()

@@ -43,6 +43,7 @@ _SIGS = {
     "ref_count_cmp_f64": (U64, [P, U64, C.c_int, C.c_double]),
     "ref_present_codes": (None, [P, U64, C.c_uint32, C.c_int, P]),
     "ref_topk": (U64, [C.c_int, P, U64, C.c_uint32, C.c_int, P]),
+    "ref_sort": (None, [C.c_int, P, P, U64, C.c_int, C.c_int, C.c_int, P]),
     "ref_filter_group_codes": (None, [P, P, P, U64, C.c_uint32, C.c_int, C.c_double, C.c_int, P, P, P]),
     "ref_join_agg": (None, [P, P, U64, P, P, U64, C.c_int, C.c_int, P, P, P]),
     "ref_group_i64": (U64, [P, P, U64, C.c_int]),
@@ -266,6 +267,19 @@ def ref_topk(values, k, desc):
     out = np.zeros(max(1, k), np.uint32)
     m = lib().ref_topk(dtype, _p(v), len(v), k, int(desc), _p(out))
     return out[:m]
+
+
+def ref_sort(values, desc, threads, nulls_last=None, validity=None) -> np.ndarray:
+    """The reference-shaped parallel full sort (ref_sort): row numbers in order."""
+    v = np.ascontiguousarray(values)
+    dtype = 2 if v.dtype.kind == "f" else 1
+    v = v.astype(np.float64 if dtype == 2 else np.int64, copy=False)
+    if nulls_last is None:
+        nulls_last = desc
+    out = np.zeros(max(1, len(v)), dtype=np.uint32)
+    lib().ref_sort(dtype, _p(v), _p(_c(validity, np.uint64)), len(v), int(desc), int(nulls_last), int(threads),
+                   _p(out))
+    return out[:len(v)]
 
 
 def ref_filter_group_codes(codes, score, salary, dict_len, op, lit, threads):

@@ -407,4 +407,47 @@ uint64_t ref_group_i64(const int64_t* keys, const double* vals, uint64_t n, int 
   return all.size();
 }
 
+// SELECT col ORDER BY col [DESC] (no LIMIT): try_typed_sort's pair loop
+// (sort.rs:270-287, 326-345: (order key, row) pairs of the non-NULL rows, NULL
+// rows collected apart, serially), then the pairs sorted as tuples in parallel
+// (sort_pairs_ord -> par_sort_unstable, sort.rs:692-698; here one std::sort
+// per thread's run and parallel pairwise merges), then assemble (773-791).
+void ref_sort(int dtype, const void* values, const uint64_t* validity, uint64_t n, int desc, int nulls_last,
+              int threads, uint32_t* out) {
+  typedef std::pair<uint64_t, uint32_t> P;
+  std::vector<P> pairs;
+  pairs.reserve(n);
+  std::vector<uint32_t> nulls;
+  for (uint64_t i = 0; i < n; ++i) {
+    if (validity && !((validity[i >> 6] >> (i & 63)) & 1ull)) {
+      nulls.push_back((uint32_t)i);
+      continue;
+    }
+    uint64_t key = dtype == 2 ? ord_f64(static_cast<const double*>(values)[i])
+                              : ((uint64_t)static_cast<const int64_t*>(values)[i] ^ (1ull << 63));
+    pairs.emplace_back(desc ? ~key : key, (uint32_t)i);
+  }
+  const uint64_t m = pairs.size();
+  const uint64_t runs = std::max<uint64_t>(1, std::min<uint64_t>((uint64_t)std::max(threads, 1), m / 4096 + 1));
+  std::vector<uint64_t> bound(runs + 1);
+  for (uint64_t r = 0; r <= runs; ++r) bound[r] = m * r / runs;
+  par_for(runs, threads, [&](uint64_t r) { std::sort(pairs.begin() + bound[r], pairs.begin() + bound[r + 1]); });
+  std::vector<P> tmp(m);
+  for (uint64_t width = 1; width < runs; width *= 2) {
+    const uint64_t merges = (runs + 2 * width - 1) / (2 * width);
+    par_for(merges, threads, [&](uint64_t j) {
+      const uint64_t a = bound[std::min(runs, 2 * width * j)], b = bound[std::min(runs, 2 * width * j + width)],
+                     e = bound[std::min(runs, 2 * width * j + 2 * width)];
+      std::merge(pairs.begin() + a, pairs.begin() + b, pairs.begin() + b, pairs.begin() + e, tmp.begin() + a);
+    });
+    pairs.swap(tmp);
+  }
+  uint64_t o = 0;
+  if (!nulls_last)
+    for (uint32_t r : nulls) out[o++] = r;
+  for (const P& p : pairs) out[o++] = p.second;
+  if (nulls_last)
+    for (uint32_t r : nulls) out[o++] = r;
+}
+
 }  // extern "C"

@@ -325,6 +325,23 @@ def test_distinct_float_equality():
     assert list(O.distinct(v)) == [0, 1, 4, 5, 6]
 
 
+@pytest.mark.parametrize("threads", [1, 3, 8])
+def test_reference_engine_sort_agrees_with_the_oracle(threads):
+    """ref_sort (pair loop + parallel tuple sort, sort.rs:270-345, 692-698) is
+    the serial oracle's full sort, NULLs included."""
+    rng = np.random.default_rng(threads)
+    for n in [0, 1, 4097, 100_003]:
+        v = rng.standard_normal(n)
+        v[::5] = 0.25
+        for desc in (False, True):
+            assert np.array_equal(O.ref_sort(v, desc, threads), O.sort(v, desc))
+    i = rng.integers(-20, 20, 50_001)
+    w = F.validity_words(rng.random(50_001) > 0.3)
+    for nl in (False, True):
+        assert np.array_equal(O.ref_sort(i, False, threads, nulls_last=nl, validity=w),
+                              O.sort(i, False, nulls_last=nl, validity=w))
+
+
 def test_reference_engine_agrees_with_the_serial_oracle():
     """The timed CPU baseline computes the same answers as the serial oracle."""
     from falcondb_b200 import workloads as W
