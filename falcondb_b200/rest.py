@@ -376,6 +376,8 @@ class RestServer:
             return 404, {"error": f"no route {method} {path}"}
         except FalconError as e:
             return 400, {"error": str(e)}
+        except Exception as e:  # a fault of this server, not of the request: say so rather than drop the connection
+            return 500, {"error": f"{type(e).__name__}: {e}"}
 
     def _drop(self, name: str) -> Tuple[int, Dict[str, Any]]:
         with self._lock:

@@ -42,6 +42,8 @@ class _FakeDb:
     def sql(self, text):
         if "SELEKT" in text:
             raise FalconError(-5, "expected 'SELECT' near 'SELEKT'")
+        if "BOOM" in text:
+            raise RuntimeError("boom")
         return _Result()
 
 
@@ -89,6 +91,8 @@ def test_errors_are_400_with_a_message(server):
     assert _call(s.port, "POST", "/load/csv", {"path": "a.csv", "table": "t"})[0] == 400
     assert _call(s.port, "POST", "/tables/t/save", {"path": "t.fdb"})[0] == 400
     assert _call(s.port, "GET", "/nowhere")[0] == 404
+    code, body = _call(s.port, "POST", "/sql", {"sql": "SELECT BOOM"})
+    assert code == 500 and "boom" in body["error"]
 
 
 def test_concurrent_requests(server):
