@@ -116,6 +116,11 @@ class fdb_serve_config(C.Structure):
     _fields_ = [("max_batch", C.c_int32), ("slots", C.c_int32), ("mem_budget", C.c_uint64)]
 
 
+class fdb_mem_stats(C.Structure):
+    _fields_ = [("in_use", C.c_uint64), ("budget", C.c_uint64), ("scratch", C.c_uint64),
+                ("pool_reserved", C.c_uint64), ("pool_used", C.c_uint64)]
+
+
 class fdb_serve_stats(C.Structure):
     _fields_ = [("wall_s", C.c_double), ("qps", C.c_double), ("p50_ms", C.c_double), ("p99_ms", C.c_double),
                 ("max_ms", C.c_double), ("mean_batch", C.c_double), ("batches", C.c_int64),
@@ -150,6 +155,7 @@ _SIGS = {
     "fdb_result_display": (C.c_char_p, [C.c_void_p]),
     "fdb_result_free": (None, [C.c_void_p]),
     "fdb_last_kernel_ms": (C.c_double, [C.c_void_p]),
+    "fdb_memory_stats": (C.c_int, [C.c_void_p, C.POINTER(fdb_mem_stats)]),
     "fdb_stream": (C.c_void_p, [C.c_void_p]),
     "fdb_synchronize": (C.c_int, [C.c_void_p]),
     "fdb_filter_mask": (C.c_int, [C.c_void_p, C.POINTER(fdb_dev_column), C.c_int32, C.c_uint64,
@@ -547,6 +553,12 @@ class Database:
     @property
     def stream(self) -> int:
         return int(lib().fdb_stream(self.handle) or 0)
+
+    def memory_stats(self) -> Dict[str, int]:
+        """Device memory the context holds (fdb_memory_stats)."""
+        st = fdb_mem_stats()
+        check(lib().fdb_memory_stats(self.handle, C.byref(st)))
+        return {k: int(getattr(st, k)) for k, _ in fdb_mem_stats._fields_}
 
     def synchronize(self) -> None:
         check(lib().fdb_synchronize(self.handle))

@@ -425,6 +425,25 @@ void fdb_result_free(fdb_result* r) { delete r; }
 
 double fdb_last_kernel_ms(const fdb_db* db) { return db ? db->ctx.last_kernel_ms : 0.0; }
 
+int fdb_memory_stats(fdb_db* db, fdb_mem_stats* out) {
+  if (!db || !out) return set_error(FDB_E_ARG, "fdb_memory_stats: bad arguments");
+  return guarded([&] {
+    std::lock_guard<std::recursive_mutex> lk(db->ctx.mu);
+    Ctx& c = db->ctx;
+    FDB_CUDA(cudaSetDevice(c.device));
+    out->in_use = c.in_use.load();
+    out->budget = c.budget;
+    out->scratch = c.scratch.bytes;
+    cudaMemPool_t pool;
+    FDB_CUDA(cudaDeviceGetDefaultMemPool(&pool, c.device));
+    unsigned long long v = 0;  // the attribute value type (cuuint64_t)
+    FDB_CUDA(cudaMemPoolGetAttribute(pool, cudaMemPoolAttrReservedMemCurrent, &v));
+    out->pool_reserved = v;
+    FDB_CUDA(cudaMemPoolGetAttribute(pool, cudaMemPoolAttrUsedMemCurrent, &v));
+    out->pool_used = v;
+  });
+}
+
 void* fdb_stream(fdb_db* db) { return db ? (void*)db->ctx.stream : nullptr; }
 
 int fdb_synchronize(fdb_db* db) {

@@ -14,6 +14,7 @@
 #include <vector>
 
 #include "../../include/falcondb_b200.h"
+#include "once.h"
 
 namespace fdb {
 

@@ -769,11 +769,8 @@ static void launch_stream_gb(Ctx& c, const fdb_dev_column* cols, uint64_t n,
   const int op_off = (int)stream_smem_bytes<NC, TR, STAGES>();
   const size_t smem = op_off + op_smem;
   auto kern = stream_kernel<Op, NC, TR, STAGES, NCW>;
-  static bool attr = false;
-  if (!attr) {
-    FDB_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, 220 * 1024));
-    attr = true;
-  }
+  static PerDeviceOnce attr;  // per instantiation and device
+  attr(c.device, [&] { FDB_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, 220 * 1024)); });
   int per_sm = 0;
   FDB_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, (NCW + 1) * 32, smem));
   if (per_sm < 1) per_sm = 1;

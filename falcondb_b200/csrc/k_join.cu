@@ -601,11 +601,8 @@ static void launch_probe_mode(Ctx& c, const fdb_dev_column* cols, uint64_t n, co
   using Op = ProbeOp<JT, DENSE>;
   const size_t smem = op_off + Op::kSmem;
   auto kern = stream_kernel<Op, NC, TR, STAGES, NCW, 8, DENSE ? FDB_PROBE_DENSE_MINB : FDB_PROBE_MINB>;
-  static bool attr = false;
-  if (!attr) {
-    FDB_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024));
-    attr = true;
-  }
+  static PerDeviceOnce attr;  // per instantiation and device
+  attr(c.device, [&] { FDB_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024)); });
   int per_sm = 0;
   FDB_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, (NCW + 1) * 32, smem));
   if (per_sm < 1) per_sm = 1;

@@ -494,11 +494,8 @@ static void launch_stream(Ctx& c, const fdb_dev_column* cols, uint64_t n, const 
   const int op_off = (int)stream_smem_bytes<NC, S::TR, S::STAGES, CBo>();
   const size_t smem = op_off + op_smem_bytes;
   auto kern = stream_kernel<Op, NC, S::TR, S::STAGES, S::NCW, CBo>;
-  static bool attr_done = false;  // per instantiation
-  if (!attr_done) {
-    FDB_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024));
-    attr_done = true;
-  }
+  static PerDeviceOnce attr_done;  // per instantiation and device
+  attr_done(c.device, [&] { FDB_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024)); });
   int per_sm = 0;
   FDB_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, (S::NCW + 1) * 32, smem));
   if (per_sm < 1) per_sm = 1;

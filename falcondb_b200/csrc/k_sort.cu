@@ -64,7 +64,8 @@ template <int DT, int MODE>
 __global__ void sort_key_kernel(DevCol col, const uint32_t* sel, uint32_t m, uint64_t* keys, uint32_t* vals,
                                 unsigned long long* vary) {
   unsigned long long o = 0, a = ~0ull;
-  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < m; i += gridDim.x * blockDim.x) {
+  for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < m;
+       i += (uint64_t)gridDim.x * blockDim.x) {
     const uint32_t row = sel ? sel[i] : i;
     const uint64_t k = sort_key_of<DT, MODE>(col, row);
     keys[i] = k;
@@ -88,7 +89,8 @@ __global__ void sort_key_kernel(DevCol col, const uint32_t* sel, uint32_t m, uin
 __global__ void distinct_heads_kernel(const uint64_t* __restrict__ keys, const uint32_t* __restrict__ rows,
                                       uint32_t m, const uint32_t* nulls, const uint64_t* nnull,
                                       unsigned long long* mask) {
-  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < m; i += gridDim.x * blockDim.x) {
+  for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < m;
+       i += (uint64_t)gridDim.x * blockDim.x) {
     if (i == 0 || keys[i] != keys[i - 1]) {
       const uint32_t r = rows[i];
       atomicOr(&mask[r >> 6], 1ull << (r & 63));
@@ -557,7 +559,8 @@ static void set_scatter_smem() {
 __global__ void pair_key_kernel(const uint32_t* __restrict__ left, const uint32_t* __restrict__ right, uint32_t n,
                                 uint64_t* keys, uint32_t* vals, unsigned long long* vary) {
   unsigned long long o = 0, a = ~0ull;
-  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+  for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n;
+       i += (uint64_t)gridDim.x * blockDim.x) {
     const uint64_t k = ((uint64_t)left[i] << 32) | (right ? right[i] : 0u);
     keys[i] = k;
     vals[i] = i;
@@ -576,7 +579,8 @@ __global__ void pair_key_kernel(const uint32_t* __restrict__ left, const uint32_
 }
 
 __global__ void pair_unpack_kernel(const uint64_t* __restrict__ keys, uint32_t n, uint32_t* left, uint32_t* right) {
-  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+  for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n;
+       i += (uint64_t)gridDim.x * blockDim.x) {
     const uint64_t k = keys[i];
     left[i] = (uint32_t)(k >> 32);
     if (right) right[i] = (uint32_t)k;
@@ -602,7 +606,8 @@ void op_sort_row_pairs(Ctx& c, uint32_t* d_left, uint32_t* d_right, uint64_t n) 
 // rows[i] = position of row i in the order: ROW_NUMBER() OVER (ORDER BY ..)
 // numbers the rows 1..n in sorted order (rank_dense, window.rs:259-300).
 __global__ void row_number_kernel(const uint32_t* order, const uint32_t* list, uint32_t n, int64_t* rn) {
-  for (uint32_t j = blockIdx.x * blockDim.x + threadIdx.x; j < n; j += gridDim.x * blockDim.x) {
+  for (uint64_t j = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; j < n;
+       j += (uint64_t)gridDim.x * blockDim.x) {
     const uint32_t o = order ? order[j] : j;
     rn[list ? list[o] : o] = (int64_t)j + 1;
   }

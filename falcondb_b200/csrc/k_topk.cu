@@ -985,11 +985,8 @@ static void launch_reg_topk(Ctx& c, const fdb_dev_column& col, uint64_t n, uint3
   const int op_off = (int)stream_smem_bytes<1, TR, STAGES>();
   const size_t smem = op_off + sizeof(RTSmem);
   auto kern = stream_kernel<RegTopkOp<DT, DESC>, 1, TR, STAGES, NCW, 8, 3, true>;  // 3 CTAs per SM, dynamic tiles
-  static bool attr = false;
-  if (!attr) {
-    FDB_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-    attr = true;
-  }
+  static PerDeviceOnce attr;  // per instantiation and device
+  attr(c.device, [&] { FDB_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem)); });
   int per_sm = 0;
   FDB_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, (NCW + 1) * 32, smem));
   if (per_sm < 1) per_sm = 1;
@@ -1057,11 +1054,8 @@ static void launch_topk_main(Ctx& c, const fdb_dev_column& col, uint64_t n, cons
   const int op_off = (int)stream_smem_bytes<1, TR, STAGES>();
   const size_t smem = op_off + topk_smem_bytes(cap);
   auto kern = stream_kernel<TopkOp, 1, TR, STAGES, NCW>;
-  static bool attr = false;
-  if (!attr) {
-    FDB_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, 220 * 1024));
-    attr = true;
-  }
+  static PerDeviceOnce attr;  // per instantiation and device
+  attr(c.device, [&] { FDB_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, 220 * 1024)); });
   int per_sm = 0;
   FDB_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, (NCW + 1) * 32, smem));
   if (per_sm < 1) per_sm = 1;
@@ -1086,11 +1080,8 @@ static void launch_warp_topk(Ctx& c, const fdb_dev_column& col, uint64_t n, Topk
     ps.out_count = nullptr;
     ps.out_t0 = t0;
     auto sk = wt_sample_kernel<DT, DESC>;
-    static bool sattr = false;
-    if (!sattr) {
-      FDB_CUDA(cudaFuncSetAttribute(sk, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)wsm));
-      sattr = true;
-    }
+    static PerDeviceOnce sattr;  // per instantiation and device
+    sattr(c.device, [&] { FDB_CUDA(cudaFuncSetAttribute(sk, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)wsm)); });
     const int grid = (int)umin64((nsamples + 2047) / 2048, (uint64_t)c.sm_count * 4);
     sk<<<grid, 256, wsm, c.stream>>>(ps, nsamples);
     FDB_CUDA(cudaGetLastError());
@@ -1108,11 +1099,8 @@ static void launch_warp_topk(Ctx& c, const fdb_dev_column& col, uint64_t n, Topk
   const int op_off = (int)stream_smem_bytes<1, TR, STAGES>();
   const size_t smem = op_off + wsm;
   auto kern = stream_kernel<WarpTopkOp<DT, DESC>, 1, TR, STAGES, NCW>;
-  static bool attr = false;
-  if (!attr) {
-    FDB_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-    attr = true;
-  }
+  static PerDeviceOnce attr;  // per instantiation and device
+  attr(c.device, [&] { FDB_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem)); });
   int per_sm = 0;
   FDB_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, (NCW + 1) * 32, smem));
   if (per_sm < 1) per_sm = 1;
@@ -1182,12 +1170,8 @@ void op_topk(Ctx& c, const fdb_dev_column& col, uint64_t n, uint32_t k, bool des
     ps.out_t0 = t0;
     const uint32_t cap = topk_cap(k, 256);
     const size_t smem = topk_smem_bytes(cap);
-    static bool attr = false;
-    if (!attr) {
-      FDB_CUDA(cudaFuncSetAttribute(topk_sample_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                    200 * 1024));
-      attr = true;
-    }
+    static PerDeviceOnce attr;  // per instantiation and device
+    attr(c.device, [&] { FDB_CUDA(cudaFuncSetAttribute(topk_sample_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024)); });
     const int grid = (int)umin64((uint64_t)c.sm_count, (nsamples + 4095) / 4096);
     topk_sample_kernel<<<grid, 256, smem, c.stream>>>(ps, nsamples);
     FDB_CUDA(cudaGetLastError());

@@ -237,6 +237,22 @@ void        fdb_result_free(fdb_result* r);
 /* Device time of the kernels of the last fdb_sql on this context, in ms. */
 double      fdb_last_kernel_ms(const fdb_db* db);
 
+/* Device memory the context holds, for monitoring (no counterpart in the
+ * reference, whose memory is the host heap).  in_use: bytes counted against
+ * the context's budget (resident tables, join tables, the operator scratch
+ * arena); budget: that cap; scratch: the arena's current size; pool_reserved /
+ * pool_used: cudaMemPoolAttrReservedMemCurrent / UsedMemCurrent of the
+ * device's default pool, which the context allocates from and which other
+ * users of that pool in the process share. */
+typedef struct fdb_mem_stats {
+    uint64_t in_use;
+    uint64_t budget;
+    uint64_t scratch;
+    uint64_t pool_reserved;
+    uint64_t pool_used;
+} fdb_mem_stats;
+int         fdb_memory_stats(fdb_db* db, fdb_mem_stats* out);
+
 /* ------------------------------------------------------------------------- */
 /* 2. Operator layer (device pointers; asynchronous on the context's stream) */
 /* ------------------------------------------------------------------------- */
