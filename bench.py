@@ -262,10 +262,19 @@ def run_gpu(args):
     per_q = {name: sum(evs[k][j][0].elapsed_time(evs[k][j][1]) for k in range(K)) / K
              for j, (name, _) in enumerate(steps)}
 
-    # Sanity: results equal the oracle-free invariants of the data.
-    assert int(r_dist.cpu().numpy().view(np.uint64)[0]) == (1 << 12) - 1
-    assert int(r_top2c.item()) == 10
-    assert list(r_top2.cpu().numpy()) == list(range(n - 1, n - 11, -1))
+    # After timing, every answer of the last step against the oracle: the
+    # FP64 SUM within 1e-12 of the serial sum, the count, the distinct set and
+    # both top-k row lists (ties by row ascending) exactly.
+    from oracle import oracle as O
+    got_sum = float(ops.to_records(r_sum, F.AGG_VALUE_DTYPE, 1)[0]["f"])
+    want_sum = O.sum_serial(t["score"])
+    assert abs(got_sum - want_sum) <= 1e-12 * abs(want_sum), (got_sum, want_sum)
+    assert int(r_cnt.item()) == O.popcount(O.cmp_mask(t["score"], F.GT, 50))
+    present = O.present_codes(t["dept"].codes, 12)
+    assert int(r_dist.cpu().numpy().view(np.uint64)[0]) == sum(1 << i for i in range(12) if present[i])
+    assert int(r_top1c.item()) == 10 and int(r_top2c.item()) == 10
+    assert list(r_top1.cpu().numpy()) == list(O.topk(t["score"], 10, True))
+    assert list(r_top2.cpu().numpy()) == list(O.topk(t["id"], 10, True))
 
     bytes_per_step = sum(BYTES_PER_ROW.values()) * n
     value = world * bytes_per_step * K / (ms / 1e3) / 1e9
@@ -299,10 +308,14 @@ def run_gpu(args):
                        "l2_flush": "not needed: every input column (400-800 MB) exceeds the 126 MB L2",
                        "parallelism": f"row shards x{world}"},
             "roofline": roof, "per_query": per_query, "e2e": e2e, "gpu_launches": LAUNCHES_PER_STEP * K,
-            "clocks": clocks,
+            "clocks": clocks, "extra_keys": ["per_query"],
         }
         if not args.no_cpu:
             result["cpu_baseline"] = cpu_baseline(t, n, args.cpu_threads)
+    if world == 1 and not args.no_configs:
+        extra = run_configs(args, db, t, n, peaks()[0])
+        result.update(extra)
+        result["extra_keys"] = ["per_query"] + list(extra)
     db.close()
     if world > 1:
         dist.barrier()
@@ -363,6 +376,260 @@ def run_e2e(args, F, t, n, db, torch, world, dist, local):
     return {"value": round(value, 2), "unit": "GB/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
             "ms_per_step": round(el / args.e2e_steps * 1e3, 3), "steps": args.e2e_steps,
             "path": "fdb_table_from_columns (pinned host) + 5 x fdb_sql"}
+
+
+# ----------------------------------------------------------------------------- the other configurations
+def run_configs(args, db, t, n, peak):
+    """One line's extra keys: the other BASELINE configurations at full size,
+    each timed with CUDA events on the library stream (K steps after 3
+    warm-ups; every input column exceeds the 126 MB L2) and checked against
+    the oracle after timing.
+
+    * filter_groupby_100M: SELECT dept, COUNT(*), SUM(score), AVG(salary)
+      WHERE score > 50 GROUP BY dept over the headline's 100M-row table
+      (20 B/row).
+    * join_{inner,left,semi,anti}: 1M-row build (key a permutation of
+      0..1M-1, payload uniform [0, 1e6)), 100M-row probe (key uniform
+      [0, 2M), value uniform [0, 1)); COUNT(*) with SUM(payload), or with
+      SUM(value) for SEMI / ANTI (8 B/probe row of key, +8 B of value).
+    * groupby_zipf: 100M rows, key Zipf(1.1) over 10M values, COUNT / SUM /
+      MIN / MAX of v, the table sized by the sizing pass inside the timed
+      call (16 B/row + 40 B/group).
+    * groupby_batched: 64 GROUP BY queries over slices of that table, sizes
+      log-uniform in [10k, 10M] rows, one captured graph against the same
+      queries one by one.
+    * serving: 10,000 queries of the four templates, Poisson at 2000 qps,
+      batched against one at a time, plus an offered-load sweep."""
+    import torch
+
+    import falcondb_b200 as F
+    from falcondb_b200 import ops, serving as S, workloads as W
+    from oracle import oracle as O
+
+    dev = torch.device("cuda", 0)
+    stream = ops.lib_stream(db)
+    K, Wm = max(3, min(args.steps, 10)), 3
+    L = F.lib()
+    extra = {}
+
+    def rate(name, ms, nbytes, **kw):
+        gbs = nbytes / (ms / 1e3) / 1e9
+        d = {"ms": round(ms, 4), "algorithmic_bytes": int(nbytes), "GB/s": round(gbs, 1),
+             "frac_of_measured_hbm": round(gbs / peak, 4), "oracle_checked": True, "steps": K, "warmup": Wm}
+        d.update(kw)
+        extra[name] = d
+
+    # --- configuration 0's query at 100M rows (the headline table) ---------
+    cols = [db.column("t", c) for c in ("dept", "score", "salary")]
+    prog = [ops.cmp(1, F.GT, 50)]
+    aggs = [(F.AGG_COUNT_STAR, 0), (F.AGG_SUM, 1), (F.AGG_AVG, 2)]
+    res = ops._bytes(F.AGG_VALUE_DTYPE.itemsize * 13 * 3, db)
+    grows = torch.empty(13, dtype=torch.int64, device=dev)
+    ca, nc = ops._cols(cols)
+    pa, npr = ops._prog(prog)
+    aa, na = ops._aggs(aggs)
+    ms = _time_steps(lambda: F.check(L.fdb_group_by_codes(db.handle, ca, nc, n, pa, npr, 0, 12, aa, na,
+                                                          res.data_ptr(), grows.data_ptr())), K, Wm, stream, torch)
+    g0 = O.group_codes(t["dept"].codes, 12, mask=O.cmp_mask(t["score"], F.GT, 50), fvals=t["score"],
+                       ivals=t["salary"])
+    rec = ops.to_records(res, F.AGG_VALUE_DTYPE).reshape(13, 3)
+    assert list(grows.cpu().numpy()[:12]) == list(g0["rows"][:12])
+    for d in range(12):
+        assert abs(rec[d, 1]["f"] - g0["fsum"][d]) <= 1e-12 * g0["fsum"][d]
+        assert rec[d, 2]["f"] == g0["isum"][d] / g0["icnt"][d]
+    rate("filter_groupby_100M", ms, 20 * n, rows=n,
+         query="SELECT dept, COUNT(*), SUM(score), AVG(salary) FROM t WHERE score > 50 GROUP BY dept")
+
+    # --- configuration 2: 1M x 100M joins ------------------------------------
+    b, p = W.join_tables(1_000_000, n, seed=7)
+    db.create_table("b", b)
+    db.create_table("p", p)
+    bk, bp = db.column("b", "key"), db.column("b", "payload")
+    pk, pv = db.column("p", "key"), db.column("p", "value")
+    out = ops._bytes(F.JOIN_AGG_DTYPE.itemsize, db)
+    ms_build = _time_steps(lambda: ops.HashTable(db, bk, bp, len(b["key"])).free(), 3, 2, stream, torch)
+    ht = ops.HashTable(db, bk, bp, len(b["key"]))
+    for jt, name in [(F.JOIN_INNER, "inner"), (F.JOIN_LEFT, "left"), (F.JOIN_SEMI, "semi"), (F.JOIN_ANTI, "anti")]:
+        val = pv if jt >= F.JOIN_SEMI else None
+        ms = _time_steps(lambda: ht.probe_agg(pk, n, jt, value=val, out=out), K, Wm, stream, torch)
+        got = ops.to_records(out, F.JOIN_AGG_DTYPE, 1)[0]
+        want = O.join_agg(b["key"], b["payload"], p["key"], p["value"], jt)
+        assert int(got["count"]) == want["count"]
+        if jt <= F.JOIN_LEFT:
+            assert int(got["sum_payload"]) == want["sum_payload"]
+        else:
+            assert abs(float(got["sum_value"]) - want["sum_value"]) <= 1e-12 * abs(want["sum_value"])
+        rate(f"join_{name}", ms, (16 if jt >= F.JOIN_SEMI else 8) * n, build_rows=len(b["key"]), probe_rows=n,
+             count=int(got["count"]), table="direct-addressed" if ht.dense else "hashed",
+             build_ms=round(ms_build, 4))
+
+    # --- configuration 3: Zipf GROUP BY, single and batched ------------------
+    g = W.groupby_table(n, distinct=10_000_000, seed=11)
+    db.create_table("g", g)
+    gk, gv = db.column("g", "key"), db.column("g", "v")
+    cap = 12_000_000
+    outb = ops._bytes(F.GROUP_I64_DTYPE.itemsize * cap, db)
+    ng = torch.empty(1, dtype=torch.int64, device=dev)
+    ms = _time_steps(lambda: ops.group_by_i64(db, gk, gv, n, capacity=cap, out=outb, ngroups=ng), K, Wm, stream,
+                     torch)
+    groups = int(ng.item())
+    rec = ops.to_records(outb, F.GROUP_I64_DTYPE, groups)
+    rec = rec[np.argsort(rec["key"], kind="stable")]
+    want = O.group_i64(g["key"], g["v"])
+    assert np.array_equal(rec["key"], want["key"]) and np.array_equal(rec["count"], want["count"])
+    assert np.array_equal(rec["min"], want["min"]) and np.array_equal(rec["max"], want["max"])
+    assert float((np.abs(rec["sum"] - want["sum"]) / np.abs(want["sum"])).max()) <= 1e-12
+    del rec, want
+    rate("groupby_zipf", ms, 16 * n + 40 * groups, rows=n, groups=groups, distinct_domain=10_000_000, zipf_s=1.1,
+         table_sizing="one pass over the keys (HyperLogLog estimate and key range) inside the timed call")
+
+    kt = torch.from_numpy(g["key"]).to(dev)
+    vt = torch.from_numpy(g["v"]).to(dev)
+    rng = np.random.default_rng(64)
+    sizes = np.minimum(np.floor(10 ** (4 + 3 * rng.random(64))).astype(np.int64), n)
+    offs = [int(rng.integers(0, n - s + 1)) for s in sizes]
+    qs = [(kt[o:o + int(s)], vt[o:o + int(s)], int(s)) for o, s in zip(offs, sizes)]
+    tuning, _ = ops.GroupByBatch.autotune(db, qs, reps=2)
+    batch = ops.GroupByBatch(db, qs, tuning=tuning)
+    ms_batch = _time_steps(batch.run, K, Wm, stream, torch)
+    bgroups = [int(batch.outs[i][1].item()) for i in range(len(qs))]
+    souts = [(ops._bytes(F.GROUP_I64_DTYPE.itemsize * (gq + 1), db), torch.empty(1, dtype=torch.int64, device=dev))
+             for gq in bgroups]
+
+    def serial():
+        for (kk, vv, sz), gq, (ob, nb2) in zip(qs, bgroups, souts):
+            ops.group_by_i64(db, kk, vv, sz, expected_groups=max(gq, 1), capacity=gq + 1, out=ob, ngroups=nb2)
+    ms_serial = _time_steps(serial, K, Wm, stream, torch)
+    assert [int(nb2.item()) for _, nb2 in souts] == bgroups
+    for i in np.argsort(sizes)[::16]:  # four queries of spread sizes against the oracle
+        o, sz = offs[i], int(sizes[i])
+        r = ops.to_records(batch.outs[i][0], F.GROUP_I64_DTYPE, bgroups[i])
+        r = r[np.argsort(r["key"], kind="stable")]
+        w = O.group_i64(g["key"][o:o + sz], g["v"][o:o + sz])
+        assert np.array_equal(r["key"], w["key"]) and np.array_equal(r["count"], w["count"])
+        assert float((np.abs(r["sum"] - w["sum"]) / np.abs(w["sum"])).max()) <= 1e-12
+    batch.free()
+    rows_total = int(sizes.sum())
+    rate("groupby_batched", ms_batch, 16 * rows_total + 40 * sum(bgroups), queries=len(qs), rows_total=rows_total,
+         groups_total=sum(bgroups), ms_serial=round(ms_serial, 4), speedup_vs_serial=round(ms_serial / ms_batch, 2),
+         qps_batched=round(len(qs) / (ms_batch / 1e3), 1), qps_serial=round(len(qs) / (ms_serial / 1e3), 1),
+         tuning={"load_factor": tuning[0], "ctas_per_sm": tuning[1], "tile_rows": tuning[2]},
+         oracle_checked_queries=4, serial="the same queries one by one, tables sized to the exact group counts")
+    del kt, vt, qs, souts
+    db.drop_table("g")
+    del g
+    torch.cuda.empty_cache()
+
+    # --- configuration 4: serving --------------------------------------------
+    extra["serving"] = serve_configuration(args, db, t, n, p, b, ht, S, O, F, torch)
+    ht.free()
+    db.drop_table("b")
+    db.drop_table("p")
+    return extra
+
+
+def serve_configuration(args, db, t, n, p, b, ht, S, O, F, torch):
+    """10,000 queries (filter-count, filter-group-by, inner join, top-k drawn
+    uniformly) over prefixes of the resident tables, prefix sizes log-uniform
+    in [10k, 100M] rows, thresholds uniform in [0, 100), Poisson arrivals at
+    2000 qps, under a 40 GB device budget: continuous batching against one
+    query at a time, then an offered-load sweep up to 3x the serial mode's
+    saturated throughput.  Every batched answer equals the one-at-a-time
+    answer; 32 of them (8 per template) are checked against the oracle."""
+    score = db.column("t", "score").raw.values
+    dept = db.column("t", "dept").raw.values
+    sal = db.column("t", "salary").raw.values
+    pkey = db.column("p", "key").raw.values
+    pval = db.column("p", "value").raw.values
+    rng = np.random.default_rng(2000)
+    nq, rate0 = args.serve_queries, 2000.0
+    kinds, rows, xs = [], [], []
+    for _ in range(nq):
+        kinds.append(int(rng.integers(0, 4)))
+        rows.append(int(min(n, np.floor(10 ** (4 + (np.log10(n) - 4) * rng.random())))))
+        xs.append(float(rng.random() * 100))
+    gaps = rng.exponential(1.0, nq)  # unit-rate Poisson gaps, scaled per offered load
+
+    def queries(qps):
+        qs, at = [], 0.0
+        for i in range(nq):
+            at += gaps[i] / qps if qps else 0.0
+            k, r, x = kinds[i], rows[i], xs[i]
+            if k == S.SERVE_COUNT:
+                q = S.count_query(score, r, x)
+            elif k == S.SERVE_GROUP:
+                q = S.group_query(score, dept, sal, 12, r, x)
+            elif k == S.SERVE_JOIN:
+                q = S.join_query(pkey, pval, ht._h.value, r, x)
+            else:
+                q = S.topk_query(score, r, x, k=10)
+            q.arrival_s = at
+            qs.append(q)
+        return qs
+
+    budget = 40 << 30
+    slots = args.serve_slots
+    S.serve_trace(db, queries(0)[:200], max_batch=128, slots=slots, mem_budget=budget)  # warm-up
+    live = queries(rate0)
+    res_b, live_b = S.serve_trace(db, live, max_batch=128, slots=slots, mem_budget=budget)
+    res_s, live_s = S.serve_trace(db, live, max_batch=1, slots=1, mem_budget=budget)
+    burst = queries(0)
+    _, sat_b = S.serve_trace(db, burst, max_batch=128, slots=slots, mem_budget=budget)
+    _, sat_s = S.serve_trace(db, burst, max_batch=1, slots=1, mem_budget=budget)
+
+    def same(a, c):
+        return (a.status == 0 and c.status == 0 and a.count == c.count and a.sum_payload == c.sum_payload
+                and list(a.group_count) == list(c.group_count) and list(a.group_sum2) == list(c.group_sum2)
+                and all(abs(x - y) <= 1e-12 * max(abs(y), 1e-300) for x, y in zip(a.group_sum0, c.group_sum0))
+                and list(a.rows[:a.count]) == list(c.rows[:c.count]))
+    assert all(same(a, c) for a, c in zip(res_b, res_s))
+    # Oracle: 8 queries per template.
+    score_h, codes_h, sal_h = t["score"], t["dept"].codes, t["salary"]
+    checked = {k: 0 for k in range(4)}
+    for q, r in zip(live, res_b):
+        if checked[q.kind] >= 8:
+            continue
+        checked[q.kind] += 1
+        m, x = q.nrows, q.threshold
+        if q.kind == S.SERVE_COUNT:
+            assert r.count == int((score_h[:m] > x).sum())
+        elif q.kind == S.SERVE_GROUP:
+            sel = score_h[:m] > x
+            c = codes_h[:m][sel]
+            assert list(r.group_count[:12]) == list(np.bincount(c, minlength=12))
+            assert list(r.group_sum2[:12]) == [int(v) for v in np.bincount(c, weights=sal_h[:m][sel].astype(float),
+                                                                          minlength=12)]
+            s0 = np.bincount(c, weights=score_h[:m][sel], minlength=12)
+            assert all(abs(r.group_sum0[j] - s0[j]) <= 1e-12 * max(abs(s0[j]), 1e-300) for j in range(12))
+        elif q.kind == S.SERVE_JOIN:
+            keys = p["key"][:m][p["value"][:m] < x / 100]
+            o = O.join_agg(b["key"], b["payload"], keys, np.zeros(len(keys)), F.JOIN_INNER)
+            assert (r.count, r.sum_payload) == (o["count"], o["sum_payload"])
+        else:
+            idx = np.nonzero(score_h[:m] < x)[0]
+            assert list(r.rows[:r.count]) == list(idx[O.topk(score_h[:m][idx], q.k, True)])
+
+    def d(st):
+        return {"qps": round(st.qps, 1), "p50_ms": round(st.p50_ms, 4), "p99_ms": round(st.p99_ms, 4),
+                "max_ms": round(st.max_ms, 4), "mean_batch": round(st.mean_batch, 2)}
+
+    # Offered-load sweep: serial at 90 % of its saturated rate, batched at 1x,
+    # 2x and 3x that saturated rate.
+    sweep = {"serial_saturated_qps": round(sat_s.qps, 1), "serial": {}, "batched": {}}
+    s90 = 0.9 * sat_s.qps
+    _, st = S.serve_trace(db, queries(s90), max_batch=1, slots=1, mem_budget=budget)
+    sweep["serial"][f"{s90:.0f}"] = d(st)
+    for mult in (1, 2, 3):
+        off = mult * sat_s.qps
+        _, st = S.serve_trace(db, queries(off), max_batch=128, slots=slots, mem_budget=budget)
+        sweep["batched"][f"{off:.0f}"] = d(st)
+    return {"unit": "queries/s", "queries": nq, "arrival_qps": rate0, "slots": slots, "max_batch": 128,
+            "mem_budget_bytes": budget, "table_rows": n, "prefix_rows": "log-uniform [10k, 100M]",
+            "at_2000qps": {"batched": d(live_b), "serial": d(live_s)},
+            "saturated": {"batched": d(sat_b), "serial": d(sat_s)},
+            "throughput_speedup": round(sat_b.qps / sat_s.qps, 2) if sat_s.qps else None,
+            "offered_load_sweep": sweep, "results_identical_batched_vs_serial": True,
+            "oracle_checked": True, "oracle_checked_queries": 32}
 
 
 # ----------------------------------------------------------------------------- CPU baseline
@@ -509,9 +776,20 @@ def run_secondary(args):
                              ngroups=ng)
         ms = _time_steps(q, K, Wm, stream, torch)
         groups = int(ng.item())
+        # After timing: every group against the oracle (keys, counts, MIN/MAX
+        # exactly; SUM within 1e-12 relative).
+        rec = ops.to_records(outb, F.GROUP_I64_DTYPE, groups)
+        rec = rec[np.argsort(rec["key"], kind="stable")]
+        want = O.group_i64(g["key"], g["v"])
+        assert np.array_equal(rec["key"], want["key"]) and np.array_equal(rec["count"], want["count"])
+        assert np.array_equal(rec["min"], want["min"]) and np.array_equal(rec["max"], want["max"])
+        assert float((np.abs(rec["sum"] - want["sum"]) / np.abs(want["sum"])).max()) <= 1e-12
+        del rec, want
         line("groupby_zipf", ms, 16 * n + 40 * groups, {"rows": n, "groups": groups, "distinct_domain": 10_000_000,
-                                                        "zipf_s": 1.1, "load_factor": lf,
-                                                        "table_sizing": "HyperLogLog estimate inside the timed call"})
+                                                        "zipf_s": 1.1, "load_factor": lf, "oracle_checked": True,
+                                                        "table_sizing": "one pass over the keys (HyperLogLog "
+                                                                        "estimate and key range) inside the timed "
+                                                                        "call"})
         db.drop_table("g")
 
     if args.workload in ("batch", "all"):
@@ -866,6 +1144,8 @@ def main():
     ap.add_argument("--e2e-steps", type=int, default=3)
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--no-configs", action="store_true",
+                    help="skip the other configurations' extra keys (1 GPU only)")
     ap.add_argument("--cpu-threads", type=int, default=0)
     ap.add_argument("--workload", default="scan",
                     choices=["scan", "filter_groupby", "join", "groupby", "batch", "sort", "rest", "serve", "serve_single",

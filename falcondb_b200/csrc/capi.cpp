@@ -558,10 +558,10 @@ int fdb_group_by_i64(fdb_db* db, const fdb_dev_column* key, const fdb_dev_column
     Ctx& c = db->ctx;
     double lf = (load_factor > 0.0 && load_factor < 1.0) ? load_factor : 0.5;
     CallScope s(db, default_scratch(c));
-    const uint64_t eg = group_by_i64_groups(s.c, *key, nrows, expected_groups);
+    const GbSizing sz = group_by_i64_sizing(s.c, *key, nrows, expected_groups);
     s.c.scratch_reset();
-    s.c.ensure_scratch(group_by_i64_scratch(eg, lf) + (16u << 20));
-    op_group_by_i64(s.c, *key, *value, nrows, prog, nterms, pred_cols, npred_cols, eg, lf, d_groups, capacity,
+    s.c.ensure_scratch(group_by_i64_scratch(sz, lf) + (16u << 20));
+    op_group_by_i64(s.c, *key, *value, nrows, prog, nterms, pred_cols, npred_cols, sz, lf, d_groups, capacity,
                     d_ngroups);
   });
 }

@@ -141,14 +141,23 @@ void op_group_by_codes(Ctx& c, const fdb_dev_column* cols, int ncols, uint64_t n
                        const fdb_pred_term* prog, int nterms, int key_col, uint32_t dict_len,
                        const fdb_agg_spec* aggs, int naggs, fdb_agg_value* d_out,
                        int64_t* d_group_rows);
-// Groups to size a hash GROUP BY table for: `expected_groups` when nonzero,
-// else a HyperLogLog estimate of the key column plus headroom (synchronises).
-uint64_t group_by_i64_groups(Ctx& c, const fdb_dev_column& key, uint64_t n, uint64_t expected_groups);
-// Scratch bytes op_group_by_i64 takes for `expected_groups` at `load_factor`.
-size_t group_by_i64_scratch(uint64_t expected_groups, double load_factor);
+// How an int64-key GROUP BY sizes its table: the groups to expect and, when
+// known, the range of the non-NULL keys.  A range that is dense enough makes
+// the table direct-addressed (one slot per key value, no hashing or probing).
+struct GbSizing {
+  uint64_t groups = 0;
+  bool has_range = false;
+  int64_t kmin = 0, kmax = 0;
+};
+// `expected_groups` when nonzero (no pass over the keys, no range), else the
+// sizing pass over the key column: estimate plus headroom, and the key range
+// (synchronises).
+GbSizing group_by_i64_sizing(Ctx& c, const fdb_dev_column& key, uint64_t n, uint64_t expected_groups);
+// Scratch bytes op_group_by_i64 takes for `s` at `load_factor`.
+size_t group_by_i64_scratch(const GbSizing& s, double load_factor);
 void op_group_by_i64(Ctx& c, const fdb_dev_column& key, const fdb_dev_column& value, uint64_t n,
                      const fdb_pred_term* prog, int nterms, const fdb_dev_column* pred_cols,
-                     int npred, uint64_t expected_groups, double load_factor,
+                     int npred, const GbSizing& s, double load_factor,
                      fdb_group_i64* d_groups, uint64_t capacity, uint64_t* d_ngroups);
 struct HashTable;  // join build side (k_join.cu)
 // Device pointers of a join build table for kernels outside k_join.cu.
@@ -173,8 +182,16 @@ void server_stop(Server* s, fdb_serve_stats* st);
 void serve_trace(fdb_db* db, Ctx& c, const fdb_serve_query* qs, int nq, const fdb_serve_config* cfg,
                  fdb_serve_result* out, fdb_serve_stats* st);
 
-// HyperLogLog estimate of the distinct keys among n INT64 values (hll.cu);
-// synchronises the context stream.
+// One sizing pass over an INT64 key column (hll.cu): a HyperLogLog estimate of
+// its distinct keys and the range of its non-NULL keys (NULL: a clear validity
+// bit, or INT64_MIN).  Synchronises the context stream.
+struct KeyStats {
+  uint64_t distinct = 0;
+  bool has_range = false;  // false when every key is NULL (or there are none)
+  int64_t kmin = 0, kmax = 0;
+};
+KeyStats key_stats_i64(Ctx& c, const fdb_dev_column& key, uint64_t n);
+// The estimate alone, over a column without NULLs.
 uint64_t estimate_distinct_i64(Ctx& c, const void* keys, uint64_t n);
 
 struct BatchPlan;
@@ -194,6 +211,32 @@ void op_distinct(Ctx& c, const fdb_dev_column& col, uint64_t n, uint32_t* d_rows
 // op_sort with, when int_as_f64, an INT64 column ordered by its f64 value.
 void op_sort_keyed(Ctx& c, const fdb_dev_column& col, uint64_t n, bool desc, bool nulls_last, bool int_as_f64,
                    uint32_t* d_rows);
+// One key of a multi-key sort (op_sort_multi).  ORDER BY keys order FLOAT64 /
+// INT64 values as the single-key sort does and a UTF8 column by `rank` (the
+// rank of each dictionary code in the sorted dictionary, equal strings equal
+// ranks; codes at or past rank_len read as NULL); DISTINCT keys only group
+// equal values together (a UTF8 DISTINCT key compares ranks when given, else
+// codes).
+struct SortKey {
+  fdb_dev_column col{};
+  bool desc = false, nulls_last = false;
+  bool distinct = false;
+  const uint32_t* rank = nullptr;  // device, rank_len entries
+  uint32_t rank_len = 0;
+};
+// Positions 0..n-1 of a row list (position p is row d_list[p], or row p when
+// d_list is null) in the order of keys[0], then keys[1], ..., then position:
+// d_pos receives n positions.  Up to 8 keys.
+void op_sort_multi(Ctx& c, const SortKey* keys, int nkeys, const uint32_t* d_list, uint64_t n, uint32_t* d_pos);
+// Scratch bytes op_sort_multi takes beyond the caller's.
+size_t sort_multi_scratch(uint64_t n);
+// SELECT DISTINCT over several columns: the positions (ascending) of the first
+// occurrence of each distinct row of `cols` over the row list; *d_count = how
+// many.  NULLs are one value per column; FLOAT64 compares with every NaN one
+// value and -0.0 equal to +0.0; UTF8 compares ranks[j] (rank_lens[j]
+// entries) when given, else codes.  ranks may be null.
+void op_distinct_multi(Ctx& c, const fdb_dev_column* cols, const uint32_t* const* ranks, const uint32_t* rank_lens,
+                       int ncols, const uint32_t* d_list, uint64_t n, uint32_t* d_pos, uint64_t* d_count);
 // Join row pairs (d_left[i], d_right[i]) put in (left, right) order in place;
 // d_right may be null (left rows only).
 void op_sort_row_pairs(Ctx& c, uint32_t* d_left, uint32_t* d_right, uint64_t n);

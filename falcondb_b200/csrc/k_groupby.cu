@@ -750,6 +750,282 @@ __global__ void gb_hash_compact_kernel(const GSlot* __restrict__ table, uint64_t
 }
 
 // ===========================================================================
+// 3. int64-key GROUP BY on a direct-addressed table
+// ===========================================================================
+// When the non-NULL keys span a range not much wider than the number of
+// groups (surrogate keys, dense id domains: the 100M-row Zipf workload's keys
+// span 0..10M-1 with 4.85M groups), the global table holds one 32-byte slot
+// per key value: slot k - kmin.  A row then needs no hash, no probe and no key
+// compare-and-swap, and its update is four fire-and-forget atomics into one
+// aligned 32-byte sector.  Each CTA still absorbs the frequent keys in a
+// shared-memory table first (the Zipf head), keyed by the slot index.  The
+// output comes out in key order, from an ordered compaction of the slots.
+struct DSlot {                 // 32 bytes, 32-byte aligned; all-zero = no row yet
+  unsigned long long count;
+  double sum;
+  unsigned long long nmin;     // ~order key of MIN (atomicMax)
+  unsigned long long max;      // order key of MAX
+};
+static_assert(sizeof(DSlot) == 32, "one sector per slot");
+
+struct SDSlot {                // CTA table slot, 32 bytes
+  unsigned int k1;             // slot index + 1 (0 = empty)
+  unsigned int count;          // a CTA sees fewer than 2^32 rows
+  double sum;
+  unsigned long long nmin;
+  unsigned long long max;
+};
+
+#ifndef FDB_GBD_SLOTS
+#define FDB_GBD_SLOTS 2048
+#endif
+constexpr uint32_t kDenseSmemSlots = FDB_GBD_SLOTS;  // power of two
+constexpr int kDenseSmemLog = __builtin_ctz(kDenseSmemSlots);
+static_assert((kDenseSmemSlots & (kDenseSmemSlots - 1)) == 0, "CTA table slots: a power of two");
+constexpr uint64_t kDenseMaxSlots = 1ull << 31;  // slot indices (and index + 1) fit 32 bits
+// Launch shape of the two-column instance (key, value): tile rows, stages,
+// consumer warps.
+#ifndef FDB_GBD_TR
+#define FDB_GBD_TR 1024
+#endif
+#ifndef FDB_GBD_ST
+#define FDB_GBD_ST 2
+#endif
+#ifndef FDB_GBD_NCW
+#define FDB_GBD_NCW 8
+#endif
+
+struct GbDenseParams {
+  PredProg prog;
+  DevCol cols[4];              // 0 = key, 1 = value, 2.. = predicate columns
+  DSlot* table;                // [slots], zeroed
+  uint64_t slots;              // kmax - kmin + 1
+  int64_t kmin;
+  DSlot* null_slot;            // the NULL key group (zeroed)
+  int* err;
+};
+
+// A value into a CTA slot.  MIN / MAX read the slot first and take the atomic
+// only when the value improves on it: after a frequent key's first few hundred
+// rows that is rare, so its rows do not queue on two 64-bit shared atomics.
+__device__ __forceinline__ void sdslot_accum(SDSlot* s, double v, bool has_v) {
+  atomicAdd(&s->count, 1u);
+  if (!has_v) return;
+  atomicAdd(&s->sum, v);
+  if (isnan(v)) return;
+  const unsigned long long k = f64_ord_key(v);
+  if (~k > *reinterpret_cast<volatile unsigned long long*>(&s->nmin)) atomicMax(&s->nmin, ~k);
+  if (k > *reinterpret_cast<volatile unsigned long long*>(&s->max)) atomicMax(&s->max, k);
+}
+
+// A value straight into its global slot (no result is used: RED operations).
+__device__ __forceinline__ void dslot_accum(DSlot* d, double v, bool has_v) {
+  atomicAdd(&d->count, 1ull);
+  if (!has_v) return;
+  atomicAdd(&d->sum, v);
+  if (isnan(v)) return;
+  const unsigned long long k = f64_ord_key(v);
+  atomicMax(&d->nmin, ~k);
+  atomicMax(&d->max, k);
+}
+
+__device__ __forceinline__ void dslot_merge(DSlot* d, const SDSlot& s) {
+  atomicAdd(&d->count, (unsigned long long)s.count);
+  if (s.sum != 0.0 || __double_as_longlong(s.sum) != 0) atomicAdd(&d->sum, s.sum);
+  if (s.nmin) atomicMax(&d->nmin, s.nmin);
+  if (s.max) atomicMax(&d->max, s.max);
+}
+
+// The CTA slot of slot index k, claiming one if free within kSmemProbe
+// probes; nullptr when it has no room there.
+__device__ __forceinline__ SDSlot* smem_dense_slot(SDSlot* tab, uint32_t k) {
+  uint32_t h = (k * 0x9E3779B1u) >> (32 - kDenseSmemLog);
+  const unsigned int k1 = k + 1u;
+  for (uint32_t probe = 0; probe < kSmemProbe; ++probe) {
+    SDSlot* s = tab + h;
+    const unsigned int cur = *reinterpret_cast<volatile unsigned int*>(&s->k1);
+    if (cur == k1) return s;
+    if (cur == 0) {
+      const unsigned int prev = atomicCAS(&s->k1, 0u, k1);
+      if (prev == 0 || prev == k1) return s;
+    }
+    h = (h + 1) & (kDenseSmemSlots - 1);
+  }
+  return nullptr;
+}
+
+struct GbDenseOp {
+  using Params = GbDenseParams;
+  struct Local {};
+  static constexpr size_t kSmem = (size_t)(kDenseSmemSlots + 1) * sizeof(SDSlot);
+
+  static __device__ void init(Local&, const Params&, unsigned char* sm, int ctid, int nct) {
+    uint64_t* w = reinterpret_cast<uint64_t*>(sm);
+    for (size_t i = ctid; i < kSmem / 8; i += nct) w[i] = 0;
+  }
+
+  template <class Acc>
+  static __device__ void step(Local&, const Params& p, unsigned char* sm, const Acc& acc, uint32_t rows, int ctid,
+                              int nct) {
+    SDSlot* tab = reinterpret_cast<SDSlot*>(sm);
+    for (uint32_t i = ctid; i < rows; i += nct) {
+      const uint64_t row = acc.row(i);
+      if (p.prog.n) {
+        GbGetter<Acc> get{p.cols, acc, i, row};
+        if (!eval_prog(p.prog, get)) continue;
+      }
+      const int64_t key = acc.template get<int64_t>(0, i);
+      const bool has_v = p.cols[1].validity ? col_valid(p.cols[1], row) : true;
+      double v = 0.0;
+      if (has_v)
+        v = p.cols[1].dtype == FDB_FLOAT64 ? acc.template get<double>(1, i)
+                                           : (double)acc.template get<int64_t>(1, i);
+      const bool kvalid = (p.cols[0].validity ? col_valid(p.cols[0], row) : true) && key != INT64_MIN;
+      if (!kvalid) {  // NULL group (i64::MIN reads as NULL)
+        sdslot_accum(tab + kDenseSmemSlots, v, has_v);
+        continue;
+      }
+      const uint64_t k = (uint64_t)key - (uint64_t)p.kmin;
+      if (k >= p.slots) {  // outside the sized range: the sizing did not see this column
+        atomicExch(p.err, kErrCapacity);
+        continue;
+      }
+      SDSlot* s = smem_dense_slot(tab, (uint32_t)k);
+      if (s)
+        sdslot_accum(s, v, has_v);
+      else
+        dslot_accum(p.table + k, v, has_v);
+    }
+  }
+
+  static __device__ void finish(Local&, const Params& p, unsigned char* sm, int ctid, int nct) {
+    const SDSlot* tab = reinterpret_cast<const SDSlot*>(sm);
+    consumer_bar(nct);
+    for (uint32_t i = ctid; i < kDenseSmemSlots; i += nct) {
+      const SDSlot s = tab[i];
+      if (s.k1) dslot_merge(p.table + (s.k1 - 1), s);
+    }
+    if (ctid == 0 && tab[kDenseSmemSlots].count) dslot_merge(p.null_slot, tab[kDenseSmemSlots]);
+  }
+};
+
+// Ordered compaction of the dense table.  Slots are cut into chunks of
+// kDenseChunk; pass 1 counts each chunk's live slots, one CTA turns the counts
+// into output offsets (and writes the NULL group after the last key), pass 2
+// writes each chunk's groups at its offset in slot (= key) order.
+constexpr uint32_t kDenseChunk = 4096;
+constexpr uint32_t kDenseCompactThreads = 256;
+
+__global__ void __launch_bounds__(kDenseCompactThreads)
+    dense_chunk_count_kernel(const DSlot* __restrict__ t, uint64_t slots, unsigned long long* chunk_off) {
+  __shared__ unsigned int wsum[kDenseCompactThreads / 32];
+  const uint64_t base = (uint64_t)blockIdx.x * kDenseChunk;
+  unsigned int live = 0;
+#pragma unroll 4
+  for (uint32_t j = threadIdx.x; j < kDenseChunk; j += kDenseCompactThreads) {
+    const uint64_t i = base + j;
+    if (i < slots) live += __ldcs(&t[i].count) != 0;
+  }
+  live = __reduce_add_sync(0xffffffffu, live);
+  if ((threadIdx.x & 31) == 0) wsum[threadIdx.x >> 5] = live;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    unsigned long long tot = 0;
+    for (int w = 0; w < kDenseCompactThreads / 32; ++w) tot += wsum[w];
+    chunk_off[blockIdx.x] = tot;
+  }
+}
+
+// One CTA: exclusive scan of the chunk counts in place, then the group count
+// and the NULL group (written last, after every key).
+__global__ void __launch_bounds__(1024)
+    dense_chunk_scan_kernel(unsigned long long* chunk_off, uint64_t nchunks, const DSlot* null_slot,
+                            fdb_group_i64* out, uint64_t cap_out, uint64_t* d_ngroups, int* err) {
+  __shared__ unsigned long long wsum[32];
+  __shared__ unsigned long long carry;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  if (threadIdx.x == 0) carry = 0;
+  __syncthreads();
+  for (uint64_t b = 0; b < nchunks; b += 1024) {
+    const uint64_t i = b + threadIdx.x;
+    const unsigned long long v = i < nchunks ? chunk_off[i] : 0;
+    unsigned long long x = v;  // inclusive warp scan
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const unsigned long long y = __shfl_up_sync(0xffffffffu, x, o);
+      if (lane >= o) x += y;
+    }
+    if (lane == 31) wsum[warp] = x;
+    __syncthreads();
+    if (warp == 0) {
+      unsigned long long w = wsum[lane];
+#pragma unroll
+      for (int o = 1; o < 32; o <<= 1) {
+        const unsigned long long y = __shfl_up_sync(0xffffffffu, w, o);
+        if (lane >= o) w += y;
+      }
+      wsum[lane] = w;  // inclusive over warps
+    }
+    __syncthreads();
+    const unsigned long long before = carry + (warp ? wsum[warp - 1] : 0) + x - v;
+    if (i < nchunks) chunk_off[i] = before;
+    __syncthreads();
+    if (threadIdx.x == 1023) carry = before + v;
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) {
+    unsigned long long total = carry;
+    const DSlot ns = *null_slot;
+    if (ns.count) {
+      if (total < cap_out) {
+        GSlot g{0, ns.count, ns.sum, ns.nmin, ns.max};
+        out[total] = gslot_group(0, g);  // key INT64_MIN
+      } else {
+        atomicExch(err, kErrCapacity);
+      }
+      ++total;
+    }
+    *d_ngroups = total;
+  }
+}
+
+__global__ void __launch_bounds__(kDenseCompactThreads)
+    dense_emit_kernel(const DSlot* __restrict__ t, uint64_t slots, int64_t kmin,
+                      const unsigned long long* __restrict__ chunk_off, fdb_group_i64* out, uint64_t cap_out,
+                      int* err) {
+  __shared__ unsigned int wcnt[kDenseCompactThreads / 32];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const uint64_t base = (uint64_t)blockIdx.x * kDenseChunk;
+  unsigned long long pos = chunk_off[blockIdx.x];
+  for (uint32_t j = 0; j < kDenseChunk; j += kDenseCompactThreads) {
+    const uint64_t i = base + j + threadIdx.x;
+    DSlot s{0, 0.0, 0, 0};
+    if (i < slots) s = t[i];
+    const bool live = s.count != 0;
+    const unsigned m = __ballot_sync(0xffffffffu, live);
+    if (lane == 0) wcnt[warp] = __popc(m);
+    __syncthreads();
+    unsigned int before = 0, total = 0;
+#pragma unroll
+    for (int w = 0; w < kDenseCompactThreads / 32; ++w) {
+      before += w < warp ? wcnt[w] : 0;
+      total += wcnt[w];
+    }
+    if (live) {
+      const unsigned long long o = pos + before + __popc(m & ((1u << lane) - 1u));
+      if (o < cap_out) {
+        GSlot g{0, s.count, s.sum, s.nmin, s.max};
+        out[o] = gslot_group(((uint64_t)kmin + i) ^ (1ull << 63), g);
+      } else {
+        atomicExch(err, kErrCapacity);
+      }
+    }
+    pos += total;
+    __syncthreads();
+  }
+}
+
+// ===========================================================================
 // Launchers
 // ===========================================================================
 constexpr uint64_t kGbTilesPerCta = 8;
@@ -952,23 +1228,52 @@ static uint64_t gb_table_capacity(uint64_t expected_groups, double load_factor) 
   return cap;
 }
 
-uint64_t group_by_i64_groups(Ctx& c, const fdb_dev_column& key, uint64_t n, uint64_t expected_groups) {
-  if (expected_groups) return expected_groups;
-  if (n == 0) return 1;
-  if (!key.values) fail(FDB_E_ARG, "column without values");
+GbSizing group_by_i64_sizing(Ctx& c, const fdb_dev_column& key, uint64_t n, uint64_t expected_groups) {
+  GbSizing s;
+  if (expected_groups) {
+    s.groups = expected_groups;
+    return s;
+  }
+  if (n == 0) {
+    s.groups = 1;
+    return s;
+  }
+  if (key.dtype != FDB_INT64) fail(FDB_E_TYPE, "hash GROUP BY needs an INT64 key");
+  const KeyStats k = key_stats_i64(c, key, n);
   // 15 % headroom over the sketch (about nine standard errors).
-  return std::min<uint64_t>(n, estimate_distinct_i64(c, key.values, n) * 115 / 100 + 64);
+  s.groups = std::min<uint64_t>(n, k.distinct * 115 / 100 + 64);
+  s.has_range = k.has_range;
+  s.kmin = k.kmin;
+  s.kmax = k.kmax;
+  return s;
 }
 
-size_t group_by_i64_scratch(uint64_t expected_groups, double load_factor) {
-  if (load_factor <= 0.0 || load_factor >= 1.0) load_factor = 0.5;
-  const uint64_t cap = gb_table_capacity(expected_groups ? expected_groups : 1, load_factor);
-  return (cap + 1) * sizeof(GSlot) + 2 * 256;  // each scratch_take rounds up to 256 bytes
+// Slots of a direct-addressed table for `s` (one per key value), or 0 when the
+// hash table is the better choice: the range must be known and its table no
+// more than twice the bytes of the hash table that the same groups would get.
+static uint64_t gb_dense_slots(const GbSizing& s, double load_factor) {
+  if (!s.has_range) return 0;
+  const uint64_t span = (uint64_t)s.kmax - (uint64_t)s.kmin;
+  if (span >= kDenseMaxSlots) return 0;
+  const uint64_t slots = span + 1;
+  const uint64_t hash_bytes = (gb_table_capacity(s.groups ? s.groups : 1, load_factor) + 1) * sizeof(GSlot);
+  return slots * sizeof(DSlot) <= 2 * hash_bytes ? slots : 0;
+}
+
+static double gb_load_factor(double lf) { return (lf <= 0.0 || lf >= 1.0) ? 0.5 : lf; }
+
+size_t group_by_i64_scratch(const GbSizing& s, double load_factor) {
+  load_factor = gb_load_factor(load_factor);
+  // Each scratch_take rounds up to 256 bytes.
+  if (const uint64_t slots = gb_dense_slots(s, load_factor))
+    return (slots + 1) * sizeof(DSlot) + (slots / kDenseChunk + 1) * 8 + 3 * 256;
+  const uint64_t cap = gb_table_capacity(s.groups ? s.groups : 1, load_factor);
+  return (cap + 1) * sizeof(GSlot) + 2 * 256;
 }
 
 void op_group_by_i64(Ctx& c, const fdb_dev_column& key, const fdb_dev_column& value, uint64_t n,
                      const fdb_pred_term* prog, int nterms, const fdb_dev_column* pred_cols,
-                     int npred, uint64_t expected_groups, double load_factor,
+                     int npred, const GbSizing& sz, double load_factor,
                      fdb_group_i64* d_groups, uint64_t capacity, uint64_t* d_ngroups) {
   if (key.dtype != FDB_INT64) fail(FDB_E_TYPE, "hash GROUP BY needs an INT64 key");
   if (value.dtype != FDB_FLOAT64 && value.dtype != FDB_INT64)
@@ -976,9 +1281,52 @@ void op_group_by_i64(Ctx& c, const fdb_dev_column& key, const fdb_dev_column& va
   if (npred < 0 || npred > 2) fail(FDB_E_ARG, "at most 2 predicate columns");
   // The CTA tables count rows in 32 bits; a CTA sees about n / grid rows.
   if (n / (uint64_t)c.sm_count >= (1ull << 31)) fail(FDB_E_ARG, "more than 2^31 rows per SM in one GROUP BY");
-  if (load_factor <= 0.0 || load_factor >= 1.0) load_factor = 0.5;
-  if (expected_groups == 0) expected_groups = n ? n : 1;
-  const uint64_t cap = gb_table_capacity(expected_groups, load_factor);
+  load_factor = gb_load_factor(load_factor);
+  fdb_dev_column all[4];
+  all[0] = key;
+  all[1] = value;
+  for (int i = 0; i < npred; ++i) all[2 + i] = pred_cols[i];
+  const int nc = 2 + npred;
+  DevCol dcols[4];
+  for (int i = 0; i < nc; ++i) {
+    if (!all[i].values && n > 0) fail(FDB_E_ARG, "column without values");
+    dcols[i] = DevCol{all[i].dtype, all[i].values, all[i].validity, all[i].validity_offset};
+  }
+
+  if (const uint64_t slots = gb_dense_slots(sz, load_factor)) {
+    // Direct-addressed table: slot k - kmin per key value, NULL group after it.
+    DSlot* table = static_cast<DSlot*>(c.scratch_take((slots + 1) * sizeof(DSlot)));
+    const uint64_t nchunks = (slots + kDenseChunk - 1) / kDenseChunk;
+    unsigned long long* chunk_off = static_cast<unsigned long long*>(c.scratch_take(nchunks * 8));
+    FDB_CUDA(cudaMemsetAsync(table, 0, (slots + 1) * sizeof(DSlot), c.stream));
+    GbDenseParams p;
+    std::memset(&p, 0, sizeof(p));
+    for (int i = 0; i < nc; ++i) p.cols[i] = dcols[i];
+    gb_fill_prog(p.prog, prog, nterms, npred, 2);
+    p.table = table;
+    p.slots = slots;
+    p.kmin = sz.kmin;
+    p.null_slot = table + slots;
+    p.err = c.d_err;
+    if (n > 0) {
+      switch (nc) {
+        case 2: launch_stream_gb<GbDenseOp, 2, FDB_GBD_TR, FDB_GBD_ST, FDB_GBD_NCW>(c, all, n, p, GbDenseOp::kSmem); break;
+        case 3: launch_stream_gb<GbDenseOp, 3, 1024, 2, FDB_GBD_NCW>(c, all, n, p, GbDenseOp::kSmem); break;
+        default: launch_stream_gb<GbDenseOp, 4, 512, 3, FDB_GBD_NCW>(c, all, n, p, GbDenseOp::kSmem); break;
+      }
+    }
+    dense_chunk_count_kernel<<<(unsigned)nchunks, kDenseCompactThreads, 0, c.stream>>>(table, slots, chunk_off);
+    FDB_CUDA(cudaGetLastError());
+    dense_chunk_scan_kernel<<<1, 1024, 0, c.stream>>>(chunk_off, nchunks, table + slots, d_groups, capacity,
+                                                      d_ngroups, c.d_err);
+    FDB_CUDA(cudaGetLastError());
+    dense_emit_kernel<<<(unsigned)nchunks, kDenseCompactThreads, 0, c.stream>>>(table, slots, sz.kmin, chunk_off,
+                                                                               d_groups, capacity, c.d_err);
+    FDB_CUDA(cudaGetLastError());
+    return;
+  }
+
+  const uint64_t cap = gb_table_capacity(sz.groups ? sz.groups : (n ? n : 1), load_factor);
   const size_t tbytes = cap * sizeof(GSlot);
   GSlot* table = static_cast<GSlot*>(c.scratch_take(tbytes + sizeof(GSlot)));
   GSlot* null_slot = table + cap;
@@ -988,15 +1336,7 @@ void op_group_by_i64(Ctx& c, const fdb_dev_column& key, const fdb_dev_column& va
 
   GbHashParams p;
   std::memset(&p, 0, sizeof(p));
-  fdb_dev_column all[4];
-  all[0] = key;
-  all[1] = value;
-  for (int i = 0; i < npred; ++i) all[2 + i] = pred_cols[i];
-  const int nc = 2 + npred;
-  for (int i = 0; i < nc; ++i) {
-    if (!all[i].values && n > 0) fail(FDB_E_ARG, "column without values");
-    p.cols[i] = DevCol{all[i].dtype, all[i].values, all[i].validity, all[i].validity_offset};
-  }
+  for (int i = 0; i < nc; ++i) p.cols[i] = dcols[i];
   gb_fill_prog(p.prog, prog, nterms, npred, 2);
   p.table = table;
   p.mask = cap - 1;

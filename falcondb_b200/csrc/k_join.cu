@@ -36,7 +36,26 @@ struct HashTable {
   bool payload_nulls = false;
   bool dense = false;        // key k lives in slot k - dmin (join_table.cuh)
   int64_t dmin = 0;
+  // Dense tables whose key range fits a CTA's shared memory as bits: bit
+  // k - dmin is set when key k has a build row.  SEMI / ANTI probes test it
+  // in shared memory and read nothing else.
+  DevBuf bits;
+  uint64_t span = 0;         // kmax - kmin + 1 (bits used)
 };
+
+// The widest key range whose presence bits a probe CTA keeps in shared
+// memory (192 KB), next to its tile ring.
+constexpr uint64_t kProbeBitsMaxSpan = 192ull * 1024 * 8;
+
+// bits[w] = presence of slots 64w .. 64w+63 (one 32-bit half per warp ballot).
+__global__ void join_bits_kernel(const unsigned int* __restrict__ cnt, uint64_t span, uint32_t* bits32) {
+  const uint64_t n32 = (span + 63) / 64 * 64;
+  for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n32; i += (uint64_t)gridDim.x * blockDim.x) {
+    const bool b = i < span && cnt[i] != 0u;
+    const unsigned m = __ballot_sync(0xffffffffu, b);
+    if ((threadIdx.x & 31) == 0) bits32[i >> 5] = m;
+  }
+}
 
 // Order keys of the smallest and largest valid build key (INT64_MIN, the
 // NULL group, excluded): out[0] = ~ord(min), out[1] = ord(max), both from a
@@ -244,6 +263,7 @@ HashTable* op_join_build(Ctx& c, const fdb_dev_column& key, const fdb_dev_column
   // Dense or hashed: the build keys' range decides (one 16-byte read back).
   bool dense = false;
   int64_t dmin = 0;
+  uint64_t span = 0;
   if (n > 0) {
     unsigned long long* range = static_cast<unsigned long long*>(c.scratch_take(16));
     FDB_CUDA(cudaMemsetAsync(range, 0, 16, c.stream));
@@ -259,6 +279,7 @@ HashTable* op_join_build(Ctx& c, const fdb_dev_column& key, const fdb_dev_column
       if (kmax - kmin < cap) {
         dense = true;
         dmin = (int64_t)kmin;
+        span = kmax - kmin + 1;
       }
     }
   }
@@ -283,6 +304,14 @@ HashTable* op_join_build(Ctx& c, const fdb_dev_column& key, const fdb_dev_column
     join_scatter_kernel<<<blocks, 256, 0, c.stream>>>(row_slot, n, static_cast<const uint32_t*>(h->off.ptr), fill,
                                                        static_cast<uint32_t*>(h->rows.ptr));
   }
+  if (dense && span <= kProbeBitsMaxSpan) {
+    const uint64_t words = (span + 63) / 64;
+    h->bits = c.alloc_buf(words * 8);
+    h->span = span;
+    const unsigned blocks = (unsigned)umin64((words * 64 + 255) / 256, (uint64_t)c.sm_count * 8);
+    join_bits_kernel<<<blocks, 256, 0, c.stream>>>(static_cast<const unsigned int*>(h->cnt.ptr), span,
+                                                    static_cast<uint32_t*>(h->bits.ptr));
+  }
   FDB_CUDA(cudaGetLastError());
   unsigned int hdup = 0;
   FDB_CUDA(cudaMemcpyAsync(&hdup, dup, 4, cudaMemcpyDeviceToHost, c.stream));
@@ -303,6 +332,7 @@ void join_free(HashTable* h) {
   c->free_buf(h->pcnt);
   c->free_buf(h->off);
   c->free_buf(h->rows);
+  c->free_buf(h->bits);
   delete h;
 }
 uint64_t join_capacity(const HashTable* h) { return h ? h->cap : 0; }
@@ -343,6 +373,8 @@ struct ProbeParams {
   JoinAggAcc* partials;   // [grid]
   unsigned int* ticket;
   fdb_join_agg* out;
+  const unsigned long long* bits;  // presence bits of a dense table's key range (ProbeBitsOp)
+  uint64_t span;
 };
 
 // Probe launch shape: ring stages, tile rows (one column), and resident CTAs
@@ -583,6 +615,52 @@ struct ProbeOp {
   }
 };
 
+// SEMI / ANTI against a dense table whose key range fits shared memory as
+// bits: every CTA copies the presence bits into shared memory once, and a row
+// then costs one shared-memory bit test (no L2 access), so the probe streams
+// its key (and value) columns at HBM speed.  Shared memory: ProbeOp's
+// reduction area, then the bits.
+template <int JT>
+struct ProbeBitsOp : ProbeOp<JT, true> {
+  static_assert(JT == FDB_JOIN_SEMI || JT == FDB_JOIN_ANTI, "presence alone answers SEMI / ANTI only");
+  using Base = ProbeOp<JT, true>;
+  using Params = ProbeParams;
+  using Local = typename Base::Local;
+  static constexpr size_t kBitsOff = (Base::kSmem + 127) / 128 * 128;
+
+  static __device__ void init(Local& st, const Params& p, unsigned char* sm, int ctid, int nct) {
+    Base::init(st, p, sm, ctid, nct);
+    unsigned long long* bits = reinterpret_cast<unsigned long long*>(sm + kBitsOff);
+    const uint64_t words = (p.span + 63) / 64;
+    for (uint64_t w = ctid; w < words; w += nct) bits[w] = __ldg(p.bits + w);
+  }
+
+  template <class Acc>
+  static __device__ void step(Local& st, const Params& p, unsigned char* sm, const Acc& acc, uint32_t rows,
+                              int ctid, int nct) {
+    const unsigned long long* bits = reinterpret_cast<const unsigned long long*>(sm + kBitsOff);
+    for (uint32_t i = ctid; i < rows; i += nct) {
+      bool match = false;
+      if (!p.key.validity || col_valid(p.key, acc.row(i))) {  // a NULL key matches nothing
+        const int64_t k = acc.template get<int64_t>(0, i);
+        if (k == INT64_MIN) {
+          match = p.cnt[p.cap] != 0u;
+        } else {
+          const uint64_t d = (uint64_t)k - (uint64_t)p.mode.dmin;
+          match = d < p.span && ((bits[d >> 6] >> (d & 63)) & 1ull);
+        }
+      }
+      if ((JT == FDB_JOIN_SEMI) == match) {
+        st.a.count += 1;
+        if (p.has_value && (!p.value.validity || col_valid(p.value, acc.row(i)))) {
+          st.a.vsum += acc.template get<double>(1, i);
+          st.a.prows += 1;
+        }
+      }
+    }
+  }
+};
+
 constexpr int kProbeMaxPerSm = 8;  // partials are sized for this many CTAs per SM
 
 template <int NC, int JT, bool DENSE>
@@ -615,8 +693,50 @@ static void launch_probe_mode(Ctx& c, const fdb_dev_column* cols, uint64_t n, co
   FDB_CUDA(cudaGetLastError());
 }
 
+// The presence-bit probe: one CTA per SM (the bits take most of its shared
+// memory), a three-stage ring when it fits beside them, else two.
+template <int NC, int JT, int STAGES>
+static void launch_probe_bits_shape(Ctx& c, const fdb_dev_column* cols, uint64_t n, const ProbeParams& p,
+                                    size_t op_smem) {
+  constexpr int TR = NC == 1 ? 2048 : 1024, NCW = 8;
+  StreamSrc<NC> src;
+  const void* bases[NC];
+  for (int i = 0; i < NC; ++i) {
+    src.base[i] = static_cast<const unsigned char*>(cols[i].values);
+    src.esize[i] = 8;
+    bases[i] = cols[i].values;
+  }
+  src.n = n;
+  src.m_end = stream_m_end(bases, NC, n);
+  const int op_off = (int)stream_smem_bytes<NC, TR, STAGES>();
+  const size_t smem = op_off + op_smem;
+  auto kern = stream_kernel<ProbeBitsOp<JT>, NC, TR, STAGES, NCW, 8, 1>;
+  static PerDeviceOnce attr;  // per instantiation and device
+  attr(c.device, [&] { FDB_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024)); });
+  const uint64_t ntiles = (src.m_end + TR - 1) / TR;
+  const int grid = (int)std::max<uint64_t>(1, umin64(ntiles ? ntiles : 1, (uint64_t)c.sm_count));
+  kern<<<grid, (NCW + 1) * 32, smem, c.stream>>>(src, p, c.d_err, op_off);
+  FDB_CUDA(cudaGetLastError());
+}
+
+template <int NC, int JT>
+static void launch_probe_bits(Ctx& c, const fdb_dev_column* cols, uint64_t n, const ProbeParams& p) {
+  constexpr int TR = NC == 1 ? 2048 : 1024;
+  const size_t op_smem = ProbeBitsOp<JT>::kBitsOff + (p.span + 63) / 64 * 8;
+  if (stream_smem_bytes<NC, TR, 3>() + op_smem <= 227 * 1024)
+    launch_probe_bits_shape<NC, JT, 3>(c, cols, n, p, op_smem);
+  else
+    launch_probe_bits_shape<NC, JT, 2>(c, cols, n, p, op_smem);
+}
+
 template <int NC, int JT>
 static void launch_probe(Ctx& c, const fdb_dev_column* cols, uint64_t n, const ProbeParams& p) {
+  if constexpr (JT == FDB_JOIN_SEMI || JT == FDB_JOIN_ANTI) {
+    if (p.bits) {
+      launch_probe_bits<NC, JT>(c, cols, n, p);
+      return;
+    }
+  }
   if (p.mode.dense)
     launch_probe_mode<NC, JT, true>(c, cols, n, p);
   else
@@ -641,6 +761,8 @@ void op_join_probe_agg(Ctx& c, const HashTable& h, const fdb_dev_column& key, co
   p.unique = h.unique ? 1 : 0;
   p.payload_nulls = h.payload_nulls ? 1 : 0;
   p.has_value = (has_value && (join_type == FDB_JOIN_SEMI || join_type == FDB_JOIN_ANTI)) ? 1 : 0;
+  p.bits = static_cast<const unsigned long long*>(h.bits.ptr);
+  p.span = h.span;
   p.partials = static_cast<JoinAggAcc*>(c.scratch_take(sizeof(JoinAggAcc) * c.sm_count * kProbeMaxPerSm));
   p.ticket = c.d_ticket;
   p.out = d_out;

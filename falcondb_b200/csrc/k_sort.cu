@@ -698,4 +698,242 @@ void op_distinct(Ctx& c, const fdb_dev_column& col, uint64_t n, uint32_t* d_rows
   op_compact_mask(c, reinterpret_cast<const uint64_t*>(heads), n, d_rows, n, d_count);
 }
 
+
+// ---------------------------------------------------------------------------
+// ORDER BY several keys, ORDER BY a text column, and DISTINCT over several
+// columns (sort_merged over several SortExprs, sort.rs:118-165; the text
+// column's dictionary ranked once and its rows sorted by rank, sort.rs:352-382;
+// dedup_batches over whole rows, select.rs:238-269).
+//
+// Positions 0..n-1 of a row list (position p is row list[p], or row p) are put
+// in order by a least-significant-key-first sequence of stable radix sorts:
+// the last key first, then each earlier key over the order so far, so ties
+// on every key keep position order, as the reference's (keys..., row)
+// comparison does.  Each pass takes the key's NULL positions out (in the
+// current order) and puts them first or last.
+// ---------------------------------------------------------------------------
+struct MKey {
+  DevCol col;
+  const uint32_t* rank;  // UTF8 ORDER BY: rank of each code in the sorted dictionary
+  uint32_t rank_len;
+  int32_t desc;
+  int32_t distinct;      // DISTINCT keys (equal exactly when the values are) instead of order keys
+};
+
+__device__ __forceinline__ bool mkey_null(const MKey& k, uint32_t row) {
+  if (k.col.validity && !col_valid(k.col, row)) return true;
+  if (k.col.dtype == FDB_UTF8) {
+    const uint32_t code = static_cast<const uint32_t*>(k.col.values)[row];
+    return code == kNullCode || (k.rank && code >= k.rank_len);
+  }
+  return false;
+}
+
+__device__ __forceinline__ uint64_t mkey_of(const MKey& k, uint32_t row) {
+  uint64_t key;
+  if (k.col.dtype == FDB_UTF8) {
+    const uint32_t code = static_cast<const uint32_t*>(k.col.values)[row];
+    key = k.rank ? k.rank[code] : code;
+  } else {
+    uint64_t b = static_cast<const uint64_t*>(k.col.values)[row];
+    if (k.distinct) {
+      if (k.col.dtype == FDB_FLOAT64) {
+        if ((b & 0x7FFFFFFFFFFFFFFFull) > 0x7FF0000000000000ull) b = 0x7FF8000000000000ull;  // NaN
+        if (b == 0x8000000000000000ull) b = 0;                                                 // -0.0
+      }
+      return b;
+    }
+    key = k.col.dtype == FDB_FLOAT64 ? f64_ord_key(__longlong_as_double((long long)b)) : (b ^ (1ull << 63));
+  }
+  return k.desc ? ~key : key;
+}
+
+__device__ __forceinline__ uint32_t list_row(const uint32_t* list, uint32_t pos) { return list ? list[pos] : pos; }
+
+__global__ void iota_u32_kernel(uint32_t* out, uint64_t n) {
+  for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x)
+    out[i] = (uint32_t)i;
+}
+
+__global__ void gather_u32_kernel(const uint32_t* __restrict__ src, const uint32_t* __restrict__ idx, uint64_t n,
+                                  uint32_t* out) {
+  for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x)
+    out[i] = src[idx[i]];
+}
+
+// Bit i of the mask: the key at position order[i] is NULL (nulls) / is not.
+// Bits past n are zero.  One 32-bit half word per warp (a ballot).
+__global__ void mkey_null_mask_kernel(MKey k, const uint32_t* list, const uint32_t* order, uint64_t n, bool nulls,
+                                      uint32_t* mask32) {
+  const uint64_t n32 = (n + 63) / 64 * 64;  // whole 64-bit words
+  for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n32; i += (uint64_t)gridDim.x * blockDim.x) {
+    bool bit = false;
+    if (i < n) bit = mkey_null(k, list_row(list, order[i])) == nulls;
+    const unsigned b = __ballot_sync(0xffffffffu, bit);
+    if ((threadIdx.x & 31) == 0) mask32[i >> 5] = b;
+  }
+}
+
+__global__ void mkey_sort_key_kernel(MKey k, const uint32_t* list, const uint32_t* sel, uint32_t m, uint64_t* keys,
+                                     uint32_t* vals, unsigned long long* vary) {
+  unsigned long long o = 0, a = ~0ull;
+  for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < m; i += (uint64_t)gridDim.x * blockDim.x) {
+    const uint32_t pos = sel[i];
+    const uint64_t key = mkey_of(k, list_row(list, pos));
+    keys[i] = key;
+    vals[i] = pos;
+    o |= key;
+    a &= key;
+  }
+#pragma unroll
+  for (int s = 16; s > 0; s >>= 1) {
+    o |= __shfl_xor_sync(0xffffffffu, o, s);
+    a &= __shfl_xor_sync(0xffffffffu, a, s);
+  }
+  if ((threadIdx.x & 31) == 0) {
+    atomicOr(&vary[0], o);
+    atomicAnd(&vary[1], a);
+  }
+}
+
+constexpr int kMaxMultiKeys = 8;
+struct MKeys {
+  MKey k[kMaxMultiKeys];
+  int32_t n;
+};
+
+// DISTINCT over several columns: position order[i] heads a run when i == 0 or
+// any column's NULL-ness or DISTINCT key differs from position order[i-1]'s;
+// its bit is set in the position mask.
+__global__ void multi_heads_kernel(MKeys ks, const uint32_t* list, const uint32_t* order, uint64_t n,
+                                   unsigned long long* mask) {
+  for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x) {
+    const uint32_t p = order[i];
+    bool head = i == 0;
+    if (!head) {
+      const uint32_t r = list_row(list, p), q = list_row(list, order[i - 1]);
+      for (int j = 0; j < ks.n && !head; ++j) {
+        const bool nr = mkey_null(ks.k[j], r), nq = mkey_null(ks.k[j], q);
+        head = nr != nq || (!nr && mkey_of(ks.k[j], r) != mkey_of(ks.k[j], q));
+      }
+    }
+    if (head) atomicOr(&mask[p >> 6], 1ull << (p & 63));
+  }
+}
+
+static MKey to_mkey(const SortKey& k) {
+  MKey m;
+  m.col = DevCol{k.col.dtype, k.col.values, k.col.validity, k.col.validity_offset};
+  m.rank = k.rank;
+  m.rank_len = k.rank_len;
+  m.desc = k.desc ? 1 : 0;
+  m.distinct = k.distinct ? 1 : 0;
+  return m;
+}
+
+size_t sort_multi_scratch(uint64_t n) {
+  const uint64_t words = (n + 63) / 64;
+  return sort_scratch_bytes(n, true) + words * 8 + 4 * n * 4 + 16 + 4096;
+}
+
+void op_sort_multi(Ctx& c, const SortKey* keys, int nkeys, const uint32_t* d_list, uint64_t n, uint32_t* d_pos) {
+  if (nkeys < 1 || nkeys > kMaxMultiKeys) fail(FDB_E_ARG, "between 1 and 8 sort keys");
+  if (n >= 0xFFFFFFFFull) fail(FDB_E_ARG, "a sort addresses rows as uint32");
+  if (n == 0) return;
+  for (int j = 0; j < nkeys; ++j) {
+    const SortKey& k = keys[j];
+    if (k.col.dtype != FDB_FLOAT64 && k.col.dtype != FDB_INT64 && k.col.dtype != FDB_UTF8)
+      fail(FDB_E_TYPE, "sort keys are FLOAT64, INT64 or UTF8 columns");
+    if (!k.col.values) fail(FDB_E_ARG, "column without values");
+    if (k.col.dtype == FDB_UTF8 && !k.distinct && !k.rank) fail(FDB_E_ARG, "text ORDER BY key without ranks");
+  }
+  set_scatter_smem();
+  c.ensure_scratch(c.scratch_top + sort_multi_scratch(n));
+  const uint32_t m = (uint32_t)n;
+  const unsigned g = (unsigned)std::max<uint64_t>(1, std::min<uint64_t>((n + 255) / 256, (uint64_t)c.sm_count * 8));
+  iota_u32_kernel<<<g, 256, 0, c.stream>>>(d_pos, n);
+  FDB_CUDA(cudaGetLastError());
+  const uint64_t words = (n + 63) / 64;
+  for (int j = nkeys - 1; j >= 0; --j) {
+    const size_t mark = c.scratch_top;
+    const SortKey& K = keys[j];
+    const MKey mk = to_mkey(K);
+    const bool nullable = K.col.validity != nullptr || K.col.dtype == FDB_UTF8;
+    const uint32_t* vsel = d_pos;
+    uint32_t* nsel = nullptr;
+    uint64_t mv = n, mnull = 0;
+    if (nullable) {
+      // Indices i (into the current order) of the non-NULL and the NULL keys,
+      // in order; both counts are read back before either list is used.
+      uint64_t* mask = static_cast<uint64_t*>(c.scratch_take(words * 8));
+      uint32_t* vidx = static_cast<uint32_t*>(c.scratch_take(n * 4));
+      uint32_t* nidx = static_cast<uint32_t*>(c.scratch_take(n * 4));
+      uint32_t* vs = static_cast<uint32_t*>(c.scratch_take(n * 4));
+      nsel = static_cast<uint32_t*>(c.scratch_take(n * 4));
+      uint64_t* cnt = static_cast<uint64_t*>(c.scratch_take(16));
+      const unsigned gw = (unsigned)std::max<uint64_t>(1, std::min<uint64_t>((words * 64 + 255) / 256,
+                                                                             (uint64_t)c.sm_count * 8));
+      mkey_null_mask_kernel<<<gw, 256, 0, c.stream>>>(mk, d_list, d_pos, n, false, reinterpret_cast<uint32_t*>(mask));
+      op_compact_mask(c, mask, n, vidx, n, cnt);
+      mkey_null_mask_kernel<<<gw, 256, 0, c.stream>>>(mk, d_list, d_pos, n, true, reinterpret_cast<uint32_t*>(mask));
+      op_compact_mask(c, mask, n, nidx, n, cnt + 1);
+      uint64_t hc[2] = {0, 0};
+      FDB_CUDA(cudaMemcpyAsync(hc, cnt, 16, cudaMemcpyDeviceToHost, c.stream));
+      FDB_CUDA(cudaStreamSynchronize(c.stream));
+      if (hc[0] + hc[1] != n) fail(FDB_E_GENERIC, "sort: valid and NULL positions do not add up");
+      mv = hc[0];
+      mnull = hc[1];
+      if (mv) gather_u32_kernel<<<g, 256, 0, c.stream>>>(d_pos, vidx, mv, vs);
+      if (mnull) gather_u32_kernel<<<g, 256, 0, c.stream>>>(d_pos, nidx, mnull, nsel);
+      vsel = vs;
+    }
+    if (mv > 0) {
+      auto kf = [&](uint64_t* k, uint32_t* v, unsigned long long* vary) {
+        const unsigned gk = (unsigned)std::max<uint64_t>(1, std::min<uint64_t>((mv + 255) / 256,
+                                                                               (uint64_t)c.sm_count * 8));
+        mkey_sort_key_kernel<<<gk, 256, 0, c.stream>>>(mk, d_list, vsel, (uint32_t)mv, k, v, vary);
+      };
+      radix_sort_pairs(c, (uint32_t)mv, kf, d_pos + (K.nulls_last ? 0 : mnull), nullptr, nullptr);
+    }
+    if (mnull)
+      FDB_CUDA(cudaMemcpyAsync(d_pos + (K.nulls_last ? mv : 0), nsel, mnull * 4, cudaMemcpyDeviceToDevice, c.stream));
+    FDB_CUDA(cudaGetLastError());
+    c.scratch_top = mark;
+  }
+  (void)m;
+}
+
+void op_distinct_multi(Ctx& c, const fdb_dev_column* cols, const uint32_t* const* ranks, const uint32_t* rank_lens,
+                       int ncols, const uint32_t* d_list, uint64_t n, uint32_t* d_pos, uint64_t* d_count) {
+  if (ncols < 1 || ncols > kMaxMultiKeys) fail(FDB_E_ARG, "DISTINCT over between 1 and 8 columns");
+  if (n >= 0xFFFFFFFFull) fail(FDB_E_ARG, "DISTINCT addresses rows as uint32");
+  if (n == 0) {
+    FDB_CUDA(cudaMemsetAsync(d_count, 0, 8, c.stream));
+    return;
+  }
+  const uint64_t words = (n + 63) / 64;
+  c.ensure_scratch(c.scratch_top + sort_multi_scratch(n) + n * 4 + words * 8 + 512);
+  uint32_t* order = static_cast<uint32_t*>(c.scratch_take(n * 4));
+  unsigned long long* heads = static_cast<unsigned long long*>(c.scratch_take(words * 8));
+  SortKey ks[kMaxMultiKeys];
+  MKeys mk;
+  mk.n = ncols;
+  for (int j = 0; j < ncols; ++j) {
+    ks[j] = SortKey{};
+    ks[j].col = cols[j];
+    ks[j].distinct = true;
+    if (ranks && ranks[j]) {
+      ks[j].rank = ranks[j];
+      ks[j].rank_len = rank_lens[j];
+    }
+    mk.k[j] = to_mkey(ks[j]);
+  }
+  op_sort_multi(c, ks, ncols, d_list, n, order);
+  FDB_CUDA(cudaMemsetAsync(heads, 0, words * 8, c.stream));
+  const unsigned g = (unsigned)std::max<uint64_t>(1, std::min<uint64_t>((n + 255) / 256, (uint64_t)c.sm_count * 8));
+  multi_heads_kernel<<<g, 256, 0, c.stream>>>(mk, d_list, order, n, heads);
+  FDB_CUDA(cudaGetLastError());
+  op_compact_mask(c, reinterpret_cast<const uint64_t*>(heads), n, d_pos, n, d_count);
+}
+
 }  // namespace fdb

@@ -833,6 +833,25 @@ static void fetch_rows(Plan& plan, const Rel& r, int rc, const uint32_t* d_rows,
   }
 }
 
+// The rank of every code of a text column's dictionary in the sorted
+// dictionary, on the device: byte-wise string order (Rust's str ordering,
+// which the reference's text sort uses, sort.rs:352-382); equal strings under
+// two codes get one rank.  The dictionary holds distinct strings, not rows, so
+// ranking it on the host is cheap; the rows are then sorted on the GPU.
+static const uint32_t* dict_ranks(Plan& plan, const RelCol& col) {
+  const std::vector<std::string>& d = *col.dict;
+  std::vector<uint32_t> idx(d.size());
+  std::iota(idx.begin(), idx.end(), 0u);
+  std::stable_sort(idx.begin(), idx.end(), [&](uint32_t a, uint32_t b) { return d[a] < d[b]; });
+  std::vector<uint32_t> rank(std::max<size_t>(d.size(), 1), 0);
+  for (size_t i = 0; i < idx.size(); ++i)
+    rank[idx[i]] = (i > 0 && d[idx[i]] == d[idx[i - 1]]) ? rank[idx[i - 1]] : (uint32_t)i;
+  uint32_t* dr = plan.dev<uint32_t>(rank.size());
+  // From pageable memory: the call returns once the source has been staged.
+  FDB_CUDA(cudaMemcpyAsync(dr, rank.data(), rank.size() * 4, cudaMemcpyHostToDevice, plan.c.stream));
+  return dr;
+}
+
 // ---------------------------------------------------------------------------
 // Scalar value model used for ORDER BY over host results.
 // ---------------------------------------------------------------------------
@@ -1042,11 +1061,11 @@ static void run_aggregates(Plan& plan, const Rel& rel, const Query& q, fdb_resul
       fdb_group_i64* d = plan.dev<fdb_group_i64>(cap);
       uint64_t* dn = plan.dev<uint64_t>(1);
       plan.c.scratch_reset();
-      const uint64_t eg = group_by_i64_groups(plan.c, col.dev, rel.nrows, 0);
+      const GbSizing sz = group_by_i64_sizing(plan.c, col.dev, rel.nrows, 0);
       plan.c.scratch_reset();
-      plan.c.ensure_scratch(group_by_i64_scratch(eg, 0.5) + (16u << 20));
+      plan.c.ensure_scratch(group_by_i64_scratch(sz, 0.5) + (16u << 20));
       op_group_by_i64(plan.c, col.dev, col.dev, rel.nrows, prog.data(), (int)prog.size(), pcols.data(),
-                      (int)pcols.size(), eg, 0.5, d, cap, dn);
+                      (int)pcols.size(), sz, 0.5, d, cap, dn);
       plan.check();
       const uint64_t ng = plan.one(dn);
       std::vector<fdb_group_i64> g = plan.to_host(d, ng);
@@ -1190,10 +1209,10 @@ static void run_group_by(Plan& plan, const Rel& rel, const Query& q, fdb_result*
     uint64_t* dn = plan.dev<uint64_t>(1);
     std::vector<fdb_group_i64> groups;
     if (rel.nrows > 0) {
-      const uint64_t eg = group_by_i64_groups(plan.c, key.dev, rel.nrows, 0);
-      plan.c.ensure_scratch(group_by_i64_scratch(eg, 0.5) + (16u << 20));
+      const GbSizing sz = group_by_i64_sizing(plan.c, key.dev, rel.nrows, 0);
+      plan.c.ensure_scratch(group_by_i64_scratch(sz, 0.5) + (16u << 20));
       op_group_by_i64(plan.c, key.dev, rel.cols[vc].dev, rel.nrows, prog.data(), (int)prog.size(), pcols.data(),
-                      (int)pcols.size(), eg, 0.5, d, cap, dn);
+                      (int)pcols.size(), sz, 0.5, d, cap, dn);
       plan.check();
       groups = plan.to_host(d, plan.one(dn));
     }
@@ -1248,6 +1267,39 @@ static void run_group_by(Plan& plan, const Rel& rel, const Query& q, fdb_result*
 // select.rs:238-457).
 static void emit_rows(Plan& plan, const Rel& rel, const std::vector<int>& outcols, const Query& q,
                       const uint32_t* d_list, uint64_t n, fdb_result* res) {
+  if (q.distinct && n > 0 && outcols.size() > 1) {
+    // Whole rows (dedup_batches, select.rs:238-269): the first occurrence of
+    // each distinct row of the projected columns, in list order.
+    if (outcols.size() > 8) fail(FDB_E_SQL, "SELECT DISTINCT over more than 8 columns is not supported");
+    std::vector<fdb_dev_column> cols;
+    std::vector<const uint32_t*> ranks;
+    std::vector<uint32_t> rank_lens;
+    for (int oc : outcols) {
+      const RelCol& col = rel.cols[oc];
+      cols.push_back(col.dev);
+      const bool text = col.dtype == FDB_UTF8 && col.dict;
+      ranks.push_back(text ? dict_ranks(plan, col) : nullptr);
+      rank_lens.push_back(text ? (uint32_t)col.dict->size() : 0u);
+    }
+    uint32_t* pos = plan.dev<uint32_t>(n);
+    uint64_t* dcount = plan.dev<uint64_t>(1);
+    plan.c.scratch_reset();
+    op_distinct_multi(plan.c, cols.data(), ranks.data(), rank_lens.data(), (int)cols.size(), d_list, n, pos, dcount);
+    plan.c.scratch_reset();
+    plan.check();
+    const uint64_t k = plan.one(dcount);
+    uint32_t* kept = pos;
+    if (d_list) {
+      kept = plan.dev<uint32_t>(std::max<uint64_t>(k, 1));
+      fdb_dev_column list{};
+      list.dtype = FDB_UTF8;  // 4-byte gather of row numbers
+      list.values = d_list;
+      op_gather(plan.c, list, pos, k, kept, nullptr);
+    }
+    for (size_t i = 0; i < outcols.size(); ++i) fetch_rows(plan, rel, outcols[i], kept, k, res->cols[i]);
+    res->rows = k;
+    return;
+  }
   if (q.distinct && n > 0) {
     const RelCol& col = rel.cols[outcols[0]];
     fdb_dev_column g = col.dev;
@@ -1338,7 +1390,6 @@ static void run_projection(Plan& plan, const Rel& rel_in, const Query& q, fdb_re
     }
   }
   for (size_t i = 0; i < outcols.size(); ++i) push_col(res, out_name(items[i]), rel.cols[outcols[i]].dtype);
-  if (q.distinct && outcols.size() != 1) fail(FDB_E_SQL, "SELECT DISTINCT over more than one column is not supported");
 
   // 1. Selected rows (all rows, or the WHERE survivors in row order).
   const uint64_t n = rel.nrows;
@@ -1469,12 +1520,61 @@ static void run_projection(Plan& plan, const Rel& rel_in, const Query& q, fdb_re
     }
   }
 
-  // 4. Everything else: bring the selected rows to the host; sort / limit there.
+  // 4. Several ORDER BY keys, a text key, or a key that is not projected:
+  //    stable radix sorts of the selected rows on the GPU, last key first
+  //    (sort_merged over several SortExprs, sort.rs:118-165; a text column by
+  //    the rank of its code in the sorted dictionary, sort.rs:352-382), then
+  //    the LIMIT.
+  if (!q.order.empty() && nsel > 0) {
+    if (q.order.size() > 8) fail(FDB_E_SQL, "ORDER BY over more than 8 keys is not supported");
+    std::vector<SortKey> keys;
+    for (const OrderItem& o : q.order) {
+      int oc = -1;
+      if (!o.ref.col.empty() && o.ref.col[0] == '#') {
+        const int pos = std::atoi(o.ref.col.c_str() + 1) - 1;
+        if (pos < 0 || pos >= (int)outcols.size()) fail(FDB_E_SQL, "bad ORDER BY reference");
+        oc = outcols[pos];
+      } else {
+        for (size_t i = 0; i < items.size() && oc < 0; ++i)
+          if (items[i].alias == o.ref.col || (items[i].col.col == o.ref.col &&
+                                              (o.ref.table.empty() || resolve(rel, o.ref) == outcols[i])))
+            oc = outcols[i];
+        if (oc < 0) oc = resolve(rel, o.ref);
+      }
+      const RelCol& col = rel.cols[oc];
+      SortKey k;
+      k.col = col.dev;
+      k.desc = o.desc;
+      k.nulls_last = o.nulls_last;
+      if (col.dtype == FDB_UTF8) {
+        if (!col.dict) fail(FDB_E_SQL, "ORDER BY a text column without a dictionary");
+        k.rank = dict_ranks(plan, col);
+        k.rank_len = (uint32_t)col.dict->size();
+      }
+      keys.push_back(k);
+    }
+    uint32_t* pos = plan.dev<uint32_t>(nsel);
+    plan.c.scratch_reset();
+    op_sort_multi(plan.c, keys.data(), (int)keys.size(), all_rows ? nullptr : d_rows, nsel, pos);
+    plan.c.scratch_reset();
+    uint32_t* order = pos;
+    if (!all_rows) {
+      order = plan.dev<uint32_t>(nsel);
+      fdb_dev_column rows_col{};
+      rows_col.dtype = FDB_UTF8;  // 4-byte gather of row numbers
+      rows_col.values = d_rows;
+      op_gather(plan.c, rows_col, pos, nsel, order, nullptr);
+    }
+    plan.check();
+    const uint64_t take = q.limit >= 0 ? std::min<uint64_t>((uint64_t)q.limit, nsel) : nsel;
+    emit_rows(plan, rel, outcols, q, order, take, res);
+    return;
+  }
+
+  // 5. No ORDER BY: the selected rows in row order, then the LIMIT.
   uint64_t take = nsel;
-  if (q.order.empty() && q.limit >= 0) take = std::min<uint64_t>(take, (uint64_t)q.limit);
+  if (q.limit >= 0) take = std::min<uint64_t>(take, (uint64_t)q.limit);
   if (q.distinct) {
-    if (!q.order.empty())
-      fail(FDB_E_SQL, "SELECT DISTINCT with ORDER BY over several keys or a text column is not supported");
     emit_rows(plan, rel, outcols, q, all_rows ? nullptr : d_rows, take, res);
     return;
   }
@@ -1486,36 +1586,6 @@ static void run_projection(Plan& plan, const Rel& rel_in, const Query& q, fdb_re
   }
   for (size_t i = 0; i < outcols.size(); ++i) fetch_rows(plan, rel, outcols[i], d_rows, take, res->cols[i]);
   res->rows = take;
-  if (!q.order.empty()) {
-    // ORDER BY may name a column that is not projected: fetch it as a hidden key.
-    std::vector<std::pair<int, OrderItem>> keys;
-    std::vector<SelItem> all_items = items;
-    size_t hidden = 0;
-    for (const OrderItem& o : q.order) {
-      int idx = -1;
-      if (!o.ref.col.empty() && o.ref.col[0] == '#') {
-        idx = std::atoi(o.ref.col.c_str() + 1) - 1;
-      } else {
-        for (size_t i = 0; i < items.size(); ++i)
-          if (items[i].alias == o.ref.col || (items[i].col.col == o.ref.col &&
-                                              (o.ref.table.empty() || resolve(rel, o.ref) == outcols[i])))
-            idx = (int)i;
-        if (idx < 0) {
-          const int rc = resolve(rel, o.ref);
-          fdb_result::Col hc;
-          hc.name = "__order" + std::to_string(hidden++);
-          hc.dtype = rel.cols[rc].dtype;
-          fetch_rows(plan, rel, rc, d_rows, take, hc);
-          res->cols.push_back(std::move(hc));
-          idx = (int)res->cols.size() - 1;
-        }
-      }
-      if (idx < 0 || idx >= (int)res->cols.size()) fail(FDB_E_SQL, "bad ORDER BY reference");
-      keys.push_back({idx, o});
-    }
-    apply_order_limit(res, keys, q.limit);
-    res->cols.resize(outcols.size());
-  }
 }
 
 // ---------------------------------------------------------------------------

@@ -301,3 +301,162 @@ def ref_join_agg(bkeys, bpay, pkeys, pval, join_type, threads):
 def ref_group_i64(keys, vals, threads):
     k, v = _c(keys, np.int64), _c(vals, np.float64)
     return int(lib().ref_group_i64(_p(k), _p(v), len(k), threads))
+
+
+# ---------------------------------------------------------------------------- reference MIN/MAX rules
+# Python restatements (small inputs only) of how the reference's own code
+# treats NaN and +-inf in MIN / MAX.  Its results depend on how the table is
+# cut into batches, so they take the batch size (65,536 rows in the
+# reference's tables).  The engine does not reproduce them; the tests use
+# these to record, case by case, where its batch-independent rule differs.
+REF_BATCH_ROWS = 65_536
+
+
+def _batches(n, batch_rows):
+    return [(s, min(n, s + batch_rows)) for s in range(0, n, batch_rows)] or [(0, 0)]
+
+
+def ref_minmax_nokey(values, is_min, validity=None, batch_rows=REF_BATCH_ROWS):
+    """No-key MIN / MAX (accumulate_typed, aggregate.rs:3286-3375).
+
+    Per batch: a FLOAT64 column with no NULL in the batch folds f64::min /
+    f64::max (NaN skipped) from +inf / -inf and contributes only when that
+    fold is finite (3308-3320, 3351-3363), so a batch holding -inf (MIN) or
+    +inf (MAX), or only NaN, contributes nothing.  Otherwise (NULLs present,
+    or an integer column) the valid values are scanned with `<` / `>` from
+    +inf / -inf (NaN never replaces the running value) and the batch
+    contributes its running value whenever it had any valid value, +inf /
+    -inf included (3322-3330, 3365-3373).  Batches combine with f64::min /
+    f64::max.  Returns None for SQL NULL."""
+    v = np.asarray(values)
+    is_float = v.dtype.kind == "f"
+    valid = (np.ones(len(v), bool) if validity is None else
+             np.array([(int(validity[i >> 6]) >> (i & 63)) & 1 == 1 for i in range(len(v))], dtype=bool))
+    fmin = lambda a, b: b if np.isnan(a) else (a if np.isnan(b) else min(a, b))
+    fmax = lambda a, b: b if np.isnan(a) else (a if np.isnan(b) else max(a, b))
+    comb = fmin if is_min else fmax
+    value = None
+    for s, e in _batches(len(v), batch_rows):
+        if e <= s:
+            continue
+        if is_float and valid[s:e].all():
+            chunk = float("inf") if is_min else float("-inf")
+            for x in v[s:e]:
+                chunk = comb(chunk, float(x))
+            if np.isfinite(chunk):
+                value = chunk if value is None else comb(value, chunk)
+            continue
+        cur = float("inf") if is_min else float("-inf")
+        anyv = False
+        for i in range(s, e):
+            if not valid[i]:
+                continue
+            x = float(v[i])
+            if (x < cur) if is_min else (x > cur):
+                cur = x
+            anyv = True
+        if anyv:
+            value = cur if value is None else comb(value, cur)
+    return value
+
+
+def ref_minmax_group(keys, values, is_min, batch_rows=REF_BATCH_ROWS):
+    """GROUP BY MIN / MAX (accumulate_batch, aggregate.rs:1092-1169, merged
+    by merge_state_entry, 1351-1390, in batch order).
+
+    Within a batch a group's first value is taken as it is, NaN included,
+    and a later value replaces it only when `<` (MIN) / `>` (MAX) holds, so a
+    leading NaN stays.  Batch states merge the same way.  Returns
+    {key: value}; NaN is a value here, not NULL."""
+    k = np.asarray(keys)
+    v = np.asarray(values, dtype=np.float64)
+    better = (lambda a, b: a < b) if is_min else (lambda a, b: a > b)
+    total = {}
+    for s, e in _batches(len(k), batch_rows):
+        state = {}
+        for i in range(s, e):
+            g, x = int(k[i]), float(v[i])
+            if g not in state or better(x, state[g]):
+                state[g] = x
+        for g, x in state.items():
+            if g not in total or better(x, total[g]):
+                total[g] = x
+    return total
+
+
+# ---------------------------------------------------------------------------- several sort keys, whole-row DISTINCT
+def _ord_u64(v: np.ndarray) -> np.ndarray:
+    """f64_ord_key (sort.rs:451-454) of a float64 array, or the sign flip of
+    an int64 array: unsigned keys whose order is the SQL order."""
+    if v.dtype.kind == "f":
+        b = np.ascontiguousarray(v, dtype=np.float64).view(np.uint64)
+        return np.where(b >> np.uint64(63) == 0, b ^ np.uint64(1 << 63), ~b)
+    return np.ascontiguousarray(v, dtype=np.int64).view(np.uint64) ^ np.uint64(1 << 63)
+
+
+def sort_multi(keys, n: int) -> np.ndarray:
+    """Rows 0..n-1 in ORDER BY order over several keys (sort_merged,
+    sort.rs:118-165): key by key, each ascending or descending with its NULLs
+    first or last; ties on every key keep row order.  `keys` is a list of
+    dicts: values (int64 / float64 array, or a list of str for a text
+    column), valid (bool array or None), desc, nulls_last.  Text compares as
+    bytes (Rust str ordering)."""
+    cols = []
+    for k in keys:
+        vals = k["values"]
+        valid = np.ones(n, bool) if k.get("valid") is None else np.asarray(k["valid"], bool)
+        if isinstance(vals, list):  # text: rank by byte-wise order
+            enc = [("" if s is None else s).encode() for s in vals]
+            order = sorted(range(n), key=lambda i: enc[i])
+            rank = np.zeros(n, np.uint64)
+            prev = None
+            r = 0
+            for j, i in enumerate(order):
+                if prev is not None and enc[i] != prev:
+                    r = j
+                rank[i] = r
+                prev = enc[i]
+            key = rank
+        else:
+            key = _ord_u64(np.asarray(vals))
+        if k["desc"]:
+            key = ~key
+        nul = ~valid
+        flag = np.where(nul, 1 if k["nulls_last"] else 0, 0 if k["nulls_last"] else 1).astype(np.uint64)
+        key = np.where(nul, np.uint64(0), key)
+        cols.append((flag, key))
+    # np.lexsort: the last key is primary; stable, so ties keep row order.
+    seq = []
+    for flag, key in reversed(cols):
+        seq += [key, flag]
+    return np.lexsort(seq).astype(np.uint32) if seq else np.arange(n, dtype=np.uint32)
+
+
+def distinct_multi(cols, n: int) -> np.ndarray:
+    """Rows (ascending) of the first occurrence of each distinct row over
+    several columns (dedup_batches, select.rs:238-269): NULL is one value per
+    column; float NaNs are one value and -0.0 equals +0.0 (norm_f64,
+    select.rs:201-204); text compares by value.  `cols`: list of dicts with
+    values (array, or list of str) and valid (bool array or None)."""
+    def cell(c, i):
+        valid = c.get("valid")
+        if valid is not None and not valid[i]:
+            return ("null",)
+        v = c["values"][i]
+        if isinstance(c["values"], list):
+            return ("s", v)
+        if np.asarray(c["values"]).dtype.kind == "f":
+            x = float(v)
+            if x != x:
+                return ("nan",)
+            return ("f", 0.0 if x == 0.0 else x)
+        return ("i", int(v))
+
+    seen = set()
+    out = []
+    for i in range(n):
+        t = tuple(cell(c, i) for c in cols)
+        if t not in seen:
+            seen.add(t)
+            out.append(i)
+    return np.asarray(out, dtype=np.uint32)

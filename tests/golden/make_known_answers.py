@@ -148,5 +148,35 @@ for rows in [100_000, 1_000_000]:
          "SELECT COUNT(*) AS n FROM bench WHERE NOT EXISTS (SELECT 1 FROM lookup WHERE lookup.lid = bench.id)",
          scalar=str(rows - rows // 10))
 
+# --- ORDER BY several keys / a text key, DISTINCT over whole rows ---------------------
+case("order_by_string", "tests/sql_integration.rs:210-216",
+     {"t": cols(name=("utf8", ["charlie", "alice", "bob"]))},
+     "SELECT * FROM t ORDER BY name ASC", rows=[["alice"], ["bob"], ["charlie"]])
+case("order_by_multi_key", "tests/sql_integration.rs:218-226",
+     {"t": cols(dept=("utf8", ["eng", "hr", "eng", "hr"]), score=("int64", [8, 9, 9, 7]))},
+     "SELECT * FROM t ORDER BY dept ASC, score DESC", head_rows=[["eng", "9"], ["eng", "8"], ["hr", "9"]])
+for direction, want in (("ASC", ["apple", "apple", "fig", "pear"]), ("DESC", ["pear", "fig", "apple", "apple"])):
+    case(f"sort_text_by_string_not_dictionary_position[{direction}]", "src/query/sort.rs:979-1001",
+         {"t": cols(s=("utf8", ["pear", "apple", "fig", "apple"]))},
+         f"SELECT s FROM t ORDER BY s {direction}", rows=[[w] for w in want])
+for order_by, want in (("s ASC", ["NULL", "NULL", "a", "b"]), ("s ASC NULLS LAST", ["a", "b", "NULL", "NULL"]),
+                       ("s DESC", ["b", "a", "NULL", "NULL"])):
+    case(f"sort_text_places_nulls[{order_by}]", "src/query/sort.rs:1003-1022",
+         {"t": cols(s=("utf8", ["b", None, "a", None]))},
+         f"SELECT s FROM t ORDER BY {order_by}", rows=[[w] for w in want])
+for direction in ("ASC", "DESC"):
+    case(f"sort_equal_strings_keep_row_order[{direction}]", "src/query/sort.rs:1024-1049",
+         {"t": cols(s=("utf8", ["x", "x", "x", "x"]), id=("int64", [10, 20, 30, 40]))},
+         f"SELECT id FROM t ORDER BY s {direction}", rows=[["10"], ["20"], ["30"], ["40"]])
+_distinct64 = ["%03d" % ((i * 37) % 64) for i in range(64)]
+case("sort_all_distinct_text_column", "src/query/sort.rs:1051-1060",
+     {"t": cols(s=("utf8", _distinct64))}, "SELECT s FROM t ORDER BY s", rows=[[w] for w in sorted(_distinct64)])
+case("sort_multi_key", "src/query/sort.rs:1747-1766",
+     {"t": cols(dept=("utf8", ["eng", "hr", "eng"]), score=("float64", [8.0, 9.0, 7.0]))},
+     "SELECT dept, score FROM t ORDER BY dept ASC, score DESC", rows=[["eng", "8"], ["eng", "7"], ["hr", "9"]])
+case("distinct_compares_whole_rows", "tests/sort_and_dedup_paths.rs:162-165",
+     {"t": cols(a=("int64", [1, 1, 1]), b=("utf8", ["x", "y", "x"]))},
+     "SELECT DISTINCT a, b FROM t", row_count=2)
+
 OUT.write_text(json.dumps({"generated_by": "tests/golden/make_known_answers.py", "cases": cases}, indent=1))
 print(f"wrote {len(cases)} cases to {OUT}")

@@ -74,6 +74,9 @@ def check_result(case: dict, res) -> None:
         if exp.get("sorted"):
             rows, want = sorted(rows), sorted(want)
         assert rows == want, f"{case['name']}: got {rows}, want {want}"
+    if "head_rows" in exp:
+        rows = res.to_rows()[:len(exp["head_rows"])]
+        assert rows == exp["head_rows"], f"{case['name']}: got {rows}, want {exp['head_rows']}"
     if "row_count" in exp:
         assert res.row_count() == exp["row_count"], f"{case['name']}: {res.row_count()} rows"
     if "first_col_sorted" in exp:

@@ -243,3 +243,76 @@ def test_hash_group_by_large_with_null_values_and_keys(db):
     rec = ops.to_records(out, F.GROUP_I64_DTYPE, g)
     rec = rec[np.argsort(rec["key"], kind="stable")]
     _same_groups(rec, _pandas_groups(keys, vals, vvalid))
+
+
+def _raw_groups(db, keys, vals, **kw):
+    """Groups in the order the kernel wrote them."""
+    out, ng = ops.group_by_i64(db, dev(keys), dev(vals) if not isinstance(vals, tuple) else vals, len(keys), **kw)
+    return ops.to_records(out, F.GROUP_I64_DTYPE, int(ng.item()))
+
+
+@pytest.mark.parametrize("kind", ["dense", "hashed"])
+def test_group_by_both_table_kinds(db, kind):
+    """The same Zipf groups through a direct-addressed table (keys spanning
+    0..D-1) and a hashed one (the keys scattered x 7919 + 3, so that their
+    range is far wider than the groups): equal answers; the direct-addressed
+    table writes its groups in key order."""
+    n, d = 3_000_000, 400_000
+    t = W.groupby_table(n, distinct=d, seed=77)
+    keys = t["key"] if kind == "dense" else t["key"] * 7919 + 3
+    raw = _raw_groups(db, keys, t["v"])
+    if kind == "dense":
+        assert np.all(np.diff(raw["key"]) > 0)
+    rec = raw[np.argsort(raw["key"], kind="stable")]
+    want = O.group_i64(keys, t["v"])
+    assert np.array_equal(rec["key"], want["key"]) and np.array_equal(rec["count"], want["count"])
+    assert np.array_equal(rec["min"], want["min"]) and np.array_equal(rec["max"], want["max"])
+    rel = np.abs(rec["sum"] - want["sum"]) / np.maximum(np.abs(want["sum"]), 1e-300)
+    assert rel.max() <= RTOL
+
+
+@pytest.mark.parametrize("lo", [np.iinfo(np.int64).min + 1, -5_000, np.iinfo(np.int64).max - 4_999])
+def test_dense_group_by_key_range_edges(db, lo):
+    """Direct-addressed tables over ranges at both ends of int64 (the slot
+    index is key - min in 64-bit two's complement), with INT64_MIN keys (the
+    NULL group, written after every key) and NULL values."""
+    n = 400_000
+    r = np.random.default_rng(abs(lo) % 1000)
+    keys = lo + r.integers(0, 5_000, n)
+    keys[::23] = np.iinfo(np.int64).min
+    vals = r.random(n) * 10 - 5
+    vvalid = r.random(n) > 0.2
+    vw = F.validity_words(vvalid)
+    raw = _raw_groups(db, keys, (dev(vals), dev(vw.view(np.int64))))
+    assert raw["key"][-1] == np.iinfo(np.int64).min  # the NULL group comes last
+    assert np.all(np.diff(raw["key"][:-1]) > 0)
+    rec = raw[np.argsort(raw["key"], kind="stable")]
+    _same_groups(rec, _pandas_groups(keys, vals, vvalid))
+
+
+def test_dense_group_by_with_filter_and_int_values(db):
+    n = 1_000_000
+    r = np.random.default_rng(31)
+    keys = r.integers(1_000, 60_000, n)
+    vals = r.integers(-10**12, 10**12, n)
+    sel = r.random(n) * 100
+    raw = _raw_groups(db, keys, vals, prog=[ops.cmp(0, F.GE, 40.0)], pred_cols=[dev(sel)])
+    assert np.all(np.diff(raw["key"]) > 0)
+    want = O.group_i64(keys, vals.astype(np.float64), mask=O.cmp_mask(sel, F.GE, 40.0))
+    assert np.array_equal(raw["key"], want["key"]) and np.array_equal(raw["count"], want["count"])
+    assert np.array_equal(raw["min"], want["min"]) and np.array_equal(raw["max"], want["max"])
+    rel = np.abs(raw["sum"] - want["sum"]) / np.maximum(np.abs(want["sum"]), 1e-300)
+    assert rel.max() <= RTOL
+
+
+def test_dense_group_by_capacity_error(db):
+    """An output buffer smaller than the groups: FDB_E_CAPACITY at the next
+    synchronisation, and the context stays usable."""
+    keys = np.arange(10_000, dtype=np.int64) % 5_000
+    vals = np.ones(10_000)
+    with pytest.raises(F.FalconError) as e:
+        ops.group_by_i64(db, dev(keys), dev(vals), len(keys), capacity=100)
+        db.synchronize()
+    assert e.value.code == -9
+    rec = _raw_groups(db, keys, vals)
+    assert len(rec) == 5_000 and np.all(rec["count"] == 2)

@@ -173,3 +173,45 @@ def test_join_dense_threshold(db, span_extra, dense):
     got = sorted(zip(left[:c].cpu().numpy().view(np.uint32).tolist(), right[:c].cpu().numpy().view(np.uint32).tolist()))
     assert got == sorted(zip(want_l.tolist(), want_r.tolist()))
     h.free()
+
+
+@pytest.mark.parametrize("kind", ["bits", "dense_wide", "hashed"])
+def test_semi_anti_on_every_table_path(db, kind):
+    """SEMI / ANTI with SUM(value) on the three probe paths: a dense table
+    whose key range fits a CTA's shared memory as presence bits (bit test
+    only), a dense table too wide for that (one 16-byte slot read), and a
+    hashed table.  Build keys with NULLs and INT64_MIN; probe keys below,
+    inside and above the range, NULL and INT64_MIN; NULL values."""
+    r = np.random.default_rng({"bits": 1, "dense_wide": 2, "hashed": 3}[kind])
+    # dense_wide: 700K keys get a 2^21-slot table, and a 2M-value range is
+    # dense there but wider than the 1.57M presence bits a CTA holds.
+    nb = {"bits": 400_000, "dense_wide": 700_000, "hashed": 400_000}[kind]
+    span = {"bits": 600_000, "dense_wide": 2_000_000, "hashed": 10**12}[kind]
+    keys = np.unique(r.integers(0, span, int(nb * 1.3)))
+    r.shuffle(keys)
+    keys = keys[:nb].astype(np.int64) - 5_000
+    nb = len(keys)
+    keys[0], keys[1] = -5_000, span - 5_001  # the range's two ends
+    keys[::1000] = I64.min
+    bvalid = r.random(nb) > 0.01
+    b = {"key": keys, "payload": r.integers(0, 1000, nb)}
+    npb = 3_000_001
+    pk = r.integers(int(keys[keys != I64.min].min()) - 100, int(keys.max()) + 100, npb)
+    pk[::777] = I64.min
+    pvalid = r.random(npb) > 0.02
+    vals = r.random(npb)
+    vvalid = r.random(npb) > 0.05
+    p = {"key": pk, "value": vals}
+    bvw, pvw = F.validity_words(bvalid), F.validity_words(pvalid)
+    h = ops.HashTable(db, (dev(keys), dev(bvw.view(np.int64))), dev(b["payload"]), nb)
+    assert h.dense == (kind != "hashed")
+    for jt in (F.JOIN_SEMI, F.JOIN_ANTI):
+        out = h.probe_agg((dev(pk), dev(pvw.view(np.int64))), npb, jt,
+                          value=(dev(vals), dev(F.validity_words(vvalid).view(np.int64))))
+        got = ops.to_records(out, F.JOIN_AGG_DTYPE, 1)[0]
+        want = O.join_agg(keys, b["payload"], pk, vals, jt, bvalid=bvw, pvalid=pvw,
+                          pvvalid=F.validity_words(vvalid))
+        assert got["count"] == want["count"]
+        assert got["payload_rows"] == want["payload_rows"]
+        assert abs(got["sum_value"] - want["sum_value"]) <= 1e-12 * abs(want["sum_value"])
+    h.free()

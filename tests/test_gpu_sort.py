@@ -201,3 +201,92 @@ def test_distinct_full_size_properties(db):
     first = torch.full((10_000_000,), n, dtype=torch.int64, device="cuda")
     first.scatter_reduce_(0, t, torch.arange(n, device="cuda"), reduce="amin")
     assert bool((first[vals] == r).all())
+
+
+def _sort_table(n, seed):
+    """id, a text column over an unsorted dictionary with NULLs, a nullable
+    INT64 column with many ties, and a FLOAT64 column with -0.0 / NaN."""
+    r = np.random.default_rng(seed)
+    labels = ["pear", "apple", "fig", "kiwi", "Zebra", "apple2", "é", "", "b", "ba"]
+    codes = r.integers(0, len(labels), n).astype(np.uint32)
+    codes[r.random(n) < 0.05] = 0xFFFFFFFF
+    sal = r.integers(0, 50, n)
+    sal_valid = r.random(n) > 0.1
+    score = np.round(r.random(n) * 20, 1)
+    score[::97] = -0.0
+    score[::131] = np.nan
+    return {"id": np.arange(n, dtype=np.int64), "dept": F.Utf8(codes, labels),
+            "salary": np.ma.MaskedArray(sal, mask=~sal_valid), "score": score}
+
+
+def _okey(t, name, desc, nulls_last=None):
+    col = t[name]
+    nl = desc if nulls_last is None else nulls_last
+    if isinstance(col, F.Utf8):
+        vals = [None if c == 0xFFFFFFFF else col.dictionary[c] for c in col.codes]
+        return {"values": vals, "valid": np.array([v is not None for v in vals]), "desc": desc, "nulls_last": nl}
+    if isinstance(col, np.ma.MaskedArray):
+        return {"values": np.ma.getdata(col), "valid": ~np.ma.getmaskarray(col), "desc": desc, "nulls_last": nl}
+    return {"values": col, "valid": None, "desc": desc, "nulls_last": nl}
+
+
+@pytest.mark.parametrize("order_by,keys", [
+    ("dept, salary DESC", [("dept", False, None), ("salary", True, None)]),
+    ("dept DESC NULLS FIRST, score", [("dept", True, False), ("score", False, None)]),
+    ("salary, score DESC, dept", [("salary", False, None), ("score", True, None), ("dept", False, None)]),
+    ("dept", [("dept", False, None)]),
+    ("score NULLS LAST, dept DESC", [("score", False, True), ("dept", True, None)]),
+])
+def test_order_by_several_keys_and_text_keys(db, order_by, keys):
+    """ORDER BY several keys and text keys on the GPU (stable radix passes,
+    last key first; text by dictionary rank) against the oracle's several-key
+    sort, with and without WHERE and LIMIT."""
+    n = 200_003
+    t = _sort_table(n, seed=len(order_by))
+    db.create_table("t", t)
+    order = O.sort_multi([_okey(t, k, d, nl) for k, d, nl in keys], n)
+    got = db.sql(f"SELECT id FROM t ORDER BY {order_by}").column(0)
+    assert np.array_equal(np.asarray(got), order)
+    got = db.sql(f"SELECT id FROM t ORDER BY {order_by} LIMIT 5000").column(0)
+    assert np.array_equal(np.asarray(got), order[:5000])
+    # With a WHERE: the selected rows' positions are sorted, then mapped back.
+    sel = np.flatnonzero(t["score"] > 5.0)
+    sub = {k: (F.Utf8(v.codes[sel], v.dictionary) if isinstance(v, F.Utf8) else v[sel]) for k, v in t.items()}
+    want = sel[O.sort_multi([_okey(sub, k, d, nl) for k, d, nl in keys], len(sel))]
+    got = db.sql(f"SELECT id FROM t WHERE score > 5 ORDER BY {order_by}").column(0)
+    assert np.array_equal(np.asarray(got), want)
+
+
+def test_distinct_over_several_columns(db):
+    """SELECT DISTINCT over several columns on the GPU: the first occurrence of
+    each distinct row, in row order, against the oracle's whole-row DISTINCT
+    (NULL one value per column; NaN one value; -0.0 equal to +0.0; text by
+    value, with one string under two codes)."""
+    n = 300_001
+    r = np.random.default_rng(5)
+    labels = ["x", "y", "x", "z"]  # "x" under two codes
+    codes = r.integers(0, 4, n).astype(np.uint32)
+    codes[::50] = 0xFFFFFFFF
+    a = r.integers(0, 30, n)
+    av = r.random(n) > 0.05
+    f = np.round(r.random(n) * 4) - 2.0
+    f[::7] = -0.0
+    f[::11] = np.nan
+    t = {"d": F.Utf8(codes, labels), "a": np.ma.MaskedArray(a, mask=~av), "f": f}
+    db.create_table("t", t)
+    dv = [None if c == 0xFFFFFFFF else labels[c] for c in codes]
+    cols = [{"values": dv, "valid": np.array([v is not None for v in dv])}, {"values": a, "valid": av},
+            {"values": f}]
+    want = O.distinct_multi(cols, n)
+    res = db.sql("SELECT DISTINCT d, a, f FROM t")
+    assert res.row_count() == len(want)
+    assert res.column(0) == [dv[i] for i in want]
+    got_a = [res.value(i, 1) for i in range(res.row_count())]
+    assert got_a == [int(a[i]) if av[i] else None for i in want]
+    # Two columns, after a WHERE.
+    sel = np.flatnonzero(a < 10)
+    want2 = sel[O.distinct_multi([{"values": a[sel], "valid": av[sel]}, {"values": f[sel]}], len(sel))]
+    res2 = db.sql("SELECT DISTINCT a, f FROM t WHERE a < 10")
+    assert res2.row_count() == len(want2)
+    got_f = np.asarray([res2.value(i, 1) for i in range(res2.row_count())], dtype=np.float64)
+    assert np.array_equal(got_f, f[want2], equal_nan=True)

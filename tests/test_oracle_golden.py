@@ -368,3 +368,64 @@ def test_reference_engine_agrees_with_the_serial_oracle():
             assert ps == o["sum_payload"]
         else:
             assert abs(vs - o["sum_value"]) <= abs(o["sum_value"]) * 1e-12
+
+
+def _key(t, name, desc=False, nulls_last=None):
+    """A sort_multi key over column `name` of a known-answer table."""
+    col = t[name]
+    if isinstance(col, F.Utf8):
+        vals = [None if c == 0xFFFFFFFF else col.dictionary[c] for c in col.codes]
+        valid = np.array([v is not None for v in vals])
+        return {"values": vals, "valid": valid, "desc": desc, "nulls_last": desc if nulls_last is None else nulls_last}
+    vd, data = _valid(col)
+    valid = None if vd is None else ~np.ma.getmaskarray(col)
+    return {"values": np.asarray(data), "valid": valid, "desc": desc,
+            "nulls_last": desc if nulls_last is None else nulls_last}
+
+
+def _cells(t, name, order):
+    col = t[name]
+    if isinstance(col, F.Utf8):
+        return ["NULL" if col.codes[r] == 0xFFFFFFFF else col.dictionary[col.codes[r]] for r in order]
+    return [str(int(col[r])) if np.asarray(col).dtype.kind == "i" else ("%g" % col[r]) for r in order]
+
+
+@pytest.mark.parametrize("name,keys,outcols", [
+    ("order_by_string", [("name", False, None)], ["name"]),
+    ("order_by_multi_key", [("dept", False, None), ("score", True, None)], ["dept", "score"]),
+    ("sort_text_by_string_not_dictionary_position[ASC]", [("s", False, None)], ["s"]),
+    ("sort_text_by_string_not_dictionary_position[DESC]", [("s", True, None)], ["s"]),
+    ("sort_text_places_nulls[s ASC]", [("s", False, None)], ["s"]),
+    ("sort_text_places_nulls[s ASC NULLS LAST]", [("s", False, True)], ["s"]),
+    ("sort_text_places_nulls[s DESC]", [("s", True, None)], ["s"]),
+    ("sort_equal_strings_keep_row_order[ASC]", [("s", False, None)], ["id"]),
+    ("sort_equal_strings_keep_row_order[DESC]", [("s", True, None)], ["id"]),
+    ("sort_all_distinct_text_column", [("s", False, None)], ["s"]),
+    ("sort_multi_key", [("dept", False, None), ("score", True, None)], ["dept", "score"]),
+])
+def test_multi_key_and_text_sort_known_answers(name, keys, outcols):
+    """sql_integration.rs:210-226 and sort.rs:979-1060, 1747-1766 restated
+    on the oracle's several-key sort (sort_merged, sort.rs:118-165; text by
+    string, sort.rs:352-382; NULLs first ascending unless NULLS LAST)."""
+    c = _case(name)
+    t = build_table(c["tables"]["t"])
+    n = len(next(iter(t.values())).codes if isinstance(next(iter(t.values())), F.Utf8) else next(iter(t.values())))
+    order = O.sort_multi([_key(t, k, d, nl) for k, d, nl in keys], n)
+    got = [list(r) for r in zip(*[_cells(t, oc, order) for oc in outcols])]
+    exp = c["expect"]
+    want = exp.get("rows") or exp.get("head_rows")
+    assert got[:len(want)] == want
+
+
+def test_distinct_whole_rows_known_answer():
+    """tests/sort_and_dedup_paths.rs:162-165 on the oracle's whole-row DISTINCT,
+    plus NULLs as one value and float equality across columns."""
+    c = _case("distinct_compares_whole_rows")
+    t = build_table(c["tables"]["t"])
+    a, b = t["a"], t["b"]
+    cols = [{"values": np.asarray(a)}, {"values": [b.dictionary[x] for x in b.codes]}]
+    assert len(O.distinct_multi(cols, 3)) == c["expect"]["row_count"]
+    x = np.array([1.0, np.nan, -0.0, 0.0, 1.0, np.nan])
+    y = np.array([5, 6, 7, 7, 5, 6])
+    yv = np.array([True, False, True, True, True, False])
+    assert list(O.distinct_multi([{"values": x}, {"values": y, "valid": yv}], 6)) == [0, 1, 2]
