@@ -171,6 +171,9 @@ _SIGS = {
     "fdb_aggregate_noalloc": (C.c_int, [C.c_void_p, C.POINTER(fdb_dev_column), C.c_int32, C.c_uint64,
                                         C.POINTER(fdb_pred_term), C.c_int32, C.POINTER(fdb_agg_spec), C.c_int32,
                                         C.c_void_p]),
+    "fdb_test_stall": (C.c_int, [C.c_void_p, C.c_uint64, C.c_uint32]),
+    "fdb_dict_remap": (C.c_int, [C.c_void_p, C.c_void_p, C.c_uint64, C.c_void_p, C.c_uint32, C.c_void_p, C.c_void_p,
+                                 C.c_uint64, C.c_void_p]),
     "fdb_distinct_codes": (C.c_int, [C.c_void_p, C.POINTER(fdb_dev_column), C.c_int32, C.c_uint64,
                                      C.POINTER(fdb_pred_term), C.c_int32, C.c_int32, C.c_uint32, C.c_void_p]),
     "fdb_group_by_codes": (C.c_int, [C.c_void_p, C.POINTER(fdb_dev_column), C.c_int32, C.c_uint64,
@@ -268,6 +271,16 @@ def validity_words(valid: np.ndarray) -> np.ndarray:
     padded = np.zeros(((n + 63) // 64) * 64, dtype=bool)
     padded[:n] = valid
     return np.packbits(padded.reshape(-1, 8), axis=1, bitorder="little").reshape(-1).view(np.uint64).copy()
+
+
+class DeviceUtf8(Utf8):
+    """A text column whose codes are already on the device (a CUDA tensor of
+    int32 holding uint32 codes, e.g. from fdb_dict_remap); create_table copies
+    them device to device."""
+
+    def __init__(self, codes, dictionary: Sequence[str]):
+        self.codes = codes
+        self.dictionary = [str(s) for s in dictionary]
 
 
 ColumnLike = Union[np.ndarray, Utf8, "np.ma.MaskedArray"]
@@ -475,7 +488,10 @@ class Database:
             keep += [values, validity]
             cols[j].name = cname.encode()
             cols[j].dtype = dtype
-            cols[j].values = values.ctypes.data if len(values) else None
+            if hasattr(values, "data_ptr"):  # device codes (DeviceUtf8)
+                cols[j].values = values.data_ptr() if len(values) else None
+            else:
+                cols[j].values = values.ctypes.data if len(values) else None
             cols[j].validity = validity.ctypes.data if validity is not None else None
         rc = lib().fdb_table_from_columns(self.handle, name.encode(), cols, len(columns), n or 0)
         check(rc)
@@ -567,7 +583,7 @@ class Database:
 
 
 __all__ = [
-    "Database", "Result", "Utf8", "DevColumn", "FalconError", "lib", "check", "version", "validity_words",
+    "Database", "Result", "Utf8", "DeviceUtf8", "DevColumn", "FalconError", "lib", "check", "version", "validity_words",
     "INT64", "FLOAT64", "UTF8", "EQ", "NE", "LT", "LE", "GT", "GE", "AGG_COUNT_STAR", "AGG_COUNT", "AGG_SUM",
     "AGG_AVG", "AGG_MIN", "AGG_MAX", "AGG_COUNT_DISTINCT", "JOIN_INNER", "JOIN_LEFT", "JOIN_SEMI", "JOIN_ANTI",
     "NO_ROW", "EXPORTED",

@@ -269,10 +269,10 @@ int64_t fdb_table_from_columns(fdb_db* db, const char* name, const fdb_column* c
           const fdb_column& hc = cols[i];
           const size_t vbytes = nrows * dtype_size(hc.dtype);
           if (vbytes)
-            FDB_CUDA(cudaMemcpyAsync(col.values.ptr, hc.values, vbytes, cudaMemcpyHostToDevice, c.upload));
+            FDB_CUDA(cudaMemcpyAsync(col.values.ptr, hc.values, vbytes, cudaMemcpyDefault, c.upload));
           if (hc.validity && nrows)
             FDB_CUDA(cudaMemcpyAsync(col.validity.ptr, hc.validity, ((nrows + 63) / 64) * 8,
-                                     cudaMemcpyHostToDevice, c.upload));
+                                     cudaMemcpyDefault, c.upload));
           if (hc.dtype == FDB_UTF8) {
             col.dict.clear();
             for (uint32_t d = 0; d < hc.dict_len; ++d) col.dict.emplace_back(hc.dict[d] ? hc.dict[d] : "");
@@ -306,9 +306,9 @@ int64_t fdb_table_from_columns(fdb_db* db, const char* name, const fdb_column* c
         FDB_CUDA(cudaEventCreateWithFlags(&col.ready, cudaEventDisableTiming));
         FDB_CUDA(cudaEventRecord(col.ready, c.stream));
         FDB_CUDA(cudaStreamWaitEvent(c.upload, col.ready, 0));
-        if (vbytes) FDB_CUDA(cudaMemcpyAsync(col.values.ptr, hc.values, vbytes, cudaMemcpyHostToDevice, c.upload));
+        if (vbytes) FDB_CUDA(cudaMemcpyAsync(col.values.ptr, hc.values, vbytes, cudaMemcpyDefault, c.upload));
         if (hc.validity && wbytes)
-          FDB_CUDA(cudaMemcpyAsync(col.validity.ptr, hc.validity, wbytes, cudaMemcpyHostToDevice, c.upload));
+          FDB_CUDA(cudaMemcpyAsync(col.validity.ptr, hc.validity, wbytes, cudaMemcpyDefault, c.upload));
         if (hc.dtype == FDB_UTF8) {
           need(hc.dict != nullptr || hc.dict_len == 0, "Utf8 column without a dictionary");
           for (uint32_t d = 0; d < hc.dict_len; ++d) col.dict.emplace_back(hc.dict[d] ? hc.dict[d] : "");
@@ -521,6 +521,25 @@ int fdb_aggregate_noalloc(fdb_db* db, const fdb_dev_column* cols, int32_t ncols,
     std::lock_guard<std::recursive_mutex> lk(db->ctx.mu);
     FDB_CUDA(cudaSetDevice(db->ctx.device));
     op_aggregate_noalloc(db->ctx, cols, ncols, nrows, prog, nterms, aggs, naggs, d_out);
+  });
+}
+
+int fdb_dict_remap(fdb_db* db, const int32_t* d_idx, uint64_t nrows, const uint64_t* d_chunk_start,
+                   uint32_t nchunks, const uint32_t* d_remap, const uint64_t* d_remap_off, uint64_t remap_len,
+                   uint32_t* d_codes) {
+  if (!db) return set_error(FDB_E_ARG, "fdb_dict_remap: db is NULL");
+  return guarded([&] {
+    CallScope s(db, default_scratch(db->ctx));
+    op_dict_remap(s.c, d_idx, nrows, d_chunk_start, nchunks, d_remap, d_remap_off, remap_len, d_codes);
+  });
+}
+
+int fdb_test_stall(fdb_db* db, uint64_t tile, uint32_t spin_limit) {
+  if (!db) return set_error(FDB_E_ARG, "fdb_test_stall: db is NULL");
+  return guarded([&] {
+    std::lock_guard<std::recursive_mutex> lk(db->ctx.mu);
+    FDB_CUDA(cudaSetDevice(db->ctx.device));
+    stream_test_stall(db->ctx, tile, spin_limit);
   });
 }
 

@@ -134,6 +134,15 @@ void op_aggregate(Ctx& c, const fdb_dev_column* cols, int ncols, uint64_t n,
 void op_aggregate_noalloc(Ctx& c, const fdb_dev_column* cols, int ncols, uint64_t n,
                           const fdb_pred_term* prog, int nterms, const fdb_agg_spec* aggs, int naggs,
                           fdb_agg_value* d_out);
+// Merged text codes of n rows from per-chunk dictionary indices (k_dict.cu):
+// chunk c holds rows [chunk_start[c], chunk_start[c+1]) (chunk_start has
+// nchunks + 1 entries, the first 0, the last n); row i's index k >= 0 maps to
+// remap[remap_off[c] + k], k < 0 to the NULL code.
+void op_dict_remap(Ctx& c, const int32_t* d_idx, uint64_t n, const uint64_t* d_chunk_start, uint32_t nchunks,
+                   const uint32_t* d_remap, const uint64_t* d_remap_off, uint64_t remap_len, uint32_t* d_codes);
+// Test hook of the bounded waits (stream.cuh StreamHook) for the streamed
+// scans of k_scan.cu on the current device; tile = ~0 clears it.
+void stream_test_stall(Ctx& c, uint64_t tile, uint32_t spin_limit);
 void op_distinct_codes(Ctx& c, const fdb_dev_column* cols, int ncols, uint64_t n,
                        const fdb_pred_term* prog, int nterms, int code_col, uint32_t dict_len,
                        uint64_t* d_bitmap);

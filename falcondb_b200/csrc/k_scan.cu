@@ -666,6 +666,16 @@ void op_aggregate_noalloc(Ctx& c, const fdb_dev_column* cols, int ncols, uint64_
   launch_stream_nc<ScanAggOp>(c, cols, ncols, n, p, ScanAggOp::kSmem);
 }
 
+// The bounded-wait test hook of this file's streamed scans (fdb_aggregate,
+// fdb_filter_count, ...): see StreamHook.  tile = ~0 clears it.
+void stream_test_stall(Ctx& c, uint64_t tile, uint32_t spin_limit) {
+  StreamHook h{};
+  h.withhold_tile1 = tile == ~0ull ? 0 : tile + 1;
+  h.spin_limit = spin_limit;
+  FDB_CUDA(cudaMemcpyToSymbolAsync(g_stream_hook, &h, sizeof(h), 0, cudaMemcpyHostToDevice, c.stream));
+  FDB_CUDA(cudaStreamSynchronize(c.stream));
+}
+
 template <typename S, typename T>
 static void launch_cmp_count(Ctx& c, const fdb_dev_column* cols, uint64_t n, const ScanAggParams& p, int op) {
   switch (op) {

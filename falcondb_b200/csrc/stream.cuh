@@ -16,6 +16,21 @@
 
 namespace fdb {
 
+// Test hook for the bounded waits (set through fdb_test_stall).  When
+// withhold_tile1 = t + 1, the producer of the CTA that is to stage tile t
+// stops before that tile's bulk copy, so its consumers' wait on the tile runs
+// out (after spin_limit polls when nonzero, else kSpinLimit): the kernel
+// records kErrTimeout and still ends.  Every copy issued before the stop has
+// been waited for by then, so none is in flight when the CTA exits.  Each
+// translation unit has its own zero (inactive) copy; only the one in
+// k_scan.cu (the aggregate scans) is ever set.
+struct StreamHook {
+  uint64_t withhold_tile1;
+  uint32_t spin_limit;
+  uint32_t _pad;
+};
+static __device__ StreamHook g_stream_hook;
+
 template <int NC>
 struct StreamSrc {
   const unsigned char* base[NC];  // device pointers to row 0 of each column
@@ -122,6 +137,8 @@ __global__ void __launch_bounds__((NCW + 1) * 32, MINB)
   __syncthreads();
 
   const uint64_t ntiles = (src.m_end + TR - 1) / TR;
+  const StreamHook hook = g_stream_hook;
+  const uint32_t spin_limit = hook.spin_limit ? hook.spin_limit : kSpinLimit;
 
   if (warp == NCW) {
     // ---------------- producer warp ----------------
@@ -143,6 +160,7 @@ __global__ void __launch_bounds__((NCW + 1) * 32, MINB)
           }
           tile_id[s] = (uint32_t)t;
         }
+        if (!DYN && hook.withhold_tile1 && t + 1 == hook.withhold_tile1) break;  // test hook only
         const uint64_t r0 = t * TR;
         const uint32_t rows = (uint32_t)umin64(TR, src.m_end - r0);
         uint32_t bytes = 0;
@@ -178,12 +196,12 @@ __global__ void __launch_bounds__((NCW + 1) * 32, MINB)
     if constexpr (DYN) {
       // The wait's outcome is made warp-uniform so that the warp collectives
       // inside Op::step stay converged; a warp that timed out stops here.
-      if (!__all_sync(0xffffffffu, mbar_wait(&full[s], ph, err))) break;
+      if (!__all_sync(0xffffffffu, mbar_wait(&full[s], ph, err, spin_limit))) break;
       const uint32_t tid = tile_id[s];
       if (tid == 0xFFFFFFFFu) break;
       t = tid;
     } else {
-      if (!dead && !mbar_wait(&full[s], ph, err)) dead = true;
+      if (!dead && !mbar_wait(&full[s], ph, err, spin_limit)) dead = true;
     }
     const uint64_t r0 = t * TR;
     const uint32_t rows = (uint32_t)umin64(TR, src.m_end - r0);

@@ -5,10 +5,19 @@ arrow_array_to_falcon, 118-231).
 The file is decoded on the host by pyarrow's multi-threaded reader, every
 column is converted to the engine's layout, and the table is uploaded once
 with ``Database.create_table``.  Text columns get ONE dictionary for the whole
-file, in first-appearance order.  The reference builds a dictionary per
-65,536-row batch (column.rs:1320-1346) and its Utf8 GROUP BY reads batch 0's
-dictionary for every batch (aggregate.rs:655-658), which mislabels groups when
-batches disagree.  A global dictionary cannot.
+file.  The reference builds a dictionary per 65,536-row batch
+(column.rs:1320-1346) and its Utf8 GROUP BY reads batch 0's dictionary for
+every batch (aggregate.rs:655-658), which mislabels groups when batches
+disagree.  A global dictionary cannot.
+
+``load_parquet`` builds that dictionary on the GPU side: text columns are
+read dictionary-encoded, the host merges only the row groups' dictionaries
+(distinct strings; merged order: chunk by chunk, each chunk's dictionary in
+its own order, which for dictionaries written in order of first appearance
+is the file's first-appearance order), each row group's indices are copied
+to the device unchanged, and fdb_dict_remap turns them into merged codes
+there.  ``read_parquet_columns`` returns host columns instead, with the
+dictionary renumbered by first appearance in the rows.
 
 Type mapping (the engine holds INT64, FLOAT64 and UTF8 columns):
 
@@ -132,11 +141,95 @@ def read_parquet_columns(path: str, columns: Optional[Sequence[str]] = None
     return out, table.num_rows
 
 
+def _merge_chunk_dictionaries(arr):
+    """The merged dictionary of a dictionary-encoded text column (strings in
+    order of first appearance in the chunks' dictionaries, chunk by chunk)
+    and, per chunk, the merged code of each of its dictionary entries.  Only
+    the dictionaries are read here: they hold distinct strings, not rows."""
+    merged: Dict[str, int] = {}
+    words: List[str] = []
+    remaps = []
+    for ch in arr.chunks:
+        d = ch.dictionary.to_pylist()
+        r = np.empty(len(d), dtype=np.uint32)
+        for j, w in enumerate(d):
+            w = str(w)
+            g = merged.get(w)
+            if g is None:
+                g = merged[w] = len(words)
+                words.append(w)
+            r[j] = g
+        remaps.append(r)
+    return words, remaps
+
+
+def _text_on_device(db: Database, arr):
+    """A dictionary-encoded text column as device codes over one merged
+    dictionary: each chunk's indices are copied to the device as they are,
+    and fdb_dict_remap turns them into merged codes there."""
+    import torch
+
+    from . import DeviceUtf8, check, lib
+    from .ops import _Fenced, _dev
+
+    pa, _, _ = _pa()
+    dev = _dev(db)
+    n = len(arr)
+    words, remaps = _merge_chunk_dictionaries(arr)
+    starts = np.zeros(len(arr.chunks) + 1, dtype=np.uint64)
+    idx = torch.empty(max(1, n), dtype=torch.int32, device=dev)
+    at = 0
+    for c, ch in enumerate(arr.chunks):
+        m = len(ch)
+        if m:
+            local = np.asarray(ch.indices.cast(pa.int32()).fill_null(-1).to_numpy(zero_copy_only=False),
+                               dtype=np.int32)
+            idx[at:at + m].copy_(torch.from_numpy(local))
+        at += m
+        starts[c + 1] = at
+    offs = np.zeros(len(remaps), dtype=np.uint64)
+    if len(remaps) > 1:
+        offs[1:] = np.cumsum([len(r) for r in remaps[:-1]])
+    remap = np.concatenate(remaps) if remaps else np.zeros(0, np.uint32)
+    d_starts = torch.from_numpy(starts.view(np.int64)).to(dev)
+    d_offs = torch.from_numpy(offs.view(np.int64)).to(dev)
+    d_remap = torch.from_numpy(np.ascontiguousarray(remap).view(np.int32) if len(remap) else
+                               np.zeros(1, np.int32)).to(dev)
+    codes = torch.empty(max(1, n), dtype=torch.int32, device=dev)
+    with _Fenced(db):
+        check(lib().fdb_dict_remap(db.handle, idx.data_ptr(), n, d_starts.data_ptr(), len(arr.chunks),
+                                   d_remap.data_ptr(), d_offs.data_ptr(), len(remap), codes.data_ptr()))
+    return DeviceUtf8(codes[:n], words), (idx, d_starts, d_offs, d_remap)
+
+
 def load_parquet(db: Database, path: str, table: str, columns: Optional[Sequence[str]] = None) -> int:
     """Read a Parquet file into device table `table` (created or replaced);
-    returns the row count."""
-    cols, n = read_parquet_columns(path, columns)
-    if not cols:
+    returns the row count.  Numeric columns are decoded on the host; text
+    columns keep their per-row-group dictionaries until the GPU merges them
+    (fdb_dict_remap), so no string and no per-row code is built on the host."""
+    pa, _, pq = _pa()
+    try:
+        schema = pq.read_schema(path)
+        want = list(columns) if columns is not None else list(schema.names)
+        text = [f.name for f in schema if f.name in want and (pa.types.is_string(f.type) or
+                                                               pa.types.is_large_string(f.type))]
+        tbl = pq.read_table(path, columns=want, use_threads=True, read_dictionary=text)
+    except (OSError, ValueError, KeyError) as e:
+        raise FalconError(-1, f"cannot read {path}: {e}") from None
+    if not tbl.column_names:
         raise FalconError(-2, f"{path}: no columns to load")
+    n = tbl.num_rows
+    cols: Dict[str, ColumnLike] = {}
+    keep = []
+    for name in tbl.column_names:
+        arr = tbl.column(name)
+        t = arr.type
+        if (pa.types.is_dictionary(t) and (pa.types.is_string(t.value_type) or pa.types.is_large_string(t.value_type))
+                and n > 0):
+            cols[name], bufs = _text_on_device(db, arr)
+            keep.append(bufs)
+        else:
+            cols[name] = _convert(name, arr)
     db.create_table(table, cols, nrows=n)
+    db.synchronize()  # the device codes were copied into the table before the buffers go
     return n

@@ -55,11 +55,10 @@ def _all_gather_bytes(buf: np.ndarray, group=None) -> List[np.ndarray]:
     return [o.cpu().numpy() for o in out]
 
 
-def combine_aggregates(local: np.ndarray, funcs: Sequence[int], group=None) -> np.ndarray:
-    """Combine every rank's no-key aggregate records (AGG_VALUE_DTYPE, one per
-    func, as fdb_aggregate returns them) into the global ones, on every rank.
-    Partials are folded in rank order, so FP64 results are repeatable."""
-    parts = [p.view(AGG_VALUE_DTYPE) for p in _all_gather_bytes(local.view(np.uint8), group)]
+def fold_aggregates(parts: Sequence[np.ndarray], funcs: Sequence[int]) -> np.ndarray:
+    """Fold per-rank no-key aggregate records (AGG_VALUE_DTYPE, one per func,
+    as fdb_aggregate returns them; parts in rank order) into the global ones.
+    FP64 partials are folded in rank order, so results are repeatable."""
     out = np.zeros(len(funcs), dtype=AGG_VALUE_DTYPE)
     for j, f in enumerate(funcs):
         recs = [p[j] for p in parts]
@@ -98,6 +97,12 @@ def combine_aggregates(local: np.ndarray, funcs: Sequence[int], group=None) -> n
     return out
 
 
+def combine_aggregates(local: np.ndarray, funcs: Sequence[int], group=None) -> np.ndarray:
+    """fold_aggregates over every rank's records, on every rank."""
+    parts = [p.view(AGG_VALUE_DTYPE) for p in _all_gather_bytes(local.view(np.uint8), group)]
+    return fold_aggregates(parts, funcs)
+
+
 def combine_presence(local_words: np.ndarray, group=None) -> np.ndarray:
     """COUNT(DISTINCT code): OR of every rank's dictionary-code presence bitmap."""
     parts = _all_gather_bytes(local_words.view(np.uint8), group)
@@ -107,16 +112,18 @@ def combine_presence(local_words: np.ndarray, group=None) -> np.ndarray:
     return out
 
 
-def combine_topk(keys: np.ndarray, rows: np.ndarray, k: int, group=None) -> Tuple[np.ndarray, np.ndarray]:
-    """Merge every rank's k best (order key, global row) pairs, each rank's
-    list padded to k, into the global k best (ascending (key, row)), on every rank."""
+def _pad_topk(keys: np.ndarray, rows: np.ndarray, k: int) -> np.ndarray:
     pk = np.full(k, np.iinfo(np.uint64).max, dtype=np.uint64)
     pr = np.full(k, np.iinfo(np.uint64).max, dtype=np.uint64)
     m = min(k, len(keys))
     pk[:m] = np.asarray(keys, dtype=np.uint64)[:m]
     pr[:m] = np.asarray(rows, dtype=np.uint64)[:m]
-    both = np.concatenate([pk, pr]).view(np.uint8)
-    parts = [p.view(np.uint64) for p in _all_gather_bytes(both, group)]
+    return np.concatenate([pk, pr])
+
+
+def fold_topk(parts: Sequence[np.ndarray], k: int) -> Tuple[np.ndarray, np.ndarray]:
+    """Merge per-rank padded (key[k], row[k]) lists into the global k best
+    (ascending (order key, global row))."""
     ak = np.concatenate([p[:k] for p in parts])
     ar = np.concatenate([p[k:] for p in parts])
     live = ~((ak == np.iinfo(np.uint64).max) & (ar == np.iinfo(np.uint64).max))
@@ -125,10 +132,16 @@ def combine_topk(keys: np.ndarray, rows: np.ndarray, k: int, group=None) -> Tupl
     return ak[order], ar[order]
 
 
-def combine_join(local: np.ndarray, group=None) -> np.ndarray:
-    """Sum every rank's join partial (JOIN_AGG_DTYPE: count, sum_payload,
+def combine_topk(keys: np.ndarray, rows: np.ndarray, k: int, group=None) -> Tuple[np.ndarray, np.ndarray]:
+    """Merge every rank's k best (order key, global row) pairs, each rank's
+    list padded to k, into the global k best (ascending (key, row)), on every rank."""
+    parts = [p.view(np.uint64) for p in _all_gather_bytes(_pad_topk(keys, rows, k).view(np.uint8), group)]
+    return fold_topk(parts, k)
+
+
+def fold_join(parts: Sequence[np.ndarray]) -> np.ndarray:
+    """Sum per-rank join partials (JOIN_AGG_DTYPE records: count, sum_payload,
     payload_rows exact; sum_value folded in rank order)."""
-    parts = [p.view(JOIN_AGG_DTYPE)[0] for p in _all_gather_bytes(local.view(np.uint8), group)]
     out = np.zeros(1, dtype=JOIN_AGG_DTYPE)
     for f in ("count", "sum_payload", "payload_rows"):
         out[0][f] = sum(int(p[f]) for p in parts)
@@ -136,6 +149,27 @@ def combine_join(local: np.ndarray, group=None) -> np.ndarray:
     for p in parts:
         acc += float(p["sum_value"])
     out[0]["sum_value"] = acc
+    return out
+
+
+def combine_join(local: np.ndarray, group=None) -> np.ndarray:
+    """fold_join over every rank's join partial, on every rank."""
+    return fold_join([p.view(JOIN_AGG_DTYPE)[0] for p in _all_gather_bytes(local.view(np.uint8), group)])
+
+
+def all_gather_parts(parts: Sequence[np.ndarray], group=None) -> List[List[np.ndarray]]:
+    """Several fixed-size byte arrays from every rank in one collective:
+    result[r][j] is rank r's array j (same sizes on every rank)."""
+    sizes = [int(np.ascontiguousarray(p).view(np.uint8).size) for p in parts]
+    flat = (np.concatenate([np.ascontiguousarray(p).view(np.uint8).ravel() for p in parts]) if parts
+            else np.zeros(0, np.uint8))
+    out = []
+    for blob in _all_gather_bytes(flat, group):
+        o, off = [], 0
+        for sz in sizes:
+            o.append(blob[off:off + sz])
+            off += sz
+        out.append(o)
     return out
 
 

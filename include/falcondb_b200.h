@@ -191,7 +191,9 @@ const char* fdb_last_error(void);
 
 /* Create (or replace) table `name` from host columns; the values are copied to
  * HBM (asynchronously on an upload stream when `host` buffers are pinned) and the
- * library owns the device copy.  Replaces the loaders falcondb_load_csv /
+ * library owns the device copy.  A values or validity pointer may also be device
+ * memory on the context's device (e.g. fdb_dict_remap's output), copied device
+ * to device after the work already queued on the context's stream.  Replaces the loaders falcondb_load_csv /
  * falcondb_load_fdb (c_ffi.rs:41-79) and Database::create_table_from_batches
  * (db.rs:180-204) for in-memory columns. Returns rows loaded or a negative code. */
 int64_t fdb_table_from_columns(fdb_db* db, const char* name, const fdb_column* cols,
@@ -313,6 +315,32 @@ int fdb_aggregate(fdb_db* db, const fdb_dev_column* cols, int32_t ncols,
 int fdb_aggregate_noalloc(fdb_db* db, const fdb_dev_column* cols, int32_t ncols,
                           uint64_t nrows, const fdb_pred_term* prog, int32_t nterms,
                           const fdb_agg_spec* aggs, int32_t naggs, fdb_agg_value* d_out);
+
+/* Merged dictionary codes of a text column read in chunks (a Parquet file's
+ * row groups, each with its own dictionary; read_parquet, parquet_io.rs:290-500,
+ * with per-batch dictionaries, column.rs:1320-1346).  Device pointers:
+ * d_idx[nrows] holds each row's index into its chunk's dictionary (negative =
+ * NULL); chunk c covers rows [d_chunk_start[c], d_chunk_start[c+1])
+ * (nchunks + 1 entries, 0 first, nrows last); d_remap[d_remap_off[c] + k] is the
+ * merged code of entry k of chunk c's dictionary (remap_len entries in all).
+ * Writes d_codes[nrows] (NULL rows: 0xFFFFFFFF), ready to be the values of an
+ * FDB_UTF8 column (fdb_table_from_columns accepts device buffers).  An index
+ * past its chunk's dictionary is reported as FDB_E_CAPACITY at the next
+ * fdb_synchronize.  Asynchronous on the context's stream. */
+int fdb_dict_remap(fdb_db* db, const int32_t* d_idx, uint64_t nrows, const uint64_t* d_chunk_start,
+                   uint32_t nchunks, const uint32_t* d_remap, const uint64_t* d_remap_off, uint64_t remap_len,
+                   uint32_t* d_codes);
+
+/* Test hook for the device-side bounded waits (no counterpart in the
+ * reference, which has no device).  After this call, the streamed scans of
+ * fdb_aggregate / fdb_filter_count / fdb_aggregate_noalloc on this context's
+ * device stop staging input before tile `tile` (a tile is a few thousand rows),
+ * so the CTA that processes it finds its wait for the tile unanswered; the wait
+ * gives up after `spin_limit` polls (0 = the normal bound), the kernel records
+ * a time-out and ends, and the next fdb_synchronize returns FDB_E_TIMEOUT.
+ * Results of calls made while the hook is set are meaningless.  tile =
+ * UINT64_MAX clears the hook; the context stays usable throughout. */
+int fdb_test_stall(fdb_db* db, uint64_t tile, uint32_t spin_limit);
 
 /* Presence bitmap of the dictionary codes that occur among rows passing `prog`
  * (present_codes, aggregate.rs:3167-3200): d_bitmap holds ceil(dict_len/64)

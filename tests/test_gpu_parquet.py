@@ -37,3 +37,39 @@ def test_parquet_load_then_group_by(db, tmp_path):
         assert got[d][0] == cnt and abs(got[d][1] - s) <= RTOL * s and got[d][2] == avg
     assert db.sql("SELECT COUNT(*) FROM pt WHERE score > 50").column(0)[0] == int((t["score"] > 50).sum())
     db.drop_table("pt")
+
+
+def test_parquet_text_columns_merged_on_the_gpu(db, tmp_path):
+    """Several row groups whose dictionaries list the departments in different
+    orders (and one that lacks most of them), NULL text values, and a second
+    text column: the loader merges the dictionaries and fdb_dict_remap
+    rewrites every row's code on the device; answers by department name equal
+    the oracle's, and every row's string equals the file's."""
+    n = 200_000
+    r = np.random.default_rng(8)
+    codes = r.integers(0, 12, n)
+    depts = np.array(W.DEPTS, dtype=object)[codes]
+    depts[:20_000] = np.where(np.arange(20_000) % 3 == 0, "d07", "d01")  # group 0: two departments
+    depts[20_000:40_000] = sorted(depts[20_000:40_000], reverse=True)    # group 1: d11 first
+    nulls = r.random(n) < 0.03
+    depts_n = [None if nulls[i] else depts[i] for i in range(n)]
+    city = np.array(["oslo", "lima", "kyiv", "pune"], dtype=object)[r.integers(0, 4, n)]
+    score = r.random(n) * 100
+    path = str(tmp_path / "m.parquet")
+    pq.write_table(pa.table({"dept": pa.array(depts_n), "city": pa.array(city.tolist()), "score": score}), path,
+                   row_group_size=20_000)
+    assert pq.ParquetFile(path).num_row_groups == 10
+    assert P.load_parquet(db, path, "m") == n
+    res = db.sql("SELECT dept, COUNT(*), SUM(score) FROM m WHERE score > 25 GROUP BY dept")
+    got = {res.column(0)[i]: (res.column(1)[i], res.column(2)[i]) for i in range(res.rows)}
+    sel = score > 25
+    dn = np.array(["" if d is None else d for d in depts_n], dtype=object)
+    for name in set(d for d in depts_n if d is not None):
+        m = sel & (dn == name)
+        want_sum = O.sum_serial(score[m])
+        assert got[name][0] == int(m.sum()) and abs(got[name][1] - want_sum) <= RTOL * want_sum
+    assert got[None][0] == int((sel & nulls).sum())  # the NULL group
+    # Row by row: the strings read back are the file's.
+    back = db.sql("SELECT dept, city FROM m")
+    assert back.column(0) == depts_n and back.column(1) == city.tolist()
+    db.drop_table("m")

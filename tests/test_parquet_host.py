@@ -86,3 +86,26 @@ def test_projection_and_errors(tmp_path):
         P.read_parquet_columns(path, ["ns"])
     with pytest.raises(FalconError):
         P.read_parquet_columns(str(tmp_path / "missing.parquet"))
+
+
+def test_chunk_dictionaries_merge_without_touching_rows():
+    """The GPU loader's host half: the row groups' dictionaries (distinct
+    strings) merge chunk by chunk into one dictionary, each chunk's entries
+    mapped to merged codes; remapping each chunk's indices through its table
+    gives every row's string (checked here on the host)."""
+    import pyarrow as pa
+
+    from falcondb_b200 import parquet as P
+
+    chunks = [pa.DictionaryArray.from_arrays(pa.array([0, 1, 1, None, 0], pa.int32()), pa.array(["b", "a"])),
+              pa.DictionaryArray.from_arrays(pa.array([2, 0, 1], pa.int32()), pa.array(["a", "c", "b"])),
+              pa.DictionaryArray.from_arrays(pa.array([0, 0], pa.int32()), pa.array(["d"]))]
+    arr = pa.chunked_array(chunks)
+    words, remaps = P._merge_chunk_dictionaries(arr)
+    assert words == ["b", "a", "c", "d"]
+    assert [list(r) for r in remaps] == [[0, 1], [1, 2, 0], [3]]
+    rows = []
+    for ch, r in zip(arr.chunks, remaps):
+        for k in ch.indices.to_pylist():
+            rows.append(None if k is None else words[r[k]])
+    assert rows == ["b", "a", "a", None, "b", "b", "a", "c", "d", "d"]
