@@ -639,6 +639,7 @@ struct ProbeBitsOp : ProbeOp<JT, true> {
   static __device__ void step(Local& st, const Params& p, unsigned char* sm, const Acc& acc, uint32_t rows,
                               int ctid, int nct) {
     const unsigned long long* bits = reinterpret_cast<const unsigned long long*>(sm + kBitsOff);
+#pragma unroll 4
     for (uint32_t i = ctid; i < rows; i += nct) {
       bool match = false;
       if (!p.key.validity || col_valid(p.key, acc.row(i))) {  // a NULL key matches nothing
@@ -693,12 +694,16 @@ static void launch_probe_mode(Ctx& c, const fdb_dev_column* cols, uint64_t n, co
   FDB_CUDA(cudaGetLastError());
 }
 
+#ifndef FDB_PROBE_BITS_NCW
+#define FDB_PROBE_BITS_NCW 16
+#endif
 // The presence-bit probe: one CTA per SM (the bits take most of its shared
 // memory), a three-stage ring when it fits beside them, else two.
 template <int NC, int JT, int STAGES>
 static void launch_probe_bits_shape(Ctx& c, const fdb_dev_column* cols, uint64_t n, const ProbeParams& p,
                                     size_t op_smem) {
-  constexpr int TR = NC == 1 ? 2048 : 1024, NCW = 8;
+  // One CTA per SM: 16 consumer warps keep enough rows in flight.
+  constexpr int TR = NC == 1 ? 2048 : 1024, NCW = FDB_PROBE_BITS_NCW;
   StreamSrc<NC> src;
   const void* bases[NC];
   for (int i = 0; i < NC; ++i) {
