@@ -698,12 +698,13 @@ static void launch_probe_mode(Ctx& c, const fdb_dev_column* cols, uint64_t n, co
 #define FDB_PROBE_BITS_NCW 16
 #endif
 // The presence-bit probe: one CTA per SM (the bits take most of its shared
-// memory), a three-stage ring when it fits beside them, else two.
-template <int NC, int JT, int STAGES>
+// memory).  The tile ring gets what is left: the largest of 3 x 2 KB-row,
+// 3 x 1 KB-row and 2 x 1 KB-row rings (per column) that fits, so that as many
+// bytes as possible are in flight per SM.
+template <int NC, int JT, int TR, int STAGES>
 static void launch_probe_bits_shape(Ctx& c, const fdb_dev_column* cols, uint64_t n, const ProbeParams& p,
                                     size_t op_smem) {
-  // One CTA per SM: 16 consumer warps keep enough rows in flight.
-  constexpr int TR = NC == 1 ? 2048 : 1024, NCW = FDB_PROBE_BITS_NCW;
+  constexpr int NCW = FDB_PROBE_BITS_NCW;
   StreamSrc<NC> src;
   const void* bases[NC];
   for (int i = 0; i < NC; ++i) {
@@ -726,12 +727,15 @@ static void launch_probe_bits_shape(Ctx& c, const fdb_dev_column* cols, uint64_t
 
 template <int NC, int JT>
 static void launch_probe_bits(Ctx& c, const fdb_dev_column* cols, uint64_t n, const ProbeParams& p) {
-  constexpr int TR = NC == 1 ? 2048 : 1024;
+  constexpr int TRB = NC == 1 ? 4096 : 2048, TRS = NC == 1 ? 2048 : 1024;
+  constexpr size_t kMax = 227 * 1024;
   const size_t op_smem = ProbeBitsOp<JT>::kBitsOff + (p.span + 63) / 64 * 8;
-  if (stream_smem_bytes<NC, TR, 3>() + op_smem <= 227 * 1024)
-    launch_probe_bits_shape<NC, JT, 3>(c, cols, n, p, op_smem);
+  if (stream_smem_bytes<NC, TRB, 3>() + op_smem <= kMax)
+    launch_probe_bits_shape<NC, JT, TRB, 3>(c, cols, n, p, op_smem);
+  else if (stream_smem_bytes<NC, TRS, 3>() + op_smem <= kMax)
+    launch_probe_bits_shape<NC, JT, TRS, 3>(c, cols, n, p, op_smem);
   else
-    launch_probe_bits_shape<NC, JT, 2>(c, cols, n, p, op_smem);
+    launch_probe_bits_shape<NC, JT, TRS, 2>(c, cols, n, p, op_smem);
 }
 
 template <int NC, int JT>

@@ -98,8 +98,10 @@ class ShardedDatabase:
         cols = [self._col(table, c) for c in names]
         spec = [(f, names.index(c) if f != AGG_COUNT_STAR else 0) for f, c in aggs]
         n = self._rows[table][1]
-        out = ops.aggregate(self.db, cols, n, list(where), spec)
-        local = ops.to_records(out, AGG_VALUE_DTYPE, len(spec))
+        # fdb_aggregate takes up to 4 aggregates per scan.
+        local = np.concatenate([ops.to_records(ops.aggregate(self.db, cols, n, list(where), spec[i:i + 4]),
+                                               AGG_VALUE_DTYPE, len(spec[i:i + 4]))
+                                for i in range(0, len(spec), 4)])
         return shard.combine_aggregates(local, [f for f, _ in aggs], self.group)
 
     def count_where(self, table: str, col: str, op: int, literal) -> int:

@@ -182,8 +182,8 @@ def _text_on_device(db: Database, arr):
     for c, ch in enumerate(arr.chunks):
         m = len(ch)
         if m:
-            local = np.asarray(ch.indices.cast(pa.int32()).fill_null(-1).to_numpy(zero_copy_only=False),
-                               dtype=np.int32)
+            local = np.array(ch.indices.cast(pa.int32()).fill_null(-1).to_numpy(zero_copy_only=False),
+                             dtype=np.int32)  # a writable copy for torch
             idx[at:at + m].copy_(torch.from_numpy(local))
         at += m
         starts[c + 1] = at

@@ -284,7 +284,7 @@ def test_distinct_over_several_columns(db):
     got_a = [res.value(i, 1) for i in range(res.row_count())]
     assert got_a == [int(a[i]) if av[i] else None for i in want]
     # Two columns, after a WHERE.
-    sel = np.flatnonzero(a < 10)
+    sel = np.flatnonzero((a < 10) & av)  # WHERE a < 10 drops the NULL rows
     want2 = sel[O.distinct_multi([{"values": a[sel], "valid": av[sel]}, {"values": f[sel]}], len(sel))]
     res2 = db.sql("SELECT DISTINCT a, f FROM t WHERE a < 10")
     assert res2.row_count() == len(want2)
