@@ -177,6 +177,7 @@ struct JoinView {
   int32_t unique;
   int32_t dense;             // key k lives in slot k - dmin (see join_table.cuh)
   int64_t dmin;
+  uint64_t span;             // dense: keys outside [dmin, dmin + span) have no slot
 };
 JoinView join_view(const HashTable* h);
 

@@ -32,12 +32,18 @@ struct JoinMode {
   int64_t dmin;   // dense: the smallest build key
   int32_t dense;
   int32_t shift;  // join_shift(cap)
+  uint64_t span;  // dense: largest build key - dmin + 1 (<= cap)
 };
 
 // Home slot of key k (stored form sk), or a value >= cap when a dense table
-// cannot hold it.
+// cannot hold it: outside [dmin, dmin + span), where no build key lies (the
+// table's slots past the span are empty, so such a key reads nothing).
 __device__ __forceinline__ uint64_t join_home(const JoinMode& m, int64_t k, uint64_t sk) {
-  return m.dense ? (uint64_t)k - (uint64_t)m.dmin : join_hash(sk, m.shift);
+  if (m.dense) {
+    const uint64_t d = (uint64_t)k - (uint64_t)m.dmin;
+    return d < m.span ? d : ~0ull;
+  }
+  return join_hash(sk, m.shift);
 }
 
 // Slot of probe key k, or kNoSlot.

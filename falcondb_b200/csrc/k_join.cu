@@ -36,11 +36,11 @@ struct HashTable {
   bool payload_nulls = false;
   bool dense = false;        // key k lives in slot k - dmin (join_table.cuh)
   int64_t dmin = 0;
+  uint64_t span = 0;         // dense: kmax - kmin + 1; probe keys outside read nothing
   // Dense tables whose key range fits a CTA's shared memory as bits: bit
   // k - dmin is set when key k has a build row.  SEMI / ANTI probes test it
   // in shared memory and read nothing else.
   DevBuf bits;
-  uint64_t span = 0;         // kmax - kmin + 1 (bits used)
 };
 
 // The widest key range whose presence bits a probe CTA keeps in shared
@@ -224,6 +224,7 @@ static JoinMode join_mode(const HashTable& h) {
   JoinMode m;
   m.dmin = h.dmin;
   m.dense = h.dense ? 1 : 0;
+  m.span = h.span;
   int b = 0;
   while ((1ull << b) < h.cap) ++b;
   m.shift = 64 - b;  // join_shift(cap)
@@ -285,6 +286,7 @@ HashTable* op_join_build(Ctx& c, const fdb_dev_column& key, const fdb_dev_column
   }
   h->dense = dense;
   h->dmin = dmin;
+  h->span = span;
   const JoinMode mode = join_mode(*h);
   if (n > 0) {
     const unsigned blocks = (unsigned)umin64((n + 255) / 256, (uint64_t)c.sm_count * 16);
@@ -307,7 +309,6 @@ HashTable* op_join_build(Ctx& c, const fdb_dev_column& key, const fdb_dev_column
   if (dense && span <= kProbeBitsMaxSpan) {
     const uint64_t words = (span + 63) / 64;
     h->bits = c.alloc_buf(words * 8);
-    h->span = span;
     const unsigned blocks = (unsigned)umin64((words * 64 + 255) / 256, (uint64_t)c.sm_count * 8);
     join_bits_kernel<<<blocks, 256, 0, c.stream>>>(static_cast<const unsigned int*>(h->cnt.ptr), span,
                                                     static_cast<uint32_t*>(h->bits.ptr));
@@ -345,6 +346,7 @@ JoinView join_view(const HashTable* h) {
   v.unique = h->unique ? 1 : 0;
   v.dense = h->dense ? 1 : 0;
   v.dmin = h->dmin;
+  v.span = h->span;
   return v;
 }
 
@@ -523,7 +525,7 @@ struct ProbeOp {
           continue;
         }
         sk[r] = (uint64_t)k ^ (1ull << 63);
-        d[r] = (uint64_t)k - (uint64_t)p.mode.dmin;
+        d[r] = join_home(p.mode, k, sk[r]);  // >= cap outside the build keys' span: no read
       }
       JSlot sl[R];
 #pragma unroll
@@ -771,7 +773,7 @@ void op_join_probe_agg(Ctx& c, const HashTable& h, const fdb_dev_column& key, co
   p.payload_nulls = h.payload_nulls ? 1 : 0;
   p.has_value = (has_value && (join_type == FDB_JOIN_SEMI || join_type == FDB_JOIN_ANTI)) ? 1 : 0;
   p.bits = static_cast<const unsigned long long*>(h.bits.ptr);
-  p.span = h.span;
+  p.span = h.bits.ptr ? h.span : 0;
   p.partials = static_cast<JoinAggAcc*>(c.scratch_take(sizeof(JoinAggAcc) * c.sm_count * kProbeMaxPerSm));
   p.ticket = c.d_ticket;
   p.out = d_out;

@@ -123,6 +123,7 @@ struct ServeG {             // a group of queries that read the same table
   int32_t ngroupq;          // GROUP queries in the group
   int32_t ncountq, njoinq;  // COUNT and JOIN queries in the group
   int32_t _pad4;
+  uint64_t span;            // dense table: keys outside [dmin, dmin + span) have no slot
 };
 
 struct ServeHeader {
@@ -351,6 +352,7 @@ __device__ void serve_probe_rows(const ServeG g, uint64_t* s0, uint32_t* m, uint
   mode.dmin = g.dmin;
   mode.dense = g.dense;
   mode.shift = join_shift(g.cap);
+  mode.span = g.span;
   const uint64_t mask = g.cap - 1;
   const uint64_t pol = l2_evict_last_policy();
   for (uint32_t base = 0; base < rows; base += kProbeIlp * kServeThreads) {
@@ -1386,6 +1388,7 @@ static bool slot_launch(Server& s, ServeSlot& sl, bool small_only) {
       d.unique = v.unique;
       d.dmin = v.dmin;
       d.dense = v.dense;
+      d.span = v.span;
     }
     for (uint64_t tk : g.tickets) put(tk);
   }
