@@ -768,12 +768,16 @@ struct DSlot {                 // 32 bytes, 32-byte aligned; all-zero = no row y
 };
 static_assert(sizeof(DSlot) == 32, "one sector per slot");
 
-struct SDSlot {                // CTA table slot, 32 bytes
-  unsigned int k1;             // slot index + 1 (0 = empty)
-  unsigned int count;          // a CTA sees fewer than 2^32 rows
-  double sum;
-  unsigned long long nmin;
-  unsigned long long max;
+// The CTA table, structure of arrays: field f of slot j is element j of
+// array f, so the lanes of a warp touching random slots spread over all 32
+// banks (32-byte array-of-structs slots put every field of every slot on 4
+// of them).  Slot kDenseSmemSlots (the last) is the NULL key group.
+struct SDTab {
+  double* sum;
+  unsigned long long* nmin;    // ~order key of MIN (atomicMax)
+  unsigned long long* max;     // order key of MAX
+  unsigned int* k1;            // slot index + 1 (0 = empty)
+  unsigned int* count;         // a CTA sees fewer than 2^32 rows
 };
 
 #ifndef FDB_GBD_SLOTS
@@ -805,17 +809,29 @@ struct GbDenseParams {
   int* err;
 };
 
-// A value into a CTA slot.  MIN / MAX read the slot first and take the atomic
-// only when the value improves on it: after a frequent key's first few hundred
-// rows that is rare, so its rows do not queue on two 64-bit shared atomics.
-__device__ __forceinline__ void sdslot_accum(SDSlot* s, double v, bool has_v) {
-  atomicAdd(&s->count, 1u);
+__device__ __forceinline__ SDTab sdtab(unsigned char* sm) {
+  constexpr uint32_t S = kDenseSmemSlots + 1;
+  SDTab t;
+  t.sum = reinterpret_cast<double*>(sm);
+  t.nmin = reinterpret_cast<unsigned long long*>(sm + 8 * S);
+  t.max = reinterpret_cast<unsigned long long*>(sm + 16 * S);
+  t.k1 = reinterpret_cast<unsigned int*>(sm + 24 * S);
+  t.count = reinterpret_cast<unsigned int*>(sm + 28 * S);
+  return t;
+}
+
+// A value into CTA slot j.  MIN / MAX read the slot first and take the atomic
+// only when the value improves on it: after a frequent key's first few
+// hundred rows that is rare, so its rows do not queue on two 64-bit shared
+// atomics.
+__device__ __forceinline__ void sdslot_accum(const SDTab& t, uint32_t j, double v, bool has_v) {
+  atomicAdd(&t.count[j], 1u);
   if (!has_v) return;
-  atomicAdd(&s->sum, v);
+  atomicAdd(&t.sum[j], v);
   if (isnan(v)) return;
   const unsigned long long k = f64_ord_key(v);
-  if (~k > *reinterpret_cast<volatile unsigned long long*>(&s->nmin)) atomicMax(&s->nmin, ~k);
-  if (k > *reinterpret_cast<volatile unsigned long long*>(&s->max)) atomicMax(&s->max, k);
+  if (~k > *reinterpret_cast<volatile unsigned long long*>(&t.nmin[j])) atomicMax(&t.nmin[j], ~k);
+  if (k > *reinterpret_cast<volatile unsigned long long*>(&t.max[j])) atomicMax(&t.max[j], k);
 }
 
 // A value straight into its global slot (no result is used: RED operations).
@@ -829,35 +845,35 @@ __device__ __forceinline__ void dslot_accum(DSlot* d, double v, bool has_v) {
   atomicMax(&d->max, k);
 }
 
-__device__ __forceinline__ void dslot_merge(DSlot* d, const SDSlot& s) {
-  atomicAdd(&d->count, (unsigned long long)s.count);
-  if (s.sum != 0.0 || __double_as_longlong(s.sum) != 0) atomicAdd(&d->sum, s.sum);
-  if (s.nmin) atomicMax(&d->nmin, s.nmin);
-  if (s.max) atomicMax(&d->max, s.max);
+__device__ __forceinline__ void dslot_merge(DSlot* d, const SDTab& t, uint32_t j) {
+  atomicAdd(&d->count, (unsigned long long)t.count[j]);
+  const double sum = t.sum[j];
+  if (__double_as_longlong(sum) != 0) atomicAdd(&d->sum, sum);
+  if (t.nmin[j]) atomicMax(&d->nmin, t.nmin[j]);
+  if (t.max[j]) atomicMax(&d->max, t.max[j]);
 }
 
 // The CTA slot of slot index k, claiming one if free within kSmemProbe
-// probes; nullptr when it has no room there.
-__device__ __forceinline__ SDSlot* smem_dense_slot(SDSlot* tab, uint32_t k) {
+// probes; -1 when it has no room there.
+__device__ __forceinline__ int smem_dense_slot(const SDTab& t, uint32_t k) {
   uint32_t h = (k * 0x9E3779B1u) >> (32 - kDenseSmemLog);
   const unsigned int k1 = k + 1u;
   for (uint32_t probe = 0; probe < kSmemProbe; ++probe) {
-    SDSlot* s = tab + h;
-    const unsigned int cur = *reinterpret_cast<volatile unsigned int*>(&s->k1);
-    if (cur == k1) return s;
+    const unsigned int cur = *reinterpret_cast<volatile unsigned int*>(&t.k1[h]);
+    if (cur == k1) return (int)h;
     if (cur == 0) {
-      const unsigned int prev = atomicCAS(&s->k1, 0u, k1);
-      if (prev == 0 || prev == k1) return s;
+      const unsigned int prev = atomicCAS(&t.k1[h], 0u, k1);
+      if (prev == 0 || prev == k1) return (int)h;
     }
     h = (h + 1) & (kDenseSmemSlots - 1);
   }
-  return nullptr;
+  return -1;
 }
 
 struct GbDenseOp {
   using Params = GbDenseParams;
   struct Local {};
-  static constexpr size_t kSmem = (size_t)(kDenseSmemSlots + 1) * sizeof(SDSlot);
+  static constexpr size_t kSmem = (size_t)(kDenseSmemSlots + 1) * 32;
 
   static __device__ void init(Local&, const Params&, unsigned char* sm, int ctid, int nct) {
     uint64_t* w = reinterpret_cast<uint64_t*>(sm);
@@ -867,7 +883,7 @@ struct GbDenseOp {
   template <class Acc>
   static __device__ void step(Local&, const Params& p, unsigned char* sm, const Acc& acc, uint32_t rows, int ctid,
                               int nct) {
-    SDSlot* tab = reinterpret_cast<SDSlot*>(sm);
+    const SDTab tab = sdtab(sm);
     for (uint32_t i = ctid; i < rows; i += nct) {
       const uint64_t row = acc.row(i);
       if (p.prog.n) {
@@ -882,7 +898,7 @@ struct GbDenseOp {
                                            : (double)acc.template get<int64_t>(1, i);
       const bool kvalid = (p.cols[0].validity ? col_valid(p.cols[0], row) : true) && key != INT64_MIN;
       if (!kvalid) {  // NULL group (i64::MIN reads as NULL)
-        sdslot_accum(tab + kDenseSmemSlots, v, has_v);
+        sdslot_accum(tab, kDenseSmemSlots, v, has_v);
         continue;
       }
       const uint64_t k = (uint64_t)key - (uint64_t)p.kmin;
@@ -890,22 +906,22 @@ struct GbDenseOp {
         atomicExch(p.err, kErrCapacity);
         continue;
       }
-      SDSlot* s = smem_dense_slot(tab, (uint32_t)k);
-      if (s)
-        sdslot_accum(s, v, has_v);
+      const int j = smem_dense_slot(tab, (uint32_t)k);
+      if (j >= 0)
+        sdslot_accum(tab, (uint32_t)j, v, has_v);
       else
         dslot_accum(p.table + k, v, has_v);
     }
   }
 
   static __device__ void finish(Local&, const Params& p, unsigned char* sm, int ctid, int nct) {
-    const SDSlot* tab = reinterpret_cast<const SDSlot*>(sm);
+    const SDTab tab = sdtab(sm);
     consumer_bar(nct);
-    for (uint32_t i = ctid; i < kDenseSmemSlots; i += nct) {
-      const SDSlot s = tab[i];
-      if (s.k1) dslot_merge(p.table + (s.k1 - 1), s);
+    for (uint32_t j = ctid; j < kDenseSmemSlots; j += nct) {
+      const unsigned int k1 = tab.k1[j];
+      if (k1) dslot_merge(p.table + (k1 - 1), tab, j);
     }
-    if (ctid == 0 && tab[kDenseSmemSlots].count) dslot_merge(p.null_slot, tab[kDenseSmemSlots]);
+    if (ctid == 0 && tab.count[kDenseSmemSlots]) dslot_merge(p.null_slot, tab, kDenseSmemSlots);
   }
 };
 

@@ -28,21 +28,24 @@ def _ord_keys(v, desc):
 
 
 def _agg_record(func, values, is_int):
+    """A partial in the layout fdb_aggregate writes (k_scan.cu): COUNT /
+    COUNT(*) as Int64 records (`i`, is_int 1); SUM, AVG, MIN and MAX as
+    Float64 records (`f`, is_int 0), an INT64 SUM being its exact total
+    converted to f64 (the reference types SUM as Float64)."""
     from oracle import oracle as O
 
     import falcondb_b200 as F
     rec = np.zeros(1, dtype=F.AGG_VALUE_DTYPE)[0]
     val, cnt = O.agg(func, values)
     rec["n"] = cnt
-    rec["is_int"] = 1 if is_int else 0
     if func in (F.AGG_COUNT_STAR, F.AGG_COUNT):
+        rec["is_int"] = 1
         rec["i"] = cnt
         rec["valid"] = 1
     elif val is not None:
         rec["valid"] = 1
         if func == F.AGG_SUM and is_int:
-            rec["i"] = int(O.sum_i64_exact(values))
-            rec["f"] = float(rec["i"])
+            rec["f"] = float(int(O.sum_i64_exact(values)))
         else:
             rec["f"] = val
     return rec
@@ -108,7 +111,7 @@ def _worker(rank, world, port):
                     assert got[j]["f"] == want
                 else:
                     assert abs(got[j]["f"] - want) <= RTOL * abs(want)
-            assert isum[0]["i"] == int(O.sum_i64_exact(t["salary"]))
+            assert isum[0]["f"] == float(int(O.sum_i64_exact(t["salary"])))
             jw = O.join_agg(bt["key"], bt["payload"], pt["key"], pt["value"], F.JOIN_INNER)
             assert (int(jg[0]["count"]), int(jg[0]["sum_payload"])) == (jw["count"], jw["sum_payload"])
             want = O.group_i64(g["key"], g["v"])
