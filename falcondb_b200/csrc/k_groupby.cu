@@ -787,6 +787,18 @@ constexpr uint32_t kDenseSmemSlots = FDB_GBD_SLOTS;  // power of two
 constexpr int kDenseSmemLog = __builtin_ctz(kDenseSmemSlots);
 static_assert((kDenseSmemSlots & (kDenseSmemSlots - 1)) == 0, "CTA table slots: a power of two");
 constexpr uint64_t kDenseMaxSlots = 1ull << 31;  // slot indices (and index + 1) fit 32 bits
+// Probes into the CTA table before a row goes to the global table.
+#ifndef FDB_GBD_PROBE
+#define FDB_GBD_PROBE 4
+#endif
+constexpr uint32_t kDenseProbe = FDB_GBD_PROBE;
+// Copies of each CTA slot's SUM, picked by lane: lanes of one warp that add to
+// the same hot slot then contend on up to kDenseSumCopies addresses, not one.
+#ifndef FDB_GBD_SUMSPLIT
+#define FDB_GBD_SUMSPLIT 1
+#endif
+constexpr uint32_t kDenseSumCopies = FDB_GBD_SUMSPLIT;
+static_assert((kDenseSumCopies & (kDenseSumCopies - 1)) == 0, "SUM copies: a power of two");
 // Launch shape of the two-column instance (key, value): tile rows, stages,
 // consumer warps.
 #ifndef FDB_GBD_TR
@@ -809,14 +821,19 @@ struct GbDenseParams {
   int* err;
 };
 
+// Shared-memory bytes of the CTA table: kDenseSumCopies SUM arrays, then
+// nmin, max, k1, count (slot kDenseSmemSlots is the NULL group).
+constexpr size_t kDenseSmemBytes = (size_t)(kDenseSmemSlots + 1) * (8 * kDenseSumCopies + 24);
+
 __device__ __forceinline__ SDTab sdtab(unsigned char* sm) {
   constexpr uint32_t S = kDenseSmemSlots + 1;
+  constexpr size_t kSums = (size_t)8 * S * kDenseSumCopies;
   SDTab t;
-  t.sum = reinterpret_cast<double*>(sm);
-  t.nmin = reinterpret_cast<unsigned long long*>(sm + 8 * S);
-  t.max = reinterpret_cast<unsigned long long*>(sm + 16 * S);
-  t.k1 = reinterpret_cast<unsigned int*>(sm + 24 * S);
-  t.count = reinterpret_cast<unsigned int*>(sm + 28 * S);
+  t.sum = reinterpret_cast<double*>(sm);  // copy c of slot j: sum[c * S + j]
+  t.nmin = reinterpret_cast<unsigned long long*>(sm + kSums);
+  t.max = reinterpret_cast<unsigned long long*>(sm + kSums + 8 * S);
+  t.k1 = reinterpret_cast<unsigned int*>(sm + kSums + 16 * S);
+  t.count = reinterpret_cast<unsigned int*>(sm + kSums + 20 * S);
   return t;
 }
 
@@ -827,7 +844,8 @@ __device__ __forceinline__ SDTab sdtab(unsigned char* sm) {
 __device__ __forceinline__ void sdslot_accum(const SDTab& t, uint32_t j, double v, bool has_v) {
   atomicAdd(&t.count[j], 1u);
   if (!has_v) return;
-  atomicAdd(&t.sum[j], v);
+  const uint32_t copy = kDenseSumCopies > 1 ? (threadIdx.x & (kDenseSumCopies - 1)) : 0;
+  atomicAdd(&t.sum[copy * (kDenseSmemSlots + 1) + j], v);
   if (isnan(v)) return;
   const unsigned long long k = f64_ord_key(v);
   if (~k > *reinterpret_cast<volatile unsigned long long*>(&t.nmin[j])) atomicMax(&t.nmin[j], ~k);
@@ -847,18 +865,20 @@ __device__ __forceinline__ void dslot_accum(DSlot* d, double v, bool has_v) {
 
 __device__ __forceinline__ void dslot_merge(DSlot* d, const SDTab& t, uint32_t j) {
   atomicAdd(&d->count, (unsigned long long)t.count[j]);
-  const double sum = t.sum[j];
+  double sum = t.sum[j];
+#pragma unroll
+  for (uint32_t c = 1; c < kDenseSumCopies; ++c) sum += t.sum[c * (kDenseSmemSlots + 1) + j];
   if (__double_as_longlong(sum) != 0) atomicAdd(&d->sum, sum);
   if (t.nmin[j]) atomicMax(&d->nmin, t.nmin[j]);
   if (t.max[j]) atomicMax(&d->max, t.max[j]);
 }
 
-// The CTA slot of slot index k, claiming one if free within kSmemProbe
+// The CTA slot of slot index k, claiming one if free within kDenseProbe
 // probes; -1 when it has no room there.
 __device__ __forceinline__ int smem_dense_slot(const SDTab& t, uint32_t k) {
   uint32_t h = (k * 0x9E3779B1u) >> (32 - kDenseSmemLog);
   const unsigned int k1 = k + 1u;
-  for (uint32_t probe = 0; probe < kSmemProbe; ++probe) {
+  for (uint32_t probe = 0; probe < kDenseProbe; ++probe) {
     const unsigned int cur = *reinterpret_cast<volatile unsigned int*>(&t.k1[h]);
     if (cur == k1) return (int)h;
     if (cur == 0) {
@@ -873,7 +893,7 @@ __device__ __forceinline__ int smem_dense_slot(const SDTab& t, uint32_t k) {
 struct GbDenseOp {
   using Params = GbDenseParams;
   struct Local {};
-  static constexpr size_t kSmem = (size_t)(kDenseSmemSlots + 1) * 32;
+  static constexpr size_t kSmem = kDenseSmemBytes;
 
   static __device__ void init(Local&, const Params&, unsigned char* sm, int ctid, int nct) {
     uint64_t* w = reinterpret_cast<uint64_t*>(sm);

@@ -634,7 +634,14 @@ struct ProbeBitsOp : ProbeOp<JT, true> {
     Base::init(st, p, sm, ctid, nct);
     unsigned long long* bits = reinterpret_cast<unsigned long long*>(sm + kBitsOff);
     const uint64_t words = (p.span + 63) / 64;
-    for (uint64_t w = ctid; w < words; w += nct) bits[w] = __ldg(p.bits + w);
+    // 16-byte loads, eight in flight per thread (the bits buffer is a pool
+    // allocation, 256-byte aligned; kBitsOff is a multiple of 128).
+    const uint64_t pairs = words / 2;
+    const uint4* src = reinterpret_cast<const uint4*>(p.bits);
+    uint4* dst = reinterpret_cast<uint4*>(bits);
+#pragma unroll 8
+    for (uint64_t w = ctid; w < pairs; w += nct) dst[w] = __ldg(src + w);
+    if ((words & 1) && ctid == 0) bits[words - 1] = __ldg(p.bits + words - 1);
   }
 
   template <class Acc>
