@@ -5,17 +5,15 @@
 // (f64_ord_key, sort.rs:451-454; the sign flip for int64; bitwise NOT for
 // DESC), so -0.0 sorts before +0.0 and NaN above +inf, as in the reference.
 //
-// A stable LSD radix sort of (order key, row) pairs with 8-bit digits, one
-// sweep per digit (the "Onesweep" scheme of Adinets and Merrill, 2022):
+// A stable LSD radix sort of (order key, row) pairs with 8-bit digits:
 //   * the key pass writes the pairs and ORs / ANDs every key, so a byte that
 //     is the same in every key costs no pass;
-//   * one more read of the keys counts the digits of every varying byte at
-//     once; their exclusive scans are every pass's global digit offsets;
-//   * per pass, radix_scatter_kernel claims 4096-key tiles in order, stages
-//     each in shared memory (TMA bulk copies, double-buffered), ranks its keys
-//     stably with warp votes, gets each digit's offset among the earlier
-//     tiles by decoupled look-back (bounded waits), permutes the tile into
-//     digit order in place and writes it out in runs;
+//   * per pass, radix_hist_kernel counts the digits of each 4096-key tile
+//     (histogram laid out digit-major, [digit][tile]); an exclusive scan of the
+//     histogram gives every (digit, tile) its output offset;
+//     radix_scatter_kernel stages each tile in shared memory (TMA bulk
+//     copies, double-buffered), ranks its keys stably with warp votes, permutes
+//     the tile into digit order in place and writes it out in runs;
 //   * the last pass writes the row numbers straight into the output.
 // Every scatter position is checked against the key count (an error, never an
 // out-of-bounds write).
@@ -104,7 +102,49 @@ __global__ void distinct_heads_kernel(const uint64_t* __restrict__ keys, const u
   }
 }
 
-// Exclusive scan of one value per thread across the block (total optional).
+// Digit counts of one tile: hist[d * ntiles + tile].  Each thread counts a
+// run of equal digits before it adds it to its warp's counters, so a byte that
+// takes few values (the exponent bytes of a float column) costs few atomics.
+__global__ void __launch_bounds__(kSortThreads) radix_hist_kernel(const uint64_t* __restrict__ keys, uint32_t m,
+                                                                  int shift, uint32_t ntiles, uint32_t* hist) {
+  __shared__ uint32_t cnt[kSortWarps][256];
+  const int tid = threadIdx.x, warp = tid >> 5;
+#pragma unroll
+  for (int w = 0; w < kSortWarps; ++w) cnt[w][tid] = 0;
+  __syncthreads();
+  const uint64_t t0 = (uint64_t)blockIdx.x * kSortTile;
+  uint64_t k[kSortItems];
+#pragma unroll
+  for (int r = 0; r < kSortItems; ++r) {
+    const uint64_t i = t0 + (uint64_t)r * kSortThreads + tid;
+    k[r] = i < m ? keys[i] : 0ull;
+  }
+  uint32_t run_d = 0, run_c = 0;
+#pragma unroll
+  for (int r = 0; r < kSortItems; ++r) {
+    const uint64_t i = t0 + (uint64_t)r * kSortThreads + tid;
+    if (i < m) {
+      const uint32_t d = (uint32_t)(k[r] >> shift) & 255u;
+      if (d != run_d && run_c) {
+        atomicAdd(&cnt[warp][run_d], run_c);
+        run_c = 0;
+      }
+      run_d = d;
+      ++run_c;
+    }
+  }
+  if (run_c) atomicAdd(&cnt[warp][run_d], run_c);
+  __syncthreads();
+  uint32_t t = 0;
+#pragma unroll
+  for (int w = 0; w < kSortWarps; ++w) t += cnt[w][tid];
+  hist[(size_t)tid * ntiles + blockIdx.x] = t;
+}
+
+// Exclusive scan of n uint32 in place: per-block sums, a scan of the sums,
+// then each block's scan offset by its sum.
+constexpr int kScanT = 1024, kScanPer = 4, kScanB = kScanT * kScanPer;
+
 __device__ uint32_t sort_block_scan(uint32_t v, uint32_t* sm, uint32_t* total) {
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
   uint32_t x = v;
@@ -131,8 +171,52 @@ __device__ uint32_t sort_block_scan(uint32_t v, uint32_t* sm, uint32_t* total) {
   return base + x - v;
 }
 
-// Stable scatter of the tiles by digit.  Persistent CTAs claim tiles in
-// order (look-back needs every earlier tile claimed); thread 0 stages each tile's keys and rows into one of two
+__global__ void sort_scan_sums_kernel(const uint32_t* in, uint64_t n, uint32_t* bsum) {
+  __shared__ uint32_t sm[32];
+  const uint64_t i0 = (uint64_t)blockIdx.x * kScanB + threadIdx.x * kScanPer;
+  uint32_t s = 0;
+#pragma unroll
+  for (int j = 0; j < kScanPer; ++j)
+    if (i0 + j < n) s += in[i0 + j];
+  uint32_t tot;
+  sort_block_scan(s, sm, &tot);
+  if (threadIdx.x == 0) bsum[blockIdx.x] = tot;
+}
+
+__global__ void sort_scan_top_kernel(uint32_t* bsum, uint64_t nb) {
+  __shared__ uint32_t sm[32];
+  const uint64_t per = (nb + blockDim.x - 1) / blockDim.x;
+  const uint64_t b0 = threadIdx.x * per;
+  uint32_t local = 0;
+  for (uint64_t i = b0; i < b0 + per && i < nb; ++i) local += bsum[i];
+  uint32_t base = sort_block_scan(local, sm, nullptr);
+  for (uint64_t i = b0; i < b0 + per && i < nb; ++i) {
+    const uint32_t v = bsum[i];
+    bsum[i] = base;
+    base += v;
+  }
+}
+
+__global__ void sort_scan_apply_kernel(uint32_t* data, uint64_t n, const uint32_t* bsum) {
+  __shared__ uint32_t sm[32];
+  const uint64_t i0 = (uint64_t)blockIdx.x * kScanB + threadIdx.x * kScanPer;
+  uint32_t v[kScanPer];
+  uint32_t s = 0;
+#pragma unroll
+  for (int j = 0; j < kScanPer; ++j) {
+    v[j] = i0 + j < n ? data[i0 + j] : 0u;
+    s += v[j];
+  }
+  uint32_t run = bsum[blockIdx.x] + sort_block_scan(s, sm, nullptr);
+#pragma unroll
+  for (int j = 0; j < kScanPer; ++j) {
+    if (i0 + j < n) data[i0 + j] = run;
+    run += v[j];
+  }
+}
+
+// Stable scatter of the tiles by digit.  Persistent CTAs take tiles
+// round-robin; thread 0 stages each tile's keys and rows into one of two
 // shared-memory buffers with TMA bulk copies, so the next tile arrives while
 // this one is ranked (a ragged last tile, whose byte count is not a multiple
 // of 16, is read with plain loads).  Warp w ranks the 512 keys
@@ -154,94 +238,8 @@ struct ScatterSmem {
   uint16_t wc[kScatterWarps][256];  // per-warp digit counts, then tile offsets (< 4096)
   uint32_t gbase[256];
   uint32_t wsum[8];
-  uint32_t tile[2];                 // the tile claimed for each stage
   uint64_t full[2];
 };
-
-// Decoupled look-back (Merrill and Garland, "Single-pass Parallel Prefix Scan
-// with Decoupled Look-back", 2016, as the "Onesweep" radix sort of Adinets and
-// Merrill, 2022, uses it): each tile publishes, per digit, first its own count
-// (AGG) and then its inclusive prefix (INC); a tile's exclusive prefix is the
-// sum of its predecessors' values back to the first INC.  Tiles are claimed
-// in order from a counter, so a tile only waits on tiles claimed before it,
-// by CTAs that are running; tile 0 waits on nothing.  Every wait is bounded.
-constexpr unsigned long long kLbAgg = 1ull << 62, kLbInc = 2ull << 62, kLbVal = (1ull << 62) - 1;
-
-__device__ __forceinline__ uint32_t lookback_prefix(unsigned long long* lb, uint64_t t, uint32_t d, uint32_t tot,
-                                                    int* err) {
-  unsigned long long* mine = lb + t * 256 + d;
-  if (t == 0) {
-    atomicExch(mine, kLbInc | tot);
-    return 0;
-  }
-  atomicExch(mine, kLbAgg | tot);
-  unsigned long long excl = 0;
-  uint64_t j = t - 1;
-  uint32_t spins = 0;
-  while (true) {
-    const unsigned long long v = *reinterpret_cast<volatile unsigned long long*>(lb + j * 256 + d);
-    if (v < kLbAgg) {  // not published yet
-      if (++spins > kSpinLimit) {
-        atomicExch(err, kErrTimeout);
-        break;
-      }
-      continue;
-    }
-    excl += v & kLbVal;
-    if (v >= kLbInc || j == 0) break;
-    --j;
-  }
-  atomicExch(mine, kLbInc | (excl + tot));
-  return (uint32_t)excl;
-}
-
-// Digit counts of every byte that varies (bit b of `bytes`) over all keys:
-// hist[b * 256 + d], for the passes' global digit offsets.  A thread counts
-// runs of equal digits among its keys before adding them, so a byte that
-// takes few values costs few shared atomics.
-__global__ void __launch_bounds__(kSortThreads)
-    radix_hist_all_kernel(const uint64_t* __restrict__ keys, uint32_t m, uint32_t bytes, uint32_t* hist) {
-  __shared__ uint32_t cnt[8 * 256];
-  for (int i = threadIdx.x; i < 8 * 256; i += kSortThreads) cnt[i] = 0;
-  __syncthreads();
-  for (uint64_t t0 = (uint64_t)blockIdx.x * kSortTile; t0 < m; t0 += (uint64_t)gridDim.x * kSortTile) {
-    uint64_t k[kSortItems];
-#pragma unroll
-    for (int r = 0; r < kSortItems; ++r) {
-      const uint64_t i = t0 + (uint64_t)r * kSortThreads + threadIdx.x;
-      k[r] = i < m ? keys[i] : 0ull;
-    }
-    for (int b = 0; b < 8; ++b) {
-      if (!((bytes >> b) & 1u)) continue;
-      uint32_t run_d = 0, run_c = 0;
-#pragma unroll
-      for (int r = 0; r < kSortItems; ++r) {
-        if (t0 + (uint64_t)r * kSortThreads + threadIdx.x < m) {
-          const uint32_t d = (uint32_t)(k[r] >> (8 * b)) & 255u;
-          if (d != run_d && run_c) {
-            atomicAdd(&cnt[b * 256 + run_d], run_c);
-            run_c = 0;
-          }
-          run_d = d;
-          ++run_c;
-        }
-      }
-      if (run_c) atomicAdd(&cnt[b * 256 + run_d], run_c);
-    }
-  }
-  __syncthreads();
-  for (int i = threadIdx.x; i < 8 * 256; i += kSortThreads)
-    if (cnt[i]) atomicAdd(&hist[i], cnt[i]);
-}
-
-// base[b * 256 + d] = the keys whose byte b is below d (one CTA of 256).
-__global__ void __launch_bounds__(256) radix_base_kernel(const uint32_t* hist, uint32_t bytes, uint32_t* base) {
-  __shared__ uint32_t sm[32];
-  for (int b = 0; b < 8; ++b) {
-    if (!((bytes >> b) & 1u)) continue;  // the same for every thread
-    base[b * 256 + threadIdx.x] = sort_block_scan(hist[b * 256 + threadIdx.x], sm, nullptr);
-  }
-}
 
 // The lanes of the warp whose d equals this lane's, d < 2^NB: one vote per bit.
 template <int NB>
@@ -271,9 +269,8 @@ __device__ __forceinline__ void sort_stage_tile(ScatterSmem& S, int s, uint64_t 
 
 __global__ void __launch_bounds__(kScatterThreads, kScatterCtasPerSm)
     radix_scatter_kernel(const uint64_t* __restrict__ kin, const uint32_t* __restrict__ vin, uint32_t m, int shift,
-                         const uint32_t* __restrict__ base, unsigned long long* lookback, unsigned int* tile_ctr,
-                         uint32_t ntiles, uint64_t* __restrict__ kout, uint32_t* __restrict__ vout, bool write_keys,
-                         int* err) {
+                         const uint32_t* __restrict__ off, uint32_t ntiles, uint64_t* __restrict__ kout,
+                         uint32_t* __restrict__ vout, bool write_keys, int* err) {
   extern __shared__ __align__(128) unsigned char smem_raw[];
   ScatterSmem& S = *reinterpret_cast<ScatterSmem*>(smem_raw);
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
@@ -292,20 +289,17 @@ __global__ void __launch_bounds__(kScatterThreads, kScatterCtasPerSm)
   uint32_t pend_it0 = 0, pend_it1 = 1;
   if (tid == 0) {
     for (int j = 0; j < 2; ++j) {
-      const uint32_t t = atomicAdd(tile_ctr, 1u);  // tiles are claimed in order
-      S.tile[j] = t;
+      const uint64_t t = blockIdx.x + (uint64_t)j * gridDim.x;
       if (t < ntiles && !sort_tile_ragged(t, ntiles, m)) {
         sort_stage_tile(S, j, t, m, kin, vin, policy);
         pending |= 1u << j;
       }
     }
   }
-  __syncthreads();
   bool dead = false;
-  for (uint32_t it = 0;; ++it) {
+  uint32_t it = 0;
+  for (uint64_t t = blockIdx.x; t < ntiles; t += gridDim.x, ++it) {
     const int s = it & 1;
-    const uint64_t t = S.tile[s];  // claims only grow: every later one is past the end too
-    if (t >= ntiles) break;
     const uint64_t t0 = t * kSortTile;
     const uint32_t tile_n = (uint32_t)umin64(kSortTile, m - t0);
     if (sort_tile_ragged(t, ntiles, m)) {
@@ -379,7 +373,7 @@ __global__ void __launch_bounds__(kScatterThreads, kScatterCtasPerSm)
         if (w < warp) dstart += S.wsum[w];
 #pragma unroll
       for (int w = 0; w < kScatterWarps; ++w) S.wc[w][tid] = (uint16_t)(S.wc[w][tid] + dstart);
-      S.gbase[tid] = base[tid] + lookback_prefix(lookback, t, tid, tot, err) - dstart;
+      S.gbase[tid] = off[(size_t)tid * ntiles + t] - dstart;
     }
     uint32_t v[kSubRounds];
 #pragma unroll
@@ -418,13 +412,9 @@ __global__ void __launch_bounds__(kScatterThreads, kScatterCtasPerSm)
     }
     fence_proxy_async_smem();  // this thread's stores to stage s come before the next bulk copy into it
     __syncthreads();           // stage s and the counters are free again
-    if (tid == 0) {
-      // This stage's next tile.  After a time-out no further copies are
-      // started, but tiles are still claimed and processed (from whatever the
-      // stage holds), so that every claimed tile publishes its counts.
-      const uint32_t tn = atomicAdd(tile_ctr, 1u);
-      S.tile[s] = tn;
-      if (!dead && tn < ntiles && !sort_tile_ragged(tn, ntiles, m)) {
+    if (tid == 0 && !dead) {  // after a time-out no further copies are started
+      const uint64_t tn = t + 2ull * gridDim.x;
+      if (tn < ntiles && !sort_tile_ragged(tn, ntiles, m)) {
         sort_stage_tile(S, s, tn, m, kin, vin, policy);
         pending |= 1u << s;
         if (s)
@@ -469,7 +459,9 @@ static void launch_sort_keys(Ctx& c, const DevCol& col, const uint32_t* sel, uin
 static size_t sort_scratch_bytes(uint64_t n, bool nullable) {
   const uint64_t words = (n + 63) / 64;
   const uint64_t ntiles = (n + kSortTile - 1) / kSortTile;
-  size_t need = 2 * n * 8 + 2 * n * 4 + ntiles * 256 * 8 + 2 * 8 * 256 * 4 + 8 + 16;
+  const uint64_t hn = 256ull * ntiles;
+  const uint64_t nb = (hn + kScanB - 1) / kScanB;
+  size_t need = 2 * n * 8 + 2 * n * 4 + hn * 4 + nb * 4 + 16;
   if (nullable) need += words * 8 + 2 * n * 4 + 16;
   return need + (2u << 20);  // + 256-byte rounding and the compaction's chunk counts
 }
@@ -521,11 +513,10 @@ static void radix_sort_pairs(Ctx& c, uint32_t m, KeysFn keys_fn, uint32_t* rows_
   uint32_t* va = static_cast<uint32_t*>(c.scratch_take(m * 4));
   uint32_t* vb = static_cast<uint32_t*>(c.scratch_take(m * 4));
   const uint32_t ntiles = (uint32_t)((m + kSortTile - 1) / kSortTile);
-  unsigned long long* lookback =
-      static_cast<unsigned long long*>(c.scratch_take((size_t)ntiles * 256 * 8));
-  uint32_t* hist = static_cast<uint32_t*>(c.scratch_take(2 * 8 * 256 * 4));  // counts, then bases
-  uint32_t* base = hist + 8 * 256;
-  unsigned int* tile_ctr = static_cast<unsigned int*>(c.scratch_take(8));
+  const uint64_t hn = 256ull * ntiles;
+  const uint64_t nb = (hn + kScanB - 1) / kScanB;
+  uint32_t* hist = static_cast<uint32_t*>(c.scratch_take(hn * 4));
+  uint32_t* bsum = static_cast<uint32_t*>(c.scratch_take(nb * 4));
   unsigned long long* vary = static_cast<unsigned long long*>(c.scratch_take(16));
   FDB_CUDA(cudaMemsetAsync(vary, 0, 8, c.stream));
   FDB_CUDA(cudaMemsetAsync(vary + 1, 0xFF, 8, c.stream));
@@ -535,30 +526,20 @@ static void radix_sort_pairs(Ctx& c, uint32_t m, KeysFn keys_fn, uint32_t* rows_
   FDB_CUDA(cudaMemcpyAsync(hv, vary, 16, cudaMemcpyDeviceToHost, c.stream));
   FDB_CUDA(cudaStreamSynchronize(c.stream));
   const uint64_t varying = hv[0] ^ hv[1];  // bits that are not the same in every key
-  uint32_t bytes = 0;                      // bit b: byte b varies (a pass)
   int last_byte = -1;
   for (int byte = 0; byte < 8; ++byte)
-    if ((varying >> (8 * byte)) & 0xFFull) {
-      bytes |= 1u << byte;
-      last_byte = byte;
-    }
-  if (bytes) {
-    // One read of the keys gives every pass's digit counts (they do not
-    // depend on the order), hence every pass's global digit offsets.
-    FDB_CUDA(cudaMemsetAsync(hist, 0, 8 * 256 * 4, c.stream));
-    const unsigned hg = (unsigned)std::min<uint64_t>(ntiles, (uint64_t)c.sm_count * 8);
-    radix_hist_all_kernel<<<hg, kSortThreads, 0, c.stream>>>(ka, m, bytes, hist);
-    radix_base_kernel<<<1, 256, 0, c.stream>>>(hist, bytes, base);
-  }
+    if ((varying >> (8 * byte)) & 0xFFull) last_byte = byte;
   const int grid = (int)std::min<uint64_t>(ntiles, (uint64_t)kScatterCtasPerSm * c.sm_count);
   for (int byte = 0; byte <= last_byte; ++byte) {
-    if (!((bytes >> byte) & 1u)) continue;  // one digit for every key: order unchanged
-    FDB_CUDA(cudaMemsetAsync(lookback, 0, (size_t)ntiles * 256 * 8, c.stream));
-    FDB_CUDA(cudaMemsetAsync(tile_ctr, 0, 4, c.stream));
+    const int shift = 8 * byte;
+    if (((varying >> shift) & 0xFFull) == 0) continue;  // one digit for every key: order unchanged
+    radix_hist_kernel<<<ntiles, kSortThreads, 0, c.stream>>>(ka, m, shift, ntiles, hist);
+    sort_scan_sums_kernel<<<(unsigned)nb, kScanT, 0, c.stream>>>(hist, hn, bsum);
+    sort_scan_top_kernel<<<1, kScanT, 0, c.stream>>>(bsum, nb);
+    sort_scan_apply_kernel<<<(unsigned)nb, kScanT, 0, c.stream>>>(hist, hn, bsum);
     const bool direct = rows_out && byte == last_byte;  // rows go straight to the output; keys are not needed
     radix_scatter_kernel<<<grid, kScatterThreads, sizeof(ScatterSmem), c.stream>>>(
-        ka, va, m, 8 * byte, base + 256 * byte, lookback, tile_ctr, ntiles, kb, direct ? rows_out : vb, !direct,
-        c.d_err);
+        ka, va, m, shift, hist, ntiles, kb, direct ? rows_out : vb, !direct, c.d_err);
     std::swap(ka, kb);
     std::swap(va, vb);
   }
