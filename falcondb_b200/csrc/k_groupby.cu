@@ -781,7 +781,7 @@ struct SDTab {
 };
 
 #ifndef FDB_GBD_SLOTS
-#define FDB_GBD_SLOTS 2048
+#define FDB_GBD_SLOTS 1024
 #endif
 constexpr uint32_t kDenseSmemSlots = FDB_GBD_SLOTS;  // power of two
 constexpr int kDenseSmemLog = __builtin_ctz(kDenseSmemSlots);
