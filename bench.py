@@ -49,6 +49,11 @@ QUERIES = {
 }
 LAUNCHES_PER_STEP = 7  # sum 1, count 1, distinct 1, top-k (sample + main) x 2
 METRIC = "scanned GB/s vs 8 TB/s HBM"
+# How the int64-key GROUP BY sizes its table in these runs.
+ZONE_SIZING = ("key range from the key column's zone maps (computed on the GPU when the table is loaded, per "
+               "65,536-row batch, as Table::append_batch computes BatchStats); no pass over the keys inside the "
+               "timed call. ms_with_sizing_pass: the same call with zone maps off, which first reads the keys once "
+               "(HyperLogLog estimate and key range)")
 
 
 def peaks():
@@ -406,9 +411,12 @@ def run_configs(args, db, t, n, peak):
       0..1M-1, payload uniform [0, 1e6)), 100M-row probe (key uniform
       [0, 2M), value uniform [0, 1)); COUNT(*) with SUM(payload), or with
       SUM(value) for SEMI / ANTI (8 B/probe row of key, +8 B of value).
+    * zone_prune: SELECT COUNT(*), SUM(score) WHERE id >= 99M through
+      fdb_sql over the headline table (id ascending), zone maps on and off:
+      host wall time per query.
     * groupby_zipf: 100M rows, key Zipf(1.1) over 10M values, COUNT / SUM /
-      MIN / MAX of v, the table sized by the sizing pass inside the timed
-      call (16 B/row + 40 B/group).
+      MIN / MAX of v, the key range from the zone maps; the same call with
+      the sizing pass beside it (16 B/row + 40 B/group).
     * groupby_batched: 64 GROUP BY queries over slices of that table, sizes
       log-uniform in [10k, 10M] rows, one captured graph against the same
       queries one by one.
@@ -454,6 +462,26 @@ def run_configs(args, db, t, n, peak):
     rate("filter_groupby_100M", ms, 20 * n, rows=n,
          query="SELECT dept, COUNT(*), SUM(score), AVG(salary) FROM t WHERE score > 50 GROUP BY dept")
 
+    # --- zone-map pruning (execute_select's batch skip, select.rs:115-137) ---
+    lo = n - n // 100
+    qz = f"SELECT COUNT(*), SUM(score) FROM t WHERE id >= {lo}"
+    walls = {}
+    for on in (0, 1):
+        db.set_option("zone_maps", on)
+        for _ in range(Wm):
+            db.sql(qz)
+        t0 = time.perf_counter()
+        for _ in range(K):
+            r = db.sql(qz)
+        walls[on] = (time.perf_counter() - t0) / K * 1e3
+        scanned = db.last_scan_rows
+        assert r.value(0, 0) == n - lo
+        assert abs(r.value(0, 1) - O.sum_serial(t["score"][lo:])) <= 1e-12 * r.value(0, 1)
+    extra["zone_prune"] = {"query": qz.replace("FROM t", "FROM t (id ascending)"), "rows": n,
+                           "ms_pruned": round(walls[1], 4), "ms_full_scan": round(walls[0], 4),
+                           "rows_scanned_pruned": scanned, "oracle_checked": True, "steps": K, "warmup": Wm,
+                           "timing": "host wall time of fdb_sql, result fetched"}
+
     # --- configuration 2: 1M x 100M joins ------------------------------------
     b, p = W.join_tables(1_000_000, n, seed=7)
     db.create_table("b", b)
@@ -484,6 +512,12 @@ def run_configs(args, db, t, n, peak):
     cap = 12_000_000
     outb = ops._bytes(F.GROUP_I64_DTYPE.itemsize * cap, db)
     ng = torch.empty(1, dtype=torch.int64, device=dev)
+    # With the key column's zone maps off, the same call first reads the keys
+    # once (HyperLogLog estimate and key range); timed too, for comparison.
+    db.set_option("zone_maps", 0)
+    ms_pass = _time_steps(lambda: ops.group_by_i64(db, gk, gv, n, capacity=cap, out=outb, ngroups=ng), K, Wm,
+                          stream, torch)
+    db.set_option("zone_maps", 1)
     ms = _time_steps(lambda: ops.group_by_i64(db, gk, gv, n, capacity=cap, out=outb, ngroups=ng), K, Wm, stream,
                      torch)
     groups = int(ng.item())
@@ -495,7 +529,7 @@ def run_configs(args, db, t, n, peak):
     assert float((np.abs(rec["sum"] - want["sum"]) / np.abs(want["sum"])).max()) <= 1e-12
     del rec, want
     rate("groupby_zipf", ms, 16 * n + 40 * groups, rows=n, groups=groups, distinct_domain=10_000_000, zipf_s=1.1,
-         table_sizing="one pass over the keys (HyperLogLog estimate and key range) inside the timed call")
+         table_sizing=ZONE_SIZING, ms_with_sizing_pass=round(ms_pass, 4))
 
     kt = torch.from_numpy(g["key"]).to(dev)
     vt = torch.from_numpy(g["v"]).to(dev)
@@ -788,6 +822,9 @@ def run_secondary(args):
         def q():
             ops.group_by_i64(db, gk, gv, n, expected_groups=0, load_factor=lf, capacity=cap, out=outb,
                              ngroups=ng)
+        db.set_option("zone_maps", 0)
+        ms_pass = _time_steps(q, K, Wm, stream, torch)
+        db.set_option("zone_maps", 1)
         ms = _time_steps(q, K, Wm, stream, torch)
         groups = int(ng.item())
         # After timing: every group against the oracle (keys, counts, MIN/MAX
@@ -801,9 +838,8 @@ def run_secondary(args):
         del rec, want
         line("groupby_zipf", ms, 16 * n + 40 * groups, {"rows": n, "groups": groups, "distinct_domain": 10_000_000,
                                                         "zipf_s": 1.1, "load_factor": lf, "oracle_checked": True,
-                                                        "table_sizing": "one pass over the keys (HyperLogLog "
-                                                                        "estimate and key range) inside the timed "
-                                                                        "call"})
+                                                        "table_sizing": ZONE_SIZING,
+                                                        "ms_with_sizing_pass": round(ms_pass, 4)})
         db.drop_table("g")
 
     if args.workload in ("batch", "all"):

@@ -127,6 +127,15 @@ class fdb_serve_stats(C.Structure):
                 ("peak_reserved", C.c_uint64), ("resident_bytes", C.c_uint64)]
 
 
+class fdb_zone(C.Structure):
+    _fields_ = [("min_i", C.c_int64), ("max_i", C.c_int64), ("min_f", C.c_double), ("max_f", C.c_double),
+                ("null_count", C.c_uint64), ("rows", C.c_uint32), ("flags", C.c_uint32)]
+
+
+ZONE_BATCH_ROWS = 65536
+ZONE_VALUES, ZONE_NAN = 1, 2
+ZONE_DTYPE = np.dtype([("min_i", "<i8"), ("max_i", "<i8"), ("min_f", "<f8"), ("max_f", "<f8"),
+                       ("null_count", "<u8"), ("rows", "<u4"), ("flags", "<u4")])
 AGG_VALUE_DTYPE = np.dtype([("f", "<f8"), ("i", "<i8"), ("n", "<i8"), ("is_int", "<i4"), ("valid", "<i4")])
 JOIN_AGG_DTYPE = np.dtype([("count", "<i8"), ("sum_payload", "<i8"), ("sum_value", "<f8"),
                            ("payload_rows", "<i8")])
@@ -155,6 +164,12 @@ _SIGS = {
     "fdb_result_display": (C.c_char_p, [C.c_void_p]),
     "fdb_result_free": (None, [C.c_void_p]),
     "fdb_last_kernel_ms": (C.c_double, [C.c_void_p]),
+    "fdb_last_scan_rows": (C.c_uint64, [C.c_void_p]),
+    "fdb_table_zone_map": (C.c_int, [C.c_void_p, C.c_char_p, C.c_char_p, C.c_void_p, C.c_uint64,
+                                     C.POINTER(C.c_uint64)]),
+    "fdb_zone_skip": (C.c_int, [C.c_void_p, C.c_char_p, C.POINTER(C.c_char_p), C.c_int32, C.POINTER(fdb_pred_term),
+                                C.c_int32, C.c_void_p, C.c_uint64, C.POINTER(C.c_uint64)]),
+    "fdb_set_option": (C.c_int, [C.c_void_p, C.c_char_p, C.c_int64]),
     "fdb_memory_stats": (C.c_int, [C.c_void_p, C.POINTER(fdb_mem_stats)]),
     "fdb_stream": (C.c_void_p, [C.c_void_p]),
     "fdb_synchronize": (C.c_int, [C.c_void_p]),
@@ -578,13 +593,49 @@ class Database:
 
     def synchronize(self) -> None:
         check(lib().fdb_synchronize(self.handle))
-        for k in list(self._keep):
-            pass
+
+    # -- zone maps ----------------------------------------------------------------------
+    def zone_map(self, table: str, column: str) -> np.ndarray:
+        """The column's zone map: one ZONE_DTYPE record per 65,536-row batch
+        (BatchStats, src/storage/stats.rs:22-52), computed when the table was
+        loaded."""
+        nb = C.c_uint64()
+        check(lib().fdb_table_zone_map(self.handle, table.encode(), column.encode(), None, 0, C.byref(nb)))
+        out = np.zeros(int(nb.value), dtype=ZONE_DTYPE)
+        if len(out):
+            check(lib().fdb_table_zone_map(self.handle, table.encode(), column.encode(), out.ctypes.data,
+                                           len(out), C.byref(nb)))
+        return out
+
+    def zone_skip(self, table: str, columns: Sequence[str], terms: Sequence["fdb_pred_term"]) -> np.ndarray:
+        """Per batch of `table`, True when the zone maps prove that no row
+        passes the WHERE program `terms` over `columns` (can_skip,
+        src/storage/stats.rs:57-113)."""
+        names = (C.c_char_p * max(1, len(columns)))(*[c.encode() for c in columns])
+        prog = (fdb_pred_term * max(1, len(terms)))(*terms)
+        nrows = self.table_row_count(table)
+        nb = (nrows + ZONE_BATCH_ROWS - 1) // ZONE_BATCH_ROWS
+        words = np.zeros(max(1, (nb + 63) // 64), dtype=np.uint64)
+        got = C.c_uint64()
+        check(lib().fdb_zone_skip(self.handle, table.encode(), names, len(columns), prog, len(terms),
+                                  words.ctypes.data, len(words), C.byref(got)))
+        bits = np.unpackbits(words.view(np.uint8), bitorder="little")[:int(got.value)]
+        return bits.astype(bool)
+
+    def set_option(self, name: str, value: int) -> None:
+        """Context option (fdb_set_option): "zone_maps" 1 / 0."""
+        check(lib().fdb_set_option(self.handle, name.encode(), int(value)))
+
+    @property
+    def last_scan_rows(self) -> int:
+        """Rows of its table that the last single-table :meth:`sql` scanned
+        after zone-map pruning."""
+        return int(lib().fdb_last_scan_rows(self.handle))
 
 
 __all__ = [
     "Database", "Result", "Utf8", "DeviceUtf8", "DevColumn", "FalconError", "lib", "check", "version", "validity_words",
     "INT64", "FLOAT64", "UTF8", "EQ", "NE", "LT", "LE", "GT", "GE", "AGG_COUNT_STAR", "AGG_COUNT", "AGG_SUM",
     "AGG_AVG", "AGG_MIN", "AGG_MAX", "AGG_COUNT_DISTINCT", "JOIN_INNER", "JOIN_LEFT", "JOIN_SEMI", "JOIN_ANTI",
-    "NO_ROW", "EXPORTED",
+    "NO_ROW", "EXPORTED", "ZONE_DTYPE", "ZONE_BATCH_ROWS", "ZONE_VALUES", "ZONE_NAN",
 ]

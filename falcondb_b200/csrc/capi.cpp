@@ -62,6 +62,7 @@ Ctx::~Ctx() {
   if (ev1) cudaEventDestroy(ev1);
   if (stream) cudaStreamDestroy(stream);
   if (upload) cudaStreamDestroy(upload);
+  if (zstream) cudaStreamDestroy(zstream);
 }
 
 // Device memory comes from the device's stream-ordered pool (cudaMallocAsync on
@@ -202,6 +203,7 @@ int fdb_open(int device, uint64_t mem_budget_bytes, fdb_db** out) {
     c.budget = mem_budget_bytes ? (size_t)mem_budget_bytes : (size_t)(free_b * 0.9);
     FDB_CUDA(cudaStreamCreateWithFlags(&c.stream, cudaStreamNonBlocking));
     FDB_CUDA(cudaStreamCreateWithFlags(&c.upload, cudaStreamNonBlocking));
+    FDB_CUDA(cudaStreamCreateWithFlags(&c.zstream, cudaStreamNonBlocking));
     // Keep freed pool blocks cached in this process (the pool belongs to this
     // process's context; nothing outlives it).
     cudaMemPool_t pool;
@@ -225,14 +227,11 @@ void fdb_close(fdb_db* db) {
   cudaSetDevice(db->ctx.device);
   cudaStreamSynchronize(db->ctx.stream);
   cudaStreamSynchronize(db->ctx.upload);
+  cudaStreamSynchronize(db->ctx.zstream);
   {
     std::lock_guard<std::recursive_mutex> lk(db->ctx.mu);
     for (auto& kv : db->ctx.tables)
-      for (auto& col : kv.second->cols) {
-        db->ctx.free_buf(col.values);
-        db->ctx.free_buf(col.validity);
-        if (col.ready) cudaEventDestroy(col.ready);
-      }
+      for (auto& col : kv.second->cols) free_column(db->ctx, col);
     db->ctx.tables.clear();
   }
   delete db;
@@ -278,6 +277,7 @@ int64_t fdb_table_from_columns(fdb_db* db, const char* name, const fdb_column* c
             for (uint32_t d = 0; d < hc.dict_len; ++d) col.dict.emplace_back(hc.dict[d] ? hc.dict[d] : "");
           }
           FDB_CUDA(cudaEventRecord(col.ready, c.upload));
+          build_zone_map(c, col, nrows);
         }
         return;
       }
@@ -315,23 +315,16 @@ int64_t fdb_table_from_columns(fdb_db* db, const char* name, const fdb_column* c
         }
         FDB_CUDA(cudaEventRecord(col.ready, c.upload));
         t->cols.push_back(std::move(col));
+        build_zone_map(c, t->cols.back(), nrows);
       }
     } catch (...) {
-      for (auto& col : t->cols) {
-        c.free_buf(col.values);
-        c.free_buf(col.validity);
-        if (col.ready) cudaEventDestroy(col.ready);
-      }
+      for (auto& col : t->cols) free_column(c, col);
       throw;
     }
     auto it = c.tables.find(name);
     if (it != c.tables.end()) {
       FDB_CUDA(cudaStreamSynchronize(c.stream));
-      for (auto& col : it->second->cols) {
-        c.free_buf(col.values);
-        c.free_buf(col.validity);
-        if (col.ready) cudaEventDestroy(col.ready);
-      }
+      for (auto& col : it->second->cols) free_column(c, col);
       c.tables.erase(it);
     }
     c.tables[name] = t;
@@ -356,11 +349,7 @@ int fdb_table_drop(fdb_db* db, const char* name) {
     if (it == c.tables.end()) fail(FDB_E_NOTFOUND, std::string("no table ") + name);
     FDB_CUDA(cudaSetDevice(c.device));
     FDB_CUDA(cudaStreamSynchronize(c.stream));
-    for (auto& col : it->second->cols) {
-      c.free_buf(col.values);
-      c.free_buf(col.validity);
-      if (col.ready) cudaEventDestroy(col.ready);
-    }
+    for (auto& col : it->second->cols) free_column(c, col);
     c.tables.erase(it);
   });
 }
@@ -385,6 +374,73 @@ int fdb_table_column(const fdb_db* db, const char* table, const char* column, fd
     out->validity = static_cast<const uint64_t*>(col.validity.ptr);
     out->validity_offset = 0;
     if (nrows) *nrows = it->second->nrows;
+  });
+}
+
+int fdb_table_zone_map(fdb_db* db, const char* table, const char* column, fdb_zone* out, uint64_t cap,
+                       uint64_t* nbatches) {
+  if (!db || !table || !column || (cap && !out)) return set_error(FDB_E_ARG, "fdb_table_zone_map: bad arguments");
+  return guarded([&] {
+    std::lock_guard<std::recursive_mutex> lk(db->ctx.mu);
+    Ctx& c = db->ctx;
+    FDB_CUDA(cudaSetDevice(c.device));
+    auto it = c.tables.find(table);
+    if (it == c.tables.end()) fail(FDB_E_NOTFOUND, std::string("no table ") + table);
+    const int ci = it->second->find(column);
+    if (ci < 0) fail(FDB_E_NOTFOUND, std::string("no column ") + column);
+    const std::vector<fdb_zone>& z = column_zones(c, it->second->cols[ci]);
+    if (nbatches) *nbatches = z.size();
+    const uint64_t m = std::min<uint64_t>(cap, z.size());
+    if (m) std::memcpy(out, z.data(), m * sizeof(fdb_zone));
+  });
+}
+
+int fdb_zone_skip(fdb_db* db, const char* table, const char* const* cols, int32_t ncols, const fdb_pred_term* prog,
+                  int32_t nterms, uint64_t* skip, uint64_t words, uint64_t* nbatches) {
+  if (!db || !table || ncols < 0 || (ncols && !cols) || nterms < 0 || (nterms && !prog) || (words && !skip))
+    return set_error(FDB_E_ARG, "fdb_zone_skip: bad arguments");
+  return guarded([&] {
+    std::lock_guard<std::recursive_mutex> lk(db->ctx.mu);
+    Ctx& c = db->ctx;
+    FDB_CUDA(cudaSetDevice(c.device));
+    auto it = c.tables.find(table);
+    if (it == c.tables.end()) fail(FDB_E_NOTFOUND, std::string("no table ") + table);
+    Table& t = *it->second;
+    std::vector<const std::vector<fdb_zone>*> zones;
+    std::vector<int32_t> dtypes;
+    for (int i = 0; i < ncols; ++i) {
+      const int ci = cols[i] ? t.find(cols[i]) : -1;
+      if (ci < 0) fail(FDB_E_NOTFOUND, std::string("no column ") + (cols[i] ? cols[i] : "(null)"));
+      zones.push_back(&column_zones(c, t.cols[ci]));
+      dtypes.push_back(t.cols[ci].dtype);
+    }
+    // Host copies of the CODE_SET bitmaps.
+    std::vector<std::vector<uint64_t>> sets((size_t)nterms);
+    for (int i = 0; i < nterms; ++i)
+      if (prog[i].kind == FDB_TERM_CODE_SET && prog[i].code_set && prog[i].lit_i > 0) {
+        sets[(size_t)i].resize(((uint64_t)prog[i].lit_i + 63) / 64);
+        FDB_CUDA(cudaMemcpyAsync(sets[(size_t)i].data(), prog[i].code_set, sets[(size_t)i].size() * 8,
+                                 cudaMemcpyDeviceToHost, c.stream));
+      }
+    FDB_CUDA(cudaStreamSynchronize(c.stream));
+    const uint64_t nb = zone_batches(t.nrows);
+    if (nbatches) *nbatches = nb;
+    const std::vector<uint8_t> out = zone_rule_out(zones, dtypes, prog, nterms, sets, nb);
+    if (words) std::memset(skip, 0, words * 8);
+    for (uint64_t b = 0; b < nb && (b >> 6) < words; ++b)
+      if (out[b]) skip[b >> 6] |= 1ull << (b & 63);
+  });
+}
+
+int fdb_set_option(fdb_db* db, const char* name, int64_t value) {
+  if (!db || !name) return set_error(FDB_E_ARG, "fdb_set_option: bad arguments");
+  return guarded([&] {
+    std::lock_guard<std::recursive_mutex> lk(db->ctx.mu);
+    if (std::strcmp(name, "zone_maps") == 0) {
+      db->ctx.zone_maps = value != 0;
+      return;
+    }
+    fail(FDB_E_ARG, std::string("unknown option ") + name);
   });
 }
 
@@ -424,6 +480,7 @@ const char* fdb_result_display(fdb_result* r) { return r ? r->display_text().c_s
 void fdb_result_free(fdb_result* r) { delete r; }
 
 double fdb_last_kernel_ms(const fdb_db* db) { return db ? db->ctx.last_kernel_ms : 0.0; }
+uint64_t fdb_last_scan_rows(const fdb_db* db) { return db ? db->ctx.last_scan_rows : 0; }
 
 int fdb_memory_stats(fdb_db* db, fdb_mem_stats* out) {
   if (!db || !out) return set_error(FDB_E_ARG, "fdb_memory_stats: bad arguments");

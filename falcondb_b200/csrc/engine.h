@@ -15,6 +15,7 @@
 
 #include "../../include/falcondb_b200.h"
 #include "once.h"
+#include "zone.h"
 
 namespace fdb {
 
@@ -50,6 +51,13 @@ struct Column {
   DevBuf validity;              // empty when the column has no NULLs
   std::vector<std::string> dict;
   cudaEvent_t ready = nullptr;  // recorded on the upload stream after the copy
+  // Zone map: one fdb_zone per 65,536-row batch, computed on the zone stream
+  // once the upload is done; the host copy is fetched on first use.
+  DevBuf zones;
+  uint64_t nzones = 0;
+  cudaEvent_t zones_ready = nullptr;
+  std::vector<fdb_zone> zhost;
+  bool zhost_valid = false;
 };
 
 struct Table {
@@ -72,6 +80,8 @@ struct Ctx {
   std::atomic<size_t> in_use{0};
   cudaStream_t stream = nullptr;         // operator stream
   cudaStream_t upload = nullptr;         // host->device copies
+  cudaStream_t zstream = nullptr;        // zone maps of freshly loaded columns
+  bool zone_maps = true;                 // option "zone_maps"
   std::recursive_mutex mu;               // serialises calls on this context
 
   // Scratch arena: a device buffer carved per operator call.  The first
@@ -85,6 +95,7 @@ struct Ctx {
   std::map<std::string, std::shared_ptr<Table>> tables;
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;
   double last_kernel_ms = 0.0;
+  uint64_t last_scan_rows = 0;           // rows of the table the last fdb_sql scanned
 
   ~Ctx();
   void* dev_alloc(size_t bytes);                 // budgeted cudaMalloc
@@ -201,6 +212,18 @@ struct KeyStats {
   int64_t kmin = 0, kmax = 0;
 };
 KeyStats key_stats_i64(Ctx& c, const fdb_dev_column& key, uint64_t n);
+
+// Zone maps (k_zone.cu, zone.cpp; pruning in zone_prune.cpp).
+// Fills d_out[0 .. zone_batches(nrows)) on stream s.
+void op_zone_map(cudaStream_t s, const Column& col, uint64_t nrows, fdb_zone* d_out);
+// (Re)computes col's zone map on the zone stream after its upload.
+void build_zone_map(Ctx& c, Column& col, uint64_t nrows);
+void free_column(Ctx& c, Column& col);
+// The host copy of col's zone map (waits for it once).
+const std::vector<fdb_zone>& column_zones(Ctx& c, Column& col);
+// The resident column whose values hold `values` (a view starting at row
+// *first_row of it), or nullptr.
+Column* column_by_values(Ctx& c, const void* values, uint64_t* table_rows, uint64_t* first_row);
 // The estimate alone, over a column without NULLs.
 uint64_t estimate_distinct_i64(Ctx& c, const void* keys, uint64_t n);
 

@@ -810,6 +810,12 @@ static_assert((kDenseSumCopies & (kDenseSumCopies - 1)) == 0, "SUM copies: a pow
 #ifndef FDB_GBD_NCW
 #define FDB_GBD_NCW 8
 #endif
+// Rows a consumer thread decodes together: their tile reads and first CTA
+// table probes are all issued before any of them is applied.
+#ifndef FDB_GBD_ROWS
+#define FDB_GBD_ROWS 4
+#endif
+constexpr uint32_t kDenseRows = FDB_GBD_ROWS;
 
 struct GbDenseParams {
   PredProg prog;
@@ -873,13 +879,21 @@ __device__ __forceinline__ void dslot_merge(DSlot* d, const SDTab& t, uint32_t j
   if (t.max[j]) atomicMax(&d->max, t.max[j]);
 }
 
+// The CTA home slot of slot index k.
+__device__ __forceinline__ uint32_t smem_dense_home(uint32_t k) {
+  return (k * 0x9E3779B1u) >> (32 - kDenseSmemLog);
+}
+
 // The CTA slot of slot index k, claiming one if free within kDenseProbe
-// probes; -1 when it has no room there.
-__device__ __forceinline__ int smem_dense_slot(const SDTab& t, uint32_t k) {
-  uint32_t h = (k * 0x9E3779B1u) >> (32 - kDenseSmemLog);
+// probes from its home slot h; -1 when it has no room there.  cur0 is a read
+// of slot h's key taken earlier.  A CTA slot's key only ever goes from 0 to
+// a slot index, so an early read can only be stale as 0, and the
+// compare-and-swap then returns the key that is really there.
+__device__ __forceinline__ int smem_dense_slot_from(const SDTab& t, uint32_t k, uint32_t h, unsigned int cur0) {
   const unsigned int k1 = k + 1u;
+  unsigned int cur = cur0;
   for (uint32_t probe = 0; probe < kDenseProbe; ++probe) {
-    const unsigned int cur = *reinterpret_cast<volatile unsigned int*>(&t.k1[h]);
+    if (probe) cur = *reinterpret_cast<volatile unsigned int*>(&t.k1[h]);
     if (cur == k1) return (int)h;
     if (cur == 0) {
       const unsigned int prev = atomicCAS(&t.k1[h], 0u, k1);
@@ -904,33 +918,64 @@ struct GbDenseOp {
   static __device__ void step(Local&, const Params& p, unsigned char* sm, const Acc& acc, uint32_t rows, int ctid,
                               int nct) {
     const SDTab tab = sdtab(sm);
-    for (uint32_t i = ctid; i < rows; i += nct) {
-      const uint64_t row = acc.row(i);
-      if (p.prog.n) {
-        GbGetter<Acc> get{p.cols, acc, i, row};
-        if (!eval_prog(p.prog, get)) continue;
+    constexpr uint32_t R = kDenseRows;
+    enum : uint8_t { kSkip, kNull, kSlot };
+    for (uint32_t i0 = ctid; i0 < rows; i0 += (uint32_t)nct * R) {
+      uint32_t k[R], h[R];
+      unsigned int cur[R];
+      double v[R];
+      uint8_t kind[R];
+      bool has_v[R];
+      // Decode every row first: key, value, its kind and its CTA home slot.
+#pragma unroll
+      for (uint32_t r = 0; r < R; ++r) {
+        const uint32_t i = i0 + r * (uint32_t)nct;
+        kind[r] = kSkip;
+        has_v[r] = false;
+        v[r] = 0.0;
+        k[r] = 0;
+        if (i >= rows) continue;
+        const uint64_t row = acc.row(i);
+        if (p.prog.n) {
+          GbGetter<Acc> get{p.cols, acc, i, row};
+          if (!eval_prog(p.prog, get)) continue;
+        }
+        const int64_t key = acc.template get<int64_t>(0, i);
+        has_v[r] = p.cols[1].validity ? col_valid(p.cols[1], row) : true;
+        if (has_v[r])
+          v[r] = p.cols[1].dtype == FDB_FLOAT64 ? acc.template get<double>(1, i)
+                                                : (double)acc.template get<int64_t>(1, i);
+        const bool kvalid = (p.cols[0].validity ? col_valid(p.cols[0], row) : true) && key != INT64_MIN;
+        if (!kvalid) {  // NULL group (i64::MIN reads as NULL)
+          kind[r] = kNull;
+          continue;
+        }
+        const uint64_t kk = (uint64_t)key - (uint64_t)p.kmin;
+        if (kk >= p.slots) {  // outside the sized range: the sizing did not see this column
+          atomicExch(p.err, kErrCapacity);
+          continue;
+        }
+        k[r] = (uint32_t)kk;
+        kind[r] = kSlot;
       }
-      const int64_t key = acc.template get<int64_t>(0, i);
-      const bool has_v = p.cols[1].validity ? col_valid(p.cols[1], row) : true;
-      double v = 0.0;
-      if (has_v)
-        v = p.cols[1].dtype == FDB_FLOAT64 ? acc.template get<double>(1, i)
-                                           : (double)acc.template get<int64_t>(1, i);
-      const bool kvalid = (p.cols[0].validity ? col_valid(p.cols[0], row) : true) && key != INT64_MIN;
-      if (!kvalid) {  // NULL group (i64::MIN reads as NULL)
-        sdslot_accum(tab, kDenseSmemSlots, v, has_v);
-        continue;
+      // Every row's first probe in flight together.
+#pragma unroll
+      for (uint32_t r = 0; r < R; ++r) {
+        h[r] = smem_dense_home(k[r]);
+        cur[r] = kind[r] == kSlot ? tab.k1[h[r]] : 0u;
       }
-      const uint64_t k = (uint64_t)key - (uint64_t)p.kmin;
-      if (k >= p.slots) {  // outside the sized range: the sizing did not see this column
-        atomicExch(p.err, kErrCapacity);
-        continue;
+#pragma unroll
+      for (uint32_t r = 0; r < R; ++r) {
+        if (kind[r] == kNull) {
+          sdslot_accum(tab, kDenseSmemSlots, v[r], has_v[r]);
+        } else if (kind[r] == kSlot) {
+          const int j = smem_dense_slot_from(tab, k[r], h[r], cur[r]);
+          if (j >= 0)
+            sdslot_accum(tab, (uint32_t)j, v[r], has_v[r]);
+          else
+            dslot_accum(p.table + k[r], v[r], has_v[r]);
+        }
       }
-      const int j = smem_dense_slot(tab, (uint32_t)k);
-      if (j >= 0)
-        sdslot_accum(tab, (uint32_t)j, v, has_v);
-      else
-        dslot_accum(p.table + k, v, has_v);
     }
   }
 
@@ -1275,6 +1320,23 @@ GbSizing group_by_i64_sizing(Ctx& c, const fdb_dev_column& key, uint64_t n, uint
     return s;
   }
   if (key.dtype != FDB_INT64) fail(FDB_E_TYPE, "hash GROUP BY needs an INT64 key");
+  // A resident column's zone map bounds its keys without a pass over them.
+  // The direct-addressed table is then taken when it has at most one slot per
+  // two rows: its zeroing and compaction cost no more than the rows' reads.
+  uint64_t table_rows = 0, first_row = 0;
+  Column* col = c.zone_maps ? column_by_values(c, key.values, &table_rows, &first_row) : nullptr;
+  int64_t zmin = 0, zmax = 0;
+  if (col && col->dtype == FDB_INT64 && first_row + n <= table_rows &&
+      zone_key_range(column_zones(c, *col), first_row, n, &zmin, &zmax)) {
+    const uint64_t span = (uint64_t)zmax - (uint64_t)zmin;
+    if (span < kDenseMaxSlots && span + 1 <= n / 2) {
+      s.groups = span + 1;
+      s.has_range = true;
+      s.kmin = zmin;
+      s.kmax = zmax;
+      return s;
+    }
+  }
   const KeyStats k = key_stats_i64(c, key, n);
   // 15 % headroom over the sketch (about nine standard errors).
   s.groups = std::min<uint64_t>(n, k.distinct * 115 / 100 + 64);

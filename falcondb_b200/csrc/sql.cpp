@@ -548,6 +548,7 @@ struct RelCol {
   int32_t dtype = 0;
   fdb_dev_column dev{};
   const std::vector<std::string>* dict = nullptr;
+  Column* src = nullptr;  // the catalog column (zone maps), for a catalog table
 };
 struct Rel {
   uint64_t nrows = 0;
@@ -585,9 +586,9 @@ struct Plan {
   }
 };
 
-static void add_table_cols(Ctx& c, Rel& r, const Table& t, const std::string& alias) {
+static void add_table_cols(Ctx& c, Rel& r, Table& t, const std::string& alias) {
   r.nrows = t.nrows;
-  for (const Column& col : t.cols) {
+  for (Column& col : t.cols) {
     RelCol rc;
     rc.name = col.name;
     rc.qual = alias.empty() ? t.name : alias;
@@ -598,6 +599,7 @@ static void add_table_cols(Ctx& c, Rel& r, const Table& t, const std::string& al
     rc.dev.validity = static_cast<const uint64_t*>(col.validity.ptr);
     rc.dev.validity_offset = 0;
     rc.dict = &col.dict;
+    rc.src = &col;
     FDB_CUDA(cudaStreamWaitEvent(c.stream, col.ready, 0));
     r.cols.push_back(rc);
   }
@@ -641,6 +643,7 @@ struct PredCompiler {
   const Rel& rel;
   std::vector<int>& local;           // local column index -> rel column
   std::vector<fdb_pred_term> terms;
+  std::vector<std::vector<uint64_t>> host_sets;  // per term: the CODE_SET bitmap on the host
 
   int local_of(int relcol) {
     for (size_t i = 0; i < local.size(); ++i)
@@ -673,6 +676,8 @@ struct PredCompiler {
     t.col = col;
     t.lit_i = (int64_t)pass.size();
     t.code_set = d;
+    host_sets.resize(terms.size());
+    host_sets.push_back(std::move(bits));
     terms.push_back(t);
   }
   void leaf_cmp(int rc, int lc, int op, const Lit& lit) {
@@ -1604,8 +1609,8 @@ static bool names_side(const ColRef& r, const std::string& table, const std::str
 
 static void run_join(Plan& plan, Query& q, const JoinSpec& js, fdb_result* res) {
   Ctx& c = plan.c;
-  const Table& L = *js.left;
-  const Table& R = *js.right;
+  Table& L = *js.left;
+  Table& R = *js.right;
   const int lk = L.find(js.lkey), rk = R.find(js.rkey);
   if (lk < 0) fail(FDB_E_NOTFOUND, "no column " + js.lkey + " in " + L.name);
   if (rk < 0) fail(FDB_E_NOTFOUND, "no column " + js.rkey + " in " + R.name);
@@ -1815,6 +1820,44 @@ const std::string& fdb_result::display_text() {
 
 namespace fdb {
 
+// Zone-map pruning (execute_select's can_skip, select.rs:115-137): the
+// relation is narrowed to the batches from the first to the last one that
+// the zone maps cannot rule out for the WHERE clause.  Batches ruled out in
+// between are still scanned (their rows fail the filter); none that could
+// hold a passing row is ever left out, so no result changes.
+static void prune_rel(Plan& plan, Rel& rel, const Query& q) {
+  if (!plan.c.zone_maps || !q.where || rel.nrows == 0) return;
+  std::vector<int> local;
+  PredCompiler pc{plan, rel, local, {}, {}};
+  pc.compile(*q.where);
+  std::vector<const std::vector<fdb_zone>*> zones;
+  std::vector<int32_t> dtypes;
+  for (int rc : local) {
+    const RelCol& col = rel.cols[(size_t)rc];
+    zones.push_back(col.src ? &column_zones(plan.c, *col.src) : nullptr);
+    dtypes.push_back(col.dtype);
+  }
+  const uint64_t nb = zone_batches(rel.nrows);
+  const std::vector<uint8_t> out =
+      zone_rule_out(zones, dtypes, pc.terms.data(), (int)pc.terms.size(), pc.host_sets, nb);
+  uint64_t b0 = 0, b1 = nb;
+  while (b0 < nb && out[b0]) ++b0;
+  while (b1 > b0 && out[b1 - 1]) --b1;
+  if (b0 == 0 && b1 == nb) return;
+  const uint64_t r0 = b0 * kZoneRows;
+  const uint64_t r1 = std::min<uint64_t>(rel.nrows, b1 * kZoneRows);
+  if (r1 <= r0) {
+    rel.nrows = 0;
+    return;
+  }
+  for (RelCol& col : rel.cols) {
+    col.dev.values = static_cast<const char*>(col.dev.values) + r0 * (uint64_t)dtype_size(col.dtype);
+    // r0 is a multiple of 65,536, so the validity view stays word-aligned.
+    if (col.dev.validity) col.dev.validity += r0 / 64;
+  }
+  rel.nrows = r1 - r0;
+}
+
 fdb_result* run_sql(Ctx& c, const std::string& sql) {
   Parser ps(sql);
   Query q = ps.query();
@@ -1857,6 +1900,8 @@ fdb_result* run_sql(Ctx& c, const std::string& sql) {
   } else {
     Rel rel;
     add_table_cols(c, rel, *find_table(c, q.table), q.alias);
+    prune_rel(plan, rel, q);
+    c.last_scan_rows = rel.nrows;
     bool all_agg = !q.items.empty();
     for (const SelItem& it : q.items) all_agg = all_agg && it.agg >= 0;
     if (q.distinct && (q.has_group || all_agg))

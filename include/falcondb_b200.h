@@ -209,6 +209,54 @@ int  fdb_table_drop(fdb_db* db, const char* name);
 int  fdb_table_column(const fdb_db* db, const char* table, const char* column,
                       fdb_dev_column* out, uint64_t* nrows);
 
+/* Zone maps (src/storage/stats.rs:22-52): the bounds and NULL count of every
+ * 65,536-row batch of a column (Table::DEFAULT_BATCH_SIZE, table.rs:339),
+ * computed on the GPU when the table is loaded, as Table::append_batch and
+ * append_batches compute BatchStats (table.rs:373, 391-404).
+ *   FDB_INT64  : min_i / max_i, exact (the reference goes through f64).
+ *   FDB_FLOAT64: min_f / max_f over the non-NaN values (f64::min / max skip
+ *                NaN); FDB_ZONE_NAN when the batch holds a NaN.
+ *   FDB_UTF8   : min_i / max_i = the smallest and largest dictionary code.
+ * FDB_ZONE_VALUES is set when the batch holds a non-NULL (for FLOAT64 a
+ * non-NULL, non-NaN) value; the bounds are meaningful only then. */
+#define FDB_ZONE_BATCH_ROWS 65536
+#define FDB_ZONE_VALUES     1
+#define FDB_ZONE_NAN        2
+typedef struct fdb_zone {
+    int64_t  min_i, max_i;
+    double   min_f, max_f;
+    uint64_t null_count;
+    uint32_t rows;
+    uint32_t flags;
+} fdb_zone;
+
+/* Copy the zone map of table.column into out[0 .. min(cap, batches)); the
+ * batch count goes to *nbatches.  out may be NULL with cap 0. */
+int  fdb_table_zone_map(fdb_db* db, const char* table, const char* column, fdb_zone* out,
+                        uint64_t cap, uint64_t* nbatches);
+
+/* The batches of `table` that a WHERE program cannot select, from the zone
+ * maps alone (BatchStats::can_skip, stats.rs:57-113): bit b of skip (LSB
+ * first, ceil(batches / 64) words) is set when no row of batch b can pass.
+ * cols[i] names the table column that the program's column i refers to;
+ * CODE_SET bitmaps are device pointers, as for the operators.  Pruning is
+ * conservative and never changes a result: a CMP leaf rules a batch out when
+ * its bounds exclude the literal (compared exactly for INT64 against an INT64
+ * literal, in float64 otherwise, as the filter compares), IS NULL when the
+ * batch has no NULL, IS NOT NULL when it is all NULL, CODE_SET when no code in
+ * the batch's code range is in the set; AND rules out when either side does,
+ * OR when both do.  NE on FLOAT64 never rules out a batch holding a NaN
+ * (NaN != x is true), which the reference's rule (stats.rs:110) misses. */
+int  fdb_zone_skip(fdb_db* db, const char* table, const char* const* cols, int32_t ncols,
+                   const fdb_pred_term* prog, int32_t nterms, uint64_t* skip, uint64_t words,
+                   uint64_t* nbatches);
+
+/* Context options.  "zone_maps" (default 1): fdb_sql scans only the batches
+ * from the first to the last one that zone maps cannot rule out, and an
+ * int64-key GROUP BY over a resident column takes its key range from the
+ * column's zone maps instead of a pass over the keys.  0 turns both off. */
+int  fdb_set_option(fdb_db* db, const char* name, int64_t value);
+
 /* Execute SQL (falcondb_sql, c_ffi.rs:86-99 -> Database::sql, db.rs:242-316).
  * *out is NULL on error.  Supported shapes (others fail with FDB_E_SQL):
  *   SELECT [DISTINCT] items FROM t [[INNER] | LEFT [OUTER] JOIN u ON t.k = u.k] [WHERE pred]
@@ -217,10 +265,12 @@ int  fdb_table_column(const fdb_db* db, const char* table, const char* column,
  *          ROW_NUMBER() OVER ([ORDER BY col [ASC|DESC]]) [AS a]
  *   pred : col op literal, IS [NOT] NULL, [NOT] IN (...), [NOT] LIKE (Utf8), AND, OR,
  *          parentheses, and [NOT] EXISTS (SELECT ... FROM u WHERE u.k = t.k).
- * ORDER BY one FLOAT64 / INT64 column runs on the GPU (fdb_topk for LIMIT <= 4096,
- * else fdb_sort); several keys or a UTF8 key are ordered on the host after the
- * fetch.  DISTINCT takes one column and runs after ORDER BY and LIMIT, as the
- * reference does (db.rs:1699-1729). */
+ * ORDER BY runs on the GPU: one FLOAT64 / INT64 key through fdb_topk (LIMIT <= 4096)
+ * or fdb_sort; several keys, or a UTF8 key (by the rank of its string), through one
+ * stable radix pass per key, last key first.  DISTINCT compares whole rows on the GPU
+ * and runs after ORDER BY and LIMIT, as the reference does (db.rs:1699-1729).  With a
+ * WHERE on one table, only the batches from the first to the last one that the zone
+ * maps cannot rule out are scanned (execute_select, select.rs:105-160). */
 int  fdb_sql(fdb_db* db, const char* sql, fdb_result** out);
 
 /* Result accessors (c_ffi.rs:103-127). */
@@ -238,6 +288,9 @@ void        fdb_result_free(fdb_result* r);
 
 /* Device time of the kernels of the last fdb_sql on this context, in ms. */
 double      fdb_last_kernel_ms(const fdb_db* db);
+/* Rows of its table that the last single-table fdb_sql scanned, after zone-map
+ * pruning (the table's row count when nothing was pruned). */
+uint64_t    fdb_last_scan_rows(const fdb_db* db);
 
 /* Device memory the context holds, for monitoring (no counterpart in the
  * reference, whose memory is the host heap).  in_use: bytes counted against

@@ -460,3 +460,162 @@ def distinct_multi(cols, n: int) -> np.ndarray:
             seen.add(t)
             out.append(i)
     return np.asarray(out, dtype=np.uint32)
+
+
+# ---------------------------------------------------------------------------- zone maps
+ZONE_BATCH_ROWS = 65_536
+ZONE_VALUES, ZONE_NAN = 1, 2
+ZONE_DTYPE = np.dtype([("min_i", "<i8"), ("max_i", "<i8"), ("min_f", "<f8"), ("max_f", "<f8"),
+                       ("null_count", "<u8"), ("rows", "<u4"), ("flags", "<u4")])
+NULL_CODE = 0xFFFFFFFF
+
+
+def _valid_bits(validity, n):
+    if validity is None:
+        return np.ones(n, bool)
+    w = np.asarray(validity, dtype=np.uint64)
+    bits = np.unpackbits(w.view(np.uint8), bitorder="little")[:n]
+    return bits.astype(bool)
+
+
+def zone_map(values, kind: str, validity=None, batch_rows: int = ZONE_BATCH_ROWS) -> np.ndarray:
+    """Per-batch bounds and NULL counts (column_stats, stats.rs:148-260, one
+    entry per Table batch, table.rs:339, 373).  kind "int" (INT64, exact
+    bounds), "float" (FLOAT64: bounds over the non-NaN values, as f64::min /
+    max skip NaN, with ZONE_NAN when a NaN is present) or "code" (UTF8:
+    smallest and largest dictionary code; NULL_CODE counts as NULL).
+    ZONE_VALUES marks a batch holding a non-NULL (non-NaN) value."""
+    v = np.asarray(values)
+    n = len(v)
+    valid = _valid_bits(validity, n)
+    nb = (n + batch_rows - 1) // batch_rows
+    out = np.zeros(nb, dtype=ZONE_DTYPE)
+    for b in range(nb):
+        s, e = b * batch_rows, min(n, (b + 1) * batch_rows)
+        x, ok = v[s:e], valid[s:e].copy()
+        if kind == "code":
+            ok &= x != NULL_CODE
+        out["rows"][b] = e - s
+        out["null_count"][b] = int((~ok).sum())
+        flags = 0
+        if kind == "float":
+            xf = x[ok].astype(np.float64)
+            if np.isnan(xf).any():
+                flags |= ZONE_NAN
+            xf = xf[~np.isnan(xf)]
+            if len(xf):
+                flags |= ZONE_VALUES
+                out["min_f"][b], out["max_f"][b] = xf.min(), xf.max()
+        else:
+            xi = x[ok].astype(np.int64)
+            if len(xi):
+                flags |= ZONE_VALUES
+                out["min_i"][b], out["max_i"][b] = xi.min(), xi.max()
+        out["flags"][b] = flags
+    return out
+
+
+# Term kinds and comparison operators of the engine's predicate programs.
+T_CMP, T_IS_NULL, T_IS_NOT_NULL, T_CODE_SET, T_AND, T_OR = range(6)
+EQ, NE, LT, LE, GT, GE = range(6)
+
+
+def _cmp_rules_out(z, kind, op, lit_is_float, lit):
+    """Can no row of batch z pass `col op lit` (can_skip_comparison,
+    stats.rs:70-113), with the filter's own arithmetic: INT64 or a code
+    against an INT64 literal compared exactly, INT64 against a FLOAT64
+    literal as float(value), FLOAT64 as double.  NULL rows fail every
+    comparison and NaN rows pass NE only."""
+    values = bool(z["flags"] & ZONE_VALUES)
+    nan = bool(z["flags"] & ZONE_NAN)
+    if kind == "float" or (kind == "int" and lit_is_float):
+        lit = float(lit)
+        lo, hi = ((float(z["min_f"]), float(z["max_f"])) if kind == "float"
+                  else (float(int(z["min_i"])), float(int(z["max_i"]))))
+        if op == NE:
+            if nan:
+                return False
+            if not values:
+                return True
+            if lit != lit:
+                return False
+            return lo == hi == lit
+        if not values or lit != lit:
+            return True
+    else:
+        if not values:
+            return True
+        lit = int(lit)
+        lo, hi = int(z["min_i"]), int(z["max_i"])
+        if op == NE:
+            return lo == hi == lit
+    return {EQ: lit < lo or lit > hi, LT: lo >= lit, LE: lo > lit, GT: hi <= lit, GE: hi < lit}[op]
+
+
+def zone_rule_out(zones, kinds, terms) -> np.ndarray:
+    """Per batch, True when the postfix program `terms` cannot pass any row
+    of it (BatchStats::can_skip, stats.rs:57-68: AND rules out when either
+    side does, OR when both do).  zones[c] / kinds[c]: the zone map and kind
+    of the program's column c.  A term is a dict: kind, and col, op,
+    lit (int or float), lit_float (bool), or set (a Python set of codes) and
+    dict_len for CODE_SET.  IS NULL rules out a batch without NULLs, IS NOT
+    NULL an all-NULL one."""
+    nb = len(zones[0]) if zones else 0
+    out = np.zeros(nb, bool)
+    for b in range(nb):
+        st = []
+        for t in terms:
+            k = t["kind"]
+            if k in (T_AND, T_OR):
+                a, c = st.pop(), st.pop()
+                st.append((a or c) if k == T_AND else (a and c))
+                continue
+            z = zones[t["col"]][b]
+            kind = kinds[t["col"]]
+            if k == T_IS_NULL:
+                st.append(int(z["null_count"]) == 0)
+            elif k == T_IS_NOT_NULL:
+                st.append(int(z["null_count"]) == int(z["rows"]))
+            elif k == T_CODE_SET:
+                if kind != "code":
+                    st.append(False)
+                elif not z["flags"] & ZONE_VALUES:
+                    st.append(True)
+                else:
+                    lo, hi = max(int(z["min_i"]), 0), min(int(z["max_i"]), t["dict_len"] - 1)
+                    st.append(not any(lo <= c <= hi for c in t["set"]))
+            else:
+                st.append(_cmp_rules_out(z, kind, t["op"], t.get("lit_float", False), t["lit"]))
+        out[b] = st.pop()
+    return out
+
+
+def ref_can_skip_cmp(values, op, lit) -> bool:
+    """The reference's own rule for one batch (column_stats + can_skip_comparison,
+    stats.rs:70-113, 148-180): bounds folded in f64 (an INT64 value goes through
+    `x as f64`, then back with `as i64`), NaN skipped by f64::min / max unless
+    every value is NaN, and `!=` ruled out when min == max == literal with no
+    NULL.  Small inputs only; the tests use it to record where the engine's
+    exact rule differs."""
+    vals = [float(x) for x in values]
+    if not vals:
+        return False
+    mn = mx = None
+    for x in vals:
+        mn = x if mn is None else (x if mn != mn else (mn if x != x else min(mn, x)))
+        mx = x if mx is None else (x if mx != mx else (mx if x != x else max(mx, x)))
+    is_int = np.asarray(values).dtype.kind in "iu"
+    if is_int:  # ScalarValue::Int64(Some(x as i64)), compared again as f64
+        mn, mx = float(int(mn)), float(int(mx))
+    lit = float(lit)
+    if op == GT:
+        return mx <= lit
+    if op == GE:
+        return mx < lit
+    if op == LT:
+        return mn >= lit
+    if op == LE:
+        return mn > lit
+    if op == EQ:
+        return lit < mn or lit > mx
+    return mn == mx == lit
