@@ -173,6 +173,8 @@ def run_gpu(args):
     t = make_table(n, seed=1 + rank)
 
     db = F.Database(local)
+    if args.tuning:
+        db.load_tuning(args.tuning)
     db.create_table("t", t)
     db.synchronize()
     cs = {c: db.column("t", c) for c in ("id", "dept", "score")}
@@ -735,6 +737,8 @@ def run_secondary(args):
 
     dev = torch.device("cuda", 0)
     db = F.Database(0)
+    if args.tuning:
+        db.load_tuning(args.tuning)
     stream = ops.lib_stream(db)
     peak, peak_kind = peaks()
     out = []
@@ -1236,6 +1240,7 @@ def main():
                              "all"],
                     help="scan = the headline line; the others print per-operator lines")
     ap.add_argument("--load-factor", type=float, default=0.5)
+    ap.add_argument("--tuning", default="", help="a launch-tuning cache (fdb_tuning_save) to load first")
     ap.add_argument("--serve-queries", type=int, default=10_000)
     ap.add_argument("--serve-slots", type=int, default=2)
     args = ap.parse_args()

@@ -132,6 +132,12 @@ class fdb_zone(C.Structure):
                 ("null_count", C.c_uint64), ("rows", C.c_uint32), ("flags", C.c_uint32)]
 
 
+class fdb_op_tuning(C.Structure):
+    _fields_ = [("ctas_per_sm", C.c_int32), ("_pad", C.c_int32), ("min_rows_per_cta", C.c_uint64)]
+
+
+TUNE_SCAN, TUNE_GROUP, TUNE_GROUP_I64, TUNE_PROBE, TUNE_TOPK = range(5)
+TUNE_KINDS = ("scan", "group", "group_i64", "probe", "topk")
 ZONE_BATCH_ROWS = 65536
 ZONE_VALUES, ZONE_NAN = 1, 2
 ZONE_DTYPE = np.dtype([("min_i", "<i8"), ("max_i", "<i8"), ("min_f", "<f8"), ("max_f", "<f8"),
@@ -170,6 +176,12 @@ _SIGS = {
     "fdb_zone_skip": (C.c_int, [C.c_void_p, C.c_char_p, C.POINTER(C.c_char_p), C.c_int32, C.POINTER(fdb_pred_term),
                                 C.c_int32, C.c_void_p, C.c_uint64, C.POINTER(C.c_uint64)]),
     "fdb_set_option": (C.c_int, [C.c_void_p, C.c_char_p, C.c_int64]),
+    "fdb_get_tuning": (C.c_int, [C.c_void_p, C.c_int32, C.POINTER(fdb_op_tuning)]),
+    "fdb_set_tuning": (C.c_int, [C.c_void_p, C.c_int32, C.POINTER(fdb_op_tuning)]),
+    "fdb_autotune_ops": (C.c_int, [C.c_void_p, C.c_uint64, C.c_int32, C.POINTER(fdb_op_tuning),
+                                   C.POINTER(C.c_double)]),
+    "fdb_tuning_save": (C.c_int, [C.c_void_p, C.c_char_p]),
+    "fdb_tuning_load": (C.c_int, [C.c_void_p, C.c_char_p]),
     "fdb_memory_stats": (C.c_int, [C.c_void_p, C.POINTER(fdb_mem_stats)]),
     "fdb_stream": (C.c_void_p, [C.c_void_p]),
     "fdb_synchronize": (C.c_int, [C.c_void_p]),
@@ -622,6 +634,40 @@ class Database:
         bits = np.unpackbits(words.view(np.uint8), bitorder="little")[:int(got.value)]
         return bits.astype(bool)
 
+    # -- launch tuning (tuning.rs:39-53's cut-offs, tuned on the device) ---------------
+    def tuning(self) -> Dict[str, Dict[str, int]]:
+        """Launch tuning of each kind of streamed operator: CTAs per SM
+        (0 = occupancy limit) and rows per CTA (0 = no minimum)."""
+        out = {}
+        for k, name in enumerate(TUNE_KINDS):
+            t = fdb_op_tuning()
+            check(lib().fdb_get_tuning(self.handle, k, C.byref(t)))
+            out[name] = {"ctas_per_sm": int(t.ctas_per_sm), "min_rows_per_cta": int(t.min_rows_per_cta)}
+        return out
+
+    def set_tuning(self, kind: Union[int, str], ctas_per_sm: int = 0, min_rows_per_cta: int = 0) -> None:
+        k = TUNE_KINDS.index(kind) if isinstance(kind, str) else int(kind)
+        t = fdb_op_tuning(ctas_per_sm, 0, min_rows_per_cta)
+        check(lib().fdb_set_tuning(self.handle, k, C.byref(t)))
+
+    def autotune(self, rows: int = 1 << 24, reps: int = 5) -> Tuple[Dict[str, Dict[str, int]], Dict[str, float]]:
+        """Time launch-shape candidates for every kind of streamed operator on
+        `rows` synthetic rows (fdb_autotune_ops) and keep the fastest.
+        Returns (choices, ms per call at `rows`)."""
+        best = (fdb_op_tuning * len(TUNE_KINDS))()
+        ms = (C.c_double * len(TUNE_KINDS))()
+        check(lib().fdb_autotune_ops(self.handle, rows, reps, best, ms))
+        return ({n: {"ctas_per_sm": int(best[k].ctas_per_sm), "min_rows_per_cta": int(best[k].min_rows_per_cta)}
+                 for k, n in enumerate(TUNE_KINDS)}, {n: float(ms[k]) for k, n in enumerate(TUNE_KINDS)})
+
+    def save_tuning(self, path: str) -> None:
+        """Write the tuning cache (JSON) for this device."""
+        check(lib().fdb_tuning_save(self.handle, str(path).encode()))
+
+    def load_tuning(self, path: str) -> None:
+        """Apply a tuning cache written on the same kind of device."""
+        check(lib().fdb_tuning_load(self.handle, str(path).encode()))
+
     def set_option(self, name: str, value: int) -> None:
         """Context option (fdb_set_option): "zone_maps" 1 / 0."""
         check(lib().fdb_set_option(self.handle, name.encode(), int(value)))
@@ -637,5 +683,5 @@ __all__ = [
     "Database", "Result", "Utf8", "DeviceUtf8", "DevColumn", "FalconError", "lib", "check", "version", "validity_words",
     "INT64", "FLOAT64", "UTF8", "EQ", "NE", "LT", "LE", "GT", "GE", "AGG_COUNT_STAR", "AGG_COUNT", "AGG_SUM",
     "AGG_AVG", "AGG_MIN", "AGG_MAX", "AGG_COUNT_DISTINCT", "JOIN_INNER", "JOIN_LEFT", "JOIN_SEMI", "JOIN_ANTI",
-    "NO_ROW", "EXPORTED", "ZONE_DTYPE", "ZONE_BATCH_ROWS", "ZONE_VALUES", "ZONE_NAN",
+    "NO_ROW", "EXPORTED", "ZONE_DTYPE", "ZONE_BATCH_ROWS", "ZONE_VALUES", "ZONE_NAN", "TUNE_KINDS",
 ]

@@ -198,6 +198,7 @@ int fdb_open(int device, uint64_t mem_budget_bytes, fdb_db** out) {
     FDB_CUDA(cudaGetDeviceProperties(&prop, device));
     if (prop.major < 10) fail(FDB_E_CUDA, "fdb_open: this build targets sm_100a (B200)");
     c.sm_count = prop.multiProcessorCount;
+    c.device_name = prop.name;
     size_t free_b = 0, total_b = 0;
     FDB_CUDA(cudaMemGetInfo(&free_b, &total_b));
     c.budget = mem_budget_bytes ? (size_t)mem_budget_bytes : (size_t)(free_b * 0.9);
@@ -728,7 +729,7 @@ int fdb_gb_batch_prepare(fdb_db* db, const fdb_gb_query* queries, int32_t nqueri
     CallScope s(db, default_scratch(db->ctx));
     std::unique_ptr<fdb_batch> b(new fdb_batch());
     b->db = db;
-    b->plan = op_gb_batch_prepare(s.c, queries, nqueries, tuning);
+    b->plan = op_gb_batch_prepare(s.c, queries, nqueries, tuning ? tuning : &s.c.tune.batch);
     *out = b.release();
   });
 }
@@ -758,7 +759,74 @@ int fdb_gb_batch_autotune(fdb_db* db, const fdb_gb_query* queries, int32_t nquer
   return guarded([&] {
     CallScope s(db, default_scratch(db->ctx));
     const double ms = op_gb_batch_autotune(s.c, queries, nqueries, reps, best);
+    s.c.tune.batch = *best;
     if (best_ms) *best_ms = ms;
+  });
+}
+
+int fdb_get_tuning(fdb_db* db, int32_t kind, fdb_op_tuning* out) {
+  if (!db || !out || kind < 0 || kind >= FDB_TUNE_KINDS) return set_error(FDB_E_ARG, "fdb_get_tuning: bad arguments");
+  std::lock_guard<std::recursive_mutex> lk(db->ctx.mu);
+  const OpTuning& t = db->ctx.tune.op[kind];
+  out->ctas_per_sm = t.ctas_per_sm;
+  out->_pad = 0;
+  out->min_rows_per_cta = t.min_rows_per_cta;
+  return FDB_OK;
+}
+
+int fdb_set_tuning(fdb_db* db, int32_t kind, const fdb_op_tuning* in) {
+  if (!db || !in || kind < 0 || kind >= FDB_TUNE_KINDS || in->ctas_per_sm < 0 || in->ctas_per_sm > 64)
+    return set_error(FDB_E_ARG, "fdb_set_tuning: bad arguments");
+  std::lock_guard<std::recursive_mutex> lk(db->ctx.mu);
+  db->ctx.tune.op[kind].ctas_per_sm = in->ctas_per_sm;
+  db->ctx.tune.op[kind].min_rows_per_cta = in->min_rows_per_cta;
+  return FDB_OK;
+}
+
+int fdb_autotune_ops(fdb_db* db, uint64_t rows, int32_t reps, fdb_op_tuning* best, double* ms_per_call) {
+  if (!db) return set_error(FDB_E_ARG, "fdb_autotune_ops: bad arguments");
+  return guarded([&] {
+    CallScope s(db, default_scratch(db->ctx));
+    op_autotune(s.c, rows, reps, best, ms_per_call);
+  });
+}
+
+int fdb_tuning_save(fdb_db* db, const char* path) {
+  if (!db || !path) return set_error(FDB_E_ARG, "fdb_tuning_save: bad arguments");
+  return guarded([&] {
+    std::string text;
+    {
+      std::lock_guard<std::recursive_mutex> lk(db->ctx.mu);
+      text = tuning_to_json(db->ctx.tune, db->ctx.device_name, db->ctx.sm_count);
+    }
+    std::FILE* f = std::fopen(path, "wb");
+    if (!f) fail(FDB_E_ARG, std::string("cannot write ") + path);
+    const size_t w = std::fwrite(text.data(), 1, text.size(), f);
+    const int closed = std::fclose(f);
+    if (w != text.size() || closed != 0) fail(FDB_E_GENERIC, std::string("short write to ") + path);
+  });
+}
+
+int fdb_tuning_load(fdb_db* db, const char* path) {
+  if (!db || !path) return set_error(FDB_E_ARG, "fdb_tuning_load: bad arguments");
+  return guarded([&] {
+    std::FILE* f = std::fopen(path, "rb");
+    if (!f) fail(FDB_E_NOTFOUND, std::string("cannot read ") + path);
+    std::string text;
+    char buf[4096];
+    size_t got;
+    while ((got = std::fread(buf, 1, sizeof(buf), f)) > 0 && text.size() < (1u << 20)) text.append(buf, got);
+    std::fclose(f);
+    TuningSet t;
+    std::string device;
+    int sms = 0;
+    const std::string err = tuning_from_json(text, &t, &device, &sms);
+    if (!err.empty()) fail(FDB_E_ARG, std::string(path) + ": " + err);
+    std::lock_guard<std::recursive_mutex> lk(db->ctx.mu);
+    if (device != db->ctx.device_name || sms != db->ctx.sm_count)
+      fail(FDB_E_ARG, std::string(path) + " was tuned on " + device + " (" + std::to_string(sms) + " SMs), not " +
+                          db->ctx.device_name + " (" + std::to_string(db->ctx.sm_count) + " SMs)");
+    db->ctx.tune = t;
   });
 }
 

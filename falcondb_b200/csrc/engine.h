@@ -15,6 +15,7 @@
 
 #include "../../include/falcondb_b200.h"
 #include "once.h"
+#include "tuning.h"
 #include "zone.h"
 
 namespace fdb {
@@ -82,6 +83,8 @@ struct Ctx {
   cudaStream_t upload = nullptr;         // host->device copies
   cudaStream_t zstream = nullptr;        // zone maps of freshly loaded columns
   bool zone_maps = true;                 // option "zone_maps"
+  std::string device_name;               // cudaDeviceProp::name
+  TuningSet tune;                        // launch tuning (fdb_set_tuning / autotune / cache)
   std::recursive_mutex mu;               // serialises calls on this context
 
   // Scratch arena: a device buffer carved per operator call.  The first
@@ -230,6 +233,9 @@ uint64_t estimate_distinct_i64(Ctx& c, const void* keys, uint64_t n);
 struct BatchPlan;
 BatchPlan* op_gb_batch_prepare(Ctx& c, const fdb_gb_query* qs, int nq, const fdb_batch_tuning* t);
 void op_gb_batch_run(BatchPlan* p);
+// Launch-shape autotuner of the streamed operators (k_tune.cu): fills
+// c.tune.op and best[FDB_TUNE_KINDS]; ms_at_rows may be null.
+void op_autotune(Ctx& c, uint64_t rows, int reps, fdb_op_tuning* best, double* ms_at_rows);
 void op_gb_batch_free(BatchPlan* p);
 double op_gb_batch_autotune(Ctx& c, const fdb_gb_query* qs, int nq, int reps, fdb_batch_tuning* best);
 void op_topk(Ctx& c, const fdb_dev_column& col, uint64_t n, uint32_t k, bool desc,

@@ -21,6 +21,7 @@
 //    to run; tests hold it to 1e-12 relative).
 #include <algorithm>
 #include <cstring>
+#include <type_traits>
 
 #include "common.cuh"
 #include "engine.h"
@@ -1130,14 +1131,14 @@ static void launch_stream_gb(Ctx& c, const fdb_dev_column* cols, uint64_t n,
   attr(c.device, [&] { FDB_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, 220 * 1024)); });
   int per_sm = 0;
   FDB_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, (NCW + 1) * 32, smem));
-  if (per_sm < 1) per_sm = 1;
-  if (per_sm > 4) per_sm = 4;
   const uint64_t ntiles = (src.m_end + TR - 1) / TR;
   // At least kGbTilesPerCta tiles per CTA: on small inputs fewer CTAs means
   // fewer partials for the last CTA to fold.
-  uint64_t want = ntiles ? (ntiles + kGbTilesPerCta - 1) / kGbTilesPerCta : (n + NCW * 32 * 8 - 1) / (NCW * 32 * 8);
-  if (want < 1) want = 1;
-  const int grid = (int)umin64(want, (uint64_t)c.sm_count * per_sm);
+  const uint64_t want =
+      ntiles ? (ntiles + kGbTilesPerCta - 1) / kGbTilesPerCta : (n + NCW * 32 * 8 - 1) / (NCW * 32 * 8);
+  constexpr int kKind =
+      std::is_same<Op, GbDenseOp>::value || std::is_same<Op, GbHashOp>::value ? FDB_TUNE_GROUP_I64 : FDB_TUNE_GROUP;
+  const int grid = tuned_grid(c.tune.op[kKind], c.sm_count, per_sm, 4, want, n);
   kern<<<grid, (NCW + 1) * 32, smem, c.stream>>>(src, p, c.d_err, op_off);
   FDB_CUDA(cudaGetLastError());
 }

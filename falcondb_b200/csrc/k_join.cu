@@ -693,12 +693,9 @@ static void launch_probe_mode(Ctx& c, const fdb_dev_column* cols, uint64_t n, co
   attr(c.device, [&] { FDB_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024)); });
   int per_sm = 0;
   FDB_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, (NCW + 1) * 32, smem));
-  if (per_sm < 1) per_sm = 1;
-  if (per_sm > kProbeMaxPerSm) per_sm = kProbeMaxPerSm;
   const uint64_t ntiles = (src.m_end + TR - 1) / TR;
-  uint64_t want = ntiles ? ntiles : (n + NCW * 32 * 8 - 1) / (NCW * 32 * 8);
-  if (want < 1) want = 1;
-  const int grid = (int)umin64(want, (uint64_t)c.sm_count * per_sm);
+  const uint64_t want = ntiles ? ntiles : (n + NCW * 32 * 8 - 1) / (NCW * 32 * 8);
+  const int grid = tuned_grid(c.tune.op[FDB_TUNE_PROBE], c.sm_count, per_sm, kProbeMaxPerSm, want, n);
   kern<<<grid, (NCW + 1) * 32, smem, c.stream>>>(src, p, c.d_err, op_off);
   FDB_CUDA(cudaGetLastError());
 }
@@ -729,7 +726,8 @@ static void launch_probe_bits_shape(Ctx& c, const fdb_dev_column* cols, uint64_t
   static PerDeviceOnce attr;  // per instantiation and device
   attr(c.device, [&] { FDB_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024)); });
   const uint64_t ntiles = (src.m_end + TR - 1) / TR;
-  const int grid = (int)std::max<uint64_t>(1, umin64(ntiles ? ntiles : 1, (uint64_t)c.sm_count));
+  // One CTA per SM: the bits take most of its shared memory.
+  const int grid = tuned_grid(c.tune.op[FDB_TUNE_PROBE], c.sm_count, 1, 1, ntiles, n);
   kern<<<grid, (NCW + 1) * 32, smem, c.stream>>>(src, p, c.d_err, op_off);
   FDB_CUDA(cudaGetLastError());
 }

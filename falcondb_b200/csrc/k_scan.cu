@@ -498,12 +498,10 @@ static void launch_stream(Ctx& c, const fdb_dev_column* cols, uint64_t n, const 
   attr_done(c.device, [&] { FDB_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024)); });
   int per_sm = 0;
   FDB_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, (S::NCW + 1) * 32, smem));
-  if (per_sm < 1) per_sm = 1;
-  if (per_sm > 4) per_sm = 4;  // per-CTA partials are sized for 4 CTAs per SM
   const uint64_t ntiles = (src.m_end + S::TR - 1) / S::TR;
-  uint64_t want = ntiles ? ntiles : (n + S::NCW * 32 * 8 - 1) / (S::NCW * 32 * 8);
-  if (want < 1) want = 1;
-  const int grid = (int)umin64(want, (uint64_t)c.sm_count * per_sm);
+  const uint64_t want = ntiles ? ntiles : (n + S::NCW * 32 * 8 - 1) / (S::NCW * 32 * 8);
+  // At most 4 CTAs per SM: the per-CTA partials are sized for that.
+  const int grid = tuned_grid(c.tune.op[FDB_TUNE_SCAN], c.sm_count, per_sm, 4, want, n);
   kern<<<grid, (S::NCW + 1) * 32, smem, c.stream>>>(src, p, c.d_err, op_off);
   FDB_CUDA(cudaGetLastError());
 }

@@ -989,11 +989,8 @@ static void launch_reg_topk(Ctx& c, const fdb_dev_column& col, uint64_t n, uint3
   attr(c.device, [&] { FDB_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem)); });
   int per_sm = 0;
   FDB_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, (NCW + 1) * 32, smem));
-  if (per_sm < 1) per_sm = 1;
-  if (per_sm > 4) per_sm = 4;
   const uint64_t ntiles = (src.m_end + TR - 1) / TR;
-  const uint64_t want = ntiles ? ntiles : 1;
-  const int grid = (int)umin64(want, (uint64_t)c.sm_count * per_sm);
+  const int grid = tuned_grid(c.tune.op[FDB_TUNE_TOPK], c.sm_count, per_sm, 4, ntiles, n);
   // Programmatic dependent launch: the grid may start (its producer warps
   // streaming tiles) while the sample pass finishes; consumers wait for it.
   cudaLaunchConfig_t cfg = {};
@@ -1058,11 +1055,9 @@ static void launch_topk_main(Ctx& c, const fdb_dev_column& col, uint64_t n, cons
   attr(c.device, [&] { FDB_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, 220 * 1024)); });
   int per_sm = 0;
   FDB_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, (NCW + 1) * 32, smem));
-  if (per_sm < 1) per_sm = 1;
-  if (per_sm > 4) per_sm = 4;  // partials are sized for 4 CTAs per SM
   const uint64_t ntiles = (src.m_end + TR - 1) / TR;
-  uint64_t want = ntiles ? ntiles : 1;
-  const int grid = (int)umin64(want, (uint64_t)c.sm_count * per_sm);
+  // At most 4 CTAs per SM: the partials are sized for that.
+  const int grid = tuned_grid(c.tune.op[FDB_TUNE_TOPK], c.sm_count, per_sm, 4, ntiles, n);
   kern<<<grid, (NCW + 1) * 32, smem, c.stream>>>(src, p, c.d_err, op_off);
   FDB_CUDA(cudaGetLastError());
 }
@@ -1103,11 +1098,8 @@ static void launch_warp_topk(Ctx& c, const fdb_dev_column& col, uint64_t n, Topk
   attr(c.device, [&] { FDB_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem)); });
   int per_sm = 0;
   FDB_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, (NCW + 1) * 32, smem));
-  if (per_sm < 1) per_sm = 1;
-  if (per_sm > 4) per_sm = 4;
   const uint64_t ntiles = (src.m_end + TR - 1) / TR;
-  const uint64_t want = ntiles ? ntiles : 1;
-  const int grid = (int)umin64(want, (uint64_t)c.sm_count * per_sm);
+  const int grid = tuned_grid(c.tune.op[FDB_TUNE_TOPK], c.sm_count, per_sm, 4, ntiles, n);
   kern<<<grid, (NCW + 1) * 32, smem, c.stream>>>(src, p, c.d_err, op_off);
   FDB_CUDA(cudaGetLastError());
 }

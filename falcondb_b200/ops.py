@@ -406,10 +406,11 @@ class GroupByBatch:
             arr[i].capacity = cap
             arr[i].d_ngroups = count.data_ptr()
         self._arr, self._nq = arr, nq
-        t = fdb_batch_tuning(*(tuning or (0.0, 0, 0)))
+        # No tuning: the context's (the last autotune's, or a loaded cache's).
+        t = fdb_batch_tuning(*tuning) if tuning else None
         h = C.c_void_p()
         with _Fenced(db):
-            check(lib().fdb_gb_batch_prepare(db.handle, arr, nq, C.byref(t), C.byref(h)))
+            check(lib().fdb_gb_batch_prepare(db.handle, arr, nq, C.byref(t) if t is not None else None, C.byref(h)))
         self._h = h
 
     def run(self) -> None:

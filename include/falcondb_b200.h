@@ -518,7 +518,8 @@ typedef struct fdb_batch fdb_batch;
 
 /* Size the queries' tables (one device arena), upload their descriptors and
  * capture the batch into a CUDA graph.  Inputs and outputs must stay valid
- * while the batch exists. */
+ * while the batch exists.  tuning NULL: the context's (the last autotune's or
+ * a loaded cache's; the defaults otherwise). */
 int fdb_gb_batch_prepare(fdb_db* db, const fdb_gb_query* queries, int32_t nqueries,
                          const fdb_batch_tuning* tuning, fdb_batch** out);
 /* Replay the batch on the context stream (asynchronous). */
@@ -526,9 +527,48 @@ int fdb_gb_batch_run(fdb_batch* b);
 void fdb_gb_batch_free(fdb_batch* b);
 /* Autotuner (replaces the reference's fixed parallel cut-offs, tuning.rs:39-53):
  * times every (load factor, CTAs per SM, tile rows) candidate on these queries
- * and returns the fastest in *best and its time per run in *best_ms. */
+ * and returns the fastest in *best and its time per run in *best_ms.  The
+ * context keeps it: fdb_gb_batch_prepare with tuning NULL uses it, and
+ * fdb_tuning_save stores it. */
 int fdb_gb_batch_autotune(fdb_db* db, const fdb_gb_query* queries, int32_t nqueries, int32_t reps,
                           fdb_batch_tuning* best, double* best_ms);
+
+/* ---- Launch tuning of the streamed operators ----------------------------------
+ * The reference sizes its parallel regions with fixed cut-offs, "rows per
+ * thread x threads" (par_min_rows / par_min_rows_per_batch_fanout,
+ * tuning.rs:39-53).  Here each kind of streamed operator has two knobs: the
+ * resident CTAs per SM of its persistent grid (0 = as many as fit, up to the
+ * kernel's own cap) and the rows each CTA must have before another CTA is
+ * launched (0 = one CTA per tile, up to the grid).  The autotuner times
+ * candidates on synthetic columns in device memory; the choices (and the
+ * batched GROUP BY's) persist in a JSON cache file. */
+#define FDB_TUNE_SCAN       0   /* filter mask / count, aggregates, COUNT(DISTINCT) */
+#define FDB_TUNE_GROUP      1   /* dictionary GROUP BY                              */
+#define FDB_TUNE_GROUP_I64  2   /* int64-key GROUP BY                               */
+#define FDB_TUNE_PROBE      3   /* join probes                                      */
+#define FDB_TUNE_TOPK       4   /* top-k                                            */
+#define FDB_TUNE_KINDS      5
+
+typedef struct fdb_op_tuning {
+    int32_t  ctas_per_sm;       /* 0 = occupancy limit                          */
+    int32_t  _pad;
+    uint64_t min_rows_per_cta;  /* 0 = no row minimum                           */
+} fdb_op_tuning;
+
+int fdb_get_tuning(fdb_db* db, int32_t kind, fdb_op_tuning* out);
+int fdb_set_tuning(fdb_db* db, int32_t kind, const fdb_op_tuning* in);
+/* Times, for each kind, CTAs per SM in {1, 2, 3, 4, occupancy} on `rows`
+ * synthetic rows and rows per CTA in {0, 2^15, 2^17, 2^19} on rows / 64, each
+ * candidate `reps` times (median), keeps the fastest in the context and
+ * returns them in best[FDB_TUNE_KINDS] (ms_per_call[FDB_TUNE_KINDS] at `rows`
+ * may be NULL).  The synthetic columns (about 40 B per row) are freed before
+ * it returns. */
+int fdb_autotune_ops(fdb_db* db, uint64_t rows, int32_t reps, fdb_op_tuning* best, double* ms_per_call);
+/* The context's tuning (every kind, and the batched GROUP BY's defaults) as a
+ * JSON file keyed by the device's name and SM count; loading a file written
+ * for another device fails with FDB_E_ARG and changes nothing. */
+int fdb_tuning_save(fdb_db* db, const char* path);
+int fdb_tuning_load(fdb_db* db, const char* path);
 
 /* ---- Serving loop ------------------------------------------------------------
  * A request loop over device-resident tables with continuous batching: queries
