@@ -413,6 +413,8 @@ def run_configs(args, db, t, n, peak):
       0..1M-1, payload uniform [0, 1e6)), 100M-row probe (key uniform
       [0, 2M), value uniform [0, 1)); COUNT(*) with SUM(payload), or with
       SUM(value) for SEMI / ANTI (8 B/probe row of key, +8 B of value).
+    * aggregate_where_100M: SELECT COUNT(*), SUM(score), AVG(salary),
+      MAX(score) WHERE score > 50 over the headline table (16 B/row).
     * zone_prune: SELECT COUNT(*), SUM(score) WHERE id >= 99M through
       fdb_sql over the headline table (id ascending), zone maps on and off:
       host wall time per query.
@@ -463,6 +465,24 @@ def run_configs(args, db, t, n, peak):
         assert rec[d, 2]["f"] == g0["isum"][d] / g0["icnt"][d]
     rate("filter_groupby_100M", ms, 20 * n, rows=n,
          query="SELECT dept, COUNT(*), SUM(score), AVG(salary) FROM t WHERE score > 50 GROUP BY dept")
+
+    # --- aggregates under one WHERE compare (execute_agg_only) ----------------
+    cols2 = [db.column("t", c) for c in ("score", "salary")]
+    aggs2 = [(F.AGG_COUNT_STAR, 0), (F.AGG_SUM, 0), (F.AGG_AVG, 1), (F.AGG_MAX, 0)]
+    res2 = ops._bytes(F.AGG_VALUE_DTYPE.itemsize * 4, db)
+    ca2, nc2 = ops._cols(cols2)
+    pa2, npr2 = ops._prog([ops.cmp(0, F.GT, 50)])
+    aa2, na2 = ops._aggs(aggs2)
+    ms = _time_steps(lambda: F.check(L.fdb_aggregate(db.handle, ca2, nc2, n, pa2, npr2, aa2, na2, res2.data_ptr())),
+                     K, Wm, stream, torch)
+    rec = ops.to_records(res2, F.AGG_VALUE_DTYPE, 4)
+    sel = t["score"] > 50
+    assert rec[0]["i"] == int(sel.sum())
+    assert abs(rec[1]["f"] - O.sum_serial(t["score"][sel])) <= 1e-12 * rec[1]["f"]
+    assert rec[2]["f"] == float(O.sum_i64_exact(t["salary"][sel])) / int(sel.sum())
+    assert rec[3]["f"] == float(t["score"][sel].max())
+    rate("aggregate_where_100M", ms, 16 * n, rows=n,
+         query="SELECT COUNT(*), SUM(score), AVG(salary), MAX(score) FROM t WHERE score > 50")
 
     # --- zone-map pruning (execute_select's batch skip, select.rs:115-137) ---
     lo = n - n // 100

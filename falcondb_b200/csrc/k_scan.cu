@@ -107,6 +107,15 @@ struct ScanAggParams {
   int32_t naggs;
   int32_t func[4];
   int32_t acol[4];
+  // FilterAggOp's decoded WHERE: one compare of column f_cmp_col (-1: none)
+  // against a literal, as double (f_cmp_f64) or as int64; f_cmp_mask holds
+  // the accepted outcomes (bit 0 unordered, 1 less, 2 equal, 3 greater).
+  int32_t f_cmp_col;
+  uint32_t f_cmp_mask;
+  int32_t f_cmp_f64;
+  uint32_t f_agg_f64;     // bit a: aggregate a's column is FLOAT64
+  double f_lit_f;
+  int64_t f_lit_i;
   AggAcc* partials;       // [gridDim.x * 4]
   unsigned int* ticket;   // zero on entry; reset by the last CTA
   fdb_agg_value* out;     // [naggs] or nullptr
@@ -293,6 +302,127 @@ __device__ __forceinline__ void fold_value(AggAcc& a, int f, T v) {
   }
   a.n++;
 }
+
+// Aggregates with at most one `col op literal` WHERE, every column NULL-free
+// and numeric (SELECT SUM(score), AVG(salary) ... WHERE score > 50).  A thread
+// takes its rows of the tile four at a time (ctid, ctid + nct, ...): it
+// compares them into a 4-bit mask, branch-free, and then each aggregate folds
+// the four rows under the mask with selects, not branches, so the aggregate
+// function and the column type are decided once per four rows (a uniform
+// branch), not per row as ScanAggOp's interpreter does.  Same accumulators,
+// partials and final pass as ScanAggOp.
+struct FilterAggOp : ScanAggOp {
+  static constexpr int R = 4;
+
+  template <typename T, class Acc>
+  static __device__ __forceinline__ void load_r(T (&x)[R], const Acc& acc, int col, const uint32_t (&i)[R],
+                                                uint32_t ok) {
+#pragma unroll
+    for (int j = 0; j < R; ++j) x[j] = ((ok >> j) & 1u) ? acc.template get<T>(col, i[j]) : T(0);
+  }
+
+  template <class Acc>
+  static __device__ __forceinline__ uint32_t pass_mask(const Params& p, const Acc& acc, const uint32_t (&i)[R],
+                                                       uint32_t ok) {
+    const int pc = p.f_cmp_col;
+    if (pc < 0) return ok;
+    const uint32_t amask = p.f_cmp_mask;
+    uint32_t m = 0;
+    if (p.f_cmp_f64) {
+      const double lit = p.f_lit_f;
+      double x[R];
+      if (p.sc.cols[pc].dtype == FDB_FLOAT64) {
+        load_r<double>(x, acc, pc, i, ok);
+      } else {
+        int64_t y[R];
+        load_r<int64_t>(y, acc, pc, i, ok);
+#pragma unroll
+        for (int j = 0; j < R; ++j) x[j] = (double)y[j];
+      }
+#pragma unroll
+      for (int j = 0; j < R; ++j) {
+        const uint32_t o = (x[j] < lit ? 1u : 0u) + (x[j] == lit ? 2u : 0u) + (x[j] > lit ? 3u : 0u);
+        m |= ((amask >> o) & 1u) << j;
+      }
+    } else {
+      const int64_t lit = p.f_lit_i;
+      int64_t x[R];
+      load_r<int64_t>(x, acc, pc, i, ok);
+#pragma unroll
+      for (int j = 0; j < R; ++j) {
+        const uint32_t o = (x[j] < lit ? 1u : 0u) + (x[j] == lit ? 2u : 0u) + (x[j] > lit ? 3u : 0u);
+        m |= ((amask >> o) & 1u) << j;
+      }
+    }
+    return m & ok;
+  }
+
+  template <typename T, class Acc>
+  static __device__ __forceinline__ void fold_r(AggAcc& a, int f, const Acc& acc, int col, const uint32_t (&i)[R],
+                                                uint32_t ok, uint32_t m) {
+    T x[R];
+    load_r<T>(x, acc, col, i, ok);
+    if (f == FDB_AGG_SUM || f == FDB_AGG_AVG) {
+      if constexpr (T(0.5) != T(0)) {
+        double s = 0.0;
+#pragma unroll
+        for (int j = 0; j < R; ++j) s += ((m >> j) & 1u) ? x[j] : 0.0;
+        a.f += s;
+      } else {
+#pragma unroll
+        for (int j = 0; j < R; ++j) {
+          const int64_t v = ((m >> j) & 1u) ? x[j] : 0;
+          i128_add(a.slo, a.shi, (uint64_t)v, v < 0 ? -1 : 0);
+        }
+      }
+      a.n += (uint64_t)__popc(m);
+      return;
+    }
+    // MIN / MAX over order keys; NaN never takes part (f64::min / max).
+#pragma unroll
+    for (int j = 0; j < R; ++j) {
+      uint64_t k;
+      bool use = (m >> j) & 1u;
+      if constexpr (T(0.5) != T(0)) {
+        use = use && !isnan(x[j]);
+        k = f64_ord_key(x[j]);
+      } else {
+        k = i64_ord_key(x[j]);
+      }
+      if (f == FDB_AGG_MIN)
+        a.m = (use && k < a.m) ? k : a.m;
+      else
+        a.m = (use && k > a.m) ? k : a.m;
+      a.n += use ? 1u : 0u;
+    }
+  }
+
+  template <class Acc>
+  static __device__ void step(Local& st, const Params& p, unsigned char*, const Acc& acc, uint32_t rows, int ctid,
+                              int nct) {
+    for (uint32_t b = 0; b < rows; b += R * (uint32_t)nct) {
+      uint32_t i[R];
+      uint32_t ok = 0;
+#pragma unroll
+      for (int j = 0; j < R; ++j) {
+        i[j] = b + (uint32_t)j * (uint32_t)nct + (uint32_t)ctid;
+        ok |= (i[j] < rows ? 1u : 0u) << j;
+      }
+      const uint32_t m = pass_mask(p, acc, i, ok);
+#pragma unroll
+      for (int a = 0; a < 4; ++a) {
+        if (a >= p.naggs) break;
+        const int f = p.func[a];
+        if (f == FDB_AGG_COUNT_STAR || f == FDB_AGG_COUNT)
+          st.a[a].n += (uint64_t)__popc(m);
+        else if ((p.f_agg_f64 >> a) & 1u)
+          fold_r<double>(st.a[a], f, acc, p.acol[a], i, ok, m);
+        else
+          fold_r<int64_t>(st.a[a], f, acc, p.acol[a], i, ok, m);
+      }
+    }
+  }
+};
 
 // Aggregates over column 0 only, no predicate, no NULLs.
 template <typename T>
@@ -592,6 +722,27 @@ void op_aggregate(Ctx& c, const fdb_dev_column* cols, int ncols, uint64_t n,
       launch_stream<ColAggOp<double>, 1>(c, cols, n, p, ScanAggOp::kSmem);
     else
       launch_stream<ColAggOp<int64_t>, 1>(c, cols, n, p, ScanAggOp::kSmem);
+    return;
+  }
+  // At most one `col op literal` and NULL-free numeric columns: FilterAggOp.
+  bool fast = nterms == 0 || (nterms == 1 && prog[0].kind == FDB_TERM_CMP);
+  for (int i = 0; i < ncols && fast; ++i) fast = cols[i].validity == nullptr && cols[i].dtype != FDB_UTF8;
+  if (fast) {
+    p.f_cmp_col = -1;
+    if (nterms == 1) {
+      const fdb_pred_term& t = prog[0];
+      p.f_cmp_col = t.col;
+      // Accepted outcomes of x op lit (bit 0 unordered, 1 less, 2 equal, 3
+      // greater): NaN passes != only, as cmp_op does.
+      static const uint32_t kAccept[6] = {0x4u, 0xBu, 0x2u, 0x6u, 0x8u, 0xCu};
+      p.f_cmp_mask = kAccept[t.op];
+      p.f_cmp_f64 = cols[t.col].dtype == FDB_FLOAT64 || t.lit_type == FDB_FLOAT64;
+      p.f_lit_f = t.lit_type == FDB_FLOAT64 ? t.lit_f : (double)t.lit_i;
+      p.f_lit_i = t.lit_i;
+    }
+    for (int a = 0; a < naggs; ++a)
+      if (aggs[a].func != FDB_AGG_COUNT_STAR && cols[aggs[a].col].dtype == FDB_FLOAT64) p.f_agg_f64 |= 1u << a;
+    launch_stream_nc<FilterAggOp>(c, cols, ncols, n, p, ScanAggOp::kSmem);
     return;
   }
   launch_stream_nc<ScanAggOp>(c, cols, ncols, n, p, ScanAggOp::kSmem);
