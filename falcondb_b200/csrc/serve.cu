@@ -55,6 +55,15 @@ constexpr int kServeMaxBatch = 256;
 #ifndef FDB_SERVE_CTAS
 #define FDB_SERVE_CTAS 3
 #endif
+// A batch's join, scan and top-k kernels run side by side (1) or one after
+// another (0).
+#ifndef FDB_SERVE_FORK
+#define FDB_SERVE_FORK 1
+#endif
+// Long-scan batches leave SM slots to the other launch slots under load (1).
+#ifndef FDB_SERVE_YIELD
+#define FDB_SERVE_YIELD 0
+#endif
 constexpr int kServeCtasPerSm = FDB_SERVE_CTAS;
 #ifndef FDB_SERVE_JOIN_CTAS
 #define FDB_SERVE_JOIN_CTAS 2
@@ -132,6 +141,9 @@ struct ServeHeader {
   uint64_t shared_units, total_units;
   uint64_t join_units;      // join groups come first: units [0, join_units) are theirs
   int32_t join_groups, _pad2;
+  // CTAs of the join, scan and top-k instances that take part (0: all).  The
+  // others end at once, leaving their SM slots to another slot's batch.
+  int32_t cta_limit[3], _pad3;
 };
 
 struct ServeArgs {
@@ -899,6 +911,8 @@ __global__ void __launch_bounds__(kServeBlock, JOIN ? kServeJoinCtasPerSm : kSer
   const uint64_t lo = JOIN ? 0 : a.hdr->join_units;
   const uint64_t shared = JOIN ? a.hdr->join_units : a.hdr->shared_units;  // end of this instance's units
   if (lo == shared) return;  // no group of this kind in the batch
+  const int32_t limit = a.hdr->cta_limit[JOIN ? 0 : 1];
+  if (limit > 0 && (int32_t)blockIdx.x >= limit) return;  // units are claimed, so fewer CTAs cover them all
   unsigned int* claim = a.claim + (JOIN ? 0 : 2);
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   for (int i = threadIdx.x; i < ng; i += kServeBlock) sm.gstart[i] = a.g[g0 + i].unit0;
@@ -1016,6 +1030,8 @@ __global__ void __launch_bounds__(kServeThreads, kServeTopkCtasPerSm) serve_topk
   const int nq = a.hdr->nq, topk0 = a.hdr->topk0;
   const int ntopk = nq - topk0;
   if (ntopk == 0) return;
+  const int32_t limit = a.hdr->cta_limit[2];
+  if (limit > 0 && (int32_t)blockIdx.x >= limit) return;
   const uint64_t shared = a.hdr->shared_units, total = a.hdr->total_units;
   for (int i = threadIdx.x; i < ntopk; i += kServeThreads) sm.start[i] = a.q[topk0 + i].tile0;
   if (threadIdx.x == 0) sm.start[ntopk] = total;
@@ -1166,17 +1182,46 @@ static void slot_capture(Server& s, ServeSlot& sl) {
   a.cand_r = static_cast<uint32_t*>(sl.d_cand_r.ptr);
   a.cand_cap = s.cand_cap;
   a.err = static_cast<int*>(sl.d_err.ptr);
+#if FDB_SERVE_FORK
+  // The join, scan and top-k instances read their own units and write their
+  // own queries' results, so the graph runs them side by side: when one runs
+  // out of units, its SMs go to the others instead of idling until it ends.
+  cudaStream_t side[2];
+  cudaEvent_t fork, joined[2];
+  for (int i = 0; i < 2; ++i) FDB_CUDA(cudaStreamCreateWithFlags(&side[i], cudaStreamNonBlocking));
+  FDB_CUDA(cudaEventCreateWithFlags(&fork, cudaEventDisableTiming));
+  for (int i = 0; i < 2; ++i) FDB_CUDA(cudaEventCreateWithFlags(&joined[i], cudaEventDisableTiming));
+#endif
   FDB_CUDA(cudaStreamBeginCapture(sl.stream, cudaStreamCaptureModeThreadLocal));
   cudaMemcpyAsync(sl.d_in.ptr, sl.h_in, kServeInBytes, cudaMemcpyHostToDevice, sl.stream);
   cudaMemsetAsync(sl.d_res.ptr, 0, kServeResBytes + 256, sl.stream);
+#if FDB_SERVE_FORK
+  cudaEventRecord(fork, sl.stream);
+  for (int i = 0; i < 2; ++i) cudaStreamWaitEvent(side[i], fork, 0);
+  serve_kernel<true><<<s.grid_join, kServeBlock, kShareSmem, side[0]>>>(a);
+  serve_topk_kernel<<<s.grid_topk, kServeThreads, 0, side[1]>>>(a);
+  serve_kernel<false><<<s.grid, kServeBlock, kShareSmem, sl.stream>>>(a);
+  for (int i = 0; i < 2; ++i) {
+    cudaEventRecord(joined[i], side[i]);
+    cudaStreamWaitEvent(sl.stream, joined[i], 0);
+  }
+#else
   serve_kernel<true><<<s.grid_join, kServeBlock, kShareSmem, sl.stream>>>(a);
   serve_kernel<false><<<s.grid, kServeBlock, kShareSmem, sl.stream>>>(a);
   serve_topk_kernel<<<s.grid_topk, kServeThreads, 0, sl.stream>>>(a);
+#endif
   serve_finish_kernel<<<kServeMaxBatch, kServeThreads, 0, sl.stream>>>(a);
   cudaMemcpyAsync(sl.h_out, sl.d_res.ptr, kServeResBytes, cudaMemcpyDeviceToHost, sl.stream);
   cudaMemcpyAsync(sl.h_err, sl.d_err.ptr, sizeof(int), cudaMemcpyDeviceToHost, sl.stream);
   cudaMemsetAsync(sl.d_err.ptr, 0, sizeof(int), sl.stream);
   FDB_CUDA(cudaStreamEndCapture(sl.stream, &sl.graph));
+#if FDB_SERVE_FORK
+  for (int i = 0; i < 2; ++i) {
+    cudaEventDestroy(joined[i]);
+    cudaStreamDestroy(side[i]);
+  }
+  cudaEventDestroy(fork);
+#endif
   FDB_CUDA(cudaGraphInstantiate(&sl.exec, sl.graph, 0));
 }
 
@@ -1402,6 +1447,22 @@ static bool slot_launch(Server& s, ServeSlot& sl, bool small_only) {
   }
   hdr->topk0 = (int32_t)sl.tickets.size();
   hdr->shared_units = units;
+  // A long-scan batch launched while short queries wait, or while another
+  // slot runs, leaves one CTA slot per SM to the other slots' batches: its
+  // persistent CTAs would otherwise hold every SM until its last unit.
+  hdr->cta_limit[0] = hdr->cta_limit[1] = hdr->cta_limit[2] = 0;
+#if FDB_SERVE_YIELD
+  if (big && s.slots.size() > 1) {
+    bool other_busy = false;
+    for (const ServeSlot& o : s.slots) other_busy |= (&o != &sl) && o.busy;
+    if (other_busy || !s.queue.empty()) {
+      const int sms = s.c->sm_count;
+      hdr->cta_limit[0] = std::max(sms, s.grid_join - sms);
+      hdr->cta_limit[1] = std::max(sms, s.grid - sms);
+      hdr->cta_limit[2] = std::max(sms, s.grid_topk - sms);
+    }
+  }
+#endif
   for (uint64_t tk : topk) {
     ServeQ& d = put(tk);
     d.tile0 = units;
