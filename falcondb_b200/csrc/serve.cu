@@ -64,6 +64,12 @@ constexpr int kServeMaxBatch = 256;
 #ifndef FDB_SERVE_YIELD
 #define FDB_SERVE_YIELD 0
 #endif
+// Queries waiting at which the short-scan slots hold off while a long-scan
+// batch runs (0: never).
+#ifndef FDB_SERVE_HOLD
+#define FDB_SERVE_HOLD 4
+#endif
+constexpr int kServeHoldBacklog = FDB_SERVE_HOLD;
 constexpr int kServeCtasPerSm = FDB_SERVE_CTAS;
 #ifndef FDB_SERVE_JOIN_CTAS
 #define FDB_SERVE_JOIN_CTAS 2
@@ -1116,6 +1122,7 @@ struct ServeSlot {
   cudaGraphExec_t exec = nullptr;
   std::vector<uint64_t> tickets;
   bool busy = false;
+  bool big = false;                // the batch in flight is of the long-scan class
 };
 
 struct ServeJob {
@@ -1472,6 +1479,7 @@ static bool slot_launch(Server& s, ServeSlot& sl, bool small_only) {
   FDB_CUDA(cudaGraphLaunch(sl.exec, sl.stream));
   FDB_CUDA(cudaEventRecord(sl.done, sl.stream));
   sl.busy = true;
+  sl.big = big;
   ++s.batches;
   s.batched_queries += (int64_t)admitted.size();
   return true;
@@ -1496,8 +1504,16 @@ static void server_loop(Server* s) {
         }
       }
       try {
-        for (size_t i = 0; i < s->slots.size(); ++i)
-          if (!s->slots[i].busy && !s->queue.empty()) progress |= slot_launch(*s, s->slots[i], i > 0);
+        for (size_t i = 0; i < s->slots.size(); ++i) {
+          if (s->slots[i].busy || s->queue.empty()) continue;
+          // Under a backlog, short-scan slots wait while a long scan runs: its
+          // persistent CTAs hold the SMs, so a batch launched beside it only
+          // queues behind it on the GPU, and the long scan itself slows down.
+          if (i > 0 && kServeHoldBacklog > 0 && s->slots[0].busy && s->slots[0].big &&
+              s->queue.size() >= (size_t)kServeHoldBacklog)
+            continue;
+          progress |= slot_launch(*s, s->slots[i], i > 0);
+        }
       } catch (const Error& e) {
         s->error = e.what();
       }
