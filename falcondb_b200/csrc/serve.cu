@@ -361,9 +361,11 @@ constexpr int kProbeIlp = 4;
 #define FDB_SERVE_PAIR_ILP 2
 #endif
 
-// fused (a join group with one query, whose value limit is `lim`): only rows
-// with v[i] < lim are probed, and their matches and payload sums are added to
-// *c / *psum instead of being written back for the queries to read.
+// Only rows with v[i] < lim are probed (lim: the largest value limit of the
+// queries that read the unit; a row at or above it counts for none of them,
+// so its match count and payload sum are left 0).  fused (a join group with
+// one query): the matches and payload sums are added to *c / *psum instead of
+// being written back for the queries to read.
 __device__ void serve_probe_rows(const ServeG g, uint64_t* s0, uint32_t* m, uint32_t rows, bool fused,
                                  const double* v, double lim, unsigned long long* c, unsigned long long* psum) {
   JoinMode mode;
@@ -385,7 +387,7 @@ __device__ void serve_probe_rows(const ServeG g, uint64_t* s0, uint32_t* m, uint
       sk[j] = 0;
       h[j] = 0;
       if (i >= rows) continue;
-      if (fused && !(v[i] < lim)) continue;
+      if (!(v[i] < lim)) continue;
       const int64_t key = (int64_t)s0[i];
       if (key == INT64_MIN) {
         if (g.cnt[g.cap] != 0u) {
@@ -765,6 +767,15 @@ __device__ void serve_shared_unit(const ServeArgs& a, const ServeG g, uint64_t t
       const ServeQ& q = a.q[g.q0];
       lim = q.thr / 100.0;
       prows = q.n > r0 ? (uint32_t)umin64(rows, q.n - r0) : 0u;
+    } else {
+      // The largest limit among the queries that read this unit, found by
+      // each warp with its lanes reading the group's descriptors in parallel.
+      for (uint32_t k = (uint32_t)lane; k < g.nq; k += 32) {
+        const ServeQ& q = a.q[g.q0 + k];
+        if (q.n > r0) lim = fmax(lim, q.thr / 100.0);
+      }
+#pragma unroll
+      for (int o = 16; o > 0; o >>= 1) lim = fmax(lim, __shfl_xor_sync(0xffffffffu, lim, o));
     }
     serve_probe_rows(g, s0, smm, prows, fused, reinterpret_cast<const double*>(s1), lim, &c, &ps);
     if (fused) {
