@@ -931,42 +931,6 @@ __device__ __forceinline__ int smem_dense_slot_from(const SDTab& t, uint32_t k, 
   return -1;
 }
 
-// Bucketed form (kDenseProbe = 4): the table is 4-slot buckets and a key
-// lives in its home bucket only; the bucket's four keys come with one 16-byte
-// read, so a key that is absent costs one shared-memory access, not four
-// dependent ones.  cur0 is that read, taken earlier (stale entries can only
-// read 0, which the compare-and-swap corrects).
-#ifndef FDB_GBD_BUCKET
-#define FDB_GBD_BUCKET 1
-#endif
-static_assert(!FDB_GBD_BUCKET || ((8 * kDenseSumCopies + 24) * (kDenseSmemSlots + 1)) % 16 == 0,
-              "the keys of a 4-slot bucket must be one aligned 16-byte word");
-static_assert(!FDB_GBD_BUCKET || kDenseProbe == 4, "a bucket is the 4 probes");
-
-__device__ __forceinline__ uint32_t smem_dense_bucket(uint32_t k) {
-  return ((k * 0x9E3779B1u) >> (32 - kDenseSmemLog)) & ~3u;
-}
-
-__device__ __forceinline__ int smem_dense_slot_bucket(const SDTab& t, uint32_t k, uint32_t b, uint4 cur) {
-  const unsigned int k1 = k + 1u;
-#pragma unroll
-  for (int attempt = 0; attempt < 4; ++attempt) {
-    const unsigned int c[4] = {cur.x, cur.y, cur.z, cur.w};
-    int empty = -1;
-#pragma unroll
-    for (int e = 3; e >= 0; --e) {
-      if (c[e] == k1) return (int)(b + e);
-      if (c[e] == 0) empty = e;
-    }
-    if (empty < 0) return -1;  // the bucket is full of other keys
-    const unsigned int prev = atomicCAS(&t.k1[b + empty], 0u, k1);
-    if (prev == 0 || prev == k1) return (int)(b + empty);
-    const volatile unsigned int* vb = &t.k1[b];  // another key took it: look again
-    cur = make_uint4(vb[0], vb[1], vb[2], vb[3]);
-  }
-  return -1;
-}
-
 struct GbDenseOp {
   using Params = GbDenseParams;
   struct Local {};
@@ -1022,31 +986,17 @@ struct GbDenseOp {
         kind[r] = kSlot;
       }
       // Every row's first probe in flight together.
-#if FDB_GBD_BUCKET
-      uint4 cb[R];
-#pragma unroll
-      for (uint32_t r = 0; r < R; ++r) {
-        h[r] = smem_dense_bucket(k[r]);
-        cb[r] = kind[r] == kSlot ? *reinterpret_cast<const uint4*>(&tab.k1[h[r]]) : make_uint4(0, 0, 0, 0);
-      }
-      (void)cur;
-#else
 #pragma unroll
       for (uint32_t r = 0; r < R; ++r) {
         h[r] = smem_dense_home(k[r]);
         cur[r] = kind[r] == kSlot ? tab.k1[h[r]] : 0u;
       }
-#endif
 #pragma unroll
       for (uint32_t r = 0; r < R; ++r) {
         if (kind[r] == kNull) {
           sdslot_accum(tab, kDenseSmemSlots, v[r], has_v[r]);
         } else if (kind[r] == kSlot) {
-#if FDB_GBD_BUCKET
-          const int j = smem_dense_slot_bucket(tab, k[r], h[r], cb[r]);
-#else
           const int j = smem_dense_slot_from(tab, k[r], h[r], cur[r]);
-#endif
           if (j >= 0)
             sdslot_accum(tab, (uint32_t)j, v[r], has_v[r]);
           else
