@@ -87,10 +87,21 @@ constexpr int kServeStages = FDB_SERVE_STAGES;
 #define FDB_SERVE_STAGE_KB 22
 #endif
 constexpr size_t kShareStage = FDB_SERVE_STAGE_KB * 1024;
+// The join instance's stages are larger: a join unit is one probe pass (each
+// thread kProbeIlp rows, all their L2 reads in flight together), and each
+// unit costs a CTA one L2 round trip, so more rows per unit means more rows
+// per round trip.
+#ifndef FDB_SERVE_JOIN_STAGE_KB
+#define FDB_SERVE_JOIN_STAGE_KB 40
+#endif
+constexpr size_t kShareStageJoin = FDB_SERVE_JOIN_STAGE_KB * 1024;
+template <bool JOIN>
+__host__ __device__ constexpr size_t share_stage() { return JOIN ? kShareStageJoin : kShareStage; }
 // Barrier block: full[stages], empty[stages], the unit of each stage, and the
 // columns each stage's consumers must load themselves (bit c: column c).
 constexpr size_t kServeBar = 128;
 constexpr size_t kShareSmem = kServeBar + kServeStages * kShareStage;
+constexpr size_t kShareSmemJoin = kServeBar + kServeStages * kShareStageJoin;
 static_assert(kServeStages * (8 + 8 + 8 + 4) <= kServeBar, "barrier block");
 
 struct ServeQ {            // device descriptor of one query
@@ -353,13 +364,80 @@ __device__ __forceinline__ void share_load(unsigned char* dst, const void* src, 
 }
 
 // Probe every staged row of a join group once: row i's build matches go to
-// m[i] and their payload sum replaces its key in s0[i].  Each thread walks
-// kProbeIlp rows together, one 32-byte slot pair (one L2 sector) per row per
-// round, so their L2 round trips overlap.
-constexpr int kProbeIlp = 4;
+// m[i] and their payload sum replaces its key in s0[i].  A direct-addressed
+// table is read with kProbeIlp rows per thread in flight together (a join
+// unit is one such pass); a hashed table with kHashIlp rows at a time, one
+// 32-byte slot pair (one L2 sector) per row per round, so their L2 round
+// trips overlap.
+#ifndef FDB_SERVE_PROBE_ILP
+#define FDB_SERVE_PROBE_ILP 8
+#endif
+constexpr int kProbeIlp = FDB_SERVE_PROBE_ILP;
+constexpr int kHashIlp = 4;
+static_assert(kProbeIlp % kHashIlp == 0, "a probe pass is whole hashed passes");
 #ifndef FDB_SERVE_PAIR_ILP
 #define FDB_SERVE_PAIR_ILP 2
 #endif
+
+// The direct-addressed probe of serve_probe_rows: per row only its slot index
+// and the slot read are kept across the loads (the key is read again from
+// shared memory to compare), so kProbeIlp reads fit in registers.
+__device__ __forceinline__ void serve_probe_dense(const ServeG& g, const JoinMode& mode, uint64_t* s0, uint32_t* m,
+                                                  uint32_t rows, bool fused, const double* v, double lim,
+                                                  unsigned long long* c, unsigned long long* psum) {
+  const uint64_t pol = l2_evict_last_policy();
+  for (uint32_t base = 0; base < rows; base += kProbeIlp * kServeThreads) {
+    uint32_t hs[kProbeIlp];
+    uint32_t todo = 0;
+#pragma unroll
+    for (int j = 0; j < kProbeIlp; ++j) {
+      const uint32_t i = base + j * kServeThreads + threadIdx.x;
+      hs[j] = 0;
+      if (i >= rows || !(v[i] < lim)) continue;
+      const int64_t key = (int64_t)s0[i];
+      if (key == INT64_MIN) continue;  // resolved below
+      const uint64_t h = join_home(mode, key, (uint64_t)key ^ (1ull << 63));
+      if (h < g.cap) {  // keys outside the build keys' span read nothing
+        hs[j] = (uint32_t)h;
+        todo |= 1u << j;
+      }
+    }
+    JSlot sl[kProbeIlp];
+#pragma unroll
+    for (int j = 0; j < kProbeIlp; ++j) {
+      sl[j].key = 0;
+      sl[j].psum = 0;
+      if ((todo >> j) & 1u)
+        asm volatile("ld.global.L2::cache_hint.v2.u64 {%0, %1}, [%2], %3;"
+                     : "=l"(sl[j].key), "=l"(sl[j].psum)
+                     : "l"(g.slots + hs[j]), "l"(pol));
+    }
+#pragma unroll
+    for (int j = 0; j < kProbeIlp; ++j) {
+      const uint32_t i = base + j * kServeThreads + threadIdx.x;
+      if (i >= rows) continue;
+      uint32_t mc = 0;
+      uint64_t ps = 0;
+      if ((todo >> j) & 1u) {
+        if (sl[j].key == (s0[i] ^ (1ull << 63))) {
+          mc = g.unique ? 1u : g.cnt[hs[j]];
+          ps = sl[j].psum;
+        }
+      } else if (v[i] < lim && (int64_t)s0[i] == INT64_MIN && g.cnt[g.cap] != 0u) {
+        mc = g.cnt[g.cap];  // the NULL-group slot after the table
+        ps = g.slots[g.cap].psum;
+      }
+      if (fused) {
+        *c += mc;
+        *psum += mc ? ps : 0ull;
+      } else {
+        m[i] = mc;
+        s0[i] = ps;
+      }
+    }
+  }
+  if (!fused) serve_bar();
+}
 
 // Only rows with v[i] < lim are probed (lim: the largest value limit of the
 // queries that read the unit; a row at or above it counts for none of them,
@@ -373,14 +451,18 @@ __device__ void serve_probe_rows(const ServeG g, uint64_t* s0, uint32_t* m, uint
   mode.dense = g.dense;
   mode.shift = join_shift(g.cap);
   mode.span = g.span;
+  if (mode.dense) {
+    serve_probe_dense(g, mode, s0, m, rows, fused, v, lim, c, psum);
+    return;
+  }
   const uint64_t mask = g.cap - 1;
   const uint64_t pol = l2_evict_last_policy();
-  for (uint32_t base = 0; base < rows; base += kProbeIlp * kServeThreads) {
-    uint64_t sk[kProbeIlp], h[kProbeIlp], ps[kProbeIlp];
-    uint32_t at[kProbeIlp];
+  for (uint32_t base = 0; base < rows; base += kHashIlp * kServeThreads) {
+    uint64_t sk[kHashIlp], h[kHashIlp], ps[kHashIlp];
+    uint32_t at[kHashIlp];
     uint32_t todo = 0;
 #pragma unroll
-    for (int j = 0; j < kProbeIlp; ++j) {
+    for (int j = 0; j < kHashIlp; ++j) {
       const uint32_t i = base + j * kServeThreads + threadIdx.x;
       at[j] = kNoSlot;
       ps[j] = 0;
@@ -398,34 +480,13 @@ __device__ void serve_probe_rows(const ServeG g, uint64_t* s0, uint32_t* m, uint
       }
       sk[j] = (uint64_t)key ^ (1ull << 63);
       h[j] = join_home(mode, key, sk[j]);
-      if (h[j] <= mask) todo |= 1u << j;  // a dense table cannot hold a key outside its range
-    }
-    if (mode.dense && todo) {
-      // Direct-addressed: key k can only be in slot k - dmin, so one 16-byte
-      // read per row resolves it.
-      JSlot sl[kProbeIlp];
-#pragma unroll
-      for (int j = 0; j < kProbeIlp; ++j) {
-        sl[j].key = 0;
-        sl[j].psum = 0;
-        if ((todo >> j) & 1u)
-          asm volatile("ld.global.L2::cache_hint.v2.u64 {%0, %1}, [%2], %3;"
-                       : "=l"(sl[j].key), "=l"(sl[j].psum)
-                       : "l"(g.slots + h[j]), "l"(pol));
-      }
-#pragma unroll
-      for (int j = 0; j < kProbeIlp; ++j)
-        if (((todo >> j) & 1u) && sl[j].key == sk[j]) {
-          at[j] = (uint32_t)h[j];
-          ps[j] = sl[j].psum;
-        }
-      todo = 0;
+      todo |= 1u << j;
     }
     // Hashed table: rounds over slot pairs, kPairIlp rows' pairs in flight at a
-    // time (fewer than kProbeIlp, to keep the registers of the pairs down).
+    // time (fewer than kHashIlp, to keep the registers of the pairs down).
     constexpr int kPairIlp = FDB_SERVE_PAIR_ILP;
 #pragma unroll
-    for (int j0 = 0; j0 < kProbeIlp; j0 += kPairIlp)
+    for (int j0 = 0; j0 < kHashIlp; j0 += kPairIlp)
     for (uint64_t round = 0; ((todo >> j0) & ((1u << kPairIlp) - 1u)) && round <= mask; ++round) {
       JSlot lo[kPairIlp], hi[kPairIlp];
 #pragma unroll
@@ -456,7 +517,7 @@ __device__ void serve_probe_rows(const ServeG g, uint64_t* s0, uint32_t* m, uint
       }
     }
 #pragma unroll
-    for (int j = 0; j < kProbeIlp; ++j) {
+    for (int j = 0; j < kHashIlp; ++j) {
       const uint32_t i = base + j * kServeThreads + threadIdx.x;
       if (i >= rows) continue;
       const uint32_t mc = at[j] == kNoSlot ? 0u : (g.unique ? 1u : g.cnt[at[j]]);
@@ -996,7 +1057,7 @@ __global__ void __launch_bounds__(kServeBlock, JOIN ? kServeJoinCtasPerSm : kSer
         for (int c = 0; c < 3; ++c) {
           if (!cols.esize[c] || ((pm >> c) & 1u)) continue;
           const unsigned char* src = static_cast<const unsigned char*>(cols.src[c]) + r0 * cols.esize[c];
-          bulk_g2s(stages + (size_t)s * kShareStage + cols.off[c], src, rows * (uint32_t)cols.esize[c], &full[s],
+          bulk_g2s(stages + (size_t)s * share_stage<JOIN>() + cols.off[c], src, rows * (uint32_t)cols.esize[c], &full[s],
                    policy);
         }
       }
@@ -1015,7 +1076,7 @@ __global__ void __launch_bounds__(kServeBlock, JOIN ? kServeJoinCtasPerSm : kSer
     const uint32_t pm = plain[s];
     if (t >= shared) break;
     const int gi = serve_find(sm.gstart, ng, t);
-    serve_shared_unit<JOIN>(a, a.g[g0 + gi], t - sm.gstart[gi], stages + (size_t)s * kShareStage, pm, sm);
+    serve_shared_unit<JOIN>(a, a.g[g0 + gi], t - sm.gstart[gi], stages + (size_t)s * share_stage<JOIN>(), pm, sm);
     // The consumers wrote the stage (probe results, plain loads): order those
     // writes before the producer's next bulk copy into it.
     fence_proxy_async_smem();
@@ -1216,7 +1277,7 @@ static void slot_capture(Server& s, ServeSlot& sl) {
 #if FDB_SERVE_FORK
   cudaEventRecord(fork, sl.stream);
   for (int i = 0; i < 2; ++i) cudaStreamWaitEvent(side[i], fork, 0);
-  serve_kernel<true><<<s.grid_join, kServeBlock, kShareSmem, side[0]>>>(a);
+  serve_kernel<true><<<s.grid_join, kServeBlock, kShareSmemJoin, side[0]>>>(a);
   serve_topk_kernel<<<s.grid_topk, kServeThreads, 0, side[1]>>>(a);
   serve_kernel<false><<<s.grid, kServeBlock, kShareSmem, sl.stream>>>(a);
   for (int i = 0; i < 2; ++i) {
@@ -1224,7 +1285,7 @@ static void slot_capture(Server& s, ServeSlot& sl) {
     cudaStreamWaitEvent(sl.stream, joined[i], 0);
   }
 #else
-  serve_kernel<true><<<s.grid_join, kServeBlock, kShareSmem, sl.stream>>>(a);
+  serve_kernel<true><<<s.grid_join, kServeBlock, kShareSmemJoin, sl.stream>>>(a);
   serve_kernel<false><<<s.grid, kServeBlock, kShareSmem, sl.stream>>>(a);
   serve_topk_kernel<<<s.grid_topk, kServeThreads, 0, sl.stream>>>(a);
 #endif
@@ -1428,7 +1489,7 @@ static bool slot_launch(Server& s, ServeSlot& sl, bool small_only) {
       const uint32_t row_bytes = 8u + (uint32_t)d.c1_bytes + (d.load_c2 ? 8u : 0u) + (g.join ? 4u : 0u);
       // A join unit is a whole number of probe passes (kProbeIlp rows per thread).
       const uint32_t quantum = g.join ? (uint32_t)(kProbeIlp * kServeThreads) : 256u;
-      d.unit_rows = (uint32_t)(kShareStage / row_bytes) / quantum * quantum;
+      d.unit_rows = (uint32_t)((g.join ? kShareStageJoin : kShareStage) / row_bytes) / quantum * quantum;
       d.off1 = 8u * d.unit_rows;
       d.off2 = d.off1 + (uint32_t)d.c1_bytes * d.unit_rows;
       d.offm = d.off2 + (d.load_c2 ? 8u : 0u) * d.unit_rows;
@@ -1545,12 +1606,12 @@ Server* server_start(fdb_db* db, Ctx& c, const fdb_serve_config* cfg) {
   s->budget = cfg && cfg->mem_budget ? cfg->mem_budget : c.budget;
   s->cfg.mem_budget = s->budget;
   s->resident = c.in_use.load();
-  FDB_CUDA(cudaFuncSetAttribute(serve_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kShareSmem));
+  FDB_CUDA(cudaFuncSetAttribute(serve_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kShareSmemJoin));
   FDB_CUDA(cudaFuncSetAttribute(serve_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kShareSmem));
   int per_sm = 0;
   FDB_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, serve_kernel<false>, kServeBlock, kShareSmem));
   s->grid = c.sm_count * std::max(1, std::min(per_sm, kServeCtasPerSm));
-  FDB_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, serve_kernel<true>, kServeBlock, kShareSmem));
+  FDB_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, serve_kernel<true>, kServeBlock, kShareSmemJoin));
   s->grid_join = c.sm_count * std::max(1, std::min(per_sm, kServeJoinCtasPerSm));
   FDB_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, serve_topk_kernel, kServeThreads, 0));
   s->grid_topk = c.sm_count * std::max(1, std::min(per_sm, kServeTopkCtasPerSm));
