@@ -394,13 +394,16 @@ struct ProbeParams {
 // JT: the join type (FDB_JOIN_*), fixed per instantiation.
 // DENSE: the table is direct-addressed (JoinMode), so a row is one 16-byte
 // slot read; FDB_PROBE_DENSE_ROWS rows per thread have their reads in flight
-// together (measured at 100M rows: 2 rows at 4 CTAs per SM 0.394 ms, 4 rows at
-// 3 CTAs 0.397 ms, 1 row through the hashed probe's loop 0.46 ms).
+// together.  The probe is bound by resident warps more than by reads per
+// thread: measured INNER / LEFT at 100M rows, 1 row per thread with no
+// minimum CTAs per SM (ptxas keeps it at 40 registers: 5 CTAs per SM) 0.305 /
+// 0.320 ms; 2 rows at 4 CTAs per SM 0.359 / 0.377 ms; 1 row at 5 or 6 CTAs
+// per SM 0.338 / 0.378 ms; 4 rows at 3 CTAs 0.341 / 0.355 ms.
 #ifndef FDB_PROBE_DENSE_ROWS
-#define FDB_PROBE_DENSE_ROWS 2
+#define FDB_PROBE_DENSE_ROWS 1
 #endif
 #ifndef FDB_PROBE_DENSE_MINB
-#define FDB_PROBE_DENSE_MINB 4
+#define FDB_PROBE_DENSE_MINB 0
 #endif
 template <int JT, bool DENSE = false>
 struct ProbeOp {

@@ -108,7 +108,7 @@ inline uint64_t stream_m_end(const void* const* bases, int nc, uint64_t n) {
 //   static __device__ void finish(Local&, const Params&, unsigned char* op_smem, int ctid, int nct);
 // step() and finish() are executed by all consumer threads; block-wide syncs
 // inside them must use consumer_bar(nct).
-// MINB: resident CTAs per SM the register allocation must allow.
+// MINB: resident CTAs per SM the register allocation must allow (0: none).
 // DYN: tiles are handed out by an atomic counter (src.tile_ctr) instead of
 // round-robin, so CTAs that run faster take more tiles and all finish
 // together.  The tile order then varies run to run, so DYN is only for ops
