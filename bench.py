@@ -730,6 +730,19 @@ def cpu_baseline(t, n, threads):
 
 
 # ----------------------------------------------------------------------------- secondary workloads
+def radix_bytes_per_row(passes: int, keys_last: bool) -> int:
+    """Algorithmic bytes per row of the radix sort: the key build (read 8,
+    write 12); per digit pass the digit count (the 8-byte keys in the first
+    pass, then the 1-byte digits that the previous scatter wrote), the scatter
+    (read 12; write 12, or only the 4-byte row in a last pass that stores no
+    keys) and, before every pass but the last, the next pass's digit (1)."""
+    b = 20
+    for p in range(passes):
+        last = p == passes - 1
+        b += (8 if p == 0 else 1) + 12 + (12 if keys_last or not last else 4) + (0 if last else 1)
+    return b
+
+
 def _time_steps(fn, K, W, stream, torch):
     """CUDA-event time of K calls of fn() on `stream` after W warm-ups."""
     for _ in range(W):
@@ -903,10 +916,7 @@ def run_secondary(args):
         db.drop_table("g")
     if args.workload in ("sort", "all"):
         # ORDER BY score DESC over 100M FLOAT64 rows, no LIMIT: an LSD radix
-        # sort of (order key, row) pairs.  Algorithmic bytes per row: the key
-        # build (read 8, write 12), per digit pass the histogram read (8) and
-        # the scatter (read 12, write 12), except that the last pass writes
-        # only the row (4) straight into the output.
+        # sort of (order key, row) pairs (bytes per row: radix_bytes_per_row).
         host_sc = W.table_t(n, seed=1)["score"]
         sc = torch.from_numpy(host_sc).to(dev)
         rows_out = torch.empty(n, dtype=torch.int32, device=dev)
@@ -923,7 +933,7 @@ def run_secondary(args):
         seen[r] = True
         assert bool(seen.all())
         del r, s_sorted, seen
-        nbytes = n * (20 + 32 * passes - 8)
+        nbytes = n * radix_bytes_per_row(passes, keys_last=False)
         sample = 10_000_000 if n >= 10_000_000 else n
         hs = sc[:sample].cpu().numpy()
         threads = args.cpu_threads or O.hardware_threads()
@@ -948,7 +958,7 @@ def run_secondary(args):
         t0 = time.perf_counter()
         O.distinct(hs_d)
         cpu_d = time.perf_counter() - t0
-        line("distinct", ms_d, n * (20 + 32 * passes + 12) + n // 4 + kept * 4,
+        line("distinct", ms_d, n * (radix_bytes_per_row(passes, keys_last=True) + 12) + n // 4 + kept * 4,
              {"rows": n, "query": "SELECT DISTINCT score FROM t", "distinct_values": kept,
               "mrows_per_s": round(n / (ms_d / 1e3) / 1e6, 1),
               "cpu_sample": {"rows": len(hs_d), "mrows_per_s": round(len(hs_d) / cpu_d / 1e6, 2), "cores": 1,

@@ -13,7 +13,9 @@
 //     histogram gives every (digit, tile) its output offset;
 //     radix_scatter_kernel stages each tile in shared memory (TMA bulk
 //     copies, double-buffered), ranks its keys stably with warp votes, permutes
-//     the tile into digit order in place and writes it out in runs;
+//     the tile into digit order in place and writes it out in runs, with the
+//     next pass's digit of each key as a byte beside it, so every pass after
+//     the first counts 1 byte per key (radix_hist_digits_kernel), not 8;
 //   * the last pass writes the row numbers straight into the output.
 // Every scatter position is checked against the key count (an error, never an
 // out-of-bounds write).
@@ -139,6 +141,57 @@ __global__ void __launch_bounds__(kSortThreads) radix_hist_kernel(const uint64_t
 #pragma unroll
   for (int w = 0; w < kSortWarps; ++w) t += cnt[w][tid];
   hist[(size_t)tid * ntiles + blockIdx.x] = t;
+}
+
+// The same counts from the digit bytes the previous pass's scatter wrote (one
+// byte per key at the key's new position): one warp per tile, eight tiles per
+// CTA, so each digit's counts of a CTA's tiles are one 32-byte store run.  A
+// lane reads eight 16-byte chunks (128 consecutive keys in 16-key runs).
+constexpr int kDigitHistWarps = 8;
+constexpr uint32_t kDigitChunks = kSortTile / 16 / 32;  // 16-byte chunks per lane
+static_assert(kSortTile % (16 * 32) == 0, "a tile is whole 16-byte chunks for every lane");
+
+__global__ void __launch_bounds__(kDigitHistWarps * 32)
+    radix_hist_digits_kernel(const uint8_t* __restrict__ dg, uint32_t m, uint32_t ntiles, uint32_t* hist) {
+  __shared__ uint32_t cnt[kDigitHistWarps][256];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const uint32_t tile = blockIdx.x * kDigitHistWarps + warp;
+#pragma unroll
+  for (int j = 0; j < 256; j += 32) cnt[warp][j + lane] = 0;
+  __syncwarp();
+  if (tile >= ntiles) return;
+  const uint64_t t0 = (uint64_t)tile * kSortTile;
+  const uint32_t n = (uint32_t)umin64(kSortTile, m - t0);
+  uint32_t run_d = 0, run_c = 0;
+  auto count = [&](uint32_t d) {
+    if (d != run_d && run_c) {
+      atomicAdd(&cnt[warp][run_d], run_c);
+      run_c = 0;
+    }
+    run_d = d;
+    ++run_c;
+  };
+  if (n == kSortTile) {
+    uint4 v[kDigitChunks];
+#pragma unroll
+    for (uint32_t r = 0; r < kDigitChunks; ++r)
+      v[r] = __ldcs(reinterpret_cast<const uint4*>(dg + t0) + r * 32 + lane);
+#pragma unroll
+    for (uint32_t r = 0; r < kDigitChunks; ++r) {
+      const uint32_t w[4] = {v[r].x, v[r].y, v[r].z, v[r].w};
+#pragma unroll
+      for (int q = 0; q < 16; ++q) count((w[q >> 2] >> ((q & 3) * 8)) & 255u);
+    }
+  } else {  // the ragged last tile: byte loads below n
+    for (uint32_t r = 0; r < kDigitChunks; ++r) {
+      const uint32_t b0 = (r * 32 + lane) * 16;
+      for (uint32_t q = 0; q < 16 && b0 + q < n; ++q) count(dg[t0 + b0 + q]);
+    }
+  }
+  if (run_c) atomicAdd(&cnt[warp][run_d], run_c);
+  __syncwarp();
+#pragma unroll
+  for (int j = 0; j < 256; j += 32) hist[(size_t)(j + lane) * ntiles + tile] = cnt[warp][j + lane];
 }
 
 // Exclusive scan of n uint32 in place: per-block sums, a scan of the sums,
@@ -270,7 +323,8 @@ __device__ __forceinline__ void sort_stage_tile(ScatterSmem& S, int s, uint64_t 
 __global__ void __launch_bounds__(kScatterThreads, kScatterCtasPerSm)
     radix_scatter_kernel(const uint64_t* __restrict__ kin, const uint32_t* __restrict__ vin, uint32_t m, int shift,
                          const uint32_t* __restrict__ off, uint32_t ntiles, uint64_t* __restrict__ kout,
-                         uint32_t* __restrict__ vout, bool write_keys, int* err) {
+                         uint32_t* __restrict__ vout, bool write_keys, uint8_t* __restrict__ dg_out, int next_shift,
+                         int* err) {
   extern __shared__ __align__(128) unsigned char smem_raw[];
   ScatterSmem& S = *reinterpret_cast<ScatterSmem*>(smem_raw);
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
@@ -404,6 +458,7 @@ __global__ void __launch_bounds__(kScatterThreads, kScatterCtasPerSm)
         const uint32_t pos = S.gbase[(uint32_t)(kk >> shift) & 255u] + i;
         if (pos < m) {
           if (write_keys) kout[pos] = kk;
+          if (dg_out) dg_out[pos] = (uint8_t)(kk >> next_shift);
           vout[pos] = S.vals[s][i];
         } else {
           atomicExch(err, kErrCapacity);
@@ -461,7 +516,7 @@ static size_t sort_scratch_bytes(uint64_t n, bool nullable) {
   const uint64_t ntiles = (n + kSortTile - 1) / kSortTile;
   const uint64_t hn = 256ull * ntiles;
   const uint64_t nb = (hn + kScanB - 1) / kScanB;
-  size_t need = 2 * n * 8 + 2 * n * 4 + hn * 4 + nb * 4 + 16;
+  size_t need = 2 * n * 8 + 2 * n * 4 + n + hn * 4 + nb * 4 + 16;
   if (nullable) need += words * 8 + 2 * n * 4 + 16;
   return need + (2u << 20);  // + 256-byte rounding and the compaction's chunk counts
 }
@@ -517,6 +572,7 @@ static void radix_sort_pairs(Ctx& c, uint32_t m, KeysFn keys_fn, uint32_t* rows_
   const uint64_t nb = (hn + kScanB - 1) / kScanB;
   uint32_t* hist = static_cast<uint32_t*>(c.scratch_take(hn * 4));
   uint32_t* bsum = static_cast<uint32_t*>(c.scratch_take(nb * 4));
+  uint8_t* dg = static_cast<uint8_t*>(c.scratch_take(m));  // the next pass's digit of each key
   unsigned long long* vary = static_cast<unsigned long long*>(c.scratch_take(16));
   FDB_CUDA(cudaMemsetAsync(vary, 0, 8, c.stream));
   FDB_CUDA(cudaMemsetAsync(vary + 1, 0xFF, 8, c.stream));
@@ -529,17 +585,25 @@ static void radix_sort_pairs(Ctx& c, uint32_t m, KeysFn keys_fn, uint32_t* rows_
   int last_byte = -1;
   for (int byte = 0; byte < 8; ++byte)
     if ((varying >> (8 * byte)) & 0xFFull) last_byte = byte;
+  int shifts[8], npass = 0;
+  for (int byte = 0; byte <= last_byte; ++byte)
+    if ((varying >> (8 * byte)) & 0xFFull) shifts[npass++] = 8 * byte;  // else one digit for every key
   const int grid = (int)std::min<uint64_t>(ntiles, (uint64_t)kScatterCtasPerSm * c.sm_count);
-  for (int byte = 0; byte <= last_byte; ++byte) {
-    const int shift = 8 * byte;
-    if (((varying >> shift) & 0xFFull) == 0) continue;  // one digit for every key: order unchanged
-    radix_hist_kernel<<<ntiles, kSortThreads, 0, c.stream>>>(ka, m, shift, ntiles, hist);
+  for (int p = 0; p < npass; ++p) {
+    const int shift = shifts[p];
+    if (p == 0)
+      radix_hist_kernel<<<ntiles, kSortThreads, 0, c.stream>>>(ka, m, shift, ntiles, hist);
+    else  // the digits the last scatter wrote
+      radix_hist_digits_kernel<<<(ntiles + kDigitHistWarps - 1) / kDigitHistWarps, kDigitHistWarps * 32, 0,
+                                 c.stream>>>(dg, m, ntiles, hist);
     sort_scan_sums_kernel<<<(unsigned)nb, kScanT, 0, c.stream>>>(hist, hn, bsum);
     sort_scan_top_kernel<<<1, kScanT, 0, c.stream>>>(bsum, nb);
     sort_scan_apply_kernel<<<(unsigned)nb, kScanT, 0, c.stream>>>(hist, hn, bsum);
-    const bool direct = rows_out && byte == last_byte;  // rows go straight to the output; keys are not needed
+    const bool last = p + 1 == npass;
+    const bool direct = rows_out && last;  // rows go straight to the output; keys are not needed
     radix_scatter_kernel<<<grid, kScatterThreads, sizeof(ScatterSmem), c.stream>>>(
-        ka, va, m, shift, hist, ntiles, kb, direct ? rows_out : vb, !direct, c.d_err);
+        ka, va, m, shift, hist, ntiles, kb, direct ? rows_out : vb, !direct, last ? nullptr : dg,
+        last ? 0 : shifts[p + 1], c.d_err);
     std::swap(ka, kb);
     std::swap(va, vb);
   }
