@@ -759,7 +759,8 @@ def _time_steps(fn, K, W, stream, torch):
 
 def run_secondary(args):
     """Per-operator lines for the other hot-path rows (not the headline):
-    filter_groupby (fused WHERE -> GROUP BY dept, 20 B/row), join (1M build x
+    filter_groupby (fused WHERE -> GROUP BY dept, 20 B/row), aggregate
+    (aggregates under one WHERE compare, 16 B/row), join (1M build x
     100M probe, INNER/LEFT/SEMI/ANTI), groupby (100M Zipf keys, 16 B/row + 40 B
     per group)."""
     import torch
@@ -810,6 +811,36 @@ def run_secondary(args):
             line("filter_groupby", ms, 20 * rows, {"rows": rows, "query": "SELECT dept, COUNT(*), SUM(score), "
                                                    "AVG(salary) FROM t WHERE score > 50 GROUP BY dept"})
             db.drop_table("t")
+
+    if args.workload in ("aggregate", "all"):
+        # Aggregates under one WHERE compare (FilterAggOp): 16 B/row of score
+        # and salary; then SUM(salary) alone under the same WHERE for scale.
+        t = W.table_t(n, seed=1)
+        db.create_table("t", t)
+        cols = [db.column("t", c) for c in ("score", "salary")]
+        L = F.lib()
+        sel = t["score"] > 50
+        ca, nc = ops._cols(cols)
+        pa, npr = ops._prog([ops.cmp(0, F.GT, 50)])
+        for name, aggs in (("aggregate_where", [(F.AGG_COUNT_STAR, 0), (F.AGG_SUM, 0), (F.AGG_AVG, 1),
+                                                (F.AGG_MAX, 0)]),
+                           ("sum_where", [(F.AGG_SUM, 1)])):
+            res = ops._bytes(F.AGG_VALUE_DTYPE.itemsize * len(aggs), db)
+            aa, na = ops._aggs(aggs)
+            ms = _time_steps(lambda: F.check(L.fdb_aggregate(db.handle, ca, nc, n, pa, npr, aa, na, res.data_ptr())),
+                             K, Wm, stream, torch)
+            rec = ops.to_records(res, F.AGG_VALUE_DTYPE, len(aggs))
+            if name == "aggregate_where":
+                assert rec[0]["i"] == int(sel.sum())
+                assert abs(rec[1]["f"] - O.sum_serial(t["score"][sel])) <= 1e-12 * rec[1]["f"]
+                assert rec[2]["f"] == float(O.sum_i64_exact(t["salary"][sel])) / int(sel.sum())
+                assert rec[3]["f"] == float(t["score"][sel].max())
+                q = "SELECT COUNT(*), SUM(score), AVG(salary), MAX(score) FROM t WHERE score > 50"
+            else:
+                assert rec[0]["f"] == float(O.sum_i64_exact(t["salary"][sel]))
+                q = "SELECT SUM(salary) FROM t WHERE score > 50"
+            line(name, ms, 16 * n, {"rows": n, "query": q})
+        db.drop_table("t")
 
     if args.workload in ("join", "all"):
         nb, npb = 1_000_000, n
@@ -1266,7 +1297,7 @@ def main():
                     help="skip the other configurations' extra keys (1 GPU only)")
     ap.add_argument("--cpu-threads", type=int, default=0)
     ap.add_argument("--workload", default="scan",
-                    choices=["scan", "filter_groupby", "join", "groupby", "batch", "sort", "parquet", "rest", "serve", "serve_single",
+                    choices=["scan", "filter_groupby", "aggregate", "join", "groupby", "batch", "sort", "parquet", "rest", "serve", "serve_single",
                              "all"],
                     help="scan = the headline line; the others print per-operator lines")
     ap.add_argument("--load-factor", type=float, default=0.5)

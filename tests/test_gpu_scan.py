@@ -248,3 +248,48 @@ def test_filtered_aggregates_fast_path(db, n):
                     assert a["n"] == cnt
                     if want is not None:
                         assert a["f"] == want
+
+
+@pytest.mark.parametrize("n", [7, 4099, 2_000_011])
+def test_filtered_aggregates_fast_path_edge_values(db, n):
+    """The fast filtered scan on the values where its accumulator forms could
+    differ from the interpreted scan's order-key / 128-bit forms: -0.0 and
+    +0.0, +-inf, NaN, and INT64 values near the limits whose sums need more
+    than 64 bits.  Values equal the oracle's; the sign of a zero MIN / MAX
+    (which f64::min / max leave unspecified) equals the interpreted scan's:
+    MAX is +0.0 and MIN -0.0 when both occur."""
+    r = rng(n + 5)
+    specials = np.array([0.0, -0.0, np.inf, -np.inf, np.nan, 1.0, -1.0])
+    f = specials[r.integers(0, len(specials), n)]
+    big = np.array([np.iinfo(np.int64).max, np.iinfo(np.int64).min, np.iinfo(np.int64).max - 7, -(1 << 62), 1 << 62,
+                    -1, 0], dtype=np.int64)
+    i = big[r.integers(0, len(big), n)]
+    cols = [dev(f), dev(i)]
+    spec = [(F.AGG_SUM, 1), (F.AGG_MIN, 0), (F.AGG_MAX, 0), (F.AGG_AVG, 1)]
+    for col, op, lit in [(1, F.GE, -(1 << 62)), (1, F.NE, 0), (0, F.NE, 5.0), (0, F.LE, 0.0), (1, F.LT, 1 << 62)]:
+        x = f if col == 0 else i
+        with np.errstate(invalid="ignore"):
+            sel = {F.NE: x != lit, F.LE: x <= lit, F.GE: x >= lit, F.LT: x < lit}[op]
+        got = ops.to_records(ops.aggregate(db, cols, n, [ops.cmp(col, op, lit)], spec), F.AGG_VALUE_DTYPE, 4)
+        slow = ops.to_records(ops.aggregate(db, cols, n, [ops.cmp(col, op, lit), ops.is_not_null(0), ops.AND()],
+                                            spec), F.AGG_VALUE_DTYPE, 4)
+        s = int(i[sel].astype(object).sum()) if sel.any() else 0
+        assert got[0]["n"] == int(sel.sum())
+        # The 128-bit sum is exact; its conversion to FLOAT64 is within an ulp.
+        assert abs(got[0]["f"] - float(s)) <= 2.0 ** -52 * abs(float(s)), (col, op, lit)
+        if sel.any():
+            assert abs(got[3]["f"] - float(s) / int(sel.sum())) <= 2.0 ** -51 * abs(float(s) / int(sel.sum()))
+        for j, func in ((1, F.AGG_MIN), (2, F.AGG_MAX)):
+            want, cnt = O.agg(func, f[sel])
+            assert got[j]["n"] == cnt and bool(got[j]["valid"]) == (want is not None)
+            if want is not None:
+                assert got[j]["f"] == want, (col, op, lit, func)
+        for j in range(4):
+            assert got[j].tobytes() == slow[j].tobytes(), (col, op, lit, j, got[j], slow[j])
+    # Signed zeros alone.
+    zeros = np.where(r.random(n) < 0.5, 0.0, -0.0)
+    got = ops.to_records(ops.aggregate(db, [dev(zeros), cols[1]], n, [ops.cmp(1, F.NE, 12345)],
+                                       [(F.AGG_MIN, 0), (F.AGG_MAX, 0)]), F.AGG_VALUE_DTYPE, 2)
+    assert got[0]["f"] == 0.0 and got[1]["f"] == 0.0
+    assert np.signbit(got[0]["f"]) == bool(np.signbit(zeros).any())
+    assert np.signbit(got[1]["f"]) == (not (~np.signbit(zeros)).any())
