@@ -190,8 +190,8 @@ struct JoinView {
   uint64_t cap;
   int32_t unique;
   int32_t dense;             // key k lives in slot k - dmin (see join_table.cuh)
-  int64_t dmin;
-  uint64_t span;             // dense: keys outside [dmin, dmin + span) have no slot
+  int64_t dmin;              // the smallest build key
+  uint64_t span;             // keys outside [dmin, dmin + span) have no slot (0: no range)
 };
 JoinView join_view(const HashTable* h);
 

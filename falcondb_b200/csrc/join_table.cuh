@@ -27,22 +27,27 @@ __device__ __forceinline__ int join_shift(uint64_t cap) { return __clzll((long l
 // it has slots (max - min < cap: surrogate keys, dense id ranges) is dense:
 // key k lives in slot k - min, so a probe is one slot read and keys outside
 // [min, min + cap) read nothing.  Otherwise keys hash (join_hash) with linear
-// probing.  The NULL-group slot (key INT64_MIN) is slot cap either way.
+// probing, and a probe key outside the build keys' [min, max] still reads
+// nothing: the range read back at build time doubles as a min/max filter, so
+// probe keys that run past the build side's (half of uniform [0, 2M) probe
+// keys against the 1M build keys 0..1M-1, say) skip the walk to an empty
+// slot that each would otherwise take.  The NULL-group slot (key INT64_MIN)
+// is slot cap either way.
 struct JoinMode {
-  int64_t dmin;   // dense: the smallest build key
+  int64_t dmin;   // the smallest build key
   int32_t dense;
   int32_t shift;  // join_shift(cap)
-  uint64_t span;  // dense: largest build key - dmin + 1 (<= cap)
+  uint64_t span;  // largest build key - dmin + 1 (dense: <= cap); 0 = no range
+                  // (an empty build side, or keys over all 2^64 values)
 };
 
-// Home slot of key k (stored form sk), or a value >= cap when a dense table
-// cannot hold it: outside [dmin, dmin + span), where no build key lies (the
-// table's slots past the span are empty, so such a key reads nothing).
+// Home slot of key k (stored form sk), or a value >= cap when the table holds
+// no key there: outside [dmin, dmin + span), where no build key lies.  A
+// dense table's slots past the span are empty; a hashed table is not read.
 __device__ __forceinline__ uint64_t join_home(const JoinMode& m, int64_t k, uint64_t sk) {
-  if (m.dense) {
-    const uint64_t d = (uint64_t)k - (uint64_t)m.dmin;
-    return d < m.span ? d : ~0ull;
-  }
+  const uint64_t d = (uint64_t)k - (uint64_t)m.dmin;
+  if (m.dense) return d < m.span ? d : ~0ull;
+  if (m.span != 0 && d >= m.span) return ~0ull;
   return join_hash(sk, m.shift);
 }
 

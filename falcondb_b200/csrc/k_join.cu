@@ -35,8 +35,8 @@ struct HashTable {
   bool unique = true;        // every key occurs once (cnt is 1 wherever set)
   bool payload_nulls = false;
   bool dense = false;        // key k lives in slot k - dmin (join_table.cuh)
-  int64_t dmin = 0;
-  uint64_t span = 0;         // dense: kmax - kmin + 1; probe keys outside read nothing
+  int64_t dmin = 0;          // the smallest build key
+  uint64_t span = 0;         // kmax - kmin + 1 (0: no range); probe keys outside read nothing
   // Dense tables whose key range fits a CTA's shared memory as bits: bit
   // k - dmin is set when key k has a build row.  SEMI / ANTI probes test it
   // in shared memory and read nothing else.
@@ -106,7 +106,12 @@ __global__ void join_insert_kernel(const int64_t* __restrict__ keys, const uint6
       s = cap;
     } else {
       const unsigned long long sk = (unsigned long long)k ^ (1ull << 63);
-      uint64_t h = join_home(mode, k, sk);  // a dense table's range fits: h < cap
+      uint64_t h = join_home(mode, k, sk);  // a build key lies in the range: h < cap
+      if (h > mask) {  // cannot happen: the range was taken over these keys
+        atomicExch(err, kErrCapacity);
+        row_slot[i] = kNoSlot;
+        continue;
+      }
       for (uint64_t probe = 0; probe <= mask; ++probe) {  // cap > distinct keys: always ends
         const unsigned long long cur = *reinterpret_cast<volatile unsigned long long*>(&slots[h].key);
         if (cur == sk) { s = h; break; }
@@ -277,11 +282,11 @@ HashTable* op_join_build(Ctx& c, const fdb_dev_column& key, const fdb_dev_column
     FDB_CUDA(cudaStreamSynchronize(c.stream));
     if (hr[1] != 0) {
       const uint64_t kmin = ~hr[0] ^ (1ull << 63), kmax = hr[1] ^ (1ull << 63);  // two's complement bits
-      if (kmax - kmin < cap) {
-        dense = true;
-        dmin = (int64_t)kmin;
-        span = kmax - kmin + 1;
-      }
+      // Both kinds keep the range: a hashed table uses it as a min/max filter
+      // on probe keys (span 0 when the keys cover all 2^64 values).
+      dmin = (int64_t)kmin;
+      span = kmax - kmin + 1;
+      dense = kmax - kmin < cap;
     }
   }
   h->dense = dense;

@@ -144,12 +144,12 @@ struct ServeG {             // a group of queries that read the same table
   const JSlot* slots;
   const unsigned int* cnt;
   uint64_t cap;
-  int64_t dmin;             // dense table: key k lives in slot k - dmin
+  int64_t dmin;             // smallest build key (dense table: key k lives in slot k - dmin)
   int32_t dense;
   int32_t ngroupq;          // GROUP queries in the group
   int32_t ncountq, njoinq;  // COUNT and JOIN queries in the group
   int32_t _pad4;
-  uint64_t span;            // dense table: keys outside [dmin, dmin + span) have no slot
+  uint64_t span;            // keys outside [dmin, dmin + span) have no slot (0: no range)
 };
 
 struct ServeHeader {
@@ -480,7 +480,7 @@ __device__ void serve_probe_rows(const ServeG g, uint64_t* s0, uint32_t* m, uint
       }
       sk[j] = (uint64_t)key ^ (1ull << 63);
       h[j] = join_home(mode, key, sk[j]);
-      todo |= 1u << j;
+      if (h[j] <= mask) todo |= 1u << j;  // keys outside the build keys' range read nothing
     }
     // Hashed table: rounds over slot pairs, kPairIlp rows' pairs in flight at a
     // time (fewer than kHashIlp, to keep the registers of the pairs down).

@@ -316,3 +316,58 @@ def test_dense_group_by_capacity_error(db):
     assert e.value.code == -9
     rec = _raw_groups(db, keys, vals)
     assert len(rec) == 5_000 and np.all(rec["count"] == 2)
+
+
+def _same_or_close_sums(got, want):
+    """SUMs: non-finite ones (inf, -inf, NaN) exactly, the rest within RTOL."""
+    fin = np.isfinite(want)
+    assert np.array_equal(got[~fin], want[~fin], equal_nan=True)
+    rel = np.abs(got[fin] - want[fin]) / np.maximum(np.abs(want[fin]), 1e-300)
+    assert rel.max(initial=0.0) <= RTOL
+
+
+@pytest.mark.parametrize("special", [False, True], ids=["plain", "nan_inf_negzero"])
+def test_dense_group_by_heavy_keys(db, special):
+    """A few keys carry most rows (every consumer warp's most frequent keys,
+    the rows whose COUNT / SUM a warp may keep in registers), the rest spread
+    over a dense 200K-key range; with NaN, +-inf and -0.0 among the heavy
+    keys' values and a NULL key group.  Every group against the oracle."""
+    n, d = 4_000_000, 200_000
+    r = np.random.default_rng(91)
+    keys = r.integers(0, d, n)
+    heavy = np.array([17, 99_999, 150_001])
+    pick = r.random(n)
+    keys[pick < 0.3] = heavy[0]
+    keys[(pick >= 0.3) & (pick < 0.45)] = heavy[1]
+    keys[(pick >= 0.45) & (pick < 0.55)] = heavy[2]
+    vals = r.random(n) * 100 - 50
+    if special:
+        hot_rows = np.flatnonzero(np.isin(keys, heavy))
+        for value, every in ((np.nan, 100_003), (np.inf, 200_003), (-np.inf, 300_007), (-0.0, 7)):
+            vals[hot_rows[::every]] = value
+        vals[np.flatnonzero(keys == heavy[2])[::50_000]] = np.nan  # a heavy key whose SUM is NaN
+    keys[::1000] = np.iinfo(np.int64).min  # the NULL group
+    raw = _raw_groups(db, keys, vals)
+    assert raw["key"][-1] == np.iinfo(np.int64).min and np.all(np.diff(raw["key"][:-1]) > 0)
+    rec = raw[np.argsort(raw["key"], kind="stable")]
+    want = O.group_i64(keys, vals)
+    assert np.array_equal(rec["key"], want["key"]) and np.array_equal(rec["count"], want["count"])
+    assert np.array_equal(rec["min"], want["min"], equal_nan=True)
+    assert np.array_equal(rec["max"], want["max"], equal_nan=True)
+    fin = np.isfinite(want["min"])
+    assert np.array_equal(np.signbit(rec["min"][fin]), np.signbit(want["min"][fin]))
+    _same_or_close_sums(rec["sum"], want["sum"])
+
+
+def test_dense_group_by_heavy_keys_null_values(db):
+    """Heavy keys whose values are partly NULL: COUNT(*) counts every row,
+    SUM / MIN / MAX skip the NULL values."""
+    n, d = 3_000_000, 100_000
+    r = np.random.default_rng(92)
+    keys = r.integers(0, d, n)
+    keys[r.random(n) < 0.5] = 4_242
+    vals = r.random(n)
+    vvalid = r.random(n) > 0.2
+    vw = F.validity_words(vvalid)
+    raw = _raw_groups(db, keys, (dev(vals), dev(vw.view(np.int64))))
+    _same_groups(raw, _pandas_groups(keys, vals, vvalid))

@@ -215,3 +215,42 @@ def test_semi_anti_on_every_table_path(db, kind):
         assert got["payload_rows"] == want["payload_rows"]
         assert abs(got["sum_value"] - want["sum_value"]) <= 1e-12 * abs(want["sum_value"])
     h.free()
+
+
+@pytest.mark.parametrize("lo,hi", [(-3_000_000_000, 3_000_000_000), (I64.min + 1, I64.max)])
+def test_hashed_table_key_range_filter(db, lo, hi):
+    """A hashed table reads nothing for probe keys outside its build keys'
+    [min, max]: keys one below the minimum and one above the maximum miss,
+    the two ends themselves match, and a build side reaching both int64
+    extremes (a range of 2^64 - 1 values) filters nothing.  Aggregates and
+    row pairs match the oracle on every join type."""
+    r = np.random.default_rng(21)
+    nb = 50_000
+    keys = r.integers(lo // 2, hi // 2, nb)
+    keys[0], keys[1] = lo, hi
+    b = {"key": keys.astype(np.int64), "payload": r.integers(0, 1000, nb)}
+    edges = [lo, hi, lo + 1, hi - 1, I64.min]
+    if lo > I64.min + 1:
+        edges += [lo - 1, I64.min + 1]
+    if hi < I64.max:
+        edges += [hi + 1, I64.max]
+    pk = np.concatenate([np.repeat(np.array(edges, dtype=np.int64), 3), r.choice(keys, 20_000),
+                         r.integers(lo // 2, hi // 2, 20_000)]).astype(np.int64)
+    r.shuffle(pk)
+    p = {"key": pk, "value": r.random(len(pk))}
+    for jt in TYPES:
+        check_agg(agg(db, b, p, jt, dense=False), O.join_agg(b["key"], b["payload"], p["key"], p["value"], jt), jt)
+    h = ops.HashTable(db, dev(b["key"]), None, nb)
+    assert not h.dense
+    for jt in TYPES:
+        want_l, want_r = O.join_pairs(b["key"], pk, jt)
+        left, right, cnt = h.probe_pairs(dev(pk), len(pk), jt, capacity=len(want_l) + 16)
+        c = int(cnt.item())
+        assert c == len(want_l), jt
+        gl = left[:c].cpu().numpy().view(np.uint32).tolist()
+        if jt <= 1:
+            gr = right[:c].cpu().numpy().view(np.uint32).tolist()
+            assert sorted(zip(gl, gr)) == sorted(zip(want_l.tolist(), want_r.tolist()))
+        else:
+            assert sorted(gl) == sorted(want_l.tolist())
+    h.free()
