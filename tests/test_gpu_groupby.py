@@ -340,7 +340,7 @@ def test_dense_group_by_heavy_keys(db, special):
     keys[pick < 0.3] = heavy[0]
     keys[(pick >= 0.3) & (pick < 0.45)] = heavy[1]
     keys[(pick >= 0.45) & (pick < 0.55)] = heavy[2]
-    vals = r.random(n) * 100 - 50
+    vals = r.random(n) * 100 + 1.0  # positive: a heavy key's SUM does not cancel to near zero
     if special:
         hot_rows = np.flatnonzero(np.isin(keys, heavy))
         for value, every in ((np.nan, 100_003), (np.inf, 200_003), (-np.inf, 300_007), (-0.0, 7)):
