@@ -39,6 +39,16 @@ def test_python_binding_covers_every_symbol():
     assert "sm_100a" in F.version()
 
 
+def test_rust_binding_in_integration_doc_covers_every_symbol():
+    """The Rust `extern "C"` block a FalconDB maintainer would add (the
+    integration guide) declares every entry point of the header."""
+    doc = (ROOT / "INTEGRATION.md").read_text()
+    block = doc[doc.index('extern "C" {'):]
+    block = block[:block.index("\n}\n")]
+    bound = set(re.findall(r"pub fn (fdb_[a-z0-9_]+)\(", block))
+    assert sorted(set(declared_symbols()) - bound) == []
+
+
 def test_open_without_gpu_fails_loudly():
     """No CPU fallback: opening a context needs a CUDA device."""
     import falcondb_b200 as F
